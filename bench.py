@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the INS2D explicit RK hot path on B200.
+
+Metric: cell-updates/s per RK4 step including all Poisson solves
+(Npx*Npy*steps / time), plus CG iterations per solve on the PCG path.
+
+Default workload: decaying 2D turbulence on a periodic 2048x2048 uniform grid,
+Re=2000, RK44, CFL 0.5, FFT pressure solve, FP64 (seeded random-phase
+streamfunction IC, E(k) ~ k^4 exp(-2(k/10)^2), unit kinetic energy).  The
+working set of a step (about 0.5 GB of FP64 fields, 32 MiB each) is larger
+than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload turb2048|turb2048_fp32|tg512|ldc64|turb2048_pcg]
+
+--impl reference times the reference algorithm's CPU restatement (the oracle
+port; the MATLAB reference itself cannot run here) on the host cores.
+Multi-GPU (torchrun): one independent replica of the workload per rank
+(weak scaling, no data-path collective), time = max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (N, domain, Re, poisson, precision, description)
+    "turb2048": dict(N=2048, L=1.0, Re=2000.0, poisson=6, precision="fp64", ic="turbulence",
+                     desc="decaying 2D turbulence 2048x2048 periodic, Re=2000, RK44, CFL 0.5, FFT Poisson, FP64"),
+    "turb2048_fp32": dict(N=2048, L=1.0, Re=2000.0, poisson=6, precision="fp32", ic="turbulence",
+                          desc="decaying 2D turbulence 2048x2048, FP32 stencils + FP64 Poisson/projection"),
+    "turb2048_pcg": dict(N=2048, L=1.0, Re=2000.0, poisson=4, precision="fp64", ic="turbulence", CG_acc=1e-10,
+                         desc="decaying 2D turbulence 2048x2048, PCG Poisson to 1e-10, FP64"),
+    "tg512": dict(N=512, L=2 * math.pi, Re=1e100, poisson=6, precision="fp64", ic="tg", dt=1e-3,
+                  desc="inviscid Taylor-Green 512x512 periodic [0,2pi]^2, RK44 dt=1e-3, FFT Poisson, FP64"),
+    "ldc64": dict(N=64, L=1.0, Re=1000.0, poisson=4, precision="fp64", ic="rest", dt=1e-3, CG_acc=1e-12,
+                  desc="lid-driven cavity 64x64, Re=1000, RK44 dt=1e-3, PCG to 1e-12, FP64"),
+}
+
+# algorithmic DRAM bytes per cell (FP64) of one launch of each kernel family
+# (each array read or written once per launch)
+def family_bytes_per_cell(fam, rk_stats):
+    if fam == "stage":
+        # V_i (16) + Vn (16) + Wt (16) + stored kV (16 on 3 of 4 RK44 stages)
+        # + earlier kV read on the last stage (48 on 1 of 4)
+        return 48 + (3 * 16 + 48) / 4.0
+    if fam == "div":
+        return 16 + 8
+    if fam == "project":
+        return 16 + 8 + 16
+    if fam == "residual":
+        return 16 + 8 + 16
+    if fam == "poisson_fft":
+        # rows r2c: 8 in + 8 out (half spectrum of complex), columns: 16, rows c2r: 8 + 8
+        return 48.0
+    return None
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(prefix="clocks_", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        with open(self.out.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def setup_case(wl, device=0):
+    import ins2d_b200
+    from ins2d_b200 import cases
+    N, L = wl["N"], wl["L"]
+    x = cases.uniform_grid(N, 0.0, L)
+    if wl["ic"] == "rest":
+        bc = cases.BC_CAVITY
+        uBC = cases.lid_uBC(1.0, L)
+    else:
+        bc = cases.BC_PERIODIC
+        uBC = None
+    opts = ins2d_b200.Options(x, x.copy(), bc, Re=wl["Re"], poisson=wl["poisson"], CG_acc=wl.get("CG_acc", 1e-12),
+                              CG_maxit=50000, uBC=uBC, RK="RK44", precision=wl["precision"], device=device)
+    if wl["ic"] == "turbulence":
+        V = cases.decaying_turbulence_ic(opts, k0=10.0, seed=2048)
+        dt = cases.cfl_dt(opts, V, 0.5)
+    elif wl["ic"] == "tg":
+        V = cases.taylor_green(opts)
+        dt = wl["dt"]
+    else:
+        V = np.zeros(opts.NV)
+        dt = wl["dt"]
+    return opts, V, dt
+
+
+def run_ours(args, wl, rank, world, local_rank):
+    import torch
+    import ins2d_b200
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    opts, V0, dt = setup_case(wl, device=local_rank)
+    stream = torch.cuda.current_stream()
+    opts.set_stream(stream.cuda_stream)
+    Vd = torch.tensor(V0, dtype=torch.float64, device="cuda")
+    pd = torch.zeros(opts.Np, dtype=torch.float64, device="cuda")
+    pd = opts.pressure_additional_solve(Vd, pd, 0.0)  # p_initial (input_check.m:126-128)
+    t = 0.0
+    # warm-up
+    _, _, st = opts.time_ERK(Vd, pd, t, dt, nsteps=args.warmup, return_stats=True)
+    t += args.warmup * dt
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    opts.profile(False)  # resets launch counters
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    _, _, st = opts.time_ERK(Vd, pd, t, dt, nsteps=args.steps, return_stats=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = opts.profile_read()
+    launches = sum(n for _, n in prof.values())
+    t += args.steps * dt
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_max = ms
+    if dist:
+        tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    cells = opts.Npx * opts.Npy
+    value = cells * args.steps * world / (ms_max / 1e3)
+
+    # end to end through the public API with host buffers: every step copies
+    # V and p from pinned host memory and reads them back
+    hV = torch.empty(opts.NV, dtype=torch.float64, pin_memory=True)
+    hp = torch.empty(opts.Np, dtype=torch.float64, pin_memory=True)
+    hV.copy_(Vd.cpu())
+    hp.copy_(pd.cpu())
+    hVn, hpn = hV.numpy(), hp.numpy()
+    from ins2d_b200 import _lib
+    import ctypes
+    lib = _lib.load()
+    ss = _lib.StepStats()
+    e_steps = max(2, min(args.steps, 20))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    tw0 = time.perf_counter()
+    for n in range(e_steps):
+        rc = lib.ins2d_erk_step(opts._ctx, hVn.ctypes.data, hpn.ctypes.data, t + n * dt, dt, ctypes.byref(ss),
+                                _lib.MEM_HOST)
+        if rc:
+            raise RuntimeError(opts._err())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - tw0) * 1e3)
+    if dist:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = cells * e_steps * world / (e2e_ms / 1e3)
+
+    # per-family device time (a separate profiled run; events add a little overhead)
+    nprof = max(2, min(args.steps, 10))
+    opts.profile(True)
+    opts.time_ERK(Vd, pd, t, dt, nsteps=nprof)
+    fam = opts.profile_read()
+    opts.profile(False)
+    peak, peak_kind = load_peaks()
+    fam_ms = {k: v[0] for k, v in fam.items()}
+    dom = max(fam_ms, key=fam_ms.get)
+    dom_launch_ms = fam[dom][0] / max(fam[dom][1], 1)
+    fkey = "poisson_fft" if (dom == "poisson" and wl["poisson"] == 6) else dom
+    bpc = family_bytes_per_cell(fkey, None)
+    roof = None
+    if bpc is not None:
+        if dom == "poisson":
+            launch_ms = fam[dom][0] / max(nprof * 4, 1)  # one solve = 3 passes
+        else:
+            launch_ms = dom_launch_ms
+        achieved = bpc * cells / (launch_ms / 1e3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                with open(tpath) as fh:
+                    traffic = json.load(fh).get(args.workload, {}).get(fkey)
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "kernel": fkey, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
+                "bytes_per_launch": bpc * cells, "launch_ms": round(launch_ms, 5),
+                "family_ms_per_step": {k: round(v / nprof, 4) for k, v in fam_ms.items()}}
+    # CPU baseline on rank 0 only at N=1
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl, budget_s=args.cpu_budget)
+    res = {
+        "metric": "cell-updates/s per RK4 step incl. Poisson solve",
+        "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if wl["precision"] == "fp64" else "f32-stencil/f64-poisson", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": wl["desc"], "grid": [opts.Npx, opts.Npy], "dt": dt,
+                   "cells": cells, "l2": "working set > 126 MB L2 (no flush)" if cells >= 1 << 20 else
+                   "small grid: L2-resident", "parallelism": f"replicas{world}"},
+        "cg_iters_per_solve": (st["iters_total"] / st["n_solves"]) if (st and st["n_solves"] and wl["poisson"] != 6)
+        else None,
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "steps": e_steps,
+                "h2d_bytes_per_step": 8 * (opts.NV + opts.Np), "d2h_bytes_per_step": 8 * (opts.NV + opts.Np)},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(wl, budget_s=25.0, steps=None):
+    """The oracle port (scipy/numpy restatement of the reference algorithm)
+    timed on the host on a bounded sample: RK44 steps of the same workload."""
+    from oracle import ins2d_ref as R
+    from ins2d_b200 import cases
+    N, L = wl["N"], wl["L"]
+    x = cases.uniform_grid(N, 0.0, L)
+    bc = cases.BC_CAVITY if wl["ic"] == "rest" else cases.BC_PERIODIC
+    uBC = cases.lid_uBC(1.0, L) if wl["ic"] == "rest" else None
+    poisson = 6 if wl["poisson"] == 6 else 4
+    t0 = time.perf_counter()
+    o = R.make_options(x, x.copy(), bc, Re=wl["Re"], poisson=poisson, CG_acc=wl.get("CG_acc", 1e-12),
+                       CG_maxit=100000, uBC=uBC, RK="RK44")
+    setup_s = time.perf_counter() - t0
+    g = o.grid
+    rng = np.random.default_rng(0)
+    if wl["ic"] == "rest":
+        V = np.zeros(g.NV)
+    elif wl["ic"] == "tg":
+        V = np.r_[np.sin(g.xu) * np.cos(g.yu), -np.cos(g.xv) * np.sin(g.yv)]
+    else:
+        V = R.initial_projection(0.1 * rng.standard_normal(g.NV), 0.0, o)
+    p = np.zeros(g.Np)
+    dt = wl.get("dt", 1e-4)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        V, p = R.time_ERK(V, p, n * dt, dt, o)
+        n += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and n >= steps) or (steps is None and (el > budget_s or n >= 50)):
+            break
+    cores = 1
+    return {"value": g.Npx * g.Npy * n / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{n} RK44 step(s) of the {N}x{N} workload with the scipy/numpy restatement "
+                      f"(sparse matvecs single-threaded; operator setup {setup_s:.1f}s excluded)"}
+
+
+def run_reference(args, wl, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    # a bounded sample: the step count is capped so the whole run takes minutes
+    warm = min(args.warmup, 1)
+    nsteps = min(steps, 3)
+    cb = cpu_baseline(wl, budget_s=1e9, steps=warm + nsteps)
+    res = {
+        "impl": "reference", "metric": "cell-updates/s per RK4 step incl. Poisson solve", "value": cb["value"],
+        "unit": "cell-updates/s", "n_gpus": world, "steps": nsteps, "warmup": warm, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": wl["desc"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(res), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="turb2048", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, wl, rank, world)
+    else:
+        run_ours(args, wl, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/* ins2d.h -- C-ABI of the B200 INS2D hot path (libins2d.so).
+ *
+ * The hot path is the explicit Runge-Kutta stage loop of the energy-conserving
+ * staggered finite-volume incompressible Navier-Stokes solver INS2D, with its
+ * right-hand side F and the pressure-Poisson projection.  The entry points
+ * below replace, one for one, the MATLAB functions a case calls through main():
+ *
+ *   ins2d_ctx_create        operators.m:1-18 + operator_*.m   (the options struct)
+ *   ins2d_set_bc_values     set_bc_vectors.m:1-706            (BC vectors at t)
+ *   ins2d_F                 spatial/F.m:1                     ([maxres,F] = F(V,C,p,T,t,options))
+ *   ins2d_divergence        check_conservation.m:37           (M*V + yM)
+ *   ins2d_pressure_poisson  solvers/pressure/pressure_poisson.m:1 (dp = pressure_poisson(f,t,options))
+ *   ins2d_pressure_additional_solve solvers/pressure/pressure_additional_solve.m:1
+ *   ins2d_erk_step          unsteady/time_ERK.m:1             ([Vnew,pnew] = time_ERK(Vn,pn,Tn,tn,dt,options))
+ *   ins2d_conservation      spatial/check_conservation.m:1    ([maxdiv,umom,vmom,k])
+ *   ins2d_laplacian         A*p with A = M*Om_inv*G           (operator_divergence.m:208)
+ * and the Fortran MEX gateway cg.F:31 ([x,iter,norm1,norm2]=cg(...)) whose role
+ * ins2d_pressure_poisson takes over with a device PCG.
+ *
+ * Conventions
+ *  - Vectors use the reference's ordering: x fastest, V = [u; v],
+ *    u(i,j) -> i + j*Nux_in, v(i,j) -> i + j*Nvx_in, p(i,j) -> i + j*Npx.
+ *  - All arithmetic is IEEE binary64 unless the context was created with
+ *    precision = INS2D_PREC_FP32_STENCIL (FP32 convection/diffusion stencils
+ *    and stage combination; divergence, Poisson solve and projection stay FP64).
+ *  - `mem` selects where array arguments live: INS2D_MEM_HOST (the call copies
+ *    in and out, host buffers owned by the caller) or INS2D_MEM_DEVICE (device
+ *    pointers on the context's device, used in place).
+ *  - Every function returns an int status (INS2D_OK = 0); the text of the last
+ *    error is ins2d_last_error(ctx).
+ *  - A context is used by one host thread at a time; distinct contexts are
+ *    independent.  Work is issued on the context's stream (ins2d_set_stream),
+ *    and each call returns after that stream has finished the call's work.
+ */
+#ifndef INS2D_H
+#define INS2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (failure modes of cg.F:262, pressure_poisson.m:58-63,
+ * boundary_conditions.m:17-40) */
+#define INS2D_OK 0
+#define INS2D_EINVAL 1      /* invalid argument / unsupported BC combination */
+#define INS2D_ENOTCONV 2    /* PCG did not reach CG_acc within CG_maxit */
+#define INS2D_EBREAKDOWN 3  /* PCG breakdown (p'Ap = 0) */
+#define INS2D_ENONFINITE 4  /* NaN/Inf met in a solve or step */
+#define INS2D_ETIMEOUT 5    /* a bounded device wait gave up */
+#define INS2D_ECUDA 6       /* CUDA runtime error */
+#define INS2D_ENOMEM 7      /* device allocation failed */
+
+/* boundary-condition types (options.BC.{u,v}.{left,right,low,up}) */
+#define INS2D_BC_DIR 0
+#define INS2D_BC_PRES 1
+#define INS2D_BC_PER 2
+#define INS2D_BC_SYM 3
+
+/* options.solversettings.poisson: 1 direct, 2 pcg+ILU, 3 cg MEX, 4 CG+DIC,
+ * 5 PETSc -> all served by the device PCG; 6 -> FFT (periodic, uniform). */
+#define INS2D_POISSON_DIRECT 1
+#define INS2D_POISSON_CG_MEX 3
+#define INS2D_POISSON_CG 4
+#define INS2D_POISSON_FFT 6
+
+#define INS2D_PREC_FP64 0
+#define INS2D_PREC_FP32_STENCIL 1
+
+#define INS2D_MEM_HOST 0
+#define INS2D_MEM_DEVICE 1
+
+#define INS2D_MAX_STAGES 8
+
+typedef struct ins2d_ctx ins2d_ctx;
+
+/* options.grid.{Nx,Ny,x,y} (mesh_generation.m:17-49): grid-line coordinates */
+typedef struct {
+  int32_t Nx, Ny;
+  const double *x; /* Nx+1 */
+  const double *y; /* Ny+1 */
+} ins2d_grid_desc;
+
+/* options.BC (boundary_conditions.m:1-40) */
+typedef struct {
+  int32_t u_left, u_right, u_low, u_up;
+  int32_t v_left, v_right, v_low, v_up;
+  int32_t bc_unsteady; /* options.BC.BC_unsteady */
+} ins2d_bc_desc;
+
+/* options.{fluid,solversettings,time} */
+typedef struct {
+  double Re;            /* options.fluid.Re */
+  int32_t poisson;      /* options.solversettings.poisson */
+  double CG_acc;        /* options.solversettings.CG_acc  (relative: ||r||/||f||) */
+  int32_t CG_maxit;     /* options.solversettings.CG_maxit */
+  int32_t p_add_solve;  /* options.solversettings.p_add_solve */
+  int32_t rk_stages;    /* s of the Butcher tableau (getRKmethod.m) */
+  double rk_A[INS2D_MAX_STAGES * INS2D_MAX_STAGES]; /* s x s, row-major */
+  double rk_b[INS2D_MAX_STAGES];
+  double rk_c[INS2D_MAX_STAGES];
+  int32_t precision;    /* INS2D_PREC_* */
+  int32_t device;       /* CUDA device ordinal */
+} ins2d_opts;
+
+/* Boundary values sampled by the caller from the case's uBC/vBC handles at
+ * time t, exactly the samples set_bc_vectors.m:52-79 takes.  NULL pressure
+ * arrays mean 0 (boundary_conditions.m:107-116); NULL time derivatives mean 0. */
+typedef struct {
+  const double *uLo, *uUp;     /* Nx+1   uBC(x, y(1)), uBC(x, y(end)) */
+  const double *uLo_i, *uUp_i; /* Nux_in uBC(xin, y(1|end)) */
+  const double *uLe_i, *uRi_i; /* Ny     uBC(x(1|end), yp) */
+  const double *vLe, *vRi;     /* Ny+1   vBC(x(1|end), y) */
+  const double *vLo_i, *vUp_i; /* Nx     vBC(xp, y(1|end)) */
+  const double *vLe_i, *vRi_i; /* Nvy_in vBC(x(1|end), yin) */
+  const double *pLe, *pRi;     /* Ny     options.BC.pLe/pRi */
+  const double *pLo, *pUp;     /* Nx     options.BC.pLo/pUp */
+  const double *dudtLe_i, *dudtRi_i; /* Ny  dudtBC(x(1|end), yp)  (BC_unsteady) */
+  const double *dvdtLo_i, *dvdtUp_i; /* Nx  dvdtBC(xp, y(1|end))  (BC_unsteady) */
+} ins2d_bc_values;
+
+/* options.grid counts (operator_mesh.m:25-110) */
+typedef struct {
+  int32_t Nx, Ny;
+  int32_t Nux_in, Nuy_in, Nvx_in, Nvy_in;
+  int32_t Npx, Npy;
+  int32_t Nu, Nv, NV, Np;
+} ins2d_sizes;
+
+/* [iter, norm1, norm2] of cg.F:15-17 (iters = 0 for the FFT path) */
+typedef struct {
+  int32_t iters;
+  double norm1; /* sqrt(||r||^2/||f||^2) */
+  double norm2; /* max|r| / (max x - min x) */
+} ins2d_solve_stats;
+
+typedef struct {
+  int32_t n_solves;
+  int32_t iters_total;
+  int32_t iters_max;
+  double norm1_max;
+} ins2d_step_stats;
+
+/* --- context (the `options` struct) ------------------------------------- */
+int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc,
+                     const ins2d_opts *opts, ins2d_ctx **out);
+int ins2d_ctx_destroy(ins2d_ctx *ctx);
+const char *ins2d_last_error(const ins2d_ctx *ctx);
+int ins2d_get_sizes(const ins2d_ctx *ctx, ins2d_sizes *out);
+/* stream: a cudaStream_t (NULL = the context's own stream) */
+int ins2d_set_stream(ins2d_ctx *ctx, void *stream);
+/* set_bc_vectors.m:1 -- boundary values at time t (steady cases call it once) */
+int ins2d_set_bc_values(ins2d_ctx *ctx, double t, const ins2d_bc_values *vals);
+/* Unsteady boundary conditions (options.BC.BC_unsteady = 1): the context calls
+ * fn(user, t, ctx) whenever the reference would call set_bc_vectors(t,options)
+ * (time_ERK.m:62,106-109, F.m:97-99, pressure_additional_solve.m:11-13); fn
+ * samples the case's uBC/vBC/dudtBC/dvdtBC at t and calls ins2d_set_bc_values.
+ * A MEX gateway implements fn with mexCallMATLAB on the case's handles. */
+typedef int (*ins2d_bc_sampler_fn)(void *user, double t, ins2d_ctx *ctx);
+int ins2d_set_bc_sampler(ins2d_ctx *ctx, ins2d_bc_sampler_fn fn, void *user);
+
+/* --- measurement ------------------------------------------------------------
+ * Kernel families of a time step.  ins2d_profile(ctx, 1) starts bracketing
+ * each family's launches with CUDA events on the context stream (and resets
+ * the counters); ins2d_profile_read returns the accumulated device time (ms)
+ * and the number of kernel launches per family since the last read, and
+ * resets them.  Launches are counted whether or not profiling is on. */
+#define INS2D_PROF_STAGE 0    /* RK stage right-hand side + combination */
+#define INS2D_PROF_DIV 1      /* divergence right-hand side of the Poisson solve */
+#define INS2D_PROF_POISSON 2  /* FFT passes or PCG kernels */
+#define INS2D_PROF_PROJECT 3  /* projection V = Vn + dt (Vtemp - c Om^-1 G dp) */
+#define INS2D_PROF_RESIDUAL 4 /* residual of the additional pressure solve */
+#define INS2D_PROF_OTHER 5    /* F, divergence, Laplacian, conservation entry points */
+#define INS2D_PROF_N 6
+int ins2d_profile(ins2d_ctx *ctx, int enable);
+int ins2d_profile_read(ins2d_ctx *ctx, double ms[INS2D_PROF_N], int64_t launches[INS2D_PROF_N]);
+
+/* --- the hot path ---------------------------------------------------------- */
+/* F.m:1 with getJacobian=0, T=0: F_out = -conv(V;C) + Diff*V + yDiff - (G*p + y_p);
+ * C = NULL means C = V; p = NULL with nopressure=1 drops the pressure terms.
+ * maxres (may be NULL) = max|F| (F.m:187). */
+int ins2d_F(ins2d_ctx *ctx, const double *V, const double *C, const double *p,
+            double t, int nopressure, double *F_out, double *maxres, int mem);
+/* f_out = M*V + yM (check_conservation.m:37); maxdiv (may be NULL) = max|f_out| */
+int ins2d_divergence(ins2d_ctx *ctx, const double *V, double *f_out, double *maxdiv, int mem);
+/* Ap = A*p, A = M*diag(Om_inv)*G (operator_divergence.m:208) */
+int ins2d_laplacian(ins2d_ctx *ctx, const double *p, double *Ap, int mem);
+/* dp = pressure_poisson(f,t,options) (pressure_poisson.m:1-106): initial
+ * guess 0; returns 0 when max|A*0 - f| < 1e-14 (:33-38); PCG to the relative
+ * residual CG_acc (cg.F:240-247) or the FFT solve (:92-104). */
+int ins2d_pressure_poisson(ins2d_ctx *ctx, const double *f, double *dp,
+                           ins2d_solve_stats *stats, int mem);
+/* p = pressure_additional_solve(V,p,T,t,options) (in place on p) */
+int ins2d_pressure_additional_solve(ins2d_ctx *ctx, const double *V, double *p, double t,
+                                    ins2d_solve_stats *stats, int mem);
+/* [V,p] = time_ERK(V,p,T,t,dt,options), in place on V and p */
+int ins2d_erk_step(ins2d_ctx *ctx, double *V, double *p, double t, double dt,
+                   ins2d_step_stats *stats, int mem);
+/* nsteps consecutive time_ERK steps from t with a fixed dt (solver_unsteady.m:72-102
+ * without process_iteration); V, p device pointers updated in place. */
+int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int32_t nsteps,
+                  ins2d_step_stats *stats, int mem);
+/* out[4] = {maxdiv, umom, vmom, k} (check_conservation.m:1-76) */
+int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4], int mem);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INS2D_H */

@@ -1,0 +1,117 @@
+"""ctypes binding of libins2d.so (include/ins2d.h).
+
+Loading fails loudly: there is no CPU fallback for the hot path.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libins2d.so")
+
+OK, EINVAL, ENOTCONV, EBREAKDOWN, ENONFINITE, ETIMEOUT, ECUDA, ENOMEM = range(8)
+STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOTCONV", 3: "EBREAKDOWN", 4: "ENONFINITE",
+                5: "ETIMEOUT", 6: "ECUDA", 7: "ENOMEM"}
+BC_CODES = {"dir": 0, "pres": 1, "per": 2, "sym": 3}
+MEM_HOST, MEM_DEVICE = 0, 1
+PREC_FP64, PREC_FP32_STENCIL = 0, 1
+MAX_STAGES = 8
+
+# every symbol include/ins2d.h declares
+EXPORTED = [
+    "ins2d_ctx_create", "ins2d_ctx_destroy", "ins2d_last_error", "ins2d_get_sizes",
+    "ins2d_set_stream", "ins2d_set_bc_values", "ins2d_set_bc_sampler", "ins2d_F",
+    "ins2d_divergence", "ins2d_laplacian", "ins2d_pressure_poisson",
+    "ins2d_pressure_additional_solve", "ins2d_erk_step", "ins2d_erk_run", "ins2d_conservation",
+    "ins2d_profile", "ins2d_profile_read",
+]
+PROF_FAMILIES = ["stage", "div", "poisson", "project", "residual", "other"]
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int32), ("Ny", ctypes.c_int32), ("x", c_double_p), ("y", c_double_p)]
+
+
+class BcDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("u_left", "u_right", "u_low", "u_up", "v_left", "v_right",
+                                               "v_low", "v_up", "bc_unsteady")]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("Re", ctypes.c_double), ("poisson", ctypes.c_int32), ("CG_acc", ctypes.c_double),
+                ("CG_maxit", ctypes.c_int32), ("p_add_solve", ctypes.c_int32), ("rk_stages", ctypes.c_int32),
+                ("rk_A", ctypes.c_double * (MAX_STAGES * MAX_STAGES)), ("rk_b", ctypes.c_double * MAX_STAGES),
+                ("rk_c", ctypes.c_double * MAX_STAGES), ("precision", ctypes.c_int32), ("device", ctypes.c_int32)]
+
+
+BC_VALUE_FIELDS = ("uLo", "uUp", "uLo_i", "uUp_i", "uLe_i", "uRi_i", "vLe", "vRi", "vLo_i", "vUp_i",
+                   "vLe_i", "vRi_i", "pLe", "pRi", "pLo", "pUp", "dudtLe_i", "dudtRi_i", "dvdtLo_i", "dvdtUp_i")
+
+
+class BcValues(ctypes.Structure):
+    _fields_ = [(n, c_double_p) for n in BC_VALUE_FIELDS]
+
+
+class Sizes(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("Nx", "Ny", "Nux_in", "Nuy_in", "Nvx_in", "Nvy_in", "Npx", "Npy",
+                                               "Nu", "Nv", "NV", "Np")]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int32), ("norm1", ctypes.c_double), ("norm2", ctypes.c_double)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("n_solves", ctypes.c_int32), ("iters_total", ctypes.c_int32), ("iters_max", ctypes.c_int32),
+                ("norm1_max", ctypes.c_double)]
+
+
+SAMPLER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p)
+
+_LIB = None
+
+
+def load():
+    """Loads libins2d.so, building it first when the sources are newer."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    from . import build as _build
+    try:
+        _build.build()
+    except Exception as e:  # no nvcc: use an existing library if present
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libins2d.so is missing and could not be built: {e}") from e
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    P = ctypes.POINTER
+    sig = {
+        "ins2d_ctx_create": (ctypes.c_int, [P(GridDesc), P(BcDesc), P(Opts), P(vp)]),
+        "ins2d_ctx_destroy": (ctypes.c_int, [vp]),
+        "ins2d_last_error": (ctypes.c_char_p, [vp]),
+        "ins2d_get_sizes": (ctypes.c_int, [vp, P(Sizes)]),
+        "ins2d_set_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_set_bc_values": (ctypes.c_int, [vp, ctypes.c_double, P(BcValues)]),
+        "ins2d_set_bc_sampler": (ctypes.c_int, [vp, SAMPLER_FN, vp]),
+        "ins2d_F": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, vp, P(ctypes.c_double),
+                                   ctypes.c_int]),
+        "ins2d_divergence": (ctypes.c_int, [vp, vp, vp, P(ctypes.c_double), ctypes.c_int]),
+        "ins2d_laplacian": (ctypes.c_int, [vp, vp, vp, ctypes.c_int]),
+        "ins2d_pressure_poisson": (ctypes.c_int, [vp, vp, vp, P(SolveStats), ctypes.c_int]),
+        "ins2d_pressure_additional_solve": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, P(SolveStats),
+                                                           ctypes.c_int]),
+        "ins2d_erk_step": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, P(StepStats),
+                                          ctypes.c_int]),
+        "ins2d_erk_run": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                         P(StepStats), ctypes.c_int]),
+        "ins2d_conservation": (ctypes.c_int, [vp, vp, ctypes.c_double, P(ctypes.c_double), ctypes.c_int]),
+        "ins2d_profile": (ctypes.c_int, [vp, ctypes.c_int]),
+        "ins2d_profile_read": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_int64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib

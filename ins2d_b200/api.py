@@ -1,0 +1,391 @@
+"""Host-side mirror of the reference's hot-path interface over libins2d.so.
+
+The reference (bsanderse/INS2D, MATLAB) exposes the path as functions of an
+``options`` struct:
+
+  [maxres,F,dF] = F(V,C,p,T,t,options,getJacobian,nopressure)   spatial/F.m:1
+  dp = pressure_poisson(f,t,options)              solvers/pressure/pressure_poisson.m:1
+  p  = pressure_additional_solve(V,p,T,t,options) solvers/pressure/pressure_additional_solve.m:1
+  [Vnew,pnew,Tnew] = time_ERK(Vn,pn,Tn,tn,dt,options)  unsteady/time_ERK.m:1
+  [maxdiv,umom,vmom,k] = check_conservation(V,T,t,options)  spatial/check_conservation.m:1
+
+Here ``options`` is an :class:`Options` (a device context built from the
+grid, the boundary-condition types, the case's uBC/vBC functions and the
+solver settings), and module-level functions with the reference's names and
+argument order call into it.  Arrays are numpy float64 vectors (host memory,
+copied in and out) or contiguous float64 CUDA tensors (used in place), in the
+reference's ordering (x fastest, V = [u; v]).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .rk import getRKmethod
+
+
+class Ins2dError(RuntimeError):
+    """Raised for a non-zero status of the C-ABI (the reference raises a
+    MATLAB error in the same situations, e.g. cg.F:262)."""
+
+    def __init__(self, status, msg):
+        super().__init__(f"{_lib.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _zero_bc(x, y, t):
+    return np.zeros(np.size(x) * np.size(y))
+
+
+def _mesh_positions(x, y, BC):
+    """xin / yin of operator_mesh.m:185-249, 272-320."""
+    L, R = BC["u"]["left"], BC["u"]["right"]
+    if L == "dir" and R == "dir":
+        xin = x[1:-1]
+    elif L == "dir" and R == "pres":
+        xin = x[1:]
+    elif L == "pres" and R == "dir":
+        xin = x[:-1]
+    elif L == "pres" and R == "pres":
+        xin = x.copy()
+    elif L == "per" and R == "per":
+        xin = x[:-1]
+    else:
+        raise ValueError(f"unsupported u-left/u-right combination {L}/{R}")
+    Lo, Up = BC["v"]["low"], BC["v"]["up"]
+    if Lo == "dir" and Up == "dir":
+        yin = y[1:-1]
+    elif Lo == "dir" and Up == "pres":
+        yin = y[1:]
+    elif Lo == "pres" and Up == "dir":
+        yin = y[:-1]
+    elif Lo == "pres" and Up == "pres":
+        yin = y.copy()
+    elif Lo == "per" and Up == "per":
+        yin = y[:-1]
+    else:
+        raise ValueError(f"unsupported v-low/v-up combination {Lo}/{Up}")
+    return xin, yin
+
+
+def _is_torch_cuda(a):
+    return hasattr(a, "is_cuda") and hasattr(a, "data_ptr") and a.is_cuda
+
+
+class _Arr:
+    """A float64 array argument: host numpy (copied) or CUDA tensor (in place)."""
+
+    def __init__(self, a, n, name):
+        if _is_torch_cuda(a):
+            import torch
+            if a.dtype != torch.float64 or not a.is_contiguous() or a.numel() != n:
+                raise ValueError(f"{name}: need a contiguous float64 CUDA tensor of {n} elements")
+            self.dev = True
+            self.obj = a
+            self.ptr = a.data_ptr()
+        else:
+            arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+            if arr.size != n:
+                raise ValueError(f"{name}: expected {n} values, got {arr.size}")
+            self.dev = False
+            self.obj = arr
+            self.ptr = arr.ctypes.data
+
+
+class Options:
+    """The ``options`` struct of the hot path, backed by a device context.
+
+    Parameters mirror the reference's case parameters: grid-line coordinates
+    ``x``, ``y`` (mesh_generation.m), boundary-condition types ``BC``
+    (``{"u": {"left":..,"right":..,"low":..,"up":..}, "v": {...}}`` with
+    'dir'/'pres'/'per'/'sym', boundary_conditions.m), the case's boundary
+    functions ``uBC(x, y, t)`` / ``vBC`` (and ``dudtBC``/``dvdtBC`` for
+    unsteady BCs), ``Re``, ``poisson`` (1-5: device PCG, 6: FFT), ``CG_acc``,
+    ``CG_maxit``, ``p_add_solve``, the RK method name, and ``precision``
+    ('fp64' or 'fp32': FP32 convection/diffusion stencils).
+    """
+
+    def __init__(self, x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_add_solve=1, RK="RK44",
+                 uBC=None, vBC=None, dudtBC=None, dvdtBC=None, pLe=0.0, pRi=0.0, pLo=0.0, pUp=0.0,
+                 precision="fp64", device=0, BC_unsteady=None):
+        self._lib = _lib.load()
+        self.x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+        self.y = np.ascontiguousarray(np.asarray(y, dtype=np.float64))
+        self.BC = {"u": dict(BC["u"]), "v": dict(BC["v"])}
+        unsteady = BC.get("BC_unsteady", 0) if BC_unsteady is None else BC_unsteady
+        self.BC_unsteady = int(unsteady)
+        self.Re = float(Re)
+        self.poisson = int(poisson)
+        self.uBC = uBC or _zero_bc
+        self.vBC = vBC or _zero_bc
+        self.dudtBC = dudtBC or _zero_bc
+        self.dvdtBC = dvdtBC or _zero_bc
+        self.pbc = (pLe, pRi, pLo, pUp)
+        self.RK = RK
+        self._ctx = ctypes.c_void_p()
+        Nx, Ny = len(self.x) - 1, len(self.y) - 1
+        g = _lib.GridDesc(Nx, Ny, self.x.ctypes.data_as(_lib.c_double_p), self.y.ctypes.data_as(_lib.c_double_p))
+        codes = []
+        for comp, sides in (("u", ("left", "right", "low", "up")), ("v", ("left", "right", "low", "up"))):
+            for sd in sides:
+                t = self.BC[comp][sd]
+                if t not in _lib.BC_CODES:
+                    raise ValueError(f"wrong BC for {comp}-{sd}: {t}")
+                codes.append(_lib.BC_CODES[t])
+        b = _lib.BcDesc(*codes, self.BC_unsteady)
+        o = _lib.Opts()
+        o.Re = self.Re
+        o.poisson = self.poisson
+        o.CG_acc = float(CG_acc)
+        o.CG_maxit = int(CG_maxit)
+        o.p_add_solve = int(p_add_solve)
+        A, bb, c = getRKmethod(RK)
+        s = len(bb)
+        o.rk_stages = s
+        for i in range(s):
+            for j in range(s):
+                o.rk_A[i * s + j] = A[i, j]
+            o.rk_b[i] = bb[i]
+            o.rk_c[i] = c[i]
+        o.precision = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32_STENCIL}[precision]
+        o.device = int(device)
+        rc = self._lib.ins2d_ctx_create(ctypes.byref(g), ctypes.byref(b), ctypes.byref(o), ctypes.byref(self._ctx))
+        if rc != 0:
+            msg = self._err()
+            self._lib.ins2d_ctx_destroy(self._ctx)
+            self._ctx = None
+            raise Ins2dError(rc, msg)
+        sz = _lib.Sizes()
+        self._lib.ins2d_get_sizes(self._ctx, ctypes.byref(sz))
+        for f, _ in _lib.Sizes._fields_:
+            setattr(self, f, int(getattr(sz, f)))
+        self.xp = (self.x[:-1] + self.x[1:]) / 2
+        self.yp = (self.y[:-1] + self.y[1:]) / 2
+        self.xin, self.yin = _mesh_positions(self.x, self.y, self.BC)
+        # positions of the unknowns (operator_mesh.m:401-409)
+        self.xu = np.tile(self.xin, self.Nuy_in)
+        self.yu = np.repeat(self.yp, self.Nux_in)
+        self.xv = np.tile(self.xp, self.Nvy_in)
+        self.yv = np.repeat(self.yin, self.Nvx_in)
+        self._sampler = None
+        if self.BC_unsteady:
+            def _cb(user, t, ctx):
+                try:
+                    self.set_bc_vectors(t)
+                    return 0
+                except Exception:  # report through the C status
+                    return _lib.EINVAL
+            self._sampler = _lib.SAMPLER_FN(_cb)
+            self._lib.ins2d_set_bc_sampler(self._ctx, self._sampler, None)
+        self.set_bc_vectors(0.0)
+
+    # -- plumbing ------------------------------------------------------------
+    def _err(self):
+        m = self._lib.ins2d_last_error(self._ctx)
+        return m.decode() if m else ""
+
+    def _check(self, rc):
+        if rc != 0:
+            raise Ins2dError(rc, self._err())
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.ins2d_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _mem(*arrs):
+        kinds = {a.dev for a in arrs if a is not None}
+        if len(kinds) > 1:
+            raise ValueError("mix of host and device arrays")
+        return _lib.MEM_DEVICE if kinds == {True} else _lib.MEM_HOST
+
+    def _like(self, ref, n):
+        if ref.dev:
+            import torch
+            return torch.empty(n, dtype=torch.float64, device=ref.obj.device)
+        return np.empty(n)
+
+    def profile(self, enable=True):
+        """Start (or stop) per-kernel-family device timing with CUDA events."""
+        self._check(self._lib.ins2d_profile(self._ctx, int(bool(enable))))
+
+    def profile_read(self):
+        """{family: (device ms, launches)} since the last read."""
+        ms = (ctypes.c_double * len(_lib.PROF_FAMILIES))()
+        n = (ctypes.c_int64 * len(_lib.PROF_FAMILIES))()
+        self._check(self._lib.ins2d_profile_read(self._ctx, ms, n))
+        return {f: (ms[i], int(n[i])) for i, f in enumerate(_lib.PROF_FAMILIES)}
+
+    def set_stream(self, stream):
+        """Issue work on a CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self._lib.ins2d_set_stream(self._ctx, ctypes.c_void_p(stream)))
+
+    # -- boundary conditions ----------------------------------------------------
+    def bc_samples(self, t):
+        """The samples set_bc_vectors.m:52-79 takes from uBC/vBC at time t."""
+        x, y, xp, yp, xin, yin = self.x, self.y, self.xp, self.yp, self.xin, self.yin
+        u, v = self.uBC, self.vBC
+        s = dict(uLo=u(x, y[0], t), uUp=u(x, y[-1], t), uLo_i=u(xin, y[0], t), uUp_i=u(xin, y[-1], t),
+                 uLe_i=u(x[0], yp, t), uRi_i=u(x[-1], yp, t), vLe=v(x[0], y, t), vRi=v(x[-1], y, t),
+                 vLo_i=v(xp, y[0], t), vUp_i=v(xp, y[-1], t), vLe_i=v(x[0], yin, t), vRi_i=v(x[-1], yin, t))
+        pLe, pRi, pLo, pUp = self.pbc
+        s.update(pLe=np.broadcast_to(pLe, (len(yp),)), pRi=np.broadcast_to(pRi, (len(yp),)),
+                 pLo=np.broadcast_to(pLo, (len(xp),)), pUp=np.broadcast_to(pUp, (len(xp),)))
+        if self.BC_unsteady:
+            s.update(dudtLe_i=self.dudtBC(x[0], yp, t), dudtRi_i=self.dudtBC(x[-1], yp, t),
+                     dvdtLo_i=self.dvdtBC(xp, y[0], t), dvdtUp_i=self.dvdtBC(xp, y[-1], t))
+        return {k: np.ascontiguousarray(np.asarray(v_, dtype=np.float64).ravel()) for k, v_ in s.items()}
+
+    def set_bc_vectors(self, t):
+        """set_bc_vectors(t,options): samples the boundary functions and sends
+        them to the device."""
+        s = self.bc_samples(t)
+        vals = _lib.BcValues()
+        keep = []
+        for name in _lib.BC_VALUE_FIELDS:
+            if name in s:
+                arr = s[name]
+                keep.append(arr)
+                setattr(vals, name, arr.ctypes.data_as(_lib.c_double_p))
+        self._check(self._lib.ins2d_set_bc_values(self._ctx, float(t), ctypes.byref(vals)))
+
+    # -- hot path ----------------------------------------------------------------
+    def F(self, V, C=None, p=None, t=0.0, nopressure=0):
+        """[maxres, F] = F(V,C,p,T,t,options,0,nopressure)."""
+        Va = _Arr(V, self.NV, "V")
+        Ca = _Arr(C, self.NV, "C") if C is not None and C is not V else None
+        pa = None if nopressure else _Arr(p, self.Np, "p")
+        out = self._like(Va, self.NV)
+        Oa = _Arr(out, self.NV, "F")
+        mem = self._mem(Va, Ca, pa, Oa)
+        mr = ctypes.c_double()
+        self._check(self._lib.ins2d_F(self._ctx, Va.ptr, Ca.ptr if Ca else None, pa.ptr if pa else None, float(t),
+                                      int(bool(nopressure)), Oa.ptr, ctypes.byref(mr), mem))
+        return mr.value, out
+
+    def divergence(self, V):
+        """M*V + yM and its max (check_conservation.m:37)."""
+        Va = _Arr(V, self.NV, "V")
+        out = self._like(Va, self.Np)
+        Oa = _Arr(out, self.Np, "f")
+        md = ctypes.c_double()
+        self._check(self._lib.ins2d_divergence(self._ctx, Va.ptr, Oa.ptr, ctypes.byref(md), self._mem(Va, Oa)))
+        return out, md.value
+
+    def laplacian(self, p):
+        """A*p with A = M*diag(Om_inv)*G."""
+        pa = _Arr(p, self.Np, "p")
+        out = self._like(pa, self.Np)
+        Oa = _Arr(out, self.Np, "Ap")
+        self._check(self._lib.ins2d_laplacian(self._ctx, pa.ptr, Oa.ptr, self._mem(pa, Oa)))
+        return out
+
+    def pressure_poisson(self, f, t=0.0, return_stats=False):
+        """dp = pressure_poisson(f,t,options)."""
+        fa = _Arr(f, self.Np, "f")
+        out = self._like(fa, self.Np)
+        Oa = _Arr(out, self.Np, "dp")
+        st = _lib.SolveStats()
+        self._check(self._lib.ins2d_pressure_poisson(self._ctx, fa.ptr, Oa.ptr, ctypes.byref(st), self._mem(fa, Oa)))
+        if return_stats:
+            return out, dict(iters=st.iters, norm1=st.norm1, norm2=st.norm2)
+        return out
+
+    def pressure_additional_solve(self, V, p, t=0.0, return_stats=False):
+        """p = pressure_additional_solve(V,p,T,t,options) (returns a new p for
+        host arrays, updates a device p in place)."""
+        Va = _Arr(V, self.NV, "V")
+        pa = _Arr(p if _is_torch_cuda(p) else np.array(p, dtype=np.float64), self.Np, "p")
+        st = _lib.SolveStats()
+        self._check(self._lib.ins2d_pressure_additional_solve(self._ctx, Va.ptr, pa.ptr, float(t), ctypes.byref(st),
+                                                              self._mem(Va, pa)))
+        if return_stats:
+            return pa.obj, dict(iters=st.iters, norm1=st.norm1, norm2=st.norm2)
+        return pa.obj
+
+    def time_ERK(self, Vn, pn, tn, dt, nsteps=1, return_stats=False):
+        """[Vnew, pnew] = time_ERK(Vn,pn,Tn,tn,dt,options); with nsteps > 1 the
+        solver_unsteady.m time loop of that many steps.  Host arrays are
+        copied (inputs untouched); device tensors are updated in place."""
+        if _is_torch_cuda(Vn):
+            Va, pa = _Arr(Vn, self.NV, "V"), _Arr(pn, self.Np, "p")
+        else:
+            Va = _Arr(np.array(Vn, dtype=np.float64), self.NV, "V")
+            pa = _Arr(np.array(pn, dtype=np.float64), self.Np, "p")
+        st = _lib.StepStats()
+        self._check(self._lib.ins2d_erk_run(self._ctx, Va.ptr, pa.ptr, float(tn), float(dt), int(nsteps),
+                                            ctypes.byref(st), self._mem(Va, pa)))
+        if return_stats:
+            return Va.obj, pa.obj, dict(n_solves=st.n_solves, iters_total=st.iters_total, iters_max=st.iters_max,
+                                        norm1_max=st.norm1_max)
+        return Va.obj, pa.obj
+
+    def check_conservation(self, V, t=0.0):
+        """[maxdiv, umom, vmom, k] = check_conservation(V,T,t,options)."""
+        Va = _Arr(V, self.NV, "V")
+        out = (ctypes.c_double * 4)()
+        self._check(self._lib.ins2d_conservation(self._ctx, Va.ptr, float(t), out, self._mem(Va)))
+        return tuple(out)
+
+    def initial_projection(self, V, t=0.0):
+        """input_check.m:95-111: project V when max|div| > 1e-12."""
+        f, maxdiv = self.divergence(V)
+        if maxdiv > 1e-12:
+            dp = self.pressure_poisson(f, t)
+            G_dp_scaled = self.F(np.zeros(self.NV), None, dp, t)[1] - self.F(np.zeros(self.NV), None, np.zeros(self.Np), t)[1]
+            # F(0,.,dp) - F(0,.,0) = -G*dp ; V - Om^-1 G dp = V + Om^-1 (that difference)
+            V = np.asarray(V, dtype=np.float64) + self.Om_inv() * G_dp_scaled
+        return V
+
+    def Om_inv(self):
+        """Om_inv (operator_mesh.m:331-352) as a host vector."""
+        hx, hy = np.diff(self.x), np.diff(self.y)
+        gx = np.zeros(len(hx) + 1)
+        gx[0], gx[-1] = hx[0] / 2, hx[-1] / 2
+        gx[1:-1] = (hx[:-1] + hx[1:]) / 2
+        gy = np.zeros(len(hy) + 1)
+        gy[0], gy[-1] = hy[0] / 2, hy[-1] / 2
+        gy[1:-1] = (hy[:-1] + hy[1:]) / 2
+        L, R = self.BC["u"]["left"], self.BC["u"]["right"]
+        gxi = {("dir", "dir"): gx[1:-1], ("dir", "pres"): gx[1:], ("pres", "dir"): gx[:-1], ("pres", "pres"): gx,
+               ("per", "per"): np.r_[gx[0] + gx[-1], gx[1:-1]]}[(L, R)]
+        Lo, Up = self.BC["v"]["low"], self.BC["v"]["up"]
+        gyi = {("dir", "dir"): gy[1:-1], ("dir", "pres"): gy[1:], ("pres", "dir"): gy[:-1], ("pres", "pres"): gy,
+               ("per", "per"): np.r_[gy[0] + gy[-1], gy[1:-1]]}[(Lo, Up)]
+        return 1.0 / np.r_[np.kron(hy, gxi), np.kron(gyi, hx)]
+
+
+# -- module-level functions with the reference's names ------------------------------
+def F(V, C, p, T, t, options, getJacobian=0, nopressure=0):
+    """[maxres,F,dF] = F(V,C,p,T,t,options,getJacobian,nopressure); the
+    Jacobian is not part of this path (dF is None)."""
+    if getJacobian:
+        raise NotImplementedError("the Jacobian of F is not part of the explicit path")
+    maxres, Fv = options.F(V, C, p, t, nopressure)
+    return maxres, Fv, None
+
+
+def pressure_poisson(f, t, options):
+    return options.pressure_poisson(f, t)
+
+
+def pressure_additional_solve(V, p, T, t, options):
+    return options.pressure_additional_solve(V, p, t)
+
+
+def time_ERK(Vn, pn, Tn, tn, dt, options):
+    V, p = options.time_ERK(Vn, pn, tn, dt)
+    return V, p, 0
+
+
+def check_conservation(V, T, t, options):
+    return options.check_conservation(V, t)

@@ -1,0 +1,828 @@
+// Context and C-ABI of libins2d.so (include/ins2d.h).
+//
+// The context plays the role of the reference's `options` struct: it holds
+// the device-resident operator tables (derived once, setup.cpp), the boundary
+// values of the current time, the Butcher tableau and the solver settings.
+// time_ERK's stage loop (unsteady/time_ERK.m:78-168) is orchestrated here on
+// the host; all arithmetic runs in the device kernels on the context stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ins2d.h"
+#include "kernels.cuh"
+#include "setup.hpp"
+
+namespace ins2d {
+void fft_prepare();
+}
+
+using namespace ins2d;
+
+struct ins2d_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  HostOps H;
+  DevOps P{};
+  ins2d_opts opts{};
+  ins2d_bc_desc bcd{};
+  bool fp32 = false;
+  int poisson = 4;
+  std::string err;
+  std::vector<void *> allocs;
+  // RK tableau shifted as in time_ERK.m:29-32
+  int s = 0;
+  double A[kMaxStages][kMaxStages] = {};
+  double c[kMaxStages] = {};
+  bool need_store[kMaxStages] = {};
+  // device work arrays
+  double *Vs = nullptr, *Wt = nullptr, *kV[kMaxStages] = {};
+  double *f = nullptr, *dp = nullptr, *wres = nullptr;
+  double *stV = nullptr, *stC = nullptr, *stO = nullptr, *stP = nullptr, *stQ = nullptr;  // host-mode staging
+  double *bcblob = nullptr;
+  size_t bc_count = 0;
+  RedScratch red;
+  FftPlan fft;
+  PcgWork pcg{};
+  PcgScalars *h_sc = nullptr;   // pinned
+  double *h_red = nullptr;      // pinned
+  // host copies of boundary samples (check_conservation.m boundary terms)
+  std::vector<double> uLe_i, uRi_i, vLo_i, vUp_i;
+  ins2d_bc_sampler_fn sampler = nullptr;
+  void *sampler_user = nullptr;
+  double bc_time = 0.0;
+  // launch counts and optional device-time profile per kernel family
+  long long launches[INS2D_PROF_N] = {};
+  bool prof = false;
+  struct Rec {
+    int fam;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+};
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                                   \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+template <typename T>
+T *dalloc(ins2d_ctx *c, size_t n) {
+  void *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) throw std::bad_alloc();
+  c->allocs.push_back(p);
+  return (T *)p;
+}
+
+Tab upload_tab(ins2d_ctx *c, const Table &t) {
+  Tab d;
+  int32_t *cc = dalloc<int32_t>(c, t.col.size());
+  double *w = dalloc<double>(c, t.w.size());
+  double *b1 = dalloc<double>(c, t.b1.size());
+  double *b2 = dalloc<double>(c, t.b2.size());
+  CK(cudaMemcpy(cc, t.col.data(), t.col.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(w, t.w.data(), t.w.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b1, t.b1.data(), t.b1.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b2, t.b2.data(), t.b2.size() * sizeof(double), cudaMemcpyHostToDevice));
+  d.c = cc;
+  d.w = w;
+  d.b1 = b1;
+  d.b2 = b2;
+  return d;
+}
+
+const double *upload_vec(ins2d_ctx *c, const std::vector<double> &v) {
+  double *d = dalloc<double>(c, v.size());
+  if (!v.empty()) CK(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return d;
+}
+
+// Layout of the boundary-value blob: {name, length}.
+struct BcSlot {
+  const double **dst;
+  int n;
+};
+
+std::vector<BcSlot> bc_slots(ins2d_ctx *c) {
+  HostOps &H = c->H;
+  BcVals &b = c->P.bc;
+  return {{&b.uLo, H.Nx + 1},   {&b.uUp, H.Nx + 1},   {&b.uLo_i, H.Nux},   {&b.uUp_i, H.Nux},
+          {&b.uLe_i, H.Ny},     {&b.uRi_i, H.Ny},     {&b.vLe, H.Ny + 1},  {&b.vRi, H.Ny + 1},
+          {&b.vLo_i, H.Nx},     {&b.vUp_i, H.Nx},     {&b.vLe_i, H.Nvy},   {&b.vRi_i, H.Nvy},
+          {&b.XvLo, H.Nux},     {&b.XvUp, H.Nux},     {&b.YuLe, H.Nvy},    {&b.YuRi, H.Nvy},
+          {&b.pLe, H.Ny},       {&b.pRi, H.Ny},       {&b.pLo, H.Nx},      {&b.pUp, H.Nx},
+          {&b.dudtLe_i, H.Ny},  {&b.dudtRi_i, H.Ny},  {&b.dvdtLo_i, H.Nx}, {&b.dvdtUp_i, H.Nx}};
+}
+
+cudaEvent_t take_event(ins2d_ctx *c) {
+  if (!c->pool.empty()) {
+    cudaEvent_t e = c->pool.back();
+    c->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+// Brackets the launches of one kernel family with CUDA events on the
+// context stream when profiling is on; counts the launches always.
+struct Prof {
+  ins2d_ctx *c;
+  int fam;
+  cudaEvent_t b = nullptr;
+  Prof(ins2d_ctx *c_, int fam_, int nlaunch) : c(c_), fam(fam_) {
+    c->launches[fam] += nlaunch;
+    if (c->prof) {
+      b = take_event(c);
+      CK(cudaEventRecord(b, c->stream));
+    }
+  }
+  ~Prof() {
+    if (c->prof && b) {
+      cudaEvent_t e = take_event(c);
+      cudaEventRecord(e, c->stream);
+      c->recs.push_back({fam, b, e});
+    }
+  }
+};
+
+int fail(ins2d_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+void setup_rk(ins2d_ctx *c) {
+  // default: classical RK44 (getRKmethod.m:313-316)
+  int s = c->opts.rk_stages;
+  double A0[kMaxStages][kMaxStages] = {}, b0[kMaxStages] = {}, c0[kMaxStages] = {};
+  if (s <= 0) {
+    s = 4;
+    A0[1][0] = 0.5;
+    A0[2][1] = 0.5;
+    A0[3][2] = 1.0;
+    b0[0] = 1.0 / 6;
+    b0[1] = 1.0 / 3;
+    b0[2] = 1.0 / 3;
+    b0[3] = 1.0 / 6;
+    c0[1] = 0.5;
+    c0[2] = 0.5;
+    c0[3] = 1.0;
+  } else {
+    for (int i = 0; i < s; ++i) {
+      for (int j = 0; j < s; ++j) A0[i][j] = c->opts.rk_A[i * s + j];
+      b0[i] = c->opts.rk_b[i];
+      c0[i] = c->opts.rk_c[i];
+    }
+  }
+  c->s = s;
+  // shifted tableau (time_ERK.m:29-32): rows 2..s of A then b'; c = [c(2:end); 1]
+  for (int i = 0; i < s; ++i)
+    for (int j = 0; j < s; ++j) c->A[i][j] = (i < s - 1) ? A0[i + 1][j] : b0[j];
+  for (int i = 0; i < s; ++i) c->c[i] = (i < s - 1) ? c0[i + 1] : 1.0;
+  for (int m = 0; m < s; ++m) {
+    c->need_store[m] = false;
+    for (int i = m + 1; i < s; ++i)
+      if (c->A[i][m] != 0.0) c->need_store[m] = true;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Poisson solve: dp = pressure_poisson(f) (or dp += ... when accumulate)
+int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st) {
+  if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
+  if (c->poisson == INS2D_POISSON_FFT) {
+    Prof pr(c, INS2D_PROF_POISSON, 3);
+    launch_fft_poisson(c->P, c->fft, f, dp, accumulate, c->stream);
+    CK(cudaGetLastError());
+    return INS2D_OK;
+  }
+  Prof pr(c, INS2D_PROF_POISSON, 2);
+  pcg_init(c->P, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
+  CK(cudaGetLastError());
+  int chunk = 4;
+  long long launched = 0;
+  for (;;) {
+    CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->h_sc->done) break;
+    if (launched > (long long)c->opts.CG_maxit + 1024)
+      return fail(c, INS2D_ETIMEOUT, "PCG: device convergence flag never set");
+    pcg_iterations(c->P, c->pcg, chunk, c->stream);
+    CK(cudaGetLastError());
+    c->launches[INS2D_PROF_POISSON] += 3LL * chunk;
+    launched += chunk;
+    chunk = std::min(chunk * 2, 128);
+  }
+  const PcgScalars &h = *c->h_sc;
+  if (st) {
+    st->iters = (int32_t)h.it;
+    st->norm1 = std::sqrt(h.rr);
+    st->norm2 = (h.maxx - h.minx) != 0.0 ? h.maxres / (h.maxx - h.minx) : 0.0;
+  }
+  if (h.status == INS2D_ENOTCONV) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "CG didn't converge in %d iterations; residual= %g", c->opts.CG_maxit,
+             std::sqrt(h.rr));
+    return fail(c, INS2D_ENOTCONV, buf);
+  }
+  if (h.status == INS2D_EBREAKDOWN) return fail(c, INS2D_EBREAKDOWN, "PCG breakdown: p'Ap = 0");
+  if (h.status == INS2D_ENONFINITE) return fail(c, INS2D_ENONFINITE, "PCG: non-finite residual");
+  pcg_finish(c->P, c->pcg, dp, accumulate, c->stream);
+  c->launches[INS2D_PROF_POISSON] += 1;
+  CK(cudaGetLastError());
+  return INS2D_OK;
+}
+
+void stats_add(ins2d_step_stats *s, const ins2d_solve_stats &o) {
+  if (!s) return;
+  s->n_solves += 1;
+  s->iters_total += o.iters;
+  s->iters_max = std::max(s->iters_max, o.iters);
+  s->norm1_max = std::max(s->norm1_max, o.norm1);
+}
+
+int sample_bc(ins2d_ctx *c, double t) {
+  if (!c->bcd.bc_unsteady) return INS2D_OK;
+  if (!c->sampler) return fail(c, INS2D_EINVAL, "unsteady boundary conditions need a sampler (ins2d_set_bc_sampler)");
+  int rc = c->sampler(c->sampler_user, t, c);
+  if (rc != INS2D_OK && c->err.empty()) c->err = "boundary sampler failed";
+  return rc;
+}
+
+// p = pressure_additional_solve(V,p,T,t,options)   (device pointers)
+int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_solve_stats *st) {
+  int rc = sample_bc(c, t);
+  if (rc) return rc;
+  {
+    Prof pr(c, INS2D_PROF_RESIDUAL, 1);
+    launch_residual(c->P, V, p, c->wres, nullptr, c->fp32, c->stream);
+  }
+  {
+    Prof pr(c, INS2D_PROF_DIV, 1);
+    launch_div(c->P, c->wres, 0.0, c->bcd.bc_unsteady ? 1.0 : 0.0, 1.0, c->f, false, c->red, c->stream);
+  }
+  CK(cudaGetLastError());
+  return solve(c, c->f, p, true, st);
+}
+
+// [V,p] = time_ERK(V,p,T,t,dt,options) on device pointers, in place.
+int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step_stats *stats) {
+  const DevOps &P = c->P;
+  int rc = sample_bc(c, t);
+  if (rc) return rc;
+  const double *dpp = nullptr;
+  for (int i = 0; i < c->s; ++i) {
+    StageArgs a{};
+    a.V = (i == 0) ? V : c->Vs;
+    a.Vn = V;
+    a.kV = c->need_store[i] ? c->kV[i] : nullptr;
+    a.nprev = 0;
+    for (int m = 0; m < i; ++m)
+      if (c->A[i][m] != 0.0) {
+        a.kprev[a.nprev] = c->kV[m];
+        a.aprev[a.nprev] = c->A[i][m];
+        ++a.nprev;
+      }
+    a.aii = c->A[i][i];
+    a.inv_dt = 1.0 / dt;
+    a.Wt = c->Wt;
+    {
+      Prof pr(c, INS2D_PROF_STAGE, 1);
+      launch_stage(P, a, c->fp32, c->stream);
+    }
+    const double ti = t + c->c[i] * dt;
+    if (c->bcd.bc_unsteady) {
+      rc = sample_bc(c, ti);
+      if (rc) return rc;
+    }
+    if (c->bcd.bc_unsteady || i > 0) {
+      // f = (M*(Vn/dt + Vtemp) + yM/dt)/c_i   (time_ERK.m:117)
+      {
+        Prof pr(c, INS2D_PROF_DIV, 1);
+        launch_div(P, c->Wt, 1.0 / dt, 0.0, 1.0 / c->c[i], c->f, false, c->red, c->stream);
+      }
+      ins2d_solve_stats st;
+      rc = solve(c, c->f, c->dp, false, &st);
+      if (rc) return rc;
+      stats_add(stats, st);
+      dpp = c->dp;
+    } else {
+      dpp = p;  // time_ERK.m:125-127
+    }
+    {
+      Prof pr(c, INS2D_PROF_PROJECT, 1);
+      launch_project(P, c->Wt, dpp, dt, c->c[i], (i == c->s - 1) ? V : c->Vs, c->stream);
+    }
+    CK(cudaGetLastError());
+  }
+  if (c->bcd.bc_unsteady && !c->opts.p_add_solve) {
+    CK(cudaMemcpyAsync(p, dpp, P.Np * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));  // p = kp(:,end)
+  } else {
+    ins2d_solve_stats st;
+    rc = additional_solve(c, V, p, t + dt, &st);
+    if (rc) return rc;
+    stats_add(stats, st);
+  }
+  return INS2D_OK;
+}
+
+// device pointer or host staging copy
+const double *in_dev(ins2d_ctx *c, const double *src, double *stage, size_t n, int mem) {
+  if (!src) return nullptr;
+  if (mem == INS2D_MEM_DEVICE) return src;
+  CK(cudaMemcpyAsync(stage, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return stage;
+}
+
+int check_mem(ins2d_ctx *c, int mem) {
+  if (mem != INS2D_MEM_HOST && mem != INS2D_MEM_DEVICE) return fail(c, INS2D_EINVAL, "mem must be INS2D_MEM_HOST or INS2D_MEM_DEVICE");
+  return INS2D_OK;
+}
+
+#define API_BEGIN \
+  if (!ctx) return INS2D_EINVAL; \
+  ctx->err.clear();              \
+  try {                          \
+    CK(cudaSetDevice(ctx->device));
+#define API_END                                                  \
+  }                                                              \
+  catch (const CudaError &e) {                                   \
+    return fail(ctx, INS2D_ECUDA, e.what());                     \
+  }                                                              \
+  catch (const std::bad_alloc &) {                               \
+    return fail(ctx, INS2D_ENOMEM, "device allocation failed");  \
+  }                                                              \
+  catch (const std::exception &e) {                              \
+    return fail(ctx, INS2D_EINVAL, e.what());                    \
+  }
+
+}  // namespace
+
+extern "C" {
+
+int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const ins2d_opts *opts, ins2d_ctx **out) {
+  if (!grid || !bc || !opts || !out || !grid->x || !grid->y) return INS2D_EINVAL;
+  *out = nullptr;
+  ins2d_ctx *c = new (std::nothrow) ins2d_ctx();
+  if (!c) return INS2D_ENOMEM;
+  c->opts = *opts;
+  c->bcd = *bc;
+  c->device = opts->device;
+  c->fp32 = opts->precision == INS2D_PREC_FP32_STENCIL;
+  c->poisson = opts->poisson;
+  int rc = INS2D_OK;
+  try {
+    if (!(opts->Re > 0)) throw std::invalid_argument("Re must be positive");
+    if (opts->precision != INS2D_PREC_FP64 && opts->precision != INS2D_PREC_FP32_STENCIL)
+      throw std::invalid_argument("unknown precision");
+    if (opts->poisson < 1 || opts->poisson > 6) throw std::invalid_argument("wrong poisson method");
+    if (opts->poisson != INS2D_POISSON_FFT && !(opts->CG_acc > 0)) throw std::invalid_argument("CG_acc must be positive");
+    if (opts->poisson != INS2D_POISSON_FFT && opts->CG_maxit < 1) throw std::invalid_argument("CG_maxit must be >= 1");
+    if (opts->rk_stages < 0 || opts->rk_stages > kMaxStages) throw std::invalid_argument("rk_stages out of range");
+    for (int i = 0; i < opts->rk_stages; ++i)
+      for (int j = i; j < opts->rk_stages; ++j)
+        if (opts->rk_A[i * opts->rk_stages + j] != 0.0) throw std::invalid_argument("Butcher tableau is not explicit");
+    CK(cudaSetDevice(c->device));
+    int bcs[8] = {bc->u_left, bc->u_right, bc->u_low, bc->u_up, bc->v_left, bc->v_right, bc->v_low, bc->v_up};
+    build_host_ops(c->H, grid->Nx, grid->Ny, grid->x, grid->y, bcs, opts->Re);
+    if (c->poisson == INS2D_POISSON_FFT) {
+      if (!c->H.fft_ok)
+        throw std::invalid_argument(
+            "Fourier transform for pressure Poisson needs periodic boundary conditions and a uniform grid");
+      if (!fft_supported(grid->Nx, grid->Ny)) throw std::invalid_argument("grid size not supported by the FFT solver");
+    }
+    setup_rk(c);
+    HostOps &H = c->H;
+    DevOps &P = c->P;
+    P.Nx = H.Nx; P.Ny = H.Ny; P.Nux = H.Nux; P.Nuy = H.Nuy; P.Nvx = H.Nvx; P.Nvy = H.Nvy;
+    P.Npx = H.Npx; P.Npy = H.Npy;
+    P.Nu = H.Nu(); P.Nv = H.Nv(); P.Np = H.Np();
+    P.invRe = 1.0 / H.Re;
+    P.AUX = upload_tab(c, H.AUX); P.SUX = upload_tab(c, H.SUX); P.AUY = upload_tab(c, H.AUY);
+    P.SUY = upload_tab(c, H.SUY); P.IVX = upload_tab(c, H.IVX); P.IVY = upload_tab(c, H.IVY);
+    P.MX = upload_tab(c, H.MX); P.MXT = upload_tab(c, H.MXT);
+    P.AVX = upload_tab(c, H.AVX); P.SVX = upload_tab(c, H.SVX); P.AVY = upload_tab(c, H.AVY);
+    P.SVY = upload_tab(c, H.SVY); P.IUX = upload_tab(c, H.IUX); P.IUY = upload_tab(c, H.IUY);
+    P.MY = upload_tab(c, H.MY); P.MYT = upload_tab(c, H.MYT);
+    P.TX = upload_tab(c, H.TX); P.TY = upload_tab(c, H.TY);
+    P.TXd = upload_vec(c, H.TXd); P.TYd = upload_vec(c, H.TYd);
+    P.hx = upload_vec(c, H.hx); P.hy = upload_vec(c, H.hy);
+    P.gxi = upload_vec(c, H.gxi); P.gyi = upload_vec(c, H.gyi);
+    P.pxl = upload_vec(c, H.pxl); P.pxr = upload_vec(c, H.pxr);
+    P.pyl = upload_vec(c, H.pyl); P.pyu = upload_vec(c, H.pyu);
+    auto reg = [&](const Regular &r, const Table &t) {
+      RegD d;
+      d.s = r.s;
+      d.lo = r.lo;
+      d.hi = r.hi;
+      d.two = r.two;
+      d.w0 = upload_vec(c, t.rw0);
+      d.w1 = upload_vec(c, t.rw1);
+      return d;
+    };
+    P.rAUX = reg(H.rAUX, H.AUX); P.rSUX = reg(H.rAUX, H.SUX);
+    P.rAUY = reg(H.rAUY, H.AUY); P.rSUY = reg(H.rAUY, H.SUY);
+    P.rIVX = reg(H.rIVX, H.IVX); P.rIVY = reg(H.rIVY, H.IVY); P.rMXT = reg(H.rMXT, H.MXT);
+    P.rAVX = reg(H.rAVX, H.AVX); P.rSVX = reg(H.rAVX, H.SVX);
+    P.rAVY = reg(H.rAVY, H.AVY); P.rSVY = reg(H.rAVY, H.SVY);
+    P.rIUX = reg(H.rIUX, H.IUX); P.rIUY = reg(H.rIUY, H.IUY); P.rMYT = reg(H.rMYT, H.MYT);
+    walker_rectangle(P);
+    if (H.fft_ok) {
+      P.fft_ax = upload_vec(c, H.fft_ax);
+      P.fft_ay = upload_vec(c, H.fft_ay);
+      P.fft_dxdy = H.fft_dxdy;
+    } else {
+      P.fft_ax = P.fft_ay = nullptr;
+      P.fft_dxdy = 0.0;
+    }
+    // boundary values (zero until ins2d_set_bc_values)
+    auto slots = bc_slots(c);
+    size_t tot = 0;
+    for (auto &s : slots) tot += (size_t)s.n;
+    c->bc_count = tot;
+    c->bcblob = dalloc<double>(c, tot);
+    CK(cudaMemset(c->bcblob, 0, tot * sizeof(double)));
+    size_t off = 0;
+    for (auto &s : slots) {
+      *s.dst = c->bcblob + off;
+      off += (size_t)s.n;
+    }
+    c->uLe_i.assign(H.Ny, 0.0); c->uRi_i.assign(H.Ny, 0.0);
+    c->vLo_i.assign(H.Nx, 0.0); c->vUp_i.assign(H.Nx, 0.0);
+    // work arrays
+    const size_t NV = (size_t)(P.Nu + P.Nv), Np = (size_t)P.Np;
+    c->Vs = dalloc<double>(c, NV);
+    c->Wt = dalloc<double>(c, NV);
+    for (int m = 0; m < c->s; ++m) c->kV[m] = c->need_store[m] ? dalloc<double>(c, NV) : nullptr;
+    c->wres = dalloc<double>(c, NV);
+    c->f = dalloc<double>(c, Np);
+    c->dp = dalloc<double>(c, Np);
+    c->stV = dalloc<double>(c, NV);
+    c->stC = dalloc<double>(c, NV);
+    c->stO = dalloc<double>(c, NV);
+    c->stP = dalloc<double>(c, Np);
+    c->stQ = dalloc<double>(c, Np);
+    const int nx = std::max(P.Nux, P.Nvx), ny = std::max(P.Nuy, P.Nvy);
+    const int maxb = ((nx + 31) / 32) * ((ny + 7) / 8) + 64;
+    c->red.partials = dalloc<double>(c, (size_t)maxb * kRedQ);
+    c->red.counter = dalloc<unsigned int>(c, 1);
+    c->red.result = dalloc<double>(c, kRedQ);
+    c->red.max_blocks = maxb;
+    CK(cudaMemset(c->red.counter, 0, sizeof(unsigned int)));
+    if (c->poisson == INS2D_POISSON_FFT) {
+      fft_prepare();
+      FftPlan &F = c->fft;
+      F.Nx = H.Nx;
+      F.Ny = H.Ny;
+      F.logx = is_pow2(H.Nx) ? (int)std::lround(std::log2((double)H.Nx)) : -1;
+      F.logy = is_pow2(H.Ny) ? (int)std::lround(std::log2((double)H.Ny)) : -1;
+      auto tw = [&](int n) {
+        std::vector<double> v(2 * (size_t)n);
+        for (int k = 0; k < n; ++k) {
+          const double ang = 2.0 * M_PI * (double)k / (double)n;
+          v[2 * k] = std::cos(ang);
+          v[2 * k + 1] = -std::sin(ang);
+        }
+        return v;
+      };
+      auto tx = tw(H.Nx), ty = tw(H.Ny);
+      F.twx = dalloc<double2>(c, H.Nx);
+      F.twy = dalloc<double2>(c, H.Ny);
+      CK(cudaMemcpy(F.twx, tx.data(), tx.size() * sizeof(double), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(F.twy, ty.data(), ty.size() * sizeof(double), cudaMemcpyHostToDevice));
+      F.spec = dalloc<double2>(c, (size_t)(H.Nx / 2 + 1) * H.Ny);
+      F.maxabs = dalloc<double>(c, 1);
+    } else {
+      PcgWork &W = c->pcg;
+      W.x = dalloc<double>(c, Np);
+      W.r = dalloc<double>(c, Np);
+      W.p = dalloc<double>(c, Np);
+      W.q = dalloc<double>(c, Np);
+      W.sc = dalloc<PcgScalars>(c, 1);
+      W.blocks = pcg_blocks(P);
+      W.partials = dalloc<double>(c, (size_t)W.blocks * 8 + 16);
+      CK(cudaMemset(W.sc, 0, sizeof(PcgScalars)));
+    }
+    CK(cudaMallocHost((void **)&c->h_sc, sizeof(PcgScalars)));
+    CK(cudaMallocHost((void **)&c->h_red, sizeof(double) * kRedQ));
+    CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    CK(cudaDeviceSynchronize());
+  } catch (const CudaError &e) {
+    c->err = e.what();
+    rc = INS2D_ECUDA;
+  } catch (const std::bad_alloc &) {
+    c->err = "device allocation failed";
+    rc = INS2D_ENOMEM;
+  } catch (const std::exception &e) {
+    c->err = e.what();
+    rc = INS2D_EINVAL;
+  }
+  if (rc != INS2D_OK) {
+    // keep the context so the caller can read ins2d_last_error, but free memory
+    for (void *p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    *out = c;
+    return rc;
+  }
+  *out = c;
+  return INS2D_OK;
+}
+
+int ins2d_ctx_destroy(ins2d_ctx *ctx) {
+  if (!ctx) return INS2D_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void *p : ctx->allocs) cudaFree(p);
+  for (auto &r : ctx->recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : ctx->pool) cudaEventDestroy(e);
+  if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
+  if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return INS2D_OK;
+}
+
+const char *ins2d_last_error(const ins2d_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int ins2d_get_sizes(const ins2d_ctx *ctx, ins2d_sizes *o) {
+  if (!ctx || !o) return INS2D_EINVAL;
+  const HostOps &H = ctx->H;
+  o->Nx = H.Nx; o->Ny = H.Ny;
+  o->Nux_in = H.Nux; o->Nuy_in = H.Nuy; o->Nvx_in = H.Nvx; o->Nvy_in = H.Nvy;
+  o->Npx = H.Npx; o->Npy = H.Npy;
+  o->Nu = (int32_t)H.Nu(); o->Nv = (int32_t)H.Nv(); o->NV = (int32_t)(H.Nu() + H.Nv()); o->Np = (int32_t)H.Np();
+  return INS2D_OK;
+}
+
+int ins2d_set_stream(ins2d_ctx *ctx, void *stream) {
+  if (!ctx) return INS2D_EINVAL;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return INS2D_OK;
+}
+
+int ins2d_profile(ins2d_ctx *ctx, int enable) {
+  if (!ctx) return INS2D_EINVAL;
+  cudaSetDevice(ctx->device);
+  for (auto &r : ctx->recs) {
+    ctx->pool.push_back(r.a);
+    ctx->pool.push_back(r.b);
+  }
+  ctx->recs.clear();
+  for (auto &l : ctx->launches) l = 0;
+  ctx->prof = enable != 0;
+  return INS2D_OK;
+}
+
+int ins2d_profile_read(ins2d_ctx *ctx, double ms[INS2D_PROF_N], int64_t launches[INS2D_PROF_N]) {
+  API_BEGIN
+  CK(cudaStreamSynchronize(ctx->stream));
+  double acc[INS2D_PROF_N] = {};
+  for (auto &r : ctx->recs) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, r.a, r.b));
+    acc[r.fam] += t;
+    ctx->pool.push_back(r.a);
+    ctx->pool.push_back(r.b);
+  }
+  ctx->recs.clear();
+  for (int k = 0; k < INS2D_PROF_N; ++k) {
+    if (ms) ms[k] = acc[k];
+    if (launches) launches[k] = ctx->launches[k];
+    ctx->launches[k] = 0;
+  }
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_set_bc_sampler(ins2d_ctx *ctx, ins2d_bc_sampler_fn fn, void *user) {
+  if (!ctx) return INS2D_EINVAL;
+  ctx->sampler = fn;
+  ctx->sampler_user = user;
+  return INS2D_OK;
+}
+
+int ins2d_set_bc_values(ins2d_ctx *ctx, double t, const ins2d_bc_values *v) {
+  if (!v) return fail(ctx, INS2D_EINVAL, "null boundary values");
+  API_BEGIN
+  HostOps &H = ctx->H;
+  auto get = [](const double *p, int n) {
+    return p ? std::vector<double>(p, p + n) : std::vector<double>((size_t)n, 0.0);
+  };
+  std::vector<double> uLo = get(v->uLo, H.Nx + 1), uUp = get(v->uUp, H.Nx + 1);
+  std::vector<double> uLo_i = get(v->uLo_i, H.Nux), uUp_i = get(v->uUp_i, H.Nux);
+  std::vector<double> uLe_i = get(v->uLe_i, H.Ny), uRi_i = get(v->uRi_i, H.Ny);
+  std::vector<double> vLe = get(v->vLe, H.Ny + 1), vRi = get(v->vRi, H.Ny + 1);
+  std::vector<double> vLo_i = get(v->vLo_i, H.Nx), vUp_i = get(v->vUp_i, H.Nx);
+  std::vector<double> vLe_i = get(v->vLe_i, H.Nvy), vRi_i = get(v->vRi_i, H.Nvy);
+  // products with the interpolation factors (set_bc_vectors.m:450-451, 492-493)
+  std::vector<double> XvLo = matvec(H.IVX.T, vLo_i), XvUp = matvec(H.IVX.T, vUp_i);
+  std::vector<double> YuLe = matvec(H.IUY.T, uLe_i), YuRi = matvec(H.IUY.T, uRi_i);
+  std::vector<double> all;
+  all.reserve(ctx->bc_count);
+  for (const auto *vec : {&uLo, &uUp, &uLo_i, &uUp_i, &uLe_i, &uRi_i, &vLe, &vRi, &vLo_i, &vUp_i, &vLe_i, &vRi_i,
+                          &XvLo, &XvUp, &YuLe, &YuRi})
+    all.insert(all.end(), vec->begin(), vec->end());
+  for (auto pr : {std::make_pair(v->pLe, H.Ny), std::make_pair(v->pRi, H.Ny), std::make_pair(v->pLo, H.Nx),
+                  std::make_pair(v->pUp, H.Nx), std::make_pair(v->dudtLe_i, H.Ny), std::make_pair(v->dudtRi_i, H.Ny),
+                  std::make_pair(v->dvdtLo_i, H.Nx), std::make_pair(v->dvdtUp_i, H.Nx)}) {
+    auto g = get(pr.first, pr.second);
+    all.insert(all.end(), g.begin(), g.end());
+  }
+  if (all.size() != ctx->bc_count) return fail(ctx, INS2D_EINVAL, "internal: boundary blob size mismatch");
+  // the blob is read by kernels queued earlier on the stream: order the update after them
+  CK(cudaMemcpyAsync(ctx->bcblob, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->uLe_i = uLe_i;
+  ctx->uRi_i = uRi_i;
+  ctx->vLo_i = vLo_i;
+  ctx->vUp_i = vUp_i;
+  ctx->bc_time = t;
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_F(ins2d_ctx *ctx, const double *V, const double *C, const double *p, double t, int nopressure,
+            double *F_out, double *maxres, int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!V || !F_out || (!nopressure && !p)) return fail(ctx, INS2D_EINVAL, "F: null argument");
+  int rc = sample_bc(ctx, t);
+  if (rc) return rc;
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv);
+  const double *dV = in_dev(ctx, V, ctx->stV, NV, mem);
+  const double *dC = (C && C != V) ? in_dev(ctx, C, ctx->stC, NV, mem) : dV;
+  const double *dP = nopressure ? nullptr : in_dev(ctx, p, ctx->stP, (size_t)ctx->P.Np, mem);
+  double *dO = mem == INS2D_MEM_DEVICE ? F_out : ctx->stO;
+  Prof pr(ctx, INS2D_PROF_OTHER, 1);
+  launch_F(ctx->P, dV, dC, dP, dO, ctx->red, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->h_red, ctx->red.result, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (mem == INS2D_MEM_HOST) CK(cudaMemcpyAsync(F_out, dO, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (maxres) *maxres = ctx->h_red[0];
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_divergence(ins2d_ctx *ctx, const double *V, double *f_out, double *maxdiv, int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!V || !f_out) return fail(ctx, INS2D_EINVAL, "divergence: null argument");
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv);
+  const double *dV = in_dev(ctx, V, ctx->stV, NV, mem);
+  double *dO = mem == INS2D_MEM_DEVICE ? f_out : ctx->stP;
+  Prof pr(ctx, INS2D_PROF_OTHER, 1);
+  launch_div(ctx->P, dV, 1.0, 0.0, 1.0, dO, true, ctx->red, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->h_red, ctx->red.result, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (mem == INS2D_MEM_HOST)
+    CK(cudaMemcpyAsync(f_out, dO, (size_t)ctx->P.Np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (maxdiv) *maxdiv = ctx->h_red[0];
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_laplacian(ins2d_ctx *ctx, const double *p, double *Ap, int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!p || !Ap) return fail(ctx, INS2D_EINVAL, "laplacian: null argument");
+  const size_t Np = (size_t)ctx->P.Np;
+  const double *dp = in_dev(ctx, p, ctx->stP, Np, mem);
+  double *dO = mem == INS2D_MEM_DEVICE ? Ap : ctx->stQ;
+  Prof pr(ctx, INS2D_PROF_OTHER, 1);
+  launch_lap(ctx->P, dp, dO, ctx->stream);
+  CK(cudaGetLastError());
+  if (mem == INS2D_MEM_HOST) CK(cudaMemcpyAsync(Ap, dO, Np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_pressure_poisson(ins2d_ctx *ctx, const double *f, double *dp, ins2d_solve_stats *stats, int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!f || !dp) return fail(ctx, INS2D_EINVAL, "pressure_poisson: null argument");
+  const size_t Np = (size_t)ctx->P.Np;
+  const double *df = in_dev(ctx, f, ctx->stP, Np, mem);
+  double *dO = mem == INS2D_MEM_DEVICE ? dp : ctx->stQ;
+  int rc = solve(ctx, df, dO, false, stats);
+  if (rc) return rc;
+  if (mem == INS2D_MEM_HOST) CK(cudaMemcpyAsync(dp, dO, Np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_pressure_additional_solve(ins2d_ctx *ctx, const double *V, double *p, double t, ins2d_solve_stats *stats,
+                                    int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!V || !p) return fail(ctx, INS2D_EINVAL, "pressure_additional_solve: null argument");
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv), Np = (size_t)ctx->P.Np;
+  const double *dV = in_dev(ctx, V, ctx->stV, NV, mem);
+  double *dP = p;
+  if (mem == INS2D_MEM_HOST) {
+    CK(cudaMemcpyAsync(ctx->stP, p, Np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    dP = ctx->stP;
+  }
+  int rc = additional_solve(ctx, dV, dP, t, stats);
+  if (rc) return rc;
+  if (mem == INS2D_MEM_HOST) CK(cudaMemcpyAsync(p, dP, Np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int32_t nsteps, ins2d_step_stats *stats,
+                  int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!V || !p || nsteps < 0) return fail(ctx, INS2D_EINVAL, "erk: bad argument");
+  if (!(dt > 0)) return fail(ctx, INS2D_EINVAL, "dt must be positive");
+  if (stats) *stats = ins2d_step_stats{0, 0, 0, 0.0};
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv), Np = (size_t)ctx->P.Np;
+  double *dV = V, *dP = p;
+  if (mem == INS2D_MEM_HOST) {
+    CK(cudaMemcpyAsync(ctx->stV, V, NV * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->stP, p, Np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    dV = ctx->stV;
+    dP = ctx->stP;
+  }
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = erk_step(ctx, dV, dP, t + n * dt, dt, stats);
+    if (rc) return rc;
+  }
+  if (mem == INS2D_MEM_HOST) {
+    CK(cudaMemcpyAsync(V, dV, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(p, dP, Np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_erk_step(ins2d_ctx *ctx, double *V, double *p, double t, double dt, ins2d_step_stats *stats, int mem) {
+  return ins2d_erk_run(ctx, V, p, t, dt, 1, stats, mem);
+}
+
+int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4], int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!V || !out) return fail(ctx, INS2D_EINVAL, "conservation: null argument");
+  int rc = sample_bc(ctx, t);
+  if (rc) return rc;
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv);
+  const double *dV = in_dev(ctx, V, ctx->stV, NV, mem);
+  Prof pr(ctx, INS2D_PROF_OTHER, 1);
+  launch_conservation(ctx->P, dV, ctx->red, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->h_red, ctx->red.result, 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const HostOps &H = ctx->H;
+  const double *r = ctx->h_red;
+  double umom = r[1], vmom = r[2], k = 0.5 * r[3] + 0.5 * r[4];
+  // Dirichlet boundary contributions (check_conservation.m:45-76)
+  auto dot = [](const std::vector<double> &a, const std::vector<double> &b, bool sq) {
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) s += (sq ? a[i] * a[i] : a[i]) * b[i];
+    return s;
+  };
+  const int *bc = H.bc;
+  if (bc[0] == BC_DIR) { umom += dot(ctx->uLe_i, H.hy, false) * H.gx[0]; k += 0.5 * dot(ctx->uLe_i, H.hy, true) * H.gx[0]; }
+  if (bc[1] == BC_DIR) { umom += dot(ctx->uRi_i, H.hy, false) * H.gx[H.Nx]; k += 0.5 * dot(ctx->uRi_i, H.hy, true) * H.gx[H.Nx]; }
+  if (bc[6] == BC_DIR) { vmom += dot(ctx->vLo_i, H.hx, false) * H.gy[0]; k += 0.5 * dot(ctx->vLo_i, H.hx, true) * H.gy[0]; }
+  if (bc[7] == BC_DIR) { vmom += dot(ctx->vUp_i, H.hx, false) * H.gy[H.Ny]; k += 0.5 * dot(ctx->vUp_i, H.hx, true) * H.gy[H.Ny]; }
+  out[0] = r[0];
+  out[1] = umom;
+  out[2] = vmom;
+  out[3] = k;
+  return INS2D_OK;
+  API_END
+}
+
+}  // extern "C"

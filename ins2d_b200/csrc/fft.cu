@@ -1,0 +1,318 @@
+// FFT pressure-Poisson solve for periodic uniform grids:
+//   dp = real(ifft2(-fft2(f) ./ Ahat)),  Ahat(0,0) = 1
+// (solvers/pressure/pressure_poisson.m:92-104, Ahat from
+// operator_divergence.m:283-284), including the early return when
+// max|fft2(f)| < 1e-14 (pressure_poisson.m:21-32).
+//
+// Three passes over HBM, each a batched 1D transform in shared memory (FP64):
+//  1. rows, real -> complex half spectrum: two real rows packed as one complex
+//     row, one complex FFT, split by Hermitian symmetry;
+//  2. columns of the half spectrum: forward FFT, multiply by -1/Ahat, inverse
+//     FFT (scaled 1/Ny), and the max |fhat| reduction;
+//  3. rows, complex half spectrum -> real: two rows packed as one complex
+//     inverse FFT (scaled 1/Nx).
+// Power-of-two lengths use radix-2 DIT/DIF with a twiddle table; other
+// lengths use a shared-memory DFT (O(N^2), small grids).
+#include "kernels.cuh"
+
+namespace ins2d {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxPow2 = 8192;
+constexpr int kMaxGeneric = 2048;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 twid(const double2 *tw, int k, bool inv) {
+  double2 w = __ldg(tw + k);
+  if (inv) w.y = -w.y;
+  return w;
+}
+__device__ __forceinline__ int brev(int k, int logn) { return (int)(__brev((unsigned)k) >> (32 - logn)); }
+
+// Shared-memory layout: one padding slot after every 8 complex values keeps
+// strided butterfly accesses free of bank conflicts.
+__device__ __forceinline__ int pd(int i) { return i + (i >> 3); }
+__host__ __device__ __forceinline__ int padded(int n) { return n + (n >> 3) + 1; }
+
+// In-place radix-2 decimation in time on G lines of length n (input in
+// bit-reversed order, output natural), three stages per pass: each thread
+// loads 8 values spaced by the first stage's half size, applies the stages in
+// registers and writes them back.  tw has n entries e^{-2 pi i k/n}.
+__device__ void dit(double2 *a, int G, int n, int logn, const double2 *tw, bool inv) {
+  const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
+  for (int s0 = 0; s0 < logn; s0 += 3) {
+    const int ns = min(3, logn - s0), R = 1 << ns, h = 1 << s0, per = n >> ns;
+    for (int g = t; g < G * per; g += nt) {
+      const int line = g / per, gg = g - line * per;
+      const int k = gg & (h - 1), blk = gg >> s0;
+      const int base = blk * R * h + k;
+      double2 *L = a + (size_t)line * ld;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) x[m] = L[pd(base + m * h)];
+#pragma unroll
+      for (int st = 0; st < 3; ++st) {
+        if (st >= ns) break;
+        const int hh = 1 << st, sh = logn - (s0 + st + 1);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          if (m >= R || (m & (2 * hh - 1)) >= hh) continue;
+          const int off = k + (m & (hh - 1)) * h;
+          const double2 y = cmul(twid(tw, off << sh, inv), x[m + hh]);
+          x[m + hh] = make_double2(x[m].x - y.x, x[m].y - y.y);
+          x[m] = make_double2(x[m].x + y.x, x[m].y + y.y);
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) L[pd(base + m * h)] = x[m];
+    }
+    __syncthreads();
+  }
+}
+
+// In-place radix-2 decimation in frequency (input natural, output
+// bit-reversed), three stages per pass from the largest half size down.
+__device__ void dif(double2 *a, int G, int n, int logn, const double2 *tw, bool inv) {
+  const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
+  for (int s_hi = logn; s_hi >= 1; s_hi -= 3) {
+    const int ns = min(3, s_hi), s_lo = s_hi - ns + 1;
+    const int R = 1 << ns, h = 1 << (s_lo - 1), per = n >> ns;
+    for (int g = t; g < G * per; g += nt) {
+      const int line = g / per, gg = g - line * per;
+      const int k = gg & (h - 1), blk = gg >> (s_lo - 1);
+      const int base = blk * R * h + k;
+      double2 *L = a + (size_t)line * ld;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) x[m] = L[pd(base + m * h)];
+#pragma unroll
+      for (int st = 2; st >= 0; --st) {
+        if (st >= ns) continue;
+        const int hh = 1 << st, sh = logn - (s_lo + st);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          if (m >= R || (m & (2 * hh - 1)) >= hh) continue;
+          const int off = k + (m & (hh - 1)) * h;
+          const double2 x0 = x[m], x1 = x[m + hh];
+          x[m] = make_double2(x0.x + x1.x, x0.y + x1.y);
+          x[m + hh] = cmul(make_double2(x0.x - x1.x, x0.y - x1.y), twid(tw, off << sh, inv));
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) L[pd(base + m * h)] = x[m];
+    }
+    __syncthreads();
+  }
+}
+
+// Plain DFT of G lines from a into b (natural order, padded layout), any n.
+__device__ void dft(const double2 *a, double2 *b, int G, int n, const double2 *tw, bool inv) {
+  const int ld = padded(n);
+  for (int o = threadIdx.x; o < G * n; o += blockDim.x) {
+    const int line = o / n, k = o - line * n;
+    const double2 *L = a + (size_t)line * ld;
+    double2 s = make_double2(0.0, 0.0);
+    int idx = 0;
+    for (int m = 0; m < n; ++m) {
+      const double2 p = cmul(L[pd(m)], twid(tw, idx, inv));
+      s.x += p.x;
+      s.y += p.y;
+      idx += k;
+      if (idx >= n) idx -= n;
+    }
+    b[(size_t)line * ld + pd(k)] = s;
+  }
+  __syncthreads();
+}
+
+// Pass 1: rows j0=2*blockIdx.x, j1=j0+1 -> half spectra.
+__global__ void __launch_bounds__(kThreads) k_rows_r2c(int Nx, int Ny, int logx, const double2 *__restrict__ tw,
+                                                       const double *__restrict__ f, double2 *__restrict__ spec) {
+  extern __shared__ double2 sm[];
+  const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
+  const bool has1 = j1 < Ny;
+  const int H = Nx / 2 + 1;
+  for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+    const double a = f[(size_t)j0 * Nx + k];
+    const double b = has1 ? f[(size_t)j1 * Nx + k] : 0.0;
+    sm[pd(logx >= 0 ? brev(k, logx) : k)] = make_double2(a, b);
+  }
+  __syncthreads();
+  const double2 *Z = sm;
+  if (logx >= 0) {
+    dit(sm, 1, Nx, logx, tw, false);
+  } else {
+    dft(sm, sm + padded(Nx), 1, Nx, tw, false);
+    Z = sm + padded(Nx);
+  }
+  for (int I = threadIdx.x; I < H; I += blockDim.x) {
+    const double2 z = Z[pd(I)], m = Z[pd((Nx - I) % Nx)];
+    spec[(size_t)j0 * H + I] = make_double2(0.5 * (z.x + m.x), 0.5 * (z.y - m.y));
+    if (has1) spec[(size_t)j1 * H + I] = make_double2(0.5 * (z.y + m.y), 0.5 * (m.x - z.x));
+  }
+}
+
+// Pass 2: G consecutive spectrum columns per block.
+__global__ void __launch_bounds__(kThreads) k_cols(int Nx, int Ny, int logy, int G, const double2 *__restrict__ tw,
+                                                   const double *__restrict__ ax, const double *__restrict__ ay,
+                                                   double dxdy, double2 *__restrict__ spec,
+                                                   unsigned long long *__restrict__ maxbits) {
+  extern __shared__ double2 sm[];
+  __shared__ double wmax[kThreads / 32];
+  const int H = Nx / 2 + 1;
+  const int c0 = blockIdx.x * G;
+  const int g_here = min(G, H - c0);
+  for (int o = threadIdx.x; o < g_here * Ny; o += blockDim.x) {
+    const int j = o / g_here, g = o - j * g_here;
+    sm[(size_t)g * padded(Ny) + pd(logy >= 0 ? brev(j, logy) : j)] = spec[(size_t)j * H + c0 + g];
+  }
+  __syncthreads();
+  double2 *A = sm;
+  const int ldy = padded(Ny);
+  if (logy >= 0) {
+    dit(sm, g_here, Ny, logy, tw, false);
+  } else {
+    dft(sm, sm + (size_t)G * ldy, g_here, Ny, tw, false);
+    A = sm + (size_t)G * ldy;
+  }
+  double lmax = 0.0;
+  for (int o = threadIdx.x; o < g_here * Ny; o += blockDim.x) {
+    const int g = o / Ny, J = o - g * Ny;
+    const int I = c0 + g;
+    double2 *slot = A + (size_t)g * ldy + pd(J);
+    const double2 F = *slot;
+    lmax = fmax(lmax, sqrt(F.x * F.x + F.y * F.y));
+    const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + I) + __ldg(ay + J));
+    *slot = make_double2(-F.x / lam, -F.y / lam);
+  }
+  __syncthreads();
+  double2 *Bout = A;
+  if (logy >= 0) {
+    dif(A, g_here, Ny, logy, tw, true);
+  } else {
+    dft(A, sm, g_here, Ny, tw, true);
+    Bout = sm;
+  }
+  const double sc = 1.0 / Ny;
+  for (int o = threadIdx.x; o < g_here * Ny; o += blockDim.x) {
+    const int j = o / g_here, g = o - j * g_here;
+    const double2 v = Bout[(size_t)g * ldy + pd(logy >= 0 ? brev(j, logy) : j)];
+    spec[(size_t)j * H + c0 + g] = make_double2(v.x * sc, v.y * sc);
+  }
+  for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, off));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = wmax[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(m));  // m >= 0: bit order = value order
+  }
+}
+
+// Pass 3: half spectra of rows j0, j1 -> real rows (scaled 1/Nx).
+__global__ void __launch_bounds__(kThreads) k_rows_c2r(int Nx, int Ny, int logx, const double2 *__restrict__ tw,
+                                                       const double2 *__restrict__ spec, double *__restrict__ out,
+                                                       int accumulate, const unsigned long long *__restrict__ maxbits) {
+  extern __shared__ double2 sm[];
+  const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
+  const bool has1 = j1 < Ny;
+  const int H = Nx / 2 + 1;
+  const double mx = __longlong_as_double((long long)*maxbits);
+  if (mx < 1e-14) {  // pressure_poisson.m:21-32: dp stays zero
+    if (!accumulate)
+      for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+        out[(size_t)j0 * Nx + k] = 0.0;
+        if (has1) out[(size_t)j1 * Nx + k] = 0.0;
+      }
+    return;
+  }
+  for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+    double2 g0, g1;
+    if (k < H) {
+      g0 = spec[(size_t)j0 * H + k];
+      g1 = has1 ? spec[(size_t)j1 * H + k] : make_double2(0.0, 0.0);
+    } else {
+      const double2 a = spec[(size_t)j0 * H + (Nx - k)];
+      const double2 b = has1 ? spec[(size_t)j1 * H + (Nx - k)] : make_double2(0.0, 0.0);
+      g0 = make_double2(a.x, -a.y);
+      g1 = make_double2(b.x, -b.y);
+    }
+    sm[pd(logx >= 0 ? brev(k, logx) : k)] = make_double2(g0.x - g1.y, g0.y + g1.x);
+  }
+  __syncthreads();
+  const double2 *W = sm;
+  if (logx >= 0) {
+    dit(sm, 1, Nx, logx, tw, true);
+  } else {
+    dft(sm, sm + padded(Nx), 1, Nx, tw, true);
+    W = sm + padded(Nx);
+  }
+  const double sc = 1.0 / Nx;
+  for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+    const double2 w = W[pd(k)];
+    if (accumulate) {
+      out[(size_t)j0 * Nx + k] += w.x * sc;
+      if (has1) out[(size_t)j1 * Nx + k] += w.y * sc;
+    } else {
+      out[(size_t)j0 * Nx + k] = w.x * sc;
+      if (has1) out[(size_t)j1 * Nx + k] = w.y * sc;
+    }
+  }
+}
+
+int ilog2_exact(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return ((1 << l) == n) ? l : -1;
+}
+
+int cols_group(int Ny, bool pow2) {
+  // two columns (32-byte row segments) per block; more for short columns
+  const size_t per = (size_t)padded(Ny) * sizeof(double2) * (pow2 ? 1 : 2);
+  int G = (int)((72 * 1024) / per);
+  if (G > 8) G = 8;
+  if (G < 1) G = 1;
+  if (Ny >= 1024 && G > 2) G = 2;
+  return G;
+}
+
+}  // namespace
+
+bool fft_supported(int Nx, int Ny) {
+  auto ok = [](int n) { return n >= 2 && ((ilog2_exact(n) >= 0 && n <= kMaxPow2) || n <= kMaxGeneric); };
+  return ok(Nx) && ok(Ny);
+}
+
+// Opt the transform kernels in to large dynamic shared memory on the current
+// device (called once per context).
+void fft_prepare() {
+  cudaFuncSetAttribute(k_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
+                        cudaStream_t s) {
+  const int Nx = plan.Nx, Ny = plan.Ny;
+  const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
+  const int G = cols_group(Ny, plan.logy >= 0);
+  const size_t smy = (size_t)G * padded(Ny) * sizeof(double2) * (plan.logy >= 0 ? 1 : 2);
+  const int pairs = (Ny + 1) / 2;
+  const int H = Nx / 2 + 1;
+  cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
+  k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, f, plan.spec);
+  k_cols<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
+                                                plan.spec, (unsigned long long *)plan.maxabs);
+  k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
+                                          (const unsigned long long *)plan.maxabs);
+}
+
+}  // namespace ins2d

@@ -1,0 +1,181 @@
+// Stencil kernels of the INS2D hot path: RK stage right-hand side, residual,
+// F, divergence, projection, Laplacian and conservation diagnostics.
+//
+// Thread mapping: one thread per (i,j) of the union of the u, v and p index
+// spaces, 32x8 thread blocks (x fastest, coalesced along rows).  Stencil
+// neighbours are served from L1/L2; each field is read from DRAM once per
+// kernel.  Reductions are deterministic: per-block partials reduced in block
+// order by the last block to finish.
+#include <cfloat>
+
+#include "kernels.cuh"
+#include "reduce.cuh"
+
+namespace ins2d {
+
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+inline dim3 grid_for(int nx, int ny) { return dim3((nx + BX - 1) / BX, (ny + BY - 1) / BY); }
+
+template <bool SAMEC>
+__global__ void __launch_bounds__(256) k_F(const __grid_constant__ DevOps P, const double *__restrict__ V,
+                                          const double *__restrict__ C, const double *__restrict__ p,
+                                          double *__restrict__ Fo, const RedScratch red) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j = blockIdx.y * BY + threadIdx.y;
+  const double *u = V, *v = V + P.Nu, *cu = C, *cv = C + P.Nu;
+  const double ypfac = p ? 1.0 : 0.0;
+  double mx[1] = {0.0};
+  const int ops[1] = {R_MAX};
+  if (i < P.Nux && j < P.Nuy) {
+    const long long idx = (long long)j * P.Nux + i;
+    double R = rhs_u<double, SAMEC>(P, u, v, cu, cv, i, j, ypfac);
+    if (p) R -= grad_x(P, p, i, j);
+    Fo[idx] = R;
+    mx[0] = fmax(mx[0], fabs(R));
+  }
+  if (i < P.Nvx && j < P.Nvy) {
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    double R = rhs_v<double, SAMEC>(P, u, v, cu, cv, i, j, ypfac);
+    if (p) R -= grad_y(P, p, i, j);
+    Fo[idx] = R;
+    mx[0] = fmax(mx[0], fabs(R));
+  }
+  grid_reduce<1>(mx, ops, red);
+}
+
+template <bool WANTMAX>
+__global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, const double *__restrict__ W,
+                                            double alpha, double beta, double gamma, double *__restrict__ f,
+                                            const RedScratch red) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j = blockIdx.y * BY + threadIdx.y;
+  double mx[1] = {0.0};
+  const int ops[1] = {R_MAX};
+  if (i < P.Npx && j < P.Npy) {
+    double d = div_in(P, W, W + P.Nu, i, j);
+    if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
+    if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
+    d *= gamma;
+    f[(long long)j * P.Npx + i] = d;
+    mx[0] = fabs(d);
+  }
+  if (WANTMAX) grid_reduce<1>(mx, ops, red);
+}
+
+__global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps P, const double *__restrict__ Wt,
+                                                const double *__restrict__ dp, double dt, double c,
+                                                double *__restrict__ Vo) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j = blockIdx.y * BY + threadIdx.y;
+  if (i < P.Nux && j < P.Nuy) {
+    const long long idx = (long long)j * P.Nux + i;
+    Vo[idx] = dt * (Wt[idx] - c * om_inv_u(P, i, j) * grad_x(P, dp, i, j));
+  }
+  if (i < P.Nvx && j < P.Nvy) {
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    Vo[idx] = dt * (Wt[idx] - c * om_inv_v(P, i, j) * grad_y(P, dp, i, j));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_correct(const __grid_constant__ DevOps P, const double *__restrict__ Vi,
+                                                const double *__restrict__ dp, double *__restrict__ Vo) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j = blockIdx.y * BY + threadIdx.y;
+  if (i < P.Nux && j < P.Nuy) {
+    const long long idx = (long long)j * P.Nux + i;
+    Vo[idx] = Vi[idx] - om_inv_u(P, i, j) * grad_x(P, dp, i, j);
+  }
+  if (i < P.Nvx && j < P.Nvy) {
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    Vo[idx] = Vi[idx] - om_inv_v(P, i, j) * grad_y(P, dp, i, j);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_lap(const __grid_constant__ DevOps P, const double *__restrict__ p,
+                                            double *__restrict__ Ap) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j = blockIdx.y * BY + threadIdx.y;
+  if (i < P.Npx && j < P.Npy) Ap[(long long)j * P.Npx + i] = lap(P, p, i, j);
+}
+
+__global__ void __launch_bounds__(256) k_conservation(const __grid_constant__ DevOps P, const double *__restrict__ V,
+                                                     const RedScratch red) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j = blockIdx.y * BY + threadIdx.y;
+  const double *u = V, *v = V + P.Nu;
+  double q[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const int ops[5] = {R_MAX, R_SUM, R_SUM, R_SUM, R_SUM};
+  if (i < P.Npx && j < P.Npy)
+    q[0] = fabs(div_in(P, u, v, i, j) + div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j));
+  if (i < P.Nux && j < P.Nuy) {
+    const double om = __ldg(P.hy + j) * __ldg(P.gxi + i);
+    const double x = u[(long long)j * P.Nux + i];
+    q[1] = om * x;
+    q[3] = om * x * x;
+  }
+  if (i < P.Nvx && j < P.Nvy) {
+    const double om = __ldg(P.gyi + j) * __ldg(P.hx + i);
+    const double x = v[(long long)j * P.Nvx + i];
+    q[2] = om * x;
+    q[4] = om * x * x;
+  }
+  grid_reduce<5>(q, ops, red);
+}
+
+__global__ void k_add(const double *__restrict__ x, double *__restrict__ y, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    y[k] += x[k];
+}
+
+}  // namespace
+
+void launch_F(const DevOps &P, const double *V, const double *C, const double *p, double *F_out,
+              const RedScratch &red, cudaStream_t s) {
+  dim3 g = grid_for(P.Nux > P.Nvx ? P.Nux : P.Nvx, P.Nuy > P.Nvy ? P.Nuy : P.Nvy);
+  if (C == nullptr || C == V)
+    k_F<true><<<g, dim3(BX, BY), 0, s>>>(P, V, V, p, F_out, red);
+  else
+    k_F<false><<<g, dim3(BX, BY), 0, s>>>(P, V, C, p, F_out, red);
+}
+
+void launch_div(const DevOps &P, const double *W, double alpha, double beta, double gamma, double *f,
+                bool want_max, const RedScratch &red, cudaStream_t s) {
+  dim3 g = grid_for(P.Npx, P.Npy);
+  if (want_max)
+    k_div<true><<<g, dim3(BX, BY), 0, s>>>(P, W, alpha, beta, gamma, f, red);
+  else
+    k_div<false><<<g, dim3(BX, BY), 0, s>>>(P, W, alpha, beta, gamma, f, red);
+}
+
+void launch_project(const DevOps &P, const double *Wt, const double *dp, double dt, double c, double *V_out,
+                    cudaStream_t s) {
+  dim3 g = grid_for(P.Nux > P.Nvx ? P.Nux : P.Nvx, P.Nuy > P.Nvy ? P.Nuy : P.Nvy);
+  k_project<<<g, dim3(BX, BY), 0, s>>>(P, Wt, dp, dt, c, V_out);
+}
+
+void launch_correct(const DevOps &P, const double *V_in, const double *dp, double *V_out, cudaStream_t s) {
+  dim3 g = grid_for(P.Nux > P.Nvx ? P.Nux : P.Nvx, P.Nuy > P.Nvy ? P.Nuy : P.Nvy);
+  k_correct<<<g, dim3(BX, BY), 0, s>>>(P, V_in, dp, V_out);
+}
+
+void launch_lap(const DevOps &P, const double *p, double *Ap, cudaStream_t s) {
+  k_lap<<<grid_for(P.Npx, P.Npy), dim3(BX, BY), 0, s>>>(P, p, Ap);
+}
+
+void launch_conservation(const DevOps &P, const double *V, const RedScratch &red, cudaStream_t s) {
+  int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
+  int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  k_conservation<<<grid_for(nx, ny), dim3(BX, BY), 0, s>>>(P, V, red);
+}
+
+void launch_add(const double *x, double *y, long long n, cudaStream_t s) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  k_add<<<(unsigned)b, 256, 0, s>>>(x, y, n);
+}
+
+}  // namespace ins2d

@@ -1,0 +1,188 @@
+// Preconditioned conjugate gradients for A dp = f, A = M Om^-1 G, with the
+// control flow and stopping rule of the reference's cg.F:158-280:
+//   x0 = 0, r0 = f, z = M^-1 r, p = z, rr0 = f'f; stop at once if rr0 <= tol^2;
+//   per iteration: q = A p; alpha = r'z / p'q; x += alpha p; r -= alpha q;
+//   converged when r'r / rr0 <= tol^2 (iter = that iteration);
+//   else z = M^-1 r; beta = r'z_new / r'z_old; p = z + beta p;
+//   error after maxit iterations;  norm1 = sqrt(r'r/rr0),
+//   norm2 = max|r| / (max x - min x) of the last iteration.
+// pressure_poisson.m:33-38's early return (max|A*0 - f| < 1e-14 -> dp = 0)
+// is folded into the first kernel.
+//
+// The reference preconditions with a diagonal incomplete Cholesky factor
+// whose forward/backward sweeps are sequential (cg.F:317-390).  Here the
+// preconditioner is the diagonal of A (Jacobi), which is parallel; iteration
+// counts therefore differ from the reference, the converged solution agrees
+// to the stated tolerance.
+//
+// Three kernels per iteration (SpMV + p'q; x/r update + r'r, r'z and the
+// norm2 extrema; p update); scalars live on the device and each kernel's last
+// block advances them, so the host only polls the convergence flag every few
+// iterations.
+#include "ins2d.h"
+#include "kernels.cuh"
+#include "reduce.cuh"
+
+namespace ins2d {
+
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+inline dim3 pgrid(const DevOps &P) { return dim3((P.Npx + BX - 1) / BX, (P.Npy + BY - 1) / BY); }
+
+__device__ __forceinline__ RedScratch red_of(const PcgWork &W) {
+  RedScratch r;
+  r.partials = W.partials;
+  r.counter = &W.sc->counter;
+  r.result = W.partials + (size_t)W.blocks * 8;  // 8 slots after the partials
+  r.max_blocks = W.blocks;
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_init(const __grid_constant__ DevOps P, const PcgWork W,
+                                              const double *__restrict__ f, double tol2, long long maxit) {
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  double q[3] = {0.0, 0.0, 0.0};
+  const int ops[3] = {R_SUM, R_SUM, R_MAX};
+  if (i < P.Npx && j < P.Npy) {
+    const long long k = (long long)j * P.Npx + i;
+    const double fv = f[k];
+    const double z = fv / lap_diag(P, i, j);
+    W.x[k] = 0.0;
+    W.r[k] = fv;
+    W.p[k] = z;
+    q[0] = fv * fv;
+    q[1] = fv * z;
+    q[2] = fabs(fv);
+  }
+  double out[3];
+  if (grid_reduce<3>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    s->tol2 = tol2;
+    s->maxit = maxit;
+    s->rr0 = out[0];
+    s->rz = out[1];
+    s->rr = 0.0;
+    s->it = 0;
+    s->status = 0;
+    s->maxx = s->minx = s->maxres = 0.0;
+    // pressure_poisson.m:33-38 and cg.F:222-227
+    s->done = (out[2] < 1e-14 || out[0] <= tol2) ? 1 : 0;
+    if (!isfinite(out[0]) || !isfinite(out[1])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_spmv(const __grid_constant__ DevOps P, const PcgWork W) {
+  if (*(volatile int *)&W.sc->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  double q[1] = {0.0};
+  const int ops[1] = {R_SUM};
+  if (i < P.Npx && j < P.Npy) {
+    const long long k = (long long)j * P.Npx + i;
+    const double aq = lap(P, W.p, i, j);
+    W.q[k] = aq;
+    q[0] = W.p[k] * aq;
+  }
+  double out[1];
+  if (grid_reduce<1>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    s->pq = out[0];
+    if (!isfinite(out[0])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    } else if (out[0] == 0.0) {
+      s->status = INS2D_EBREAKDOWN;
+      s->done = 1;
+    } else {
+      s->alpha = s->rz / out[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P, const PcgWork W) {
+  if (*(volatile int *)&W.sc->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  const double alpha = W.sc->alpha;
+  double q[5] = {0.0, 0.0, -DBL_MAX, DBL_MAX, 0.0};
+  const int ops[5] = {R_SUM, R_SUM, R_MAX, R_MIN, R_MAX};
+  if (i < P.Npx && j < P.Npy) {
+    const long long k = (long long)j * P.Npx + i;
+    const double x = W.x[k] + alpha * W.p[k];
+    const double r = W.r[k] - alpha * W.q[k];
+    W.x[k] = x;
+    W.r[k] = r;
+    q[0] = r * r;
+    q[1] = r * (r / lap_diag(P, i, j));
+    q[2] = x;
+    q[3] = x;
+    q[4] = fabs(r);
+  }
+  double out[5];
+  if (grid_reduce<5>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    s->it += 1;
+    s->rr = out[0] / s->rr0;
+    s->maxx = out[2];
+    s->minx = out[3];
+    s->maxres = out[4];
+    if (!isfinite(s->rr) || !isfinite(out[1])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    } else if (s->rr <= s->tol2) {
+      s->done = 1;
+    } else if (s->it >= s->maxit) {
+      s->status = INS2D_ENOTCONV;
+      s->done = 1;
+    } else {
+      s->beta = out[1] / s->rz;
+      s->rz = out[1];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pupdate(const __grid_constant__ DevOps P, const PcgWork W) {
+  if (*(volatile int *)&W.sc->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  if (i < P.Npx && j < P.Npy) {
+    const long long k = (long long)j * P.Npx + i;
+    W.p[k] = W.r[k] / lap_diag(P, i, j) + W.sc->beta * W.p[k];
+  }
+}
+
+__global__ void k_copy_out(const double *__restrict__ x, double *__restrict__ dp, long long n, int accumulate) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    dp[k] = accumulate ? dp[k] + x[k] : x[k];
+}
+
+}  // namespace
+
+int pcg_blocks(const DevOps &P) {
+  dim3 g = pgrid(P);
+  return (int)(g.x * g.y);
+}
+
+void pcg_init(const DevOps &P, const PcgWork &W, const double *f, double tol, long long maxit, cudaStream_t s) {
+  k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
+}
+
+void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
+  const dim3 g = pgrid(P), b(BX, BY);
+  for (int it = 0; it < n; ++it) {
+    k_spmv<<<g, b, 0, s>>>(P, W);
+    k_update<<<g, b, 0, s>>>(P, W);
+    k_pupdate<<<g, b, 0, s>>>(P, W);
+  }
+}
+
+void pcg_finish(const DevOps &P, const PcgWork &W, double *dp, bool accumulate, cudaStream_t s) {
+  long long n = P.Np;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_copy_out<<<(unsigned)blocks, 256, 0, s>>>(W.x, dp, n, accumulate ? 1 : 0);
+}
+
+}  // namespace ins2d

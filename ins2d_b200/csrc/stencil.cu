@@ -1,0 +1,539 @@
+// Column-walking evaluation of the momentum right-hand side
+//   R = -conv(V) + Diff*V + yDiff - y_p     (F.m:137-145 without G*p)
+// for the RK stage kernel (time_ERK.m:90-101) and the residual of the
+// additional pressure solve (pressure_additional_solve.m:11-13).
+//
+// Each thread owns one column i and walks a run of rows j.  Its 1D x-table
+// rows (Au_ux, Su_ux, Iv_uy(x), ... at i and i+1) are loaded into registers
+// once per run; the y-faces (u at uy, vbar at uy, du/dy, v at vy, dv/dy) are
+// computed once per face and slid down the column, so per point only the few
+// field values of the stencil are loaded.  Warps with threadIdx.y == 0 walk u
+// points, threadIdx.y == 1 walk v points of the same columns, so both share
+// their field rows in L1.  Boundary rows of the operators use the same tables
+// (the boundary elimination lives in the table entries), so there is one
+// code path for every boundary-condition combination.
+#include "kernels.cuh"
+
+namespace ins2d {
+
+namespace {
+
+constexpr int WX = 64;  // columns per block (two warps per walker)
+constexpr int RUN = 32; // rows per column run
+
+template <typename S>
+struct XRow {  // one row of an x-table in registers
+  int c0, c1, c2;
+  S w0, w1, w2, b1, b2;
+};
+template <typename S>
+struct XRowW {  // weights of a second table that shares the columns
+  S w0, w1, w2, b1, b2;
+};
+
+template <typename S>
+__device__ __forceinline__ XRow<S> xrow(const Tab &T, int r) {
+  XRow<S> x;
+  const int32_t *c = T.c + kT * r;
+  const double *w = T.w + kT * r;
+  x.c0 = __ldg(c);
+  x.c1 = __ldg(c + 1);
+  x.c2 = __ldg(c + 2);
+  x.w0 = S(__ldg(w));
+  x.w1 = S(__ldg(w + 1));
+  x.w2 = S(__ldg(w + 2));
+  x.b1 = S(__ldg(T.b1 + r));
+  x.b2 = S(__ldg(T.b2 + r));
+  return x;
+}
+template <typename S>
+__device__ __forceinline__ XRowW<S> xroww(const Tab &T, int r) {
+  XRowW<S> x;
+  const double *w = T.w + kT * r;
+  x.w0 = S(__ldg(w));
+  x.w1 = S(__ldg(w + 1));
+  x.w2 = S(__ldg(w + 2));
+  x.b1 = S(__ldg(T.b1 + r));
+  x.b2 = S(__ldg(T.b2 + r));
+  return x;
+}
+
+// loads the (up to three) entries of a row of f at the columns of x
+template <typename S>
+struct Trip {
+  S a0, a1, a2;
+};
+template <typename S>
+__device__ __forceinline__ Trip<S> load3(const double *__restrict__ row, const XRow<S> &x) {
+  Trip<S> t;
+  t.a0 = S(__ldg(row + x.c0));
+  t.a1 = S(__ldg(row + x.c1));
+  t.a2 = (x.w2 != S(0)) ? S(__ldg(row + x.c2)) : S(0);
+  return t;
+}
+template <typename S>
+__device__ __forceinline__ S dot3(const XRow<S> &x, const Trip<S> &t) {
+  return x.w0 * t.a0 + x.w1 * t.a1 + x.w2 * t.a2;
+}
+template <typename S>
+__device__ __forceinline__ S dot3(const XRowW<S> &x, const Trip<S> &t) {
+  return x.w0 * t.a0 + x.w1 * t.a1 + x.w2 * t.a2;
+}
+
+// a y-table row (warp-uniform)
+template <typename S>
+struct YRow {
+  int c0, c1, c2;
+  S w0, w1, w2, b1, b2;
+};
+template <typename S>
+__device__ __forceinline__ YRow<S> yrow(const Tab &T, int r) {
+  YRow<S> y;
+  const int32_t *c = T.c + kT * r;
+  const double *w = T.w + kT * r;
+  y.c0 = __ldg(c);
+  y.c1 = __ldg(c + 1);
+  y.c2 = __ldg(c + 2);
+  y.w0 = S(__ldg(w));
+  y.w1 = S(__ldg(w + 1));
+  y.w2 = S(__ldg(w + 2));
+  y.b1 = S(__ldg(T.b1 + r));
+  y.b2 = S(__ldg(T.b2 + r));
+  return y;
+}
+
+struct Epi {
+  int mode;  // 0: RK stage, 1: residual of the additional solve
+  // stage
+  const double *Vn;
+  double *kV;
+  const double *kprev[kMaxStages];
+  double aprev[kMaxStages];
+  int nprev;
+  double aii, inv_dt;
+  double *Wt;
+  // residual
+  const double *p;
+  double *w;
+  double *kV_next;
+};
+
+__device__ __forceinline__ void epilogue_stage(const Epi &e, long long idx, double oi, double R) {
+  const double k = oi * R;
+  if (e.kV) e.kV[idx] = k;
+  double vt = 0.0;
+  for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * e.kprev[m][idx];
+  vt += e.aii * k;
+  e.Wt[idx] = e.Vn[idx] * e.inv_dt + vt;
+}
+
+// ---------------------------------------------------------------------------
+// u walker
+template <typename S>
+__device__ void walk_u(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+                       int i, int j0, int j1) {
+  if (i >= P.Nux) return;
+  j1 = min(j1, P.Nuy);
+  if (j0 >= j1) return;
+  const S ire = S(P.invRe);
+  const XRow<S> ax0 = xrow<S>(P.AUX, i), ax1 = xrow<S>(P.AUX, i + 1);
+  const XRowW<S> sx0 = xroww<S>(P.SUX, i), sx1 = xroww<S>(P.SUX, i + 1);
+  const XRow<S> ix = xrow<S>(P.IVX, i);
+  const S gx = S(__ldg(P.gxi + i));
+  const S pl = S(__ldg(P.pxl + i)), pr = S(__ldg(P.pxr + i));
+  const S uLo = S(__ldg(P.bc.uLo_i + i)), uUp = S(__ldg(P.bc.uUp_i + i));
+  const S xvlo = S(__ldg(P.bc.XvLo + i)), xvup = S(__ldg(P.bc.XvUp + i));
+  // gradient row (residual mode)
+  XRow<double> gt{};
+  if (e.mode == 1) gt = xrow<double>(P.MXT, i);
+  // face at row r: u_uy, du/dy, vbar_uy
+  auto face = [&](int r, S &uy, S &sy, S &vf) {
+    const YRow<S> ay = yrow<S>(P.AUY, r);
+    const double *__restrict__ sw = P.SUY.w + kT * r;
+    const S s0 = S(__ldg(sw)), s1 = S(__ldg(sw + 1)), s2 = S(__ldg(sw + 2));
+    const S f0 = S(__ldg(u + (long long)ay.c0 * P.Nux + i));
+    const S f1 = S(__ldg(u + (long long)ay.c1 * P.Nux + i));
+    const S f2 = (ay.w2 != S(0) || s2 != S(0)) ? S(__ldg(u + (long long)ay.c2 * P.Nux + i)) : S(0);
+    uy = ay.w0 * f0 + ay.w1 * f1 + ay.w2 * f2 + ay.b1 * uLo + ay.b2 * uUp;
+    sy = s0 * f0 + s1 * f1 + s2 * f2 + S(__ldg(P.SUY.b1 + r)) * uLo + S(__ldg(P.SUY.b2 + r)) * uUp;
+    const YRow<S> iy = yrow<S>(P.IVY, r);
+    S acc = S(0);
+    if (iy.w0 != S(0)) acc += iy.w0 * dot3(ix, load3(v + (long long)iy.c0 * P.Nvx, ix));
+    if (iy.w1 != S(0)) acc += iy.w1 * dot3(ix, load3(v + (long long)iy.c1 * P.Nvx, ix));
+    if (iy.w2 != S(0)) acc += iy.w2 * dot3(ix, load3(v + (long long)iy.c2 * P.Nvx, ix));
+    vf = acc + ix.b1 * S(__ldg(P.bc.vLe + r)) + ix.b2 * S(__ldg(P.bc.vRi + r)) + iy.b1 * xvlo + iy.b2 * xvup;
+  };
+  S uy0, sy0, vf0;
+  face(j0, uy0, sy0, vf0);
+  for (int j = j0; j < j1; ++j) {
+    S uy1, sy1, vf1;
+    face(j + 1, uy1, sy1, vf1);
+    const double *__restrict__ row = u + (long long)j * P.Nux;
+    const S ule = S(__ldg(P.bc.uLe_i + j)), uri = S(__ldg(P.bc.uRi_i + j));
+    const Trip<S> t0 = load3(row, ax0), t1 = load3(row, ax1);
+    const S uxl = dot3(ax0, t0) + ax0.b1 * ule + ax0.b2 * uri;
+    const S uxr = dot3(ax1, t1) + ax1.b1 * ule + ax1.b2 * uri;
+    const S sxl = dot3(sx0, t0) + sx0.b1 * ule + sx0.b2 * uri;
+    const S sxr = dot3(sx1, t1) + sx1.b1 * ule + sx1.b2 * uri;
+    const S hy = S(__ldg(P.hy + j));
+    const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
+    const S duvdy = vf1 * uy1 - vf0 * uy0;
+    const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
+    const S ypx = hy * S(__ldg(P.bc.pLe + j)) * pl + hy * S(__ldg(P.bc.pRi + j)) * pr;
+    const double R = (double)(-(du2dx + duvdy) + d2u - ypx);
+    const long long idx = (long long)j * P.Nux + i;
+    const double hyd = __ldg(P.hy + j);
+    const double oi = 1.0 / (hyd * (double)__ldg(P.gxi + i));
+    if (e.mode == 0) {
+      epilogue_stage(e, idx, oi, R);
+    } else {
+      const double *prow = e.p + (long long)j * P.Npx;
+      const double g = -hyd * (gt.w0 * __ldg(prow + gt.c0) + gt.w1 * __ldg(prow + gt.c1) +
+                               (gt.w2 != 0.0 ? gt.w2 * __ldg(prow + gt.c2) : 0.0));
+      e.w[idx] = oi * (R - g);
+      if (e.kV_next) e.kV_next[idx] = oi * R;
+    }
+    uy0 = uy1;
+    sy0 = sy1;
+    vf0 = vf1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// v walker
+template <typename S>
+__device__ void walk_v(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+                       int i, int j0, int j1) {
+  if (i >= P.Nvx) return;
+  j1 = min(j1, P.Nvy);
+  if (j0 >= j1) return;
+  const S ire = S(P.invRe);
+  const XRow<S> vx0 = xrow<S>(P.AVX, i), vx1 = xrow<S>(P.AVX, i + 1);
+  const XRowW<S> sv0 = xroww<S>(P.SVX, i), sv1 = xroww<S>(P.SVX, i + 1);
+  const XRow<S> ux0 = xrow<S>(P.IUX, i), ux1 = xrow<S>(P.IUX, i + 1);
+  const S hx = S(__ldg(P.hx + i));
+  const S vLo = S(__ldg(P.bc.vLo_i + i)), vUp = S(__ldg(P.bc.vUp_i + i));
+  const S pLo = S(__ldg(P.bc.pLo + i)), pUp = S(__ldg(P.bc.pUp + i));
+  const S uLo0 = S(__ldg(P.bc.uLo + i)), uUp0 = S(__ldg(P.bc.uUp + i));
+  const S uLo1 = S(__ldg(P.bc.uLo + i + 1)), uUp1 = S(__ldg(P.bc.uUp + i + 1));
+  auto face = [&](int r, S &vy, S &sy) {
+    const YRow<S> ay = yrow<S>(P.AVY, r);
+    const double *__restrict__ sw = P.SVY.w + kT * r;
+    const S s0 = S(__ldg(sw)), s1 = S(__ldg(sw + 1)), s2 = S(__ldg(sw + 2));
+    const S f0 = S(__ldg(v + (long long)ay.c0 * P.Nvx + i));
+    const S f1 = S(__ldg(v + (long long)ay.c1 * P.Nvx + i));
+    const S f2 = (ay.w2 != S(0) || s2 != S(0)) ? S(__ldg(v + (long long)ay.c2 * P.Nvx + i)) : S(0);
+    vy = ay.w0 * f0 + ay.w1 * f1 + ay.w2 * f2 + ay.b1 * vLo + ay.b2 * vUp;
+    sy = s0 * f0 + s1 * f1 + s2 * f2 + S(__ldg(P.SVY.b1 + r)) * vLo + S(__ldg(P.SVY.b2 + r)) * vUp;
+  };
+  S vy0, sy0;
+  face(j0, vy0, sy0);
+  for (int j = j0; j < j1; ++j) {
+    S vy1, sy1;
+    face(j + 1, vy1, sy1);
+    const double *__restrict__ row = v + (long long)j * P.Nvx;
+    const S vle = S(__ldg(P.bc.vLe_i + j)), vri = S(__ldg(P.bc.vRi_i + j));
+    const Trip<S> t0 = load3(row, vx0), t1 = load3(row, vx1);
+    const S vxl = dot3(vx0, t0) + vx0.b1 * vle + vx0.b2 * vri;
+    const S vxr = dot3(vx1, t1) + vx1.b1 * vle + vx1.b2 * vri;
+    const S svl = dot3(sv0, t0) + sv0.b1 * vle + sv0.b2 * vri;
+    const S svr = dot3(sv1, t1) + sv1.b1 * vle + sv1.b2 * vri;
+    // ubar at vx faces r = i, i+1 (row j of Iu_vx's y-factor)
+    const YRow<S> iy = yrow<S>(P.IUY, j);
+    S ufl = S(0), ufr = S(0);
+    if (iy.w0 != S(0)) {
+      const double *ur = u + (long long)iy.c0 * P.Nux;
+      ufl += iy.w0 * dot3(ux0, load3(ur, ux0));
+      ufr += iy.w0 * dot3(ux1, load3(ur, ux1));
+    }
+    if (iy.w1 != S(0)) {
+      const double *ur = u + (long long)iy.c1 * P.Nux;
+      ufl += iy.w1 * dot3(ux0, load3(ur, ux0));
+      ufr += iy.w1 * dot3(ux1, load3(ur, ux1));
+    }
+    if (iy.w2 != S(0)) {
+      const double *ur = u + (long long)iy.c2 * P.Nux;
+      ufl += iy.w2 * dot3(ux0, load3(ur, ux0));
+      ufr += iy.w2 * dot3(ux1, load3(ur, ux1));
+    }
+    const S yle = S(__ldg(P.bc.YuLe + j)), yri = S(__ldg(P.bc.YuRi + j));
+    ufl += iy.b1 * uLo0 + iy.b2 * uUp0 + ux0.b1 * yle + ux0.b2 * yri;
+    ufr += iy.b1 * uLo1 + iy.b2 * uUp1 + ux1.b1 * yle + ux1.b2 * yri;
+    const S duvdx = ufr * vxr - ufl * vxl;
+    const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
+    const S d2v = S(__ldg(P.gyi + j)) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
+    const S ypy = hx * pLo * S(__ldg(P.pyl + j)) + hx * pUp * S(__ldg(P.pyu + j));
+    const double R = (double)(-(duvdx + dv2dy) + d2v - ypy);
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    const double oi = 1.0 / (__ldg(P.gyi + j) * __ldg(P.hx + i));
+    if (e.mode == 0) {
+      epilogue_stage(e, idx, oi, R);
+    } else {
+      const YRow<double> gy = yrow<double>(P.MYT, j);
+      const double g = -__ldg(P.hx + i) *
+                       (gy.w0 * __ldg(e.p + (long long)gy.c0 * P.Npx + i) + gy.w1 * __ldg(e.p + (long long)gy.c1 * P.Npx + i) +
+                        (gy.w2 != 0.0 ? gy.w2 * __ldg(e.p + (long long)gy.c2 * P.Npx + i) : 0.0));
+      e.w[idx] = oi * (R - g);
+      if (e.kV_next) e.kV_next[idx] = oi * R;
+    }
+    vy0 = vy1;
+    sy0 = sy1;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Fast walkers for interior tiles: every table row used by the tile is a
+// regular two-point stencil (RegD) without boundary terms, so addresses follow
+// from the column/row index and the weights come from the regular weight
+// arrays; boundary values do not enter.
+template <typename S>
+__device__ __forceinline__ S rw(const double *w, int r) {
+  return S(__ldg(w + r));
+}
+
+template <typename S>
+__device__ void fast_u(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+                       int i, int j0, int j1) {
+  const S ire = S(P.invRe);
+  const int cA = i + P.rAUX.s, cI = i + P.rIVX.s;
+  const S a00 = rw<S>(P.rAUX.w0, i), a01 = rw<S>(P.rAUX.w1, i);
+  const S a10 = rw<S>(P.rAUX.w0, i + 1), a11 = rw<S>(P.rAUX.w1, i + 1);
+  const S s00 = rw<S>(P.rSUX.w0, i), s01 = rw<S>(P.rSUX.w1, i);
+  const S s10 = rw<S>(P.rSUX.w0, i + 1), s11 = rw<S>(P.rSUX.w1, i + 1);
+  const S iv0 = rw<S>(P.rIVX.w0, i), iv1 = rw<S>(P.rIVX.w1, i);
+  const S gx = S(__ldg(P.gxi + i));
+  const bool twoA = P.rAUX.two, twoAy = P.rAUY.two, twoIx = P.rIVX.two, twoIy = P.rIVY.two;
+  auto vx = [&](const double *row) {
+    S r = iv0 * S(__ldg(row + cI));
+    if (twoIx) r += iv1 * S(__ldg(row + cI + 1));
+    return r;
+  };
+  auto face = [&](int r, S &uy, S &sy, S &vf) {
+    const double *col = u + (long long)(r + P.rAUY.s) * P.Nux + i;
+    const S f0 = S(__ldg(col));
+    const S f1 = twoAy ? S(__ldg(col + P.Nux)) : S(0);
+    uy = rw<S>(P.rAUY.w0, r) * f0 + rw<S>(P.rAUY.w1, r) * f1;
+    sy = rw<S>(P.rSUY.w0, r) * f0 + rw<S>(P.rSUY.w1, r) * f1;
+    const double *vr = v + (long long)(r + P.rIVY.s) * P.Nvx;
+    S acc = rw<S>(P.rIVY.w0, r) * vx(vr);
+    if (twoIy) acc += rw<S>(P.rIVY.w1, r) * vx(vr + P.Nvx);
+    vf = acc;
+  };
+  S uy0, sy0, vf0;
+  face(j0, uy0, sy0, vf0);
+  for (int j = j0; j < j1; ++j) {
+    S uy1, sy1, vf1;
+    face(j + 1, uy1, sy1, vf1);
+    const double *__restrict__ row = u + (long long)j * P.Nux;
+    const S um = S(__ldg(row + cA)), u0 = S(__ldg(row + cA + 1));
+    const S up = twoA ? S(__ldg(row + cA + 2)) : S(0);
+    const S uxl = a00 * um + a01 * u0, uxr = a10 * u0 + a11 * up;
+    const S sxl = s00 * um + s01 * u0, sxr = s10 * u0 + s11 * up;
+    const double hyd = __ldg(P.hy + j);
+    const S hy = S(hyd);
+    const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
+    const S duvdy = vf1 * uy1 - vf0 * uy0;
+    const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
+    const double R = (double)(-(du2dx + duvdy) + d2u);
+    const long long idx = (long long)j * P.Nux + i;
+    const double oi = 1.0 / (hyd * (double)__ldg(P.gxi + i));
+    if (e.mode == 0) {
+      epilogue_stage(e, idx, oi, R);
+    } else {
+      const double *prow = e.p + (long long)j * P.Npx + i + P.rMXT.s;
+      double g = __ldg(P.rMXT.w0 + i) * __ldg(prow);
+      if (P.rMXT.two) g += __ldg(P.rMXT.w1 + i) * __ldg(prow + 1);
+      g *= -hyd;
+      e.w[idx] = oi * (R - g);
+      if (e.kV_next) e.kV_next[idx] = oi * R;
+    }
+    uy0 = uy1;
+    sy0 = sy1;
+    vf0 = vf1;
+  }
+}
+
+template <typename S>
+__device__ void fast_v(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+                       int i, int j0, int j1) {
+  const S ire = S(P.invRe);
+  const int cV = i + P.rAVX.s;
+  const int cU0 = i + P.rIUX.s, cU1 = cU0 + 1;
+  const S v00 = rw<S>(P.rAVX.w0, i), v01 = rw<S>(P.rAVX.w1, i);
+  const S v10 = rw<S>(P.rAVX.w0, i + 1), v11 = rw<S>(P.rAVX.w1, i + 1);
+  const S s00 = rw<S>(P.rSVX.w0, i), s01 = rw<S>(P.rSVX.w1, i);
+  const S s10 = rw<S>(P.rSVX.w0, i + 1), s11 = rw<S>(P.rSVX.w1, i + 1);
+  const S wu00 = rw<S>(P.rIUX.w0, i), wu01 = rw<S>(P.rIUX.w1, i);
+  const S wu10 = rw<S>(P.rIUX.w0, i + 1), wu11 = rw<S>(P.rIUX.w1, i + 1);
+  const double hxd = __ldg(P.hx + i);
+  const S hx = S(hxd);
+  const bool twoV = P.rAVX.two, twoVy = P.rAVY.two, twoUx = P.rIUX.two, twoUy = P.rIUY.two;
+  auto face = [&](int r, S &vy, S &sy) {
+    const double *col = v + (long long)(r + P.rAVY.s) * P.Nvx + i;
+    const S f0 = S(__ldg(col));
+    const S f1 = twoVy ? S(__ldg(col + P.Nvx)) : S(0);
+    vy = rw<S>(P.rAVY.w0, r) * f0 + rw<S>(P.rAVY.w1, r) * f1;
+    sy = rw<S>(P.rSVY.w0, r) * f0 + rw<S>(P.rSVY.w1, r) * f1;
+  };
+  auto ux = [&](const double *row, S &l, S &r) {
+    const S a = S(__ldg(row + cU0)), b = S(__ldg(row + cU1));
+    l = wu00 * a;
+    r = wu10 * b;
+    if (twoUx) {
+      l += wu01 * b;
+      r += wu11 * S(__ldg(row + cU1 + 1));
+    }
+  };
+  S vy0, sy0;
+  face(j0, vy0, sy0);
+  for (int j = j0; j < j1; ++j) {
+    S vy1, sy1;
+    face(j + 1, vy1, sy1);
+    const double *__restrict__ row = v + (long long)j * P.Nvx;
+    const S vm = S(__ldg(row + cV)), v0 = S(__ldg(row + cV + 1));
+    const S vp = twoV ? S(__ldg(row + cV + 2)) : S(0);
+    const S vxl = v00 * vm + v01 * v0, vxr = v10 * v0 + v11 * vp;
+    const S svl = s00 * vm + s01 * v0, svr = s10 * v0 + s11 * vp;
+    const double *ur = u + (long long)(j + P.rIUY.s) * P.Nux;
+    S l0, r0;
+    ux(ur, l0, r0);
+    const S wy0 = rw<S>(P.rIUY.w0, j);
+    S ufl = wy0 * l0, ufr = wy0 * r0;
+    if (twoUy) {
+      S l1, r1;
+      ux(ur + P.Nux, l1, r1);
+      const S wy1 = rw<S>(P.rIUY.w1, j);
+      ufl += wy1 * l1;
+      ufr += wy1 * r1;
+    }
+    const S duvdx = ufr * vxr - ufl * vxl;
+    const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
+    const double gyd = __ldg(P.gyi + j);
+    const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
+    const double R = (double)(-(duvdx + dv2dy) + d2v);
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    const double oi = 1.0 / (gyd * hxd);
+    if (e.mode == 0) {
+      epilogue_stage(e, idx, oi, R);
+    } else {
+      const double *pc = e.p + (long long)(j + P.rMYT.s) * P.Npx + i;
+      double g = __ldg(P.rMYT.w0 + j) * __ldg(pc);
+      if (P.rMYT.two) g += __ldg(P.rMYT.w1 + j) * __ldg(pc + P.Npx);
+      g *= -hxd;
+      e.w[idx] = oi * (R - g);
+      if (e.kV_next) e.kV_next[idx] = oi * R;
+    }
+    vy0 = vy1;
+    sy0 = sy1;
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(WX * 2) k_walk_fast(const __grid_constant__ DevOps P, const double *__restrict__ V,
+                                                      const __grid_constant__ Epi e) {
+  const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
+  const int i = bx * WX + threadIdx.x;
+  const int j0 = by * RUN, j1 = j0 + RUN;
+  const double *u = V, *v = V + P.Nu;
+  if (threadIdx.y == 0)
+    fast_u<S>(P, u, v, e, i, j0, j1);
+  else
+    fast_v<S>(P, u, v, e, i, j0, j1);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(WX * 2) k_walk(const __grid_constant__ DevOps P, const double *__restrict__ V,
+                                                 const __grid_constant__ Epi e) {
+  if ((int)blockIdx.x >= P.fbx0 && (int)blockIdx.x < P.fbx1 && (int)blockIdx.y >= P.fby0 &&
+      (int)blockIdx.y < P.fby1)
+    return;  // interior tile: handled by k_walk_fast
+  const int i = blockIdx.x * WX + threadIdx.x;
+  const int j0 = blockIdx.y * RUN, j1 = j0 + RUN;
+  const double *u = V, *v = V + P.Nu;
+  if (threadIdx.y == 0)
+    walk_u<S>(P, u, v, e, i, j0, j1);
+  else
+    walk_v<S>(P, u, v, e, i, j0, j1);
+}
+
+void launch_walk(const DevOps &P, const double *V, const Epi &e, bool fp32, cudaStream_t s) {
+  const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
+  const int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  dim3 g((nx + WX - 1) / WX, (ny + RUN - 1) / RUN);
+  const bool has_fast = P.fbx1 > P.fbx0 && P.fby1 > P.fby0;
+  if (has_fast) {
+    dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
+    if (fp32)
+      k_walk_fast<float><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
+    else
+      k_walk_fast<double><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
+  }
+  if (fp32)
+    k_walk<float><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
+  else
+    k_walk<double><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
+}
+
+}  // namespace
+
+// The rectangle of tiles whose every column and row lies in the regular
+// ranges the fast walkers need (both walkers of a block must qualify).
+void walker_rectangle(DevOps &P) {
+  auto in = [](const RegD &r, int a, int b) { return a >= r.lo && b < r.hi; };  // rows a..b inclusive
+  const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
+  const int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  const int nbx = (nx + WX - 1) / WX, nby = (ny + RUN - 1) / RUN;
+  int bx0 = -1, bx1 = -1, by0 = -1, by1 = -1;
+  for (int bx = 0; bx < nbx; ++bx) {
+    const int i0 = bx * WX, i1 = i0 + WX;  // columns i0..i1-1
+    const bool ok = i1 <= P.Nux && i1 <= P.Nvx && in(P.rAUX, i0, i1) && in(P.rIVX, i0, i1 - 1) &&
+                    in(P.rMXT, i0, i1 - 1) && in(P.rAVX, i0, i1) && in(P.rIUX, i0, i1);
+    if (ok) {
+      if (bx0 < 0) bx0 = bx;
+      bx1 = bx + 1;
+    }
+  }
+  for (int by = 0; by < nby; ++by) {
+    const int j0 = by * RUN, j1 = j0 + RUN;  // rows j0..j1-1
+    const bool ok = j1 <= P.Nuy && j1 <= P.Nvy && in(P.rAUY, j0, j1) && in(P.rIVY, j0, j1) && in(P.rAVY, j0, j1) &&
+                    in(P.rIUY, j0, j1 - 1) && in(P.rMYT, j0, j1 - 1);
+    if (ok) {
+      if (by0 < 0) by0 = by;
+      by1 = by + 1;
+    }
+  }
+  if (bx0 < 0 || by0 < 0) bx0 = bx1 = by0 = by1 = 0;
+  P.fbx0 = bx0;
+  P.fbx1 = bx1;
+  P.fby0 = by0;
+  P.fby1 = by1;
+}
+
+void launch_stage(const DevOps &P, const StageArgs &a, bool fp32, cudaStream_t s) {
+  Epi e{};
+  e.mode = 0;
+  e.Vn = a.Vn;
+  e.kV = a.kV;
+  for (int m = 0; m < a.nprev; ++m) {
+    e.kprev[m] = a.kprev[m];
+    e.aprev[m] = a.aprev[m];
+  }
+  e.nprev = a.nprev;
+  e.aii = a.aii;
+  e.inv_dt = a.inv_dt;
+  e.Wt = a.Wt;
+  launch_walk(P, a.V, e, fp32, s);
+}
+
+void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next, bool fp32,
+                     cudaStream_t s) {
+  Epi e{};
+  e.mode = 1;
+  e.p = p;
+  e.w = w;
+  e.kV_next = kV_next;
+  launch_walk(P, V, e, fp32, s);
+}
+
+}  // namespace ins2d

@@ -41,14 +41,24 @@ def grid_stretched(N, a=0.0, b=1.0, beta=1.5):
     return a + (b - a) * (z + 1) / 2
 
 
-def smooth_bc(seed):
-    """Smooth, time-dependent boundary values (so every BC vector is non-zero)."""
+def is_closed(bc):
+    """No outflow ('pres') boundary: the pressure matrix is singular and the
+    boundary data must carry zero net normal flux for a consistent system."""
+    return "pres" not in (bc["u"]["left"], bc["u"]["right"], bc["v"]["low"], bc["v"]["up"])
+
+
+def smooth_bc(seed, closed=False):
+    """Smooth, time-dependent boundary values (so every BC vector is non-zero).
+    closed=True makes the normal components (u on left/right, v on low/up)
+    zero, as a closed domain needs."""
     rng = np.random.default_rng(seed)
     a = rng.uniform(0.5, 1.5, 6)
 
     def uBC(x, y, t):
         x = np.atleast_1d(np.asarray(x, float))
         y = np.atleast_1d(np.asarray(y, float))
+        if closed and len(x) == 1 and len(y) > 1:
+            return np.zeros(len(y))
         X = np.tile(x, len(y)) if len(y) > 1 else x
         Y = np.repeat(y, len(x)) if len(y) > 1 else np.full(len(x), y[0])
         return a[0] * np.sin(2 * X + a[1] * Y + t) + a[2] * 0.3
@@ -56,6 +66,8 @@ def smooth_bc(seed):
     def vBC(x, y, t):
         x = np.atleast_1d(np.asarray(x, float))
         y = np.atleast_1d(np.asarray(y, float))
+        if closed and len(y) == 1 and len(x) > 1:
+            return np.zeros(len(x))
         X = np.tile(x, len(y)) if len(y) > 1 else x
         Y = np.repeat(y, len(x)) if len(y) > 1 else np.full(len(x), y[0])
         return a[3] * np.cos(a[4] * X - 3 * Y + 0.5 * t) + 0.1 * a[5]

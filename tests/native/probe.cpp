@@ -1,0 +1,53 @@
+// Test-only probe: exposes the host-side operator tables of setup.cpp to the
+// CPU tests (no CUDA), so the derivation can be checked against the oracle's
+// assembled sparse matrices.
+#include <cstring>
+#include <string>
+
+#include "setup.hpp"
+
+using namespace ins2d;
+
+static std::string g_err;
+
+extern "C" const char *probe_error() { return g_err.c_str(); }
+
+extern "C" void *probe_build(int Nx, int Ny, const double *x, const double *y, const int *bc, double Re) {
+  HostOps *H = new HostOps();
+  try {
+    build_host_ops(*H, Nx, Ny, x, y, bc, Re);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    delete H;
+    return nullptr;
+  }
+  return H;
+}
+
+extern "C" void probe_free(void *h) { delete (HostOps *)h; }
+
+extern "C" int probe_sizes(void *h, int *out) {
+  HostOps *H = (HostOps *)h;
+  out[0] = H->Nux; out[1] = H->Nuy; out[2] = H->Nvx; out[3] = H->Nvy; out[4] = H->Npx; out[5] = H->Npy;
+  return 0;
+}
+
+extern "C" int probe_table(void *h, const char *name, int *nrows, int *ncols, const int **col, const double **w,
+                           const double **b1, const double **b2) {
+  HostOps *H = (HostOps *)h;
+  const Table *t = nullptr;
+  struct { const char *n; const Table *t; } all[] = {
+      {"AUX", &H->AUX}, {"SUX", &H->SUX}, {"AUY", &H->AUY}, {"SUY", &H->SUY}, {"IVX", &H->IVX}, {"IVY", &H->IVY},
+      {"MX", &H->MX},   {"MXT", &H->MXT}, {"AVX", &H->AVX}, {"SVX", &H->SVX}, {"AVY", &H->AVY}, {"SVY", &H->SVY},
+      {"IUX", &H->IUX}, {"IUY", &H->IUY}, {"MY", &H->MY},   {"MYT", &H->MYT}, {"TX", &H->TX},   {"TY", &H->TY}};
+  for (auto &a : all)
+    if (std::strcmp(a.n, name) == 0) t = a.t;
+  if (!t) return 1;
+  *nrows = t->nrows;
+  *ncols = t->ncols;
+  *col = t->col.data();
+  *w = t->w.data();
+  *b1 = t->b1.data();
+  *b2 = t->b2.data();
+  return 0;
+}
