@@ -269,13 +269,16 @@ int sample_bc(ins2d_ctx *c, double t) {
   return rc;
 }
 
-// p = pressure_additional_solve(V,p,T,t,options)   (device pointers)
-int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_solve_stats *st) {
+// p = pressure_additional_solve(V,p,T,t,options)   (device pointers); when
+// kV_next is given it also receives Om^-1 R(V) (the next step's first-stage
+// right-hand side).
+int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_solve_stats *st,
+                     double *kV_next = nullptr) {
   int rc = sample_bc(c, t);
   if (rc) return rc;
   {
     Prof pr(c, INS2D_PROF_RESIDUAL, 1);
-    launch_residual(c->P, V, p, c->wres, nullptr, c->fp32, c->stream);
+    launch_residual(c->P, V, p, c->wres, kV_next, c->fp32, c->stream);
   }
   {
     Prof pr(c, INS2D_PROF_DIV, 1);
@@ -286,27 +289,35 @@ int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_s
 }
 
 // [V,p] = time_ERK(V,p,T,t,dt,options) on device pointers, in place.
-int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step_stats *stats) {
+// k0_cached: kV[0] already holds Om^-1 R(V) (steady BCs, the previous step of
+// the same run computed it in its additional solve); on return *cache_next
+// says whether kV[0] holds it for the next step.
+int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step_stats *stats, bool k0_cached,
+             bool *cache_next) {
   const DevOps &P = c->P;
+  if (cache_next) *cache_next = false;
   int rc = sample_bc(c, t);
   if (rc) return rc;
   const double *dpp = nullptr;
   for (int i = 0; i < c->s; ++i) {
-    StageArgs a{};
-    a.V = (i == 0) ? V : c->Vs;
-    a.Vn = V;
-    a.kV = c->need_store[i] ? c->kV[i] : nullptr;
-    a.nprev = 0;
-    for (int m = 0; m < i; ++m)
-      if (c->A[i][m] != 0.0) {
-        a.kprev[a.nprev] = c->kV[m];
-        a.aprev[a.nprev] = c->A[i][m];
-        ++a.nprev;
-      }
-    a.aii = c->A[i][i];
-    a.inv_dt = 1.0 / dt;
-    a.Wt = c->Wt;
-    {
+    if (i == 0 && k0_cached && !c->bcd.bc_unsteady) {
+      Prof pr(c, INS2D_PROF_STAGE, 1);
+      launch_stage_cached(c->kV[0], V, c->A[0][0], 1.0 / dt, c->Wt, P.Nu + P.Nv, c->stream);
+    } else {
+      StageArgs a{};
+      a.V = (i == 0) ? V : c->Vs;
+      a.Vn = V;
+      a.kV = (c->need_store[i] || i == 0) ? c->kV[i] : nullptr;
+      a.nprev = 0;
+      for (int m = 0; m < i; ++m)
+        if (c->A[i][m] != 0.0) {
+          a.kprev[a.nprev] = c->kV[m];
+          a.aprev[a.nprev] = c->A[i][m];
+          ++a.nprev;
+        }
+      a.aii = c->A[i][i];
+      a.inv_dt = 1.0 / dt;
+      a.Wt = c->Wt;
       Prof pr(c, INS2D_PROF_STAGE, 1);
       launch_stage(P, a, c->fp32, c->stream);
     }
@@ -339,9 +350,11 @@ int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step
     CK(cudaMemcpyAsync(p, dpp, P.Np * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));  // p = kp(:,end)
   } else {
     ins2d_solve_stats st;
-    rc = additional_solve(c, V, p, t + dt, &st);
+    const bool cache = cache_next && !c->bcd.bc_unsteady;
+    rc = additional_solve(c, V, p, t + dt, &st, cache ? c->kV[0] : nullptr);
     if (rc) return rc;
     stats_add(stats, st);
+    if (cache) *cache_next = true;
   }
   return INS2D_OK;
 }
@@ -436,6 +449,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
       d.lo = r.lo;
       d.hi = r.hi;
       d.two = r.two;
+      d.n = t.ncols;
       d.w0 = upload_vec(c, t.rw0);
       d.w1 = upload_vec(c, t.rw1);
       return d;
@@ -446,6 +460,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     P.rAVX = reg(H.rAVX, H.AVX); P.rSVX = reg(H.rAVX, H.SVX);
     P.rAVY = reg(H.rAVY, H.AVY); P.rSVY = reg(H.rAVY, H.SVY);
     P.rIUX = reg(H.rIUX, H.IUX); P.rIUY = reg(H.rIUY, H.IUY); P.rMYT = reg(H.rMYT, H.MYT);
+    P.rMX = reg(H.rMX, H.MX); P.rMY = reg(H.rMY, H.MY);
     walker_rectangle(P);
     if (H.fft_ok) {
       P.fft_ax = upload_vec(c, H.fft_ax);
@@ -473,7 +488,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     const size_t NV = (size_t)(P.Nu + P.Nv), Np = (size_t)P.Np;
     c->Vs = dalloc<double>(c, NV);
     c->Wt = dalloc<double>(c, NV);
-    for (int m = 0; m < c->s; ++m) c->kV[m] = c->need_store[m] ? dalloc<double>(c, NV) : nullptr;
+    for (int m = 0; m < c->s; ++m) c->kV[m] = (c->need_store[m] || m == 0) ? dalloc<double>(c, NV) : nullptr;
     c->wres = dalloc<double>(c, NV);
     c->f = dalloc<double>(c, Np);
     c->dp = dalloc<double>(c, Np);
@@ -773,9 +788,12 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
     dV = ctx->stV;
     dP = ctx->stP;
   }
+  bool cached = false;
   for (int n = 0; n < nsteps; ++n) {
-    int rc = erk_step(ctx, dV, dP, t + n * dt, dt, stats);
+    bool next = false;
+    int rc = erk_step(ctx, dV, dP, t + n * dt, dt, stats, cached, n + 1 < nsteps ? &next : nullptr);
     if (rc) return rc;
+    cached = next;
   }
   if (mem == INS2D_MEM_HOST) {
     CK(cudaMemcpyAsync(V, dV, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -40,9 +40,10 @@ struct BcVals {
 // Regular interior of a 1D table: rows [lo,hi) are w0[r]*f[r+s] + w1[r]*f[r+s+1]
 // without boundary terms (two = 0: w1 is zero in the whole range).
 struct RegD {
-  int s, lo, hi, two;
+  int s, lo, hi, two, n;  // n: column count (indices wrap modulo n)
   const double *w0, *w1;
 };
+__device__ __forceinline__ int wrapn(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
 
 struct DevOps {
   int Nx, Ny, Nux, Nuy, Nvx, Nvy, Npx, Npy;
@@ -59,7 +60,7 @@ struct DevOps {
   BcVals bc;
   // fast-walker data: regular ranges (pairs share ranges) and the block
   // rectangle [fbx0,fbx1) x [fby0,fby1) whose tiles lie inside all of them
-  RegD rAUX, rSUX, rAUY, rSUY, rIVX, rIVY, rMXT, rAVX, rSVX, rAVY, rSVY, rIUX, rIUY, rMYT;
+  RegD rAUX, rSUX, rAUY, rSUY, rIVX, rIVY, rMXT, rAVX, rSVX, rAVY, rSVY, rIUX, rIUY, rMYT, rMX, rMY;
   int fbx0, fbx1, fby0, fby1;
 };
 
@@ -207,6 +208,29 @@ __device__ __forceinline__ double div_bc(const DevOps &P, const double *uLe, con
          __ldg(P.hx + i) * (__ldg(P.MY.b1 + j) * __ldg(vLo + i) + __ldg(P.MY.b2 + j) * __ldg(vUp + i));
 }
 // (A p)(i,j), A = M Om^-1 G = -(hy_j TX + hx_i TY)
+__device__ __forceinline__ bool in_reg(const RegD &r, int row) { return row >= r.lo && row < r.hi; }
+// regular-row versions (no tables, no boundary terms)
+__device__ __forceinline__ double reg_x(const RegD &r, int row, const double *__restrict__ f, long long base) {
+  const int c0 = wrapn(row + r.s, r.n);
+  double a = __ldg(r.w0 + row) * __ldg(f + base + c0);
+  if (r.two) a += __ldg(r.w1 + row) * __ldg(f + base + wrapn(c0 + 1, r.n));
+  return a;
+}
+__device__ __forceinline__ double reg_y(const RegD &r, int row, const double *__restrict__ f, int stride, int i) {
+  const int c0 = wrapn(row + r.s, r.n);
+  double a = __ldg(r.w0 + row) * __ldg(f + (long long)c0 * stride + i);
+  if (r.two) a += __ldg(r.w1 + row) * __ldg(f + (long long)wrapn(c0 + 1, r.n) * stride + i);
+  return a;
+}
+__device__ __forceinline__ double grad_x_fast(const DevOps &P, const double *__restrict__ p, int i, int j) {
+  if (in_reg(P.rMXT, i)) return -__ldg(P.hy + j) * reg_x(P.rMXT, i, p, (long long)j * P.Npx);
+  return grad_x(P, p, i, j);
+}
+__device__ __forceinline__ double grad_y_fast(const DevOps &P, const double *__restrict__ p, int i, int j) {
+  if (in_reg(P.rMYT, j)) return -__ldg(P.hx + i) * reg_y(P.rMYT, j, p, P.Npx, i);
+  return grad_y(P, p, i, j);
+}
+
 __device__ __forceinline__ double lap(const DevOps &P, const double *__restrict__ p, int i, int j) {
   return -(__ldg(P.hy + j) * tab_x<double>(P.TX, i, p, (long long)j * P.Npx) +
            __ldg(P.hx + i) * tab_y<double>(P.TY, j, p, P.Npx, i));

@@ -170,33 +170,38 @@ __global__ void __launch_bounds__(kThreads) k_cols(int Nx, int Ny, int logy, int
   const int H = Nx / 2 + 1;
   const int c0 = blockIdx.x * G;
   const int g_here = min(G, H - c0);
+  // power-of-two columns: forward decimation in frequency (natural order in,
+  // bit-reversed out), scaling in bit-reversed order, inverse decimation in
+  // time (bit-reversed in, natural out) -- no permutation pass is needed
+  const int ldy = padded(Ny);
   for (int o = threadIdx.x; o < g_here * Ny; o += blockDim.x) {
     const int j = o / g_here, g = o - j * g_here;
-    sm[(size_t)g * padded(Ny) + pd(logy >= 0 ? brev(j, logy) : j)] = spec[(size_t)j * H + c0 + g];
+    sm[(size_t)g * ldy + pd(j)] = spec[(size_t)j * H + c0 + g];
   }
   __syncthreads();
   double2 *A = sm;
-  const int ldy = padded(Ny);
   if (logy >= 0) {
-    dit(sm, g_here, Ny, logy, tw, false);
+    dif(sm, g_here, Ny, logy, tw, false);
   } else {
     dft(sm, sm + (size_t)G * ldy, g_here, Ny, tw, false);
     A = sm + (size_t)G * ldy;
   }
   double lmax = 0.0;
   for (int o = threadIdx.x; o < g_here * Ny; o += blockDim.x) {
-    const int g = o / Ny, J = o - g * Ny;
+    const int g = o / Ny, pos = o - g * Ny;
+    const int J = logy >= 0 ? brev(pos, logy) : pos;
     const int I = c0 + g;
-    double2 *slot = A + (size_t)g * ldy + pd(J);
+    double2 *slot = A + (size_t)g * ldy + pd(pos);
     const double2 F = *slot;
     lmax = fmax(lmax, sqrt(F.x * F.x + F.y * F.y));
     const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + I) + __ldg(ay + J));
-    *slot = make_double2(-F.x / lam, -F.y / lam);
+    const double r = -1.0 / lam;
+    *slot = make_double2(F.x * r, F.y * r);
   }
   __syncthreads();
   double2 *Bout = A;
   if (logy >= 0) {
-    dif(A, g_here, Ny, logy, tw, true);
+    dit(A, g_here, Ny, logy, tw, true);
   } else {
     dft(A, sm, g_here, Ny, tw, true);
     Bout = sm;
@@ -204,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) k_cols(int Nx, int Ny, int logy, int
   const double sc = 1.0 / Ny;
   for (int o = threadIdx.x; o < g_here * Ny; o += blockDim.x) {
     const int j = o / g_here, g = o - j * g_here;
-    const double2 v = Bout[(size_t)g * ldy + pd(logy >= 0 ? brev(j, logy) : j)];
+    const double2 v = Bout[(size_t)g * ldy + pd(j)];
     spec[(size_t)j * H + c0 + g] = make_double2(v.x * sc, v.y * sc);
   }
   for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, off));

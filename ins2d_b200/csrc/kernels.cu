@@ -55,9 +55,16 @@ __global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, c
   double mx[1] = {0.0};
   const int ops[1] = {R_MAX};
   if (i < P.Npx && j < P.Npy) {
-    double d = div_in(P, W, W + P.Nu, i, j);
-    if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
-    if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
+    double d;
+    if (in_reg(P.rMX, i) && in_reg(P.rMY, j)) {
+      // interior cell: regular rows of Mx and My, no boundary contribution
+      d = __ldg(P.hy + j) * reg_x(P.rMX, i, W, (long long)j * P.Nux) +
+          __ldg(P.hx + i) * reg_y(P.rMY, j, W + P.Nu, P.Nvx, i);
+    } else {
+      d = div_in(P, W, W + P.Nu, i, j);
+      if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
+      if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
+    }
     d *= gamma;
     f[(long long)j * P.Npx + i] = d;
     mx[0] = fabs(d);
@@ -72,11 +79,11 @@ __global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps 
   const int j = blockIdx.y * BY + threadIdx.y;
   if (i < P.Nux && j < P.Nuy) {
     const long long idx = (long long)j * P.Nux + i;
-    Vo[idx] = dt * (Wt[idx] - c * om_inv_u(P, i, j) * grad_x(P, dp, i, j));
+    Vo[idx] = dt * (Wt[idx] - c * om_inv_u(P, i, j) * grad_x_fast(P, dp, i, j));
   }
   if (i < P.Nvx && j < P.Nvy) {
     const long long idx = P.Nu + (long long)j * P.Nvx + i;
-    Vo[idx] = dt * (Wt[idx] - c * om_inv_v(P, i, j) * grad_y(P, dp, i, j));
+    Vo[idx] = dt * (Wt[idx] - c * om_inv_v(P, i, j) * grad_y_fast(P, dp, i, j));
   }
 }
 
@@ -125,6 +132,12 @@ __global__ void __launch_bounds__(256) k_conservation(const __grid_constant__ De
   grid_reduce<5>(q, ops, red);
 }
 
+__global__ void k_stage_cached(const double *__restrict__ kV0, const double *__restrict__ Vn, double aii,
+                               double inv_dt, double *__restrict__ Wt, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    Wt[k] = Vn[k] * inv_dt + aii * kV0[k];
+}
+
 __global__ void k_add(const double *__restrict__ x, double *__restrict__ y, long long n) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
     y[k] += x[k];
@@ -169,6 +182,13 @@ void launch_conservation(const DevOps &P, const double *V, const RedScratch &red
   int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
   int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   k_conservation<<<grid_for(nx, ny), dim3(BX, BY), 0, s>>>(P, V, red);
+}
+
+void launch_stage_cached(const double *kV0, const double *Vn, double aii, double inv_dt, double *Wt, long long n,
+                         cudaStream_t s) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 32) b = 148 * 32;
+  k_stage_cached<<<(unsigned)b, 256, 0, s>>>(kV0, Vn, aii, inv_dt, Wt, n);
 }
 
 void launch_add(const double *x, double *y, long long n, cudaStream_t s) {

@@ -55,6 +55,10 @@ void launch_correct(const DevOps &P, const double *V_in, const double *dp, doubl
 void launch_lap(const DevOps &P, const double *p, double *Ap, cudaStream_t s);
 // red.result = {max|M V + yM|, sum Omu u, sum Omv v, sum Omu u^2, sum Omv v^2}
 void launch_conservation(const DevOps &P, const double *V, const RedScratch &red, cudaStream_t s);
+// first RK stage when kV0 = Om^-1 R(Vn) is already known (it is the residual
+// of the previous step's additional pressure solve): Wt = Vn/dt + aii*kV0
+void launch_stage_cached(const double *kV0, const double *Vn, double aii, double inv_dt, double *Wt, long long n,
+                         cudaStream_t s);
 // y += x
 void launch_add(const double *x, double *y, long long n, cudaStream_t s);
 

@@ -278,17 +278,20 @@ Table make_table(const Sp &Pre, const BC1 &bc, const std::string &name) {
 }
 
 Regular find_regular(Table &T) {
+  // Rows r whose entries sit at columns (r+s) and (r+s+1) taken modulo the
+  // column count (periodic wrap rows qualify), without boundary terms.
   Regular R;
-  const int n = T.nrows;
+  const int n = T.nrows, nc = T.ncols;
   T.rw0.assign((size_t)n, 0.0);
   T.rw1.assign((size_t)n, 0.0);
-  if (n == 0) return R;
+  if (n == 0 || nc < 3) return R;
+  auto md = [nc](int c) { return ((c % nc) + nc) % nc; };
   auto is_reg = [&](int r, int s) {
-    if (r + s < 0 || r + s + 1 >= T.ncols) return false;  // both columns valid indices
     if (T.b1[r] != 0.0 || T.b2[r] != 0.0) return false;
+    if (T.T.rows[r].empty()) return false;
     for (auto &jv : T.T.rows[r])
-      if (jv.first != r + s && jv.first != r + s + 1) return false;
-    return !T.T.rows[r].empty();
+      if (jv.first != md(r + s) && jv.first != md(r + s + 1)) return false;
+    return true;
   };
   const int mid = n / 2;
   if (T.T.rows[mid].empty()) return R;
@@ -303,7 +306,7 @@ Regular find_regular(Table &T) {
   R.two = 0;
   for (int r = lo; r < hi; ++r)
     for (auto &jv : T.T.rows[r]) {
-      if (jv.first == r + s + 1) {
+      if (jv.first == md(r + s + 1)) {
         R.two = 1;
         T.rw1[r] = jv.second;
       } else {
@@ -564,6 +567,8 @@ void build_host_ops(HostOps &H, int Nx, int Ny, const double *x, const double *y
   H.rIUY = find_regular(H.IUY);
   H.rMXT = find_regular(H.MXT);
   H.rMYT = find_regular(H.MYT);
+  H.rMX = find_regular(H.MX);
+  H.rMY = find_regular(H.MY);
 
   // --- Laplacian A = M*Om_inv*G (operator_divergence.m:208) -----------------
   H.TX = make_table(mul(mul(H.MX.T, Sp::diag(recip(H.gxi))), transpose(H.MX.T)), "A(x)");

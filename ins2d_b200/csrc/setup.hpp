@@ -93,7 +93,7 @@ struct HostOps {
   // y_px / y_py patterns (set_bc_vectors.m:154-176)
   std::vector<double> pxl, pxr, pyl, pyu;
   // regular interior ranges (pairs intersected): used by the fast walker
-  Regular rAUX, rAUY, rIVX, rIVY, rMXT, rAVX, rAVY, rIUX, rIUY, rMYT;
+  Regular rAUX, rAUY, rIVX, rIVY, rMXT, rAVX, rAVY, rIUX, rIUY, rMYT, rMX, rMY;
   // FFT Poisson symbol factors (operator_divergence.m:268-291)
   bool fft_ok = false;
   std::vector<double> fft_ax, fft_ay;  // (1/dx^2) sin^2(I pi/Npx), (1/dy^2) sin^2(J pi/Npy)

@@ -292,74 +292,117 @@ __device__ __forceinline__ S rw(const double *w, int r) {
   return S(__ldg(w + r));
 }
 
+// Raw loads of one row of the u walker: the x-face values of row j, the
+// field values of the y-face j+1 and the epilogue input; issued one row ahead
+// of their use so each warp keeps two rows of loads in flight.
+template <typename S>
+struct URaw {
+  S um, u0, up, f0, f1, va0, va1, vb0, vb1;
+  double ep;
+};
+
 template <typename S>
 __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
                        int i, int j0, int j1) {
   const S ire = S(P.invRe);
-  const int cA = i + P.rAUX.s, cI = i + P.rIVX.s;
+  // columns (modulo the row length for periodic wraps)
+  const int cA0 = wrapn(i + P.rAUX.s, P.rAUX.n), cA1 = wrapn(cA0 + 1, P.rAUX.n), cA2 = wrapn(cA1 + 1, P.rAUX.n);
+  const int cI0 = wrapn(i + P.rIVX.s, P.rIVX.n), cI1 = wrapn(cI0 + 1, P.rIVX.n);
   const S a00 = rw<S>(P.rAUX.w0, i), a01 = rw<S>(P.rAUX.w1, i);
   const S a10 = rw<S>(P.rAUX.w0, i + 1), a11 = rw<S>(P.rAUX.w1, i + 1);
   const S s00 = rw<S>(P.rSUX.w0, i), s01 = rw<S>(P.rSUX.w1, i);
   const S s10 = rw<S>(P.rSUX.w0, i + 1), s11 = rw<S>(P.rSUX.w1, i + 1);
   const S iv0 = rw<S>(P.rIVX.w0, i), iv1 = rw<S>(P.rIVX.w1, i);
   const S gx = S(__ldg(P.gxi + i));
+  const double gxd = __ldg(P.gxi + i);
   const bool twoA = P.rAUX.two, twoAy = P.rAUY.two, twoIx = P.rIVX.two, twoIy = P.rIVY.two;
-  auto vx = [&](const double *row) {
-    S r = iv0 * S(__ldg(row + cI));
-    if (twoIx) r += iv1 * S(__ldg(row + cI + 1));
-    return r;
+  const int sAy = P.rAUY.s, sIy = P.rIVY.s;
+  const long long Nux = P.Nux, Nvx = P.Nvx;
+  // raw values of face r (u column at rows r+sAy, r+sAy+1; v rows r+sIy, r+sIy+1)
+  auto load_face = [&](int r, URaw<S> &q) {
+    const int ra = wrapn(r + sAy, P.rAUY.n);
+    q.f0 = S(__ldg(u + (long long)ra * Nux + i));
+    q.f1 = twoAy ? S(__ldg(u + (long long)wrapn(ra + 1, P.rAUY.n) * Nux + i)) : S(0);
+    const int rv = wrapn(r + sIy, P.rIVY.n);
+    const double *vr = v + (long long)rv * Nvx;
+    q.va0 = S(__ldg(vr + cI0));
+    q.va1 = twoIx ? S(__ldg(vr + cI1)) : S(0);
+    if (twoIy) {
+      const double *vr1 = v + (long long)wrapn(rv + 1, P.rIVY.n) * Nvx;
+      q.vb0 = S(__ldg(vr1 + cI0));
+      q.vb1 = twoIx ? S(__ldg(vr1 + cI1)) : S(0);
+    } else {
+      q.vb0 = q.vb1 = S(0);
+    }
   };
-  auto face = [&](int r, S &uy, S &sy, S &vf) {
-    const double *col = u + (long long)(r + P.rAUY.s) * P.Nux + i;
-    const S f0 = S(__ldg(col));
-    const S f1 = twoAy ? S(__ldg(col + P.Nux)) : S(0);
-    uy = rw<S>(P.rAUY.w0, r) * f0 + rw<S>(P.rAUY.w1, r) * f1;
-    sy = rw<S>(P.rSUY.w0, r) * f0 + rw<S>(P.rSUY.w1, r) * f1;
-    const double *vr = v + (long long)(r + P.rIVY.s) * P.Nvx;
-    S acc = rw<S>(P.rIVY.w0, r) * vx(vr);
-    if (twoIy) acc += rw<S>(P.rIVY.w1, r) * vx(vr + P.Nvx);
-    vf = acc;
+  auto face = [&](int r, const URaw<S> &q, S &uy, S &sy, S &vf) {
+    uy = rw<S>(P.rAUY.w0, r) * q.f0 + rw<S>(P.rAUY.w1, r) * q.f1;
+    sy = rw<S>(P.rSUY.w0, r) * q.f0 + rw<S>(P.rSUY.w1, r) * q.f1;
+    vf = rw<S>(P.rIVY.w0, r) * (iv0 * q.va0 + iv1 * q.va1) + rw<S>(P.rIVY.w1, r) * (iv0 * q.vb0 + iv1 * q.vb1);
+  };
+  auto load_row = [&](int j, URaw<S> &q) {
+    const double *row = u + (long long)j * Nux;
+    q.um = S(__ldg(row + cA0));
+    q.u0 = S(__ldg(row + cA1));
+    q.up = twoA ? S(__ldg(row + cA2)) : S(0);
+    load_face(j + 1, q);
+    const long long idx = (long long)j * Nux + i;
+    q.ep = (e.mode == 0) ? __ldg(e.Vn + idx) : 0.0;
   };
   S uy0, sy0, vf0;
-  face(j0, uy0, sy0, vf0);
+  {
+    URaw<S> q0;
+    load_face(j0, q0);
+    face(j0, q0, uy0, sy0, vf0);
+  }
+  URaw<S> cur;
+  load_row(j0, cur);
   for (int j = j0; j < j1; ++j) {
+    URaw<S> nxt;
+    if (j + 1 < j1) load_row(j + 1, nxt);
     S uy1, sy1, vf1;
-    face(j + 1, uy1, sy1, vf1);
-    const double *__restrict__ row = u + (long long)j * P.Nux;
-    const S um = S(__ldg(row + cA)), u0 = S(__ldg(row + cA + 1));
-    const S up = twoA ? S(__ldg(row + cA + 2)) : S(0);
-    const S uxl = a00 * um + a01 * u0, uxr = a10 * u0 + a11 * up;
-    const S sxl = s00 * um + s01 * u0, sxr = s10 * u0 + s11 * up;
+    face(j + 1, cur, uy1, sy1, vf1);
+    const S uxl = a00 * cur.um + a01 * cur.u0, uxr = a10 * cur.u0 + a11 * cur.up;
+    const S sxl = s00 * cur.um + s01 * cur.u0, sxr = s10 * cur.u0 + s11 * cur.up;
     const double hyd = __ldg(P.hy + j);
     const S hy = S(hyd);
     const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
     const S duvdy = vf1 * uy1 - vf0 * uy0;
     const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
     const double R = (double)(-(du2dx + duvdy) + d2u);
-    const long long idx = (long long)j * P.Nux + i;
-    const double oi = 1.0 / (hyd * (double)__ldg(P.gxi + i));
+    const long long idx = (long long)j * Nux + i;
+    const double oi = 1.0 / (hyd * gxd);
     if (e.mode == 0) {
-      epilogue_stage(e, idx, oi, R);
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = cur.ep * e.inv_dt + vt;
     } else {
-      const double *prow = e.p + (long long)j * P.Npx + i + P.rMXT.s;
-      double g = __ldg(P.rMXT.w0 + i) * __ldg(prow);
-      if (P.rMXT.two) g += __ldg(P.rMXT.w1 + i) * __ldg(prow + 1);
-      g *= -hyd;
+      const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
       e.w[idx] = oi * (R - g);
       if (e.kV_next) e.kV_next[idx] = oi * R;
     }
     uy0 = uy1;
     sy0 = sy1;
     vf0 = vf1;
+    cur = nxt;
   }
 }
+
+template <typename S>
+struct VRaw {
+  S vm, v0, vp, f0, f1, ua0, ua1, ua2, ub0, ub1, ub2;
+  double ep;
+};
 
 template <typename S>
 __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
                        int i, int j0, int j1) {
   const S ire = S(P.invRe);
-  const int cV = i + P.rAVX.s;
-  const int cU0 = i + P.rIUX.s, cU1 = cU0 + 1;
+  const int cV0 = wrapn(i + P.rAVX.s, P.rAVX.n), cV1 = wrapn(cV0 + 1, P.rAVX.n), cV2 = wrapn(cV1 + 1, P.rAVX.n);
+  const int cU0 = wrapn(i + P.rIUX.s, P.rIUX.n), cU1 = wrapn(cU0 + 1, P.rIUX.n), cU2 = wrapn(cU1 + 1, P.rIUX.n);
   const S v00 = rw<S>(P.rAVX.w0, i), v01 = rw<S>(P.rAVX.w1, i);
   const S v10 = rw<S>(P.rAVX.w0, i + 1), v11 = rw<S>(P.rAVX.w1, i + 1);
   const S s00 = rw<S>(P.rSVX.w0, i), s01 = rw<S>(P.rSVX.w1, i);
@@ -369,63 +412,81 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
   const double hxd = __ldg(P.hx + i);
   const S hx = S(hxd);
   const bool twoV = P.rAVX.two, twoVy = P.rAVY.two, twoUx = P.rIUX.two, twoUy = P.rIUY.two;
-  auto face = [&](int r, S &vy, S &sy) {
-    const double *col = v + (long long)(r + P.rAVY.s) * P.Nvx + i;
-    const S f0 = S(__ldg(col));
-    const S f1 = twoVy ? S(__ldg(col + P.Nvx)) : S(0);
-    vy = rw<S>(P.rAVY.w0, r) * f0 + rw<S>(P.rAVY.w1, r) * f1;
-    sy = rw<S>(P.rSVY.w0, r) * f0 + rw<S>(P.rSVY.w1, r) * f1;
+  const int sVy = P.rAVY.s, sUy = P.rIUY.s;
+  const long long Nux = P.Nux, Nvx = P.Nvx;
+  auto load_face = [&](int r, VRaw<S> &q) {
+    const int ra = wrapn(r + sVy, P.rAVY.n);
+    q.f0 = S(__ldg(v + (long long)ra * Nvx + i));
+    q.f1 = twoVy ? S(__ldg(v + (long long)wrapn(ra + 1, P.rAVY.n) * Nvx + i)) : S(0);
   };
-  auto ux = [&](const double *row, S &l, S &r) {
-    const S a = S(__ldg(row + cU0)), b = S(__ldg(row + cU1));
-    l = wu00 * a;
-    r = wu10 * b;
-    if (twoUx) {
-      l += wu01 * b;
-      r += wu11 * S(__ldg(row + cU1 + 1));
+  auto face = [&](int r, const VRaw<S> &q, S &vy, S &sy) {
+    vy = rw<S>(P.rAVY.w0, r) * q.f0 + rw<S>(P.rAVY.w1, r) * q.f1;
+    sy = rw<S>(P.rSVY.w0, r) * q.f0 + rw<S>(P.rSVY.w1, r) * q.f1;
+  };
+  auto load_row = [&](int j, VRaw<S> &q) {
+    const double *row = v + (long long)j * Nvx;
+    q.vm = S(__ldg(row + cV0));
+    q.v0 = S(__ldg(row + cV1));
+    q.vp = twoV ? S(__ldg(row + cV2)) : S(0);
+    const int ru = wrapn(j + sUy, P.rIUY.n);
+    const double *ur = u + (long long)ru * Nux;
+    q.ua0 = S(__ldg(ur + cU0));
+    q.ua1 = S(__ldg(ur + cU1));
+    q.ua2 = twoUx ? S(__ldg(ur + cU2)) : S(0);
+    if (twoUy) {
+      const double *ur1 = u + (long long)wrapn(ru + 1, P.rIUY.n) * Nux;
+      q.ub0 = S(__ldg(ur1 + cU0));
+      q.ub1 = S(__ldg(ur1 + cU1));
+      q.ub2 = twoUx ? S(__ldg(ur1 + cU2)) : S(0);
+    } else {
+      q.ub0 = q.ub1 = q.ub2 = S(0);
     }
+    load_face(j + 1, q);
+    const long long idx = P.Nu + (long long)j * Nvx + i;
+    q.ep = (e.mode == 0) ? __ldg(e.Vn + idx) : 0.0;
   };
   S vy0, sy0;
-  face(j0, vy0, sy0);
+  {
+    VRaw<S> q0;
+    load_face(j0, q0);
+    face(j0, q0, vy0, sy0);
+  }
+  VRaw<S> cur;
+  load_row(j0, cur);
   for (int j = j0; j < j1; ++j) {
+    VRaw<S> nxt;
+    if (j + 1 < j1) load_row(j + 1, nxt);
     S vy1, sy1;
-    face(j + 1, vy1, sy1);
-    const double *__restrict__ row = v + (long long)j * P.Nvx;
-    const S vm = S(__ldg(row + cV)), v0 = S(__ldg(row + cV + 1));
-    const S vp = twoV ? S(__ldg(row + cV + 2)) : S(0);
-    const S vxl = v00 * vm + v01 * v0, vxr = v10 * v0 + v11 * vp;
-    const S svl = s00 * vm + s01 * v0, svr = s10 * v0 + s11 * vp;
-    const double *ur = u + (long long)(j + P.rIUY.s) * P.Nux;
-    S l0, r0;
-    ux(ur, l0, r0);
-    const S wy0 = rw<S>(P.rIUY.w0, j);
-    S ufl = wy0 * l0, ufr = wy0 * r0;
-    if (twoUy) {
-      S l1, r1;
-      ux(ur + P.Nux, l1, r1);
-      const S wy1 = rw<S>(P.rIUY.w1, j);
-      ufl += wy1 * l1;
-      ufr += wy1 * r1;
-    }
+    face(j + 1, cur, vy1, sy1);
+    const S vxl = v00 * cur.vm + v01 * cur.v0, vxr = v10 * cur.v0 + v11 * cur.vp;
+    const S svl = s00 * cur.vm + s01 * cur.v0, svr = s10 * cur.v0 + s11 * cur.vp;
+    // ubar at vx faces i, i+1: IUY row j times IUX rows i, i+1
+    const S la = wu00 * cur.ua0 + wu01 * cur.ua1, ra = wu10 * cur.ua1 + wu11 * cur.ua2;
+    const S lb = wu00 * cur.ub0 + wu01 * cur.ub1, rb = wu10 * cur.ub1 + wu11 * cur.ub2;
+    const S wy0 = rw<S>(P.rIUY.w0, j), wy1 = rw<S>(P.rIUY.w1, j);
+    const S ufl = wy0 * la + wy1 * lb, ufr = wy0 * ra + wy1 * rb;
     const S duvdx = ufr * vxr - ufl * vxl;
     const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
     const double gyd = __ldg(P.gyi + j);
     const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
     const double R = (double)(-(duvdx + dv2dy) + d2v);
-    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    const long long idx = P.Nu + (long long)j * Nvx + i;
     const double oi = 1.0 / (gyd * hxd);
     if (e.mode == 0) {
-      epilogue_stage(e, idx, oi, R);
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = cur.ep * e.inv_dt + vt;
     } else {
-      const double *pc = e.p + (long long)(j + P.rMYT.s) * P.Npx + i;
-      double g = __ldg(P.rMYT.w0 + j) * __ldg(pc);
-      if (P.rMYT.two) g += __ldg(P.rMYT.w1 + j) * __ldg(pc + P.Npx);
-      g *= -hxd;
+      const double g = -hxd * reg_y(P.rMYT, j, e.p, P.Npx, i);
       e.w[idx] = oi * (R - g);
       if (e.kV_next) e.kV_next[idx] = oi * R;
     }
     vy0 = vy1;
     sy0 = sy1;
+    cur = nxt;
   }
 }
 
