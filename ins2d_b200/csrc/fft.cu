@@ -273,6 +273,240 @@ __global__ void __launch_bounds__(kThreads) k_rows_c2r(int Nx, int Ny, int logx,
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Register groups of up to three radix-2 stages on 8 values x[m] at positions
+// base + m*h (h = half size of the smallest stage of the group, k = base mod h).
+__device__ __forceinline__ void group_dif(double2 (&x)[8], int ns, int k, int h, int s_lo, int logn,
+                                          const double2 *tw, bool inv) {
+#pragma unroll
+  for (int st = 2; st >= 0; --st) {
+    if (st >= ns) continue;
+    const int hh = 1 << st, sh = logn - (s_lo + st);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      if ((m & (2 * hh - 1)) >= hh || m + hh >= (1 << ns)) continue;
+      const int off = k + (m & (hh - 1)) * h;
+      const double2 x0 = x[m], x1 = x[m + hh];
+      x[m] = make_double2(x0.x + x1.x, x0.y + x1.y);
+      x[m + hh] = cmul(make_double2(x0.x - x1.x, x0.y - x1.y), twid(tw, off << sh, inv));
+    }
+  }
+}
+__device__ __forceinline__ void group_dit(double2 (&x)[8], int ns, int k, int h, int s0, int logn,
+                                          const double2 *tw, bool inv) {
+#pragma unroll
+  for (int st = 0; st < 3; ++st) {
+    if (st >= ns) break;
+    const int hh = 1 << st, sh = logn - (s0 + st + 1);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      if ((m & (2 * hh - 1)) >= hh || m + hh >= (1 << ns)) continue;
+      const int off = k + (m & (hh - 1)) * h;
+      const double2 y = cmul(twid(tw, off << sh, inv), x[m + hh]);
+      x[m + hh] = make_double2(x[m].x - y.x, x[m].y - y.y);
+      x[m] = make_double2(x[m].x + y.x, x[m].y + y.y);
+    }
+  }
+}
+
+// Shared-memory passes over stages s_top down to s_bot (DIF) / s_bot up to
+// s_top (DIT), three stages per pass.
+__device__ void dif_range(double2 *a, int G, int n, int logn, const double2 *tw, bool inv, int s_top, int s_bot) {
+  const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
+  for (int s_hi = s_top; s_hi >= s_bot; s_hi -= 3) {
+    const int ns = min(3, s_hi - s_bot + 1), s_lo = s_hi - ns + 1;
+    const int R = 1 << ns, h = 1 << (s_lo - 1), per = n >> ns;
+    for (int g = t; g < G * per; g += nt) {
+      const int line = g / per, gg = g - line * per;
+      const int k = gg & (h - 1), blk = gg >> (s_lo - 1);
+      const int base = blk * R * h + k;
+      double2 *L = a + (size_t)line * ld;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) x[m] = L[pd(base + m * h)];
+      group_dif(x, ns, k, h, s_lo, logn, tw, inv);
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) L[pd(base + m * h)] = x[m];
+    }
+    __syncthreads();
+  }
+}
+__device__ void dit_range(double2 *a, int G, int n, int logn, const double2 *tw, bool inv, int s_bot, int s_top) {
+  const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
+  for (int s0 = s_bot - 1; s0 < s_top; s0 += 3) {
+    const int ns = min(3, s_top - s0), R = 1 << ns, h = 1 << s0, per = n >> ns;
+    for (int g = t; g < G * per; g += nt) {
+      const int line = g / per, gg = g - line * per;
+      const int k = gg & (h - 1), blk = gg >> s0;
+      const int base = blk * R * h + k;
+      double2 *L = a + (size_t)line * ld;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) x[m] = L[pd(base + m * h)];
+      group_dit(x, ns, k, h, s0, logn, tw, inv);
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        if (m < R) L[pd(base + m * h)] = x[m];
+    }
+    __syncthreads();
+  }
+}
+
+// --- power-of-two lengths >= 64: first and last radix-8 passes fused with
+// the global loads/stores, no permutation passes --------------------------------
+
+// rows j0, j1 -> half spectra (forward DIF; bit-reversed result read back
+// during the Hermitian split)
+__global__ void __launch_bounds__(kThreads) k_rows_r2c_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
+                                                         const double *__restrict__ f, double2 *__restrict__ spec) {
+  extern __shared__ double2 sm[];
+  const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
+  const bool has1 = j1 < Ny;
+  const int H = Nx / 2 + 1, per = Nx >> 3;
+  const double *r0 = f + (size_t)j0 * Nx, *r1 = f + (size_t)j1 * Nx;
+  for (int k = threadIdx.x; k < per; k += blockDim.x) {
+    double2 x[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) x[m] = make_double2(__ldg(r0 + k + m * per), has1 ? __ldg(r1 + k + m * per) : 0.0);
+    group_dif(x, 3, k, per, L - 2, L, tw, false);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
+  }
+  __syncthreads();
+  dif_range(sm, 1, Nx, L, tw, false, L - 3, 1);
+  for (int I = threadIdx.x; I < H; I += blockDim.x) {
+    const double2 z = sm[pd(brev(I, L))], m = sm[pd(brev((Nx - I) & (Nx - 1), L))];
+    spec[(size_t)j0 * H + I] = make_double2(0.5 * (z.x + m.x), 0.5 * (z.y - m.y));
+    if (has1) spec[(size_t)j1 * H + I] = make_double2(0.5 * (z.y + m.y), 0.5 * (m.x - z.x));
+  }
+}
+
+// G spectrum columns: forward DIF, -1/Ahat scaling fused with the last DIF and
+// first DIT passes, inverse DIT; max |fhat| reduction
+__global__ void __launch_bounds__(kThreads) k_cols_f(int Nx, int Ny, int L, int G, const double2 *__restrict__ tw,
+                                                     const double *__restrict__ ax, const double *__restrict__ ay,
+                                                     double dxdy, double2 *__restrict__ spec,
+                                                     unsigned long long *__restrict__ maxbits) {
+  extern __shared__ double2 sm[];
+  __shared__ double wmax[kThreads / 32];
+  const int H = Nx / 2 + 1, per = Ny >> 3, ld = padded(Ny);
+  const int c0 = blockIdx.x * G;
+  const int g_here = min(G, H - c0);
+  for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
+    const int k = gidx / g_here, line = gidx - k * g_here;
+    double2 x[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) x[m] = spec[(size_t)(k + m * per) * H + c0 + line];
+    group_dif(x, 3, k, per, L - 2, L, tw, false);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) sm[(size_t)line * ld + pd(k + m * per)] = x[m];
+  }
+  __syncthreads();
+  dif_range(sm, g_here, Ny, L, tw, false, L - 3, 4);
+  double lmax = 0.0;
+  for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
+    const int line = gidx / per, k = gidx - line * per;
+    double2 *Ls = sm + (size_t)line * ld;
+    const int I = c0 + line;
+    double2 x[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) x[m] = Ls[pd(8 * k + m)];
+    group_dif(x, 3, 0, 1, 1, L, tw, false);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int J = brev(8 * k + m, L);
+      const double2 F = x[m];
+      lmax = fmax(lmax, sqrt(F.x * F.x + F.y * F.y));
+      const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + I) + __ldg(ay + J));
+      const double r = -1.0 / lam;
+      x[m] = make_double2(F.x * r, F.y * r);
+    }
+    group_dit(x, 3, 0, 1, 0, L, tw, true);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) Ls[pd(8 * k + m)] = x[m];
+  }
+  __syncthreads();
+  dit_range(sm, g_here, Ny, L, tw, true, 4, L - 3);
+  const double sc = 1.0 / Ny;
+  for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
+    const int k = gidx / g_here, line = gidx - k * g_here;
+    double2 x[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) x[m] = sm[(size_t)line * ld + pd(k + m * per)];
+    group_dit(x, 3, k, per, L - 3, L, tw, true);
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+      spec[(size_t)(k + m * per) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
+  }
+  for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, off));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = wmax[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mm = fmax(mm, wmax[w]);
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(mm));
+  }
+}
+
+// half spectra of rows j0, j1 -> real rows (inverse DIF, bit-reversed result
+// read back in natural order)
+__global__ void __launch_bounds__(kThreads) k_rows_c2r_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
+                                                         const double2 *__restrict__ spec, double *__restrict__ out,
+                                                         int accumulate, const unsigned long long *__restrict__ maxbits) {
+  extern __shared__ double2 sm[];
+  const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
+  const bool has1 = j1 < Ny;
+  const int H = Nx / 2 + 1, per = Nx >> 3;
+  const double mx = __longlong_as_double((long long)*maxbits);
+  if (mx < 1e-14) {  // pressure_poisson.m:21-32: dp stays zero
+    if (!accumulate)
+      for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+        out[(size_t)j0 * Nx + k] = 0.0;
+        if (has1) out[(size_t)j1 * Nx + k] = 0.0;
+      }
+    return;
+  }
+  const double2 *s0 = spec + (size_t)j0 * H, *s1 = spec + (size_t)j1 * H;
+  for (int k = threadIdx.x; k < per; k += blockDim.x) {
+    double2 x[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int q = k + m * per;
+      double2 g0, g1;
+      if (q < H) {
+        g0 = s0[q];
+        g1 = has1 ? s1[q] : make_double2(0.0, 0.0);
+      } else {
+        const double2 a = s0[Nx - q];
+        const double2 b = has1 ? s1[Nx - q] : make_double2(0.0, 0.0);
+        g0 = make_double2(a.x, -a.y);
+        g1 = make_double2(b.x, -b.y);
+      }
+      x[m] = make_double2(g0.x - g1.y, g0.y + g1.x);
+    }
+    group_dif(x, 3, k, per, L - 2, L, tw, true);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
+  }
+  __syncthreads();
+  dif_range(sm, 1, Nx, L, tw, true, L - 3, 1);
+  const double sc = 1.0 / Nx;
+  for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
+    const double2 w = sm[pd(brev(k, L))];
+    if (accumulate) {
+      out[(size_t)j0 * Nx + k] += w.x * sc;
+      if (has1) out[(size_t)j1 * Nx + k] += w.y * sc;
+    } else {
+      out[(size_t)j0 * Nx + k] = w.x * sc;
+      if (has1) out[(size_t)j1 * Nx + k] = w.y * sc;
+    }
+  }
+}
+
 int ilog2_exact(int n) {
   int l = 0;
   while ((1 << l) < n) ++l;
@@ -299,6 +533,9 @@ bool fft_supported(int Nx, int Ny) {
 // Opt the transform kernels in to large dynamic shared memory on the current
 // device (called once per context).
 void fft_prepare() {
+  cudaFuncSetAttribute(k_rows_r2c_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_cols_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_rows_c2r_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -313,11 +550,23 @@ void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, d
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
   cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
-  k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, f, plan.spec);
-  k_cols<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
-                                                plan.spec, (unsigned long long *)plan.maxabs);
-  k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
-                                          (const unsigned long long *)plan.maxabs);
+  const bool fx = plan.logx >= 6, fy = plan.logy >= 6;  // fused-pass kernels
+  if (fx)
+    k_rows_r2c_f<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, f, plan.spec);
+  else
+    k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, f, plan.spec);
+  if (fy)
+    k_cols_f<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
+                                                    plan.spec, (unsigned long long *)plan.maxabs);
+  else
+    k_cols<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
+                                                  plan.spec, (unsigned long long *)plan.maxabs);
+  if (fx)
+    k_rows_c2r_f<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
+                                              (const unsigned long long *)plan.maxabs);
+  else
+    k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
+                                            (const unsigned long long *)plan.maxabs);
 }
 
 }  // namespace ins2d
