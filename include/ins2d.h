@@ -204,6 +204,28 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
 /* out[4] = {maxdiv, umom, vmom, k} (check_conservation.m:1-76) */
 int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4], int mem);
 
+/* --- allocation-free FFT solve ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (an application that gives the whole GPU to its own memory pool, a
+ * plugin inside a host that owns the allocator, a real-time loop where
+ * cudaMalloc must not run): dp = real(ifft2(-fft2(f)./Ahat)) on a periodic
+ * uniform Nx x Ny grid with spacings dx, dy -- the FFT branch of
+ * pressure_poisson.m:92-104 with its early return -- for device arrays f, dp
+ * on the current device and a cudaStream_t stream (NULL = default stream).
+ * Allocates nothing: the scratch lives in one static device array of
+ * about 8.5 MB that every GPU loading the library keeps until exit.
+ * Limits: 2 <= Nx, Ny <= INS2D_NOALLOC_MAX_N, Nx*Ny <= INS2D_NOALLOC_MAX_CELLS,
+ * and sizes the FFT path supports; other sizes return INS2D_EINVAL.
+ * The first call on a device looks up the array's device address and sets
+ * kernel attributes; make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  Returns
+ * after the stream has finished the call's work. */
+#define INS2D_NOALLOC_MAX_N 4096
+#define INS2D_NOALLOC_MAX_CELLS (1 << 20)
+int ins2d_fft_poisson_noalloc(const double *f, double *dp, int32_t Nx, int32_t Ny, double dx, double dy,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,7 +22,7 @@ EXPORTED = [
     "ins2d_set_stream", "ins2d_set_bc_values", "ins2d_set_bc_sampler", "ins2d_F",
     "ins2d_divergence", "ins2d_laplacian", "ins2d_pressure_poisson",
     "ins2d_pressure_additional_solve", "ins2d_erk_step", "ins2d_erk_run", "ins2d_conservation",
-    "ins2d_profile", "ins2d_profile_read",
+    "ins2d_profile", "ins2d_profile_read", "ins2d_fft_poisson_noalloc",
 ]
 PROF_FAMILIES = ["stage", "div", "poisson", "project", "residual", "other"]
 
@@ -108,6 +108,8 @@ def load():
         "ins2d_conservation": (ctypes.c_int, [vp, vp, ctypes.c_double, P(ctypes.c_double), ctypes.c_int]),
         "ins2d_profile": (ctypes.c_int, [vp, ctypes.c_int]),
         "ins2d_profile_read": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_int64)]),
+        "ins2d_fft_poisson_noalloc": (ctypes.c_int, [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                     ctypes.c_double, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
