@@ -92,7 +92,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.out,
+                                          "-i", str(self.gpu), "-lms", "50"], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -172,6 +172,7 @@ def run_ours(args, wl, rank, world, local_rank):
         dist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
+    time.sleep(0.3)  # let nvidia-smi start sampling before the timed region
     opts.profile(False)  # resets launch counters
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -344,8 +345,8 @@ def run_reference(args, wl, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="turb2048", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-budget", type=float, default=20.0)

@@ -25,25 +25,28 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
-    if not force and not _stale():
+def build(force=False, verbose=False, out=None, defines=(), objdir=None):
+    """Compiles the library (to `out`, default ins2d_b200/libins2d.so); extra
+    -D definitions select launch-shape tunables."""
+    target = out or LIB
+    if not force and out is None and not _stale():
         return LIB
-    objdir = os.path.join(HERE, "_build")
+    objdir = objdir or os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
-        cmd = [NVCC] + ARCH + common + ["-lineinfo", "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [NVCC] + ARCH + common + ["-D" + d for d in defines] + ["-lineinfo", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = target + ".tmp"
     subprocess.check_call([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":

@@ -216,7 +216,28 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
     CK(cudaGetLastError());
     return INS2D_OK;
   }
-  Prof pr(c, INS2D_PROF_POISSON, 2);
+  Prof pr(c, INS2D_PROF_POISSON, pcg_use_block(c->P) ? 1 : 2);
+  if (pcg_use_block(c->P)) {
+    pcg_solve_block(c->P, c->pcg, f, dp, c->opts.CG_acc, c->opts.CG_maxit, accumulate, c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const PcgScalars &h = *c->h_sc;
+    if (st) {
+      st->iters = (int32_t)h.it;
+      st->norm1 = std::sqrt(h.rr);
+      st->norm2 = (h.maxx - h.minx) != 0.0 ? h.maxres / (h.maxx - h.minx) : 0.0;
+    }
+    if (h.status == INS2D_ENOTCONV) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "CG didn't converge in %d iterations; residual= %g", c->opts.CG_maxit,
+               std::sqrt(h.rr));
+      return fail(c, INS2D_ENOTCONV, buf);
+    }
+    if (h.status == INS2D_EBREAKDOWN) return fail(c, INS2D_EBREAKDOWN, "PCG breakdown: p'Ap = 0");
+    if (h.status == INS2D_ENONFINITE) return fail(c, INS2D_ENONFINITE, "PCG: non-finite residual");
+    return INS2D_OK;
+  }
   pcg_init(c->P, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
   CK(cudaGetLastError());
   int chunk = 4;
@@ -441,6 +462,15 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     P.TXd = upload_vec(c, H.TXd); P.TYd = upload_vec(c, H.TYd);
     P.hx = upload_vec(c, H.hx); P.hy = upload_vec(c, H.hy);
     P.gxi = upload_vec(c, H.gxi); P.gyi = upload_vec(c, H.gyi);
+    {
+      auto rec = [](const std::vector<double> &v) {
+        std::vector<double> r(v.size());
+        for (size_t k = 0; k < v.size(); ++k) r[k] = 1.0 / v[k];
+        return r;
+      };
+      P.rhx = upload_vec(c, rec(H.hx)); P.rhy = upload_vec(c, rec(H.hy));
+      P.rgxi = upload_vec(c, rec(H.gxi)); P.rgyi = upload_vec(c, rec(H.gyi));
+    }
     P.pxl = upload_vec(c, H.pxl); P.pxr = upload_vec(c, H.pxr);
     P.pyl = upload_vec(c, H.pyl); P.pyu = upload_vec(c, H.pyu);
     auto reg = [&](const Regular &r, const Table &t) {

@@ -54,6 +54,7 @@ struct DevOps {
   Tab TX, TY;
   const double *TXd, *TYd;
   const double *hx, *hy, *gxi, *gyi;
+  const double *rhx, *rhy, *rgxi, *rgyi;  // reciprocals (Om^-1 = 1/(hy gxi) as (1/hy)(1/gxi))
   const double *pxl, *pxr, *pyl, *pyu;
   const double *fft_ax, *fft_ay;
   double fft_dxdy;
@@ -238,11 +239,13 @@ __device__ __forceinline__ double lap(const DevOps &P, const double *__restrict_
 __device__ __forceinline__ double lap_diag(const DevOps &P, int i, int j) {
   return -(__ldg(P.hy + j) * __ldg(P.TXd + i) + __ldg(P.hx + i) * __ldg(P.TYd + j));
 }
+// Om_inv (operator_mesh.m:335,342) as a product of 1D reciprocals (within
+// one rounding of 1/(hy*gxi))
 __device__ __forceinline__ double om_inv_u(const DevOps &P, int i, int j) {
-  return 1.0 / (__ldg(P.hy + j) * __ldg(P.gxi + i));
+  return __ldg(P.rhy + j) * __ldg(P.rgxi + i);
 }
 __device__ __forceinline__ double om_inv_v(const DevOps &P, int i, int j) {
-  return 1.0 / (__ldg(P.gyi + j) * __ldg(P.hx + i));
+  return __ldg(P.rgyi + j) * __ldg(P.rhx + i);
 }
 
 }  // namespace ins2d

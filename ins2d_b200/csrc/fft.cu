@@ -19,7 +19,16 @@ namespace ins2d {
 
 namespace {
 
-constexpr int kThreads = 256;
+#ifndef INS2D_FFT_THREADS
+#define INS2D_FFT_THREADS 256
+#endif
+#ifndef INS2D_FFT_COLS_MINB
+#define INS2D_FFT_COLS_MINB 1
+#endif
+#ifndef INS2D_FFT_COLS_G
+#define INS2D_FFT_COLS_G 2
+#endif
+constexpr int kThreads = INS2D_FFT_THREADS;
 constexpr int kMaxPow2 = 8192;
 constexpr int kMaxGeneric = 2048;
 
@@ -387,7 +396,7 @@ __global__ void __launch_bounds__(kThreads) k_rows_r2c_f(int Nx, int Ny, int L, 
 
 // G spectrum columns: forward DIF, -1/Ahat scaling fused with the last DIF and
 // first DIT passes, inverse DIT; max |fhat| reduction
-__global__ void __launch_bounds__(kThreads) k_cols_f(int Nx, int Ny, int L, int G, const double2 *__restrict__ tw,
+__global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx, int Ny, int L, int G, const double2 *__restrict__ tw,
                                                      const double *__restrict__ ax, const double *__restrict__ ay,
                                                      double dxdy, double2 *__restrict__ spec,
                                                      unsigned long long *__restrict__ maxbits) {
@@ -519,7 +528,7 @@ int cols_group(int Ny, bool pow2) {
   int G = (int)((72 * 1024) / per);
   if (G > 8) G = 8;
   if (G < 1) G = 1;
-  if (Ny >= 1024 && G > 2) G = 2;
+  if (Ny >= 1024 && G > INS2D_FFT_COLS_G) G = INS2D_FFT_COLS_G;
   return G;
 }
 

@@ -93,5 +93,11 @@ void pcg_init(const DevOps &P, const PcgWork &W, const double *f, double tol, lo
 void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s);
 void pcg_finish(const DevOps &P, const PcgWork &W, double *dp, bool accumulate, cudaStream_t s);
 int pcg_blocks(const DevOps &P);
+// Small grids: the whole solve in one thread block (dp written or accumulated
+// when converged; status/iterations in W.sc)
+constexpr long long kPcgBlockMaxCells = 16384;
+bool pcg_use_block(const DevOps &P);
+void pcg_solve_block(const DevOps &P, const PcgWork &W, const double *f, double *dp, double tol, long long maxit,
+                     bool accumulate, cudaStream_t s);
 
 }  // namespace ins2d

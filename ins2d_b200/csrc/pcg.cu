@@ -158,7 +158,146 @@ __global__ void k_copy_out(const double *__restrict__ x, double *__restrict__ dp
     dp[k] = accumulate ? dp[k] + x[k] : x[k];
 }
 
+
+// ---------------------------------------------------------------------------
+// Whole solve in one thread block (small grids): same algorithm and stopping
+// rule, block-level reductions in a fixed order, no host round trips.
+constexpr int kBlockThreads = 1024;
+
+template <int NQ>
+__device__ void block_reduce(double (&v)[NQ], const int (&ops)[NQ], double (*sh)[NQ]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+    for (int off = 16; off > 0; off >>= 1) v[q] = red_combine(v[q], __shfl_down_sync(0xffffffffu, v[q], off), ops[q]);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sh[warp][q] = v[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double a = sh[0][q];
+    for (int w = 1; w < nw; ++w) a = red_combine(a, sh[w][q], ops[q]);
+    v[q] = a;  // every thread gets the block result
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_constant__ DevOps P, const PcgWork W,
+                                                               const double *__restrict__ f, double *__restrict__ dp,
+                                                               double tol2, long long maxit, int accumulate) {
+  __shared__ double sh[kBlockThreads / 32][5];
+  const int Npx = P.Npx;
+  const long long Np = P.Np;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *__restrict__ x = W.x, *__restrict__ r = W.r, *__restrict__ p = W.p, *__restrict__ q = W.q;
+  // init (cg.F:207-229 with x_in = 0)
+  double a3[3] = {0.0, 0.0, 0.0};
+  const int op3[3] = {R_SUM, R_SUM, R_MAX};
+  for (long long k = tid; k < Np; k += nt) {
+    const int i = (int)(k % Npx), j = (int)(k / Npx);
+    const double fv = f[k];
+    const double z = fv / lap_diag(P, i, j);
+    x[k] = 0.0;
+    r[k] = fv;
+    p[k] = z;
+    a3[0] += fv * fv;
+    a3[1] += fv * z;
+    a3[2] = fmax(a3[2], fabs(fv));
+  }
+  block_reduce<3>(a3, op3, (double(*)[3])sh);
+  const double rr0 = a3[0];
+  double rz = a3[1];
+  double rr = 0.0, maxx = 0.0, minx = 0.0, maxres = 0.0;
+  long long it = 0;
+  int status = 0;
+  bool done = (a3[2] < 1e-14 || rr0 <= tol2);  // pressure_poisson.m:33-38, cg.F:222-227
+  if (!isfinite(rr0) || !isfinite(rz)) {
+    status = INS2D_ENONFINITE;
+    done = true;
+  }
+  const int op1[1] = {R_SUM};
+  const int op5[5] = {R_SUM, R_SUM, R_MAX, R_MIN, R_MAX};
+  while (!done) {
+    double a1[1] = {0.0};
+    for (long long k = tid; k < Np; k += nt) {
+      const int i = (int)(k % Npx), j = (int)(k / Npx);
+      const double aq = lap(P, p, i, j);
+      q[k] = aq;
+      a1[0] += p[k] * aq;
+    }
+    block_reduce<1>(a1, op1, (double(*)[1])sh);
+    const double pq = a1[0];
+    if (!isfinite(pq)) {
+      status = INS2D_ENONFINITE;
+      break;
+    }
+    if (pq == 0.0) {
+      status = INS2D_EBREAKDOWN;
+      break;
+    }
+    const double alpha = rz / pq;
+    double a5[5] = {0.0, 0.0, -DBL_MAX, DBL_MAX, 0.0};
+    for (long long k = tid; k < Np; k += nt) {
+      const int i = (int)(k % Npx), j = (int)(k / Npx);
+      const double xv = x[k] + alpha * p[k];
+      const double rv = r[k] - alpha * q[k];
+      x[k] = xv;
+      r[k] = rv;
+      a5[0] += rv * rv;
+      a5[1] += rv * (rv / lap_diag(P, i, j));
+      a5[2] = fmax(a5[2], xv);
+      a5[3] = fmin(a5[3], xv);
+      a5[4] = fmax(a5[4], fabs(rv));
+    }
+    block_reduce<5>(a5, op5, (double(*)[5])sh);
+    ++it;
+    rr = a5[0] / rr0;
+    maxx = a5[2];
+    minx = a5[3];
+    maxres = a5[4];
+    if (!isfinite(rr) || !isfinite(a5[1])) {
+      status = INS2D_ENONFINITE;
+      break;
+    }
+    if (rr <= tol2) break;
+    if (it >= maxit) {
+      status = INS2D_ENOTCONV;
+      break;
+    }
+    const double beta = a5[1] / rz;
+    rz = a5[1];
+    for (long long k = tid; k < Np; k += nt) {
+      const int i = (int)(k % Npx), j = (int)(k / Npx);
+      p[k] = r[k] / lap_diag(P, i, j) + beta * p[k];
+    }
+    __syncthreads();
+  }
+  if (status == 0)
+    for (long long k = tid; k < Np; k += nt) dp[k] = accumulate ? dp[k] + x[k] : x[k];
+  if (tid == 0) {
+    PcgScalars *s = W.sc;
+    s->rr0 = rr0;
+    s->rr = rr;
+    s->it = it;
+    s->maxx = maxx;
+    s->minx = minx;
+    s->maxres = maxres;
+    s->status = status;
+    s->done = 1;
+    s->tol2 = tol2;
+    s->maxit = maxit;
+  }
+}
+
 }  // namespace
+
+bool pcg_use_block(const DevOps &P) { return P.Np <= kPcgBlockMaxCells; }
+
+void pcg_solve_block(const DevOps &P, const PcgWork &W, const double *f, double *dp, double tol, long long maxit,
+                     bool accumulate, cudaStream_t s) {
+  k_pcg_block<<<1, kBlockThreads, 0, s>>>(P, W, f, dp, tol * tol, maxit, accumulate ? 1 : 0);
+}
 
 int pcg_blocks(const DevOps &P) {
   dim3 g = pgrid(P);

@@ -18,8 +18,15 @@ namespace ins2d {
 
 namespace {
 
-constexpr int WX = 64;  // columns per block (two warps per walker)
-constexpr int RUN = 32; // rows per column run
+// launch shape (compile-time tunables)
+#ifndef INS2D_WALK_RUN
+#define INS2D_WALK_RUN 16
+#endif
+#ifndef INS2D_WALK_MINB
+#define INS2D_WALK_MINB 5
+#endif
+constexpr int WX = 64;               // columns per block (two warps per walker)
+constexpr int RUN = INS2D_WALK_RUN;  // rows per column run
 
 template <typename S>
 struct XRow {  // one row of an x-table in registers
@@ -183,7 +190,7 @@ __device__ void walk_u(const DevOps &P, const double *__restrict__ u, const doub
     const double R = (double)(-(du2dx + duvdy) + d2u - ypx);
     const long long idx = (long long)j * P.Nux + i;
     const double hyd = __ldg(P.hy + j);
-    const double oi = 1.0 / (hyd * (double)__ldg(P.gxi + i));
+    const double oi = __ldg(P.rhy + j) * __ldg(P.rgxi + i);
     if (e.mode == 0) {
       epilogue_stage(e, idx, oi, R);
     } else {
@@ -265,7 +272,7 @@ __device__ void walk_v(const DevOps &P, const double *__restrict__ u, const doub
     const S ypy = hx * pLo * S(__ldg(P.pyl + j)) + hx * pUp * S(__ldg(P.pyu + j));
     const double R = (double)(-(duvdx + dv2dy) + d2v - ypy);
     const long long idx = P.Nu + (long long)j * P.Nvx + i;
-    const double oi = 1.0 / (__ldg(P.gyi + j) * __ldg(P.hx + i));
+    const double oi = __ldg(P.rgyi + j) * __ldg(P.rhx + i);
     if (e.mode == 0) {
       epilogue_stage(e, idx, oi, R);
     } else {
@@ -314,7 +321,7 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
   const S s10 = rw<S>(P.rSUX.w0, i + 1), s11 = rw<S>(P.rSUX.w1, i + 1);
   const S iv0 = rw<S>(P.rIVX.w0, i), iv1 = rw<S>(P.rIVX.w1, i);
   const S gx = S(__ldg(P.gxi + i));
-  const double gxd = __ldg(P.gxi + i);
+  const double rgx = __ldg(P.rgxi + i);
   const bool twoA = P.rAUX.two, twoAy = P.rAUY.two, twoIx = P.rIVX.two, twoIy = P.rIVY.two;
   const int sAy = P.rAUY.s, sIy = P.rIVY.s;
   const long long Nux = P.Nux, Nvx = P.Nvx;
@@ -371,7 +378,7 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
     const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
     const double R = (double)(-(du2dx + duvdy) + d2u);
     const long long idx = (long long)j * Nux + i;
-    const double oi = 1.0 / (hyd * gxd);
+    const double oi = __ldg(P.rhy + j) * rgx;
     if (e.mode == 0) {
       const double k = oi * R;
       if (e.kV) e.kV[idx] = k;
@@ -410,6 +417,7 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
   const S wu00 = rw<S>(P.rIUX.w0, i), wu01 = rw<S>(P.rIUX.w1, i);
   const S wu10 = rw<S>(P.rIUX.w0, i + 1), wu11 = rw<S>(P.rIUX.w1, i + 1);
   const double hxd = __ldg(P.hx + i);
+  const double rhx = __ldg(P.rhx + i);
   const S hx = S(hxd);
   const bool twoV = P.rAVX.two, twoVy = P.rAVY.two, twoUx = P.rIUX.two, twoUy = P.rIUY.two;
   const int sVy = P.rAVY.s, sUy = P.rIUY.s;
@@ -471,7 +479,7 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
     const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
     const double R = (double)(-(duvdx + dv2dy) + d2v);
     const long long idx = P.Nu + (long long)j * Nvx + i;
-    const double oi = 1.0 / (gyd * hxd);
+    const double oi = __ldg(P.rgyi + j) * rhx;
     if (e.mode == 0) {
       const double k = oi * R;
       if (e.kV) e.kV[idx] = k;
@@ -491,7 +499,7 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
 }
 
 template <typename S>
-__global__ void __launch_bounds__(WX * 2) k_walk_fast(const __grid_constant__ DevOps P, const double *__restrict__ V,
+__global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_fast(const __grid_constant__ DevOps P, const double *__restrict__ V,
                                                       const __grid_constant__ Epi e) {
   const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
   const int i = bx * WX + threadIdx.x;
