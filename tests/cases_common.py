@@ -73,3 +73,28 @@ def smooth_bc(seed, closed=False):
         return a[3] * np.cos(a[4] * X - 3 * Y + 0.5 * t) + 0.1 * a[5]
 
     return uBC, vBC
+
+
+def unsteady_bc(seed):
+    """The boundary functions of smooth_bc(seed) with their time derivatives
+    (for BC_unsteady = 1 cases): returns uBC, vBC, dudtBC, dvdtBC."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(0.5, 1.5, 6)
+    uBC, vBC = smooth_bc(seed)
+
+    def _xy(x, y):
+        x = np.atleast_1d(np.asarray(x, float))
+        y = np.atleast_1d(np.asarray(y, float))
+        X = np.tile(x, len(y)) if len(y) > 1 else x
+        Y = np.repeat(y, len(x)) if len(y) > 1 else np.full(len(x), y[0])
+        return X, Y
+
+    def dudtBC(x, y, t):
+        X, Y = _xy(x, y)
+        return a[0] * np.cos(2 * X + a[1] * Y + t)
+
+    def dvdtBC(x, y, t):
+        X, Y = _xy(x, y)
+        return -0.5 * a[3] * np.sin(a[4] * X - 3 * Y + 0.5 * t)
+
+    return uBC, vBC, dudtBC, dvdtBC
