@@ -65,6 +65,14 @@ extern "C" {
 #define INS2D_POISSON_CG 4
 #define INS2D_POISSON_FFT 6
 
+/* preconditioner of the device PCG (poisson 1-5).  The reference's cg.F uses
+ * a diagonal incomplete Cholesky factor (sequential sweeps, cg.F:317-390);
+ * the device offers a multigrid V-cycle (default) or the Jacobi diagonal.
+ * Either way CG iterates to the same relative residual CG_acc. */
+#define INS2D_PRECOND_DEFAULT 0 /* multigrid where the grid allows it, else Jacobi */
+#define INS2D_PRECOND_JACOBI 1
+#define INS2D_PRECOND_MG 2
+
 #define INS2D_PREC_FP64 0
 #define INS2D_PREC_FP32_STENCIL 1
 
@@ -102,6 +110,7 @@ typedef struct {
   double rk_c[INS2D_MAX_STAGES];
   int32_t precision;    /* INS2D_PREC_* */
   int32_t device;       /* CUDA device ordinal */
+  int32_t precond;      /* INS2D_PRECOND_* (0 = default) */
 } ins2d_opts;
 
 /* Boundary values sampled by the caller from the case's uBC/vBC handles at
@@ -225,6 +234,42 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
 #define INS2D_NOALLOC_MAX_CELLS (1 << 20)
 int ins2d_fft_poisson_noalloc(const double *f, double *dp, int32_t Nx, int32_t Ny, double dx, double dy,
                               void *stream);
+
+/* --- ensembles ------------------------------------------------------------
+ * No single counterpart in the reference: the reference runs one case per
+ * MATLAB process (main.m); ensembles of independent flows (different grids,
+ * boundary conditions and Re, e.g. snapshot generation for reduced-order
+ * models, process_iteration.m:79-87) are many such runs.  Here the members
+ * are advanced together: each phase of a time step is one launch over all
+ * members, and the Poisson solves are one persistent launch whose thread
+ * blocks take members from a queue.  Members are full contexts (their
+ * operators, boundary values, F, conservation, ... are reached through
+ * ins2d_ens_member); the ensemble owns each member's state V, p.
+ * Restrictions: steady boundary conditions, the PCG pressure solver
+ * (poisson 1-5), the same device, precision, CG_acc, CG_maxit and RK method
+ * for all members, at most 262144 pressure cells per member. */
+typedef struct ins2d_ens ins2d_ens;
+int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_desc *bcs,
+                     const ins2d_opts *opts, ins2d_ens **out);
+int ins2d_ens_destroy(ins2d_ens *e);
+const char *ins2d_ens_last_error(const ins2d_ens *e);
+int32_t ins2d_ens_size(const ins2d_ens *e);
+/* member context (owned by the ensemble; NULL when m is out of range) */
+ins2d_ctx *ins2d_ens_member(ins2d_ens *e, int32_t m);
+int ins2d_ens_set_stream(ins2d_ens *e, void *stream);
+/* member state V (NV values), p (Np values) in or out */
+int ins2d_ens_set_state(ins2d_ens *e, int32_t m, const double *V, const double *p, int mem);
+int ins2d_ens_get_state(ins2d_ens *e, int32_t m, double *V, double *p, int mem);
+/* device pointers of a member's state (valid for the ensemble's lifetime) */
+int ins2d_ens_state_ptr(ins2d_ens *e, int32_t m, double **V, double **p);
+/* nsteps of time_ERK for every member with the same t, dt; stats: n entries
+ * (per member, accumulated over the run) or NULL.  A member whose solve fails
+ * makes the call return that status, naming the member. */
+int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_step_stats *stats);
+/* launch shape of the member solves chosen by the tuner on the first run
+ * (threads per member, resident blocks) and the tuner's timings (ms of one
+ * solve phase with 512 and with 256 threads per member) */
+int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[2]);
 
 #ifdef __cplusplus
 }

@@ -6,7 +6,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libins2d.so")
+# INS2D_LIBRARY selects another build of the library (launch-shape variants)
+LIB_PATH = os.environ.get("INS2D_LIBRARY") or os.path.join(HERE, "libins2d.so")
 
 OK, EINVAL, ENOTCONV, EBREAKDOWN, ENONFINITE, ETIMEOUT, ECUDA, ENOMEM = range(8)
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOTCONV", 3: "EBREAKDOWN", 4: "ENONFINITE",
@@ -14,6 +15,7 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOTCONV", 3: "EBREAKDOWN", 4: "ENONFI
 BC_CODES = {"dir": 0, "pres": 1, "per": 2, "sym": 3}
 MEM_HOST, MEM_DEVICE = 0, 1
 PREC_FP64, PREC_FP32_STENCIL = 0, 1
+PRECOND_CODES = {"default": 0, "jacobi": 1, "mg": 2}
 MAX_STAGES = 8
 
 # every symbol include/ins2d.h declares
@@ -23,6 +25,9 @@ EXPORTED = [
     "ins2d_divergence", "ins2d_laplacian", "ins2d_pressure_poisson",
     "ins2d_pressure_additional_solve", "ins2d_erk_step", "ins2d_erk_run", "ins2d_conservation",
     "ins2d_profile", "ins2d_profile_read", "ins2d_fft_poisson_noalloc",
+    "ins2d_ens_create", "ins2d_ens_destroy", "ins2d_ens_last_error", "ins2d_ens_size", "ins2d_ens_member",
+    "ins2d_ens_set_stream", "ins2d_ens_set_state", "ins2d_ens_get_state", "ins2d_ens_state_ptr",
+    "ins2d_ens_erk_run", "ins2d_ens_solve_shape",
 ]
 PROF_FAMILIES = ["stage", "div", "poisson", "project", "residual", "other"]
 
@@ -42,7 +47,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("Re", ctypes.c_double), ("poisson", ctypes.c_int32), ("CG_acc", ctypes.c_double),
                 ("CG_maxit", ctypes.c_int32), ("p_add_solve", ctypes.c_int32), ("rk_stages", ctypes.c_int32),
                 ("rk_A", ctypes.c_double * (MAX_STAGES * MAX_STAGES)), ("rk_b", ctypes.c_double * MAX_STAGES),
-                ("rk_c", ctypes.c_double * MAX_STAGES), ("precision", ctypes.c_int32), ("device", ctypes.c_int32)]
+                ("rk_c", ctypes.c_double * MAX_STAGES), ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("precond", ctypes.c_int32)]
 
 
 BC_VALUE_FIELDS = ("uLo", "uUp", "uLo_i", "uUp_i", "uLe_i", "uRi_i", "vLe", "vRi", "vLo_i", "vUp_i",
@@ -79,7 +85,8 @@ def load():
         return _LIB
     from . import build as _build
     try:
-        _build.build()
+        if not os.environ.get("INS2D_LIBRARY"):
+            _build.build()
     except Exception as e:  # no nvcc: use an existing library if present
         if not os.path.exists(LIB_PATH):
             raise RuntimeError(f"libins2d.so is missing and could not be built: {e}") from e
@@ -110,6 +117,17 @@ def load():
         "ins2d_profile_read": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_int64)]),
         "ins2d_fft_poisson_noalloc": (ctypes.c_int, [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                                      ctypes.c_double, vp]),
+        "ins2d_ens_create": (ctypes.c_int, [ctypes.c_int32, P(GridDesc), P(BcDesc), P(Opts), P(vp)]),
+        "ins2d_ens_destroy": (ctypes.c_int, [vp]),
+        "ins2d_ens_last_error": (ctypes.c_char_p, [vp]),
+        "ins2d_ens_size": (ctypes.c_int32, [vp]),
+        "ins2d_ens_member": (vp, [vp, ctypes.c_int32]),
+        "ins2d_ens_set_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_ens_set_state": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int]),
+        "ins2d_ens_get_state": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int]),
+        "ins2d_ens_state_ptr": (ctypes.c_int, [vp, ctypes.c_int32, P(vp), P(vp)]),
+        "ins2d_ens_erk_run": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32, P(StepStats)]),
+        "ins2d_ens_solve_shape": (ctypes.c_int, [vp, P(ctypes.c_int32), P(ctypes.c_int32), P(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -103,14 +103,17 @@ class Options:
     'dir'/'pres'/'per'/'sym', boundary_conditions.m), the case's boundary
     functions ``uBC(x, y, t)`` / ``vBC`` (and ``dudtBC``/``dvdtBC`` for
     unsteady BCs), ``Re``, ``poisson`` (1-5: device PCG, 6: FFT), ``CG_acc``,
-    ``CG_maxit``, ``p_add_solve``, the RK method name, and ``precision``
-    ('fp64' or 'fp32': FP32 convection/diffusion stencils).
+    ``CG_maxit``, ``p_add_solve``, the RK method name, ``precision``
+    ('fp64' or 'fp32': FP32 convection/diffusion stencils) and ``precond``
+    (PCG preconditioner: 'default' = multigrid where the grid allows it,
+    'mg', or 'jacobi').
     """
 
     def __init__(self, x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_add_solve=1, RK="RK44",
                  uBC=None, vBC=None, dudtBC=None, dvdtBC=None, pLe=0.0, pRi=0.0, pLo=0.0, pUp=0.0,
-                 precision="fp64", device=0, BC_unsteady=None):
+                 precision="fp64", device=0, BC_unsteady=None, precond="default", _handle=None):
         self._lib = _lib.load()
+        self._owner = _handle is None
         self.x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
         self.y = np.ascontiguousarray(np.asarray(y, dtype=np.float64))
         self.BC = {"u": dict(BC["u"]), "v": dict(BC["v"])}
@@ -151,12 +154,18 @@ class Options:
             o.rk_c[i] = c[i]
         o.precision = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32_STENCIL}[precision]
         o.device = int(device)
-        rc = self._lib.ins2d_ctx_create(ctypes.byref(g), ctypes.byref(b), ctypes.byref(o), ctypes.byref(self._ctx))
-        if rc != 0:
-            msg = self._err()
-            self._lib.ins2d_ctx_destroy(self._ctx)
-            self._ctx = None
-            raise Ins2dError(rc, msg)
+        o.precond = _lib.PRECOND_CODES[precond]
+        self._desc = (g, b, o)  # kept for ensembles
+        if _handle is not None:
+            self._ctx = ctypes.c_void_p(_handle)
+        else:
+            rc = self._lib.ins2d_ctx_create(ctypes.byref(g), ctypes.byref(b), ctypes.byref(o),
+                                            ctypes.byref(self._ctx))
+            if rc != 0:
+                msg = self._err()
+                self._lib.ins2d_ctx_destroy(self._ctx)
+                self._ctx = None
+                raise Ins2dError(rc, msg)
         sz = _lib.Sizes()
         self._lib.ins2d_get_sizes(self._ctx, ctypes.byref(sz))
         for f, _ in _lib.Sizes._fields_:
@@ -170,7 +179,7 @@ class Options:
         self.xv = np.tile(self.xp, self.Nvy_in)
         self.yv = np.repeat(self.yin, self.Nvx_in)
         self._sampler = None
-        if self.BC_unsteady:
+        if self.BC_unsteady and _handle is None:
             def _cb(user, t, ctx):
                 try:
                     self.set_bc_vectors(t)
@@ -179,7 +188,8 @@ class Options:
                     return _lib.EINVAL
             self._sampler = _lib.SAMPLER_FN(_cb)
             self._lib.ins2d_set_bc_sampler(self._ctx, self._sampler, None)
-        self.set_bc_vectors(0.0)
+        if _handle is None:
+            self.set_bc_vectors(0.0)
 
     # -- plumbing ------------------------------------------------------------
     def _err(self):
@@ -192,7 +202,8 @@ class Options:
 
     def close(self):
         if getattr(self, "_ctx", None):
-            self._lib.ins2d_ctx_destroy(self._ctx)
+            if getattr(self, "_owner", True):
+                self._lib.ins2d_ctx_destroy(self._ctx)
             self._ctx = None
 
     def __del__(self):
@@ -362,6 +373,142 @@ class Options:
         gyi = {("dir", "dir"): gy[1:-1], ("dir", "pres"): gy[1:], ("pres", "dir"): gy[:-1], ("pres", "pres"): gy,
                ("per", "per"): np.r_[gy[0] + gy[-1], gy[1:-1]]}[(Lo, Up)]
         return 1.0 / np.r_[np.kron(hy, gxi), np.kron(gyi, hx)]
+
+
+class Ensemble:
+    """Independent flows advanced together (ins2d_ens_*): ``members`` is a
+    list of dicts of :class:`Options` keyword arguments (x, y, BC, Re, uBC,
+    vBC, CG_acc, ...); every phase of a time step is one launch over all
+    members and the Poisson solves one persistent launch.  ``member(m)`` is
+    the member's :class:`Options` (its F, conservation, boundary values);
+    the ensemble holds each member's state (set_state / get_state)."""
+
+    def __init__(self, members):
+        self._lib = _lib.load()
+        self.members = []
+        # describe every member with an Options-like set of descriptors (no
+        # context is created for the descriptors themselves)
+        descs = [_describe(**kw) for kw in members]
+        n = len(descs)
+        G = (_lib.GridDesc * n)(*[d[0] for d in descs])
+        B = (_lib.BcDesc * n)(*[d[1] for d in descs])
+        O = (_lib.Opts * n)(*[d[2] for d in descs])
+        self._keep = descs
+        self._e = ctypes.c_void_p()
+        rc = self._lib.ins2d_ens_create(n, G, B, O, ctypes.byref(self._e))
+        if rc != 0:
+            msg = self._lib.ins2d_ens_last_error(self._e)
+            self._lib.ins2d_ens_destroy(self._e)
+            self._e = None
+            raise Ins2dError(rc, msg.decode() if msg else "")
+        for m, kw in enumerate(members):
+            h = self._lib.ins2d_ens_member(self._e, m)
+            opts = Options(_handle=h, **kw)
+            opts.set_bc_vectors(0.0)
+            self.members.append(opts)
+
+    def __len__(self):
+        return len(self.members)
+
+    def member(self, m):
+        return self.members[m]
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self._lib.ins2d_ens_last_error(self._e)
+            raise Ins2dError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_e", None):
+            for o in self.members:
+                o._ctx = None
+            self._lib.ins2d_ens_destroy(self._e)
+            self._e = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        self._check(self._lib.ins2d_ens_set_stream(self._e, ctypes.c_void_p(stream)))
+
+    def set_state(self, m, V, p):
+        o = self.members[m]
+        Va, pa = _Arr(V, o.NV, "V"), _Arr(p, o.Np, "p")
+        self._check(self._lib.ins2d_ens_set_state(self._e, m, Va.ptr, pa.ptr, Options._mem(Va, pa)))
+
+    def get_state(self, m, V=None, p=None):
+        """The member's (V, p), into the given host arrays when passed."""
+        o = self.members[m]
+        V = np.empty(o.NV) if V is None else V
+        p = np.empty(o.Np) if p is None else p
+        Va, pa = _Arr(V, o.NV, "V"), _Arr(p, o.Np, "p")
+        if Va.obj is not V or pa.obj is not p:
+            raise ValueError("get_state: output arrays must be contiguous float64")
+        self._check(self._lib.ins2d_ens_get_state(self._e, m, Va.ptr, pa.ptr, Options._mem(Va, pa)))
+        return V, p
+
+    def state_tensors(self, m):
+        """The member's device state as (V, p) torch CUDA tensors (views)."""
+        import torch
+        Vp, pp = ctypes.c_void_p(), ctypes.c_void_p()
+        self._check(self._lib.ins2d_ens_state_ptr(self._e, m, ctypes.byref(Vp), ctypes.byref(pp)))
+        o = self.members[m]
+        return _cuda_view(Vp.value, o.NV), _cuda_view(pp.value, o.Np)
+
+    def time_ERK(self, t, dt, nsteps=1):
+        """nsteps of time_ERK for every member; returns per-member stats."""
+        n = len(self.members)
+        st = (_lib.StepStats * n)()
+        self._check(self._lib.ins2d_ens_erk_run(self._e, float(t), float(dt), int(nsteps), st))
+        return [dict(n_solves=s.n_solves, iters_total=s.iters_total, iters_max=s.iters_max, norm1_max=s.norm1_max)
+                for s in st]
+
+    def solve_shape(self):
+        th, bl = ctypes.c_int32(), ctypes.c_int32()
+        ms = (ctypes.c_double * 2)()
+        self._check(self._lib.ins2d_ens_solve_shape(self._e, ctypes.byref(th), ctypes.byref(bl), ms))
+        return dict(threads=th.value, blocks=bl.value, tuned_ms={512: ms[0], 256: ms[1]})
+
+
+def _describe(x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_add_solve=1, RK="RK44",
+              precision="fp64", device=0, precond="default", **_ignored):
+    """C descriptors (grid, BC, options) of one case, as Options builds them."""
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+    y = np.ascontiguousarray(np.asarray(y, dtype=np.float64))
+    g = _lib.GridDesc(len(x) - 1, len(y) - 1, x.ctypes.data_as(_lib.c_double_p), y.ctypes.data_as(_lib.c_double_p))
+    codes = [_lib.BC_CODES[BC[c][sd]] for c in ("u", "v") for sd in ("left", "right", "low", "up")]
+    b = _lib.BcDesc(*codes, int(BC.get("BC_unsteady", 0)))
+    o = _lib.Opts()
+    o.Re = float(Re)
+    o.poisson = int(poisson)
+    o.CG_acc = float(CG_acc)
+    o.CG_maxit = int(CG_maxit)
+    o.p_add_solve = int(p_add_solve)
+    A, bb, c = getRKmethod(RK)
+    s = len(bb)
+    o.rk_stages = s
+    for i in range(s):
+        for j in range(s):
+            o.rk_A[i * s + j] = A[i, j]
+        o.rk_b[i] = bb[i]
+        o.rk_c[i] = c[i]
+    o.precision = {"fp64": _lib.PREC_FP64, "fp32": _lib.PREC_FP32_STENCIL}[precision]
+    o.device = int(device)
+    o.precond = _lib.PRECOND_CODES[precond]
+    return g, b, o, x, y
+
+
+def _cuda_view(ptr, n):
+    """A float64 CUDA tensor viewing n values at a device pointer."""
+    import torch
+
+    class _Iface:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2}
+
+    return torch.as_tensor(_Iface(), device="cuda")
 
 
 # -- module-level functions with the reference's names ------------------------------

@@ -70,7 +70,9 @@ def tanh_grid(N, a, b, stretch):
     def ratio(d):
         z = np.tanh(d * s) / np.tanh(d)
         h = np.diff(z)
-        return np.max(np.maximum(h[1:] / h[:-1], h[:-1] / h[1:]))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r = np.maximum(h[1:] / h[:-1], h[:-1] / h[1:])
+        return np.inf if not np.all(np.isfinite(r)) else np.max(r)
 
     lo, hi = 1e-6, 20.0
     if ratio(hi) < stretch:

@@ -18,6 +18,7 @@
 #include "ins2d.h"
 #include "kernels.cuh"
 #include "setup.hpp"
+#include "mg_host.hpp"
 
 namespace ins2d {
 void fft_prepare();
@@ -51,6 +52,8 @@ struct ins2d_ctx {
   RedScratch red;
   FftPlan fft;
   PcgWork pcg{};
+  bool use_mg = false;
+  MgD mg{};
   PcgScalars *h_sc = nullptr;   // pinned
   double *h_red = nullptr;      // pinned
   // host copies of boundary samples (check_conservation.m boundary terms)
@@ -216,9 +219,13 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
     CK(cudaGetLastError());
     return INS2D_OK;
   }
-  Prof pr(c, INS2D_PROF_POISSON, pcg_use_block(c->P) ? 1 : 2);
-  if (pcg_use_block(c->P)) {
-    pcg_solve_block(c->P, c->pcg, f, dp, c->opts.CG_acc, c->opts.CG_maxit, accumulate, c->stream);
+  const bool block = c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P);
+  Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
+  if (block) {
+    if (c->use_mg)
+      pcg_solve_block_mg(c->P, c->mg, c->pcg, f, dp, c->opts.CG_acc, c->opts.CG_maxit, accumulate, c->stream);
+    else
+      pcg_solve_block(c->P, c->pcg, f, dp, c->opts.CG_acc, c->opts.CG_maxit, accumulate, c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -238,9 +245,12 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
     if (h.status == INS2D_ENONFINITE) return fail(c, INS2D_ENONFINITE, "PCG: non-finite residual");
     return INS2D_OK;
   }
-  pcg_init(c->P, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
+  if (c->use_mg)
+    pcg_init_mg(c->P, c->mg, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
+  else
+    pcg_init(c->P, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
   CK(cudaGetLastError());
-  int chunk = 4;
+  int chunk = c->use_mg ? 2 : 4;
   long long launched = 0;
   for (;;) {
     CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
@@ -248,11 +258,16 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
     if (c->h_sc->done) break;
     if (launched > (long long)c->opts.CG_maxit + 1024)
       return fail(c, INS2D_ETIMEOUT, "PCG: device convergence flag never set");
-    pcg_iterations(c->P, c->pcg, chunk, c->stream);
+    if (c->use_mg) {
+      pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->stream);
+      c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
+    } else {
+      pcg_iterations(c->P, c->pcg, chunk, c->stream);
+      c->launches[INS2D_PROF_POISSON] += 3LL * chunk;
+    }
     CK(cudaGetLastError());
-    c->launches[INS2D_PROF_POISSON] += 3LL * chunk;
     launched += chunk;
-    chunk = std::min(chunk * 2, 128);
+    chunk = c->use_mg ? 4 : std::min(chunk * 2, 128);
   }
   const PcgScalars &h = *c->h_sc;
   if (st) {
@@ -432,6 +447,8 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     if (opts->poisson < 1 || opts->poisson > 6) throw std::invalid_argument("wrong poisson method");
     if (opts->poisson != INS2D_POISSON_FFT && !(opts->CG_acc > 0)) throw std::invalid_argument("CG_acc must be positive");
     if (opts->poisson != INS2D_POISSON_FFT && opts->CG_maxit < 1) throw std::invalid_argument("CG_maxit must be >= 1");
+    if (opts->precond < INS2D_PRECOND_DEFAULT || opts->precond > INS2D_PRECOND_MG)
+      throw std::invalid_argument("wrong preconditioner");
     if (opts->rk_stages < 0 || opts->rk_stages > kMaxStages) throw std::invalid_argument("rk_stages out of range");
     for (int i = 0; i < opts->rk_stages; ++i)
       for (int j = i; j < opts->rk_stages; ++j)
@@ -567,6 +584,18 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
       W.blocks = pcg_blocks(P);
       W.partials = dalloc<double>(c, (size_t)W.blocks * 8 + 16);
       CK(cudaMemset(W.sc, 0, sizeof(PcgScalars)));
+      if (opts->precond != INS2D_PRECOND_JACOBI) {
+        std::vector<MgHostLevel> lv;
+        try {
+          lv = mg_build_levels(H);
+        } catch (const std::runtime_error &e) {
+          if (opts->precond == INS2D_PRECOND_MG) throw std::invalid_argument(e.what());
+        }
+        if (!lv.empty()) {
+          mg_setup_device(lv, c->mg, [c](size_t n) { return dalloc<double>(c, n); }, nullptr);
+          c->use_mg = true;
+        }
+      }
     }
     CK(cudaMallocHost((void **)&c->h_sc, sizeof(PcgScalars)));
     CK(cudaMallocHost((void **)&c->h_red, sizeof(double) * kRedQ));
@@ -871,6 +900,432 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
   out[3] = k;
   return INS2D_OK;
   API_END
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Ensembles: many independent flows (different grids, boundary conditions,
+// Re) advanced together.  Each member is a full context (its operator
+// tables, multigrid hierarchy, work arrays); the ensemble adds the members'
+// state (V, p), a device table of member descriptors and the tile work lists,
+// so every phase of a time step is ONE launch over all members: the stage
+// and residual walkers over the members' tiles, the divergence and
+// projection over their cells, and the Poisson solves as a persistent launch
+// whose thread blocks take members from a queue (largest first) and run each
+// member's whole PCG.  A step is captured once as a CUDA graph and replayed.
+// The solve launch shape (threads per member) is chosen by timing the
+// candidates on the first run.
+struct ins2d_ens {
+  int device = 0;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  std::vector<ins2d_ctx *> mem;
+  std::vector<double *> V, p;  // member state (owned by the member contexts' allocations)
+  std::string err;
+  bool fp32 = false;
+  double tol2 = 0.0;
+  long long maxit = 0;
+  // device tables
+  EnsMemberD *d_mem = nullptr;
+  std::vector<MgD *> d_mg;
+  int4 *d_fast = nullptr, *d_gen = nullptr, *d_cells = nullptr;
+  int n_fast = 0, n_gen = 0, n_cells = 0;
+  int *d_order = nullptr;
+  unsigned *d_queue = nullptr;
+  EnsStats *d_stats = nullptr;
+  std::vector<void *> allocs;
+  bool uploaded = false;
+  // launch shape of the member solves (autotuned) and the step graphs
+  int solve_threads = 0, solve_blocks = 0;
+  double tuned_ms[2] = {0.0, 0.0};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt[2] = {0.0, 0.0};
+};
+
+namespace {
+
+int ens_fail(ins2d_ens *e, int code, const std::string &msg) {
+  if (e) e->err = msg;
+  return code;
+}
+
+template <typename T>
+T *ens_alloc(ins2d_ens *e, size_t n) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
+  e->allocs.push_back(p);
+  return (T *)p;
+}
+
+void ens_release_graphs(ins2d_ens *e) {
+  for (auto &g : e->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// descriptor table, work lists and member order (largest first)
+void ens_upload(ins2d_ens *e) {
+  const int n = (int)e->mem.size();
+  std::vector<EnsMemberD> h(n);
+  std::vector<int4> fast, gen, cells;
+  for (int m = 0; m < n; ++m) {
+    ins2d_ctx *c = e->mem[m];
+    EnsMemberD &d = h[m];
+    d = EnsMemberD{};
+    d.P = c->P;
+    d.V = e->V[m];
+    d.p = e->p[m];
+    d.Vs = c->Vs;
+    d.Wt = c->Wt;
+    for (int k = 0; k < kMaxStages; ++k) d.kV[k] = c->kV[k];
+    d.f = c->f;
+    d.dp = c->dp;
+    d.wres = c->wres;
+    d.W = c->pcg;
+    d.mg = c->use_mg ? e->d_mg[m] : nullptr;
+    walk_tiles(c->P, m, fast, gen);
+    cell_tiles(c->P, m, cells);
+  }
+  std::vector<int> order(n);
+  for (int m = 0; m < n; ++m) order[m] = m;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e->mem[a]->P.Np > e->mem[b]->P.Np; });
+  if (!e->d_mem) {
+    e->d_mem = ens_alloc<EnsMemberD>(e, n);
+    e->d_order = ens_alloc<int>(e, n);
+    e->d_queue = ens_alloc<unsigned>(e, 2);
+    e->d_stats = ens_alloc<EnsStats>(e, n);
+    e->d_fast = ens_alloc<int4>(e, fast.size());
+    e->d_gen = ens_alloc<int4>(e, gen.size());
+    e->d_cells = ens_alloc<int4>(e, cells.size());
+    CK(cudaMemset(e->d_queue, 0, 2 * sizeof(unsigned)));
+  }
+  CK(cudaMemcpy(e->d_mem, h.data(), n * sizeof(EnsMemberD), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->d_order, order.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  if (!fast.empty()) CK(cudaMemcpy(e->d_fast, fast.data(), fast.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  if (!gen.empty()) CK(cudaMemcpy(e->d_gen, gen.data(), gen.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(e->d_cells, cells.data(), cells.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  e->n_fast = (int)fast.size();
+  e->n_gen = (int)gen.size();
+  e->n_cells = (int)cells.size();
+  e->uploaded = true;
+}
+
+int sm_count(int device) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+  return v > 0 ? v : 1;
+}
+
+void ens_solve(ins2d_ens *e, int which) {
+  launch_pcg_members(e->d_mem, e->d_order, (int)e->mem.size(), which, e->tol2, e->maxit, e->d_queue, e->d_stats,
+                     e->solve_threads, e->solve_blocks, e->stream);
+}
+
+// one time step of every member (time_ERK.m with steady boundary conditions)
+void ens_step(ins2d_ens *e, double dt, bool k0_cached) {
+  const ins2d_ctx *c0 = e->mem[0];
+  const int s = c0->s;
+  for (int i = 0; i < s; ++i) {
+    if (i == 0 && k0_cached) {
+      launch_stage_cached_ens(e->d_mem, e->d_cells, e->n_cells, c0->A[0][0], 1.0 / dt, e->stream);
+    } else {
+      EnsWalk w{};
+      w.mode = 0;
+      w.stage = i;
+      w.store = (c0->need_store[i] || i == 0) ? 1 : 0;
+      w.use_vs = i > 0;
+      for (int m = 0; m < i; ++m)
+        if (c0->A[i][m] != 0.0) {
+          w.kidx[w.nprev] = m;
+          w.aprev[w.nprev] = c0->A[i][m];
+          ++w.nprev;
+        }
+      w.aii = c0->A[i][i];
+      w.inv_dt = 1.0 / dt;
+      launch_walk_ens(e->d_mem, e->d_fast, e->n_fast, e->d_gen, e->n_gen, w, e->fp32, e->stream);
+    }
+    if (i > 0) {
+      launch_div_ens(e->d_mem, e->d_cells, e->n_cells, 0, 1.0 / dt, 1.0 / c0->c[i], e->stream);
+      ens_solve(e, 0);
+    }
+    launch_project_ens(e->d_mem, e->d_cells, e->n_cells, dt, c0->c[i], i == 0 ? 1 : 0, i == s - 1 ? 1 : 0,
+                       e->stream);
+  }
+  // additional pressure solve; its residual is the next step's first stage
+  EnsWalk w{};
+  w.mode = 1;
+  w.cache = 1;
+  launch_walk_ens(e->d_mem, e->d_fast, e->n_fast, e->d_gen, e->n_gen, w, e->fp32, e->stream);
+  launch_div_ens(e->d_mem, e->d_cells, e->n_cells, 1, 0.0, 1.0, e->stream);
+  ens_solve(e, 1);
+}
+
+// Times the member solve with each candidate launch shape on the current
+// right-hand sides (the solves are repeatable: x0 = 0, deterministic
+// reductions) and keeps the fastest.
+void ens_autotune(ins2d_ens *e) {
+  const int sms = sm_count(e->device), n = (int)e->mem.size();
+  const int cand[2] = {512, 256};
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  int best = -1;
+  float best_ms = 0.f;
+  for (int k = 0; k < 2; ++k) {
+    e->solve_threads = cand[k];
+    e->solve_blocks = std::min(n, sms * (512 / cand[k]));
+    ens_solve(e, 0);  // warm-up
+    CK(cudaEventRecord(a, e->stream));
+    ens_solve(e, 0);
+    CK(cudaEventRecord(b, e->stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    e->tuned_ms[k] = ms;
+    if (best < 0 || ms < best_ms) {
+      best = k;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  e->solve_threads = cand[best];
+  e->solve_blocks = std::min(n, sms * (512 / cand[best]));
+}
+
+#define ENS_BEGIN                 \
+  if (!e) return INS2D_EINVAL;    \
+  e->err.clear();                 \
+  try {                           \
+    CK(cudaSetDevice(e->device));
+#define ENS_END                                                     \
+  }                                                                 \
+  catch (const CudaError &x) {                                      \
+    return ens_fail(e, INS2D_ECUDA, x.what());                      \
+  }                                                                 \
+  catch (const std::bad_alloc &) {                                  \
+    return ens_fail(e, INS2D_ENOMEM, "device allocation failed");   \
+  }                                                                 \
+  catch (const std::exception &x) {                                 \
+    return ens_fail(e, INS2D_EINVAL, x.what());                     \
+  }
+
+}  // namespace
+
+extern "C" {
+
+int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_desc *bcs, const ins2d_opts *opts,
+                     ins2d_ens **out) {
+  if (!out || n < 1 || !grids || !bcs || !opts) return INS2D_EINVAL;
+  *out = nullptr;
+  ins2d_ens *e = new (std::nothrow) ins2d_ens();
+  if (!e) return INS2D_ENOMEM;
+  int rc = INS2D_OK;
+  std::string msg;
+  for (int m = 0; m < n && rc == INS2D_OK; ++m) {
+    const ins2d_opts &o = opts[m];
+    if (bcs[m].bc_unsteady) {
+      rc = INS2D_EINVAL;
+      msg = "ensemble members need steady boundary conditions";
+    } else if (o.poisson == INS2D_POISSON_FFT) {
+      rc = INS2D_EINVAL;
+      msg = "ensemble members use the PCG pressure solver (poisson 1-5)";
+    } else if (o.device != opts[0].device || o.precision != opts[0].precision || o.CG_acc != opts[0].CG_acc ||
+               o.CG_maxit != opts[0].CG_maxit || o.rk_stages != opts[0].rk_stages ||
+               std::memcmp(o.rk_A, opts[0].rk_A, sizeof(o.rk_A)) != 0 ||
+               std::memcmp(o.rk_c, opts[0].rk_c, sizeof(o.rk_c)) != 0 ||
+               std::memcmp(o.rk_b, opts[0].rk_b, sizeof(o.rk_b)) != 0) {
+      rc = INS2D_EINVAL;
+      msg = "ensemble members must share device, precision, CG_acc, CG_maxit and the RK method";
+    }
+    if (rc) break;
+    ins2d_ctx *c = nullptr;
+    rc = ins2d_ctx_create(&grids[m], &bcs[m], &o, &c);
+    if (rc) {
+      msg = std::string("member ") + std::to_string(m) + ": " + (c ? c->err : std::string("create failed"));
+      if (c) ins2d_ctx_destroy(c);
+      break;
+    }
+    e->mem.push_back(c);
+    if ((long long)c->P.Np > 262144) {
+      rc = INS2D_EINVAL;
+      msg = "ensemble members are limited to 262144 pressure cells";
+    }
+  }
+  if (rc == INS2D_OK) {
+    try {
+      e->device = opts[0].device;
+      CK(cudaSetDevice(e->device));
+      e->fp32 = e->mem[0]->fp32;
+      e->tol2 = opts[0].CG_acc * opts[0].CG_acc;
+      e->maxit = opts[0].CG_maxit;
+      for (ins2d_ctx *c : e->mem) {
+        e->V.push_back(dalloc<double>(c, (size_t)(c->P.Nu + c->P.Nv)));
+        e->p.push_back(dalloc<double>(c, (size_t)c->P.Np));
+        CK(cudaMemset(e->V.back(), 0, (size_t)(c->P.Nu + c->P.Nv) * sizeof(double)));
+        CK(cudaMemset(e->p.back(), 0, (size_t)c->P.Np * sizeof(double)));
+        MgD *dm = nullptr;
+        if (c->use_mg) {
+          dm = ens_alloc<MgD>(e, 1);
+          CK(cudaMemcpy(dm, &c->mg, sizeof(MgD), cudaMemcpyHostToDevice));
+        }
+        e->d_mg.push_back(dm);
+      }
+      CK(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking));
+      e->stream = e->own_stream;
+      CK(cudaDeviceSynchronize());
+    } catch (const CudaError &x) {
+      rc = INS2D_ECUDA;
+      msg = x.what();
+    } catch (const std::bad_alloc &) {
+      rc = INS2D_ENOMEM;
+      msg = "device allocation failed";
+    }
+  }
+  if (rc != INS2D_OK) {
+    e->err = msg;
+    *out = e;  // the caller reads the message, then destroys
+    return rc;
+  }
+  *out = e;
+  return INS2D_OK;
+}
+
+int ins2d_ens_destroy(ins2d_ens *e) {
+  if (!e) return INS2D_OK;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  ens_release_graphs(e);
+  for (void *p : e->allocs) cudaFree(p);
+  for (ins2d_ctx *c : e->mem) ins2d_ctx_destroy(c);
+  if (e->own_stream) cudaStreamDestroy(e->own_stream);
+  delete e;
+  return INS2D_OK;
+}
+
+const char *ins2d_ens_last_error(const ins2d_ens *e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int32_t ins2d_ens_size(const ins2d_ens *e) { return e ? (int32_t)e->mem.size() : 0; }
+
+ins2d_ctx *ins2d_ens_member(ins2d_ens *e, int32_t m) {
+  if (!e || m < 0 || m >= (int32_t)e->mem.size()) return nullptr;
+  return e->mem[m];
+}
+
+int ins2d_ens_set_stream(ins2d_ens *e, void *stream) {
+  if (!e) return INS2D_EINVAL;
+  e->stream = stream ? (cudaStream_t)stream : e->own_stream;
+  ens_release_graphs(e);
+  return INS2D_OK;
+}
+
+int ins2d_ens_set_state(ins2d_ens *e, int32_t m, const double *V, const double *p, int mem) {
+  ENS_BEGIN
+  if (m < 0 || m >= (int32_t)e->mem.size() || !V || !p) return ens_fail(e, INS2D_EINVAL, "set_state: bad argument");
+  if (mem != INS2D_MEM_HOST && mem != INS2D_MEM_DEVICE) return ens_fail(e, INS2D_EINVAL, "bad mem");
+  const ins2d_ctx *c = e->mem[m];
+  const cudaMemcpyKind k = mem == INS2D_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(e->V[m], V, (size_t)(c->P.Nu + c->P.Nv) * sizeof(double), k, e->stream));
+  CK(cudaMemcpyAsync(e->p[m], p, (size_t)c->P.Np * sizeof(double), k, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return INS2D_OK;
+  ENS_END
+}
+
+int ins2d_ens_get_state(ins2d_ens *e, int32_t m, double *V, double *p, int mem) {
+  ENS_BEGIN
+  if (m < 0 || m >= (int32_t)e->mem.size() || !V || !p) return ens_fail(e, INS2D_EINVAL, "get_state: bad argument");
+  if (mem != INS2D_MEM_HOST && mem != INS2D_MEM_DEVICE) return ens_fail(e, INS2D_EINVAL, "bad mem");
+  const ins2d_ctx *c = e->mem[m];
+  const cudaMemcpyKind k = mem == INS2D_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(V, e->V[m], (size_t)(c->P.Nu + c->P.Nv) * sizeof(double), k, e->stream));
+  CK(cudaMemcpyAsync(p, e->p[m], (size_t)c->P.Np * sizeof(double), k, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return INS2D_OK;
+  ENS_END
+}
+
+int ins2d_ens_state_ptr(ins2d_ens *e, int32_t m, double **V, double **p) {
+  if (!e || m < 0 || m >= (int32_t)e->mem.size() || !V || !p) return INS2D_EINVAL;
+  *V = e->V[m];
+  *p = e->p[m];
+  return INS2D_OK;
+}
+
+int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_step_stats *stats) {
+  ENS_BEGIN
+  (void)t;  // steady boundary conditions: the step does not depend on t
+  if (nsteps < 0 || !(dt > 0)) return ens_fail(e, INS2D_EINVAL, "erk_run: bad argument");
+  const int n = (int)e->mem.size();
+  if (!e->uploaded) ens_upload(e);
+  CK(cudaMemsetAsync(e->d_stats, 0, n * sizeof(EnsStats), e->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    const int g = k > 0 ? 1 : 0;  // graph 1: first stage from the cached residual
+    if (e->solve_threads == 0) {
+      // first use: one direct step, then tune the solve launch on the
+      // right-hand side it left behind (re-solving it changes no state: the
+      // tuner writes dp, which every stage overwrites); the step's
+      // statistics are kept
+      e->solve_threads = 512;
+      e->solve_blocks = std::min(n, sm_count(e->device));
+      ens_step(e, dt, g == 1);
+      std::vector<EnsStats> keep(n);
+      CK(cudaMemcpyAsync(keep.data(), e->d_stats, n * sizeof(EnsStats), cudaMemcpyDeviceToHost, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      ens_autotune(e);
+      CK(cudaMemcpyAsync(e->d_stats, keep.data(), n * sizeof(EnsStats), cudaMemcpyHostToDevice, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      continue;
+    }
+    if (!e->graph[g] || e->graph_dt[g] != dt) {
+      if (e->graph[g]) {
+        cudaGraphExecDestroy(e->graph[g]);
+        e->graph[g] = nullptr;
+      }
+      cudaGraph_t gr;
+      CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+      ens_step(e, dt, g == 1);
+      CK(cudaStreamEndCapture(e->stream, &gr));
+      cudaError_t ie = cudaGraphInstantiate(&e->graph[g], gr, 0);
+      cudaGraphDestroy(gr);
+      CK(ie);
+      e->graph_dt[g] = dt;
+    }
+    CK(cudaGraphLaunch(e->graph[g], e->stream));
+  }
+  std::vector<EnsStats> hs(n);
+  CK(cudaMemcpyAsync(hs.data(), e->d_stats, n * sizeof(EnsStats), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  int first_bad = -1;
+  for (int m = 0; m < n; ++m) {
+    if (stats) {
+      stats[m].n_solves = (int32_t)hs[m].n_solves;
+      stats[m].iters_total = (int32_t)hs[m].iters_total;
+      stats[m].iters_max = (int32_t)hs[m].iters_max;
+      stats[m].norm1_max = hs[m].norm1_max;
+    }
+    if (hs[m].status != 0 && first_bad < 0) first_bad = m;
+  }
+  if (first_bad >= 0) {
+    const int st = hs[first_bad].status;
+    return ens_fail(e, st, std::string("member ") + std::to_string(first_bad) +
+                               (st == INS2D_ENOTCONV ? ": CG didn't converge" : ": solve failed"));
+  }
+  return INS2D_OK;
+  ENS_END
+}
+
+int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[2]) {
+  if (!e) return INS2D_EINVAL;
+  if (threads) *threads = e->solve_threads;
+  if (blocks) *blocks = e->solve_blocks;
+  if (tuned_ms) {
+    tuned_ms[0] = e->tuned_ms[0];
+    tuned_ms[1] = e->tuned_ms[1];
+  }
+  return INS2D_OK;
 }
 
 }  // extern "C"

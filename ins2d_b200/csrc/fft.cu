@@ -25,6 +25,9 @@ namespace {
 #ifndef INS2D_FFT_COLS_MINB
 #define INS2D_FFT_COLS_MINB 1
 #endif
+#ifndef INS2D_FFT_COLS_BUDGET
+#define INS2D_FFT_COLS_BUDGET 72  // KB of shared memory per column block
+#endif
 #ifndef INS2D_FFT_COLS_G
 #define INS2D_FFT_COLS_G 2
 #endif
@@ -525,7 +528,7 @@ int ilog2_exact(int n) {
 int cols_group(int Ny, bool pow2) {
   // two columns (32-byte row segments) per block; more for short columns
   const size_t per = (size_t)padded(Ny) * sizeof(double2) * (pow2 ? 1 : 2);
-  int G = (int)((72 * 1024) / per);
+  int G = (int)((INS2D_FFT_COLS_BUDGET * 1024) / per);
   if (G > 8) G = 8;
   if (G < 1) G = 1;
   if (Ny >= 1024 && G > INS2D_FFT_COLS_G) G = INS2D_FFT_COLS_G;

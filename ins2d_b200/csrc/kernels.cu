@@ -6,6 +6,7 @@
 // neighbours are served from L1/L2; each field is read from DRAM once per
 // kernel.  Reductions are deterministic: per-block partials reduced in block
 // order by the last block to finish.
+#include <algorithm>
 #include <cfloat>
 
 #include "kernels.cuh"
@@ -46,6 +47,22 @@ __global__ void __launch_bounds__(256) k_F(const __grid_constant__ DevOps P, con
   grid_reduce<1>(mx, ops, red);
 }
 
+// f(i,j) = (M W + alpha yM + beta ydM)(i,j) * gamma
+__device__ __forceinline__ double div_cell(const DevOps &P, const double *__restrict__ W, double alpha, double beta,
+                                           double gamma, int i, int j) {
+  double d;
+  if (in_reg(P.rMX, i) && in_reg(P.rMY, j)) {
+    // interior cell: regular rows of Mx and My, no boundary contribution
+    d = __ldg(P.hy + j) * reg_x(P.rMX, i, W, (long long)j * P.Nux) +
+        __ldg(P.hx + i) * reg_y(P.rMY, j, W + P.Nu, P.Nvx, i);
+  } else {
+    d = div_in(P, W, W + P.Nu, i, j);
+    if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
+    if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
+  }
+  return d * gamma;
+}
+
 template <bool WANTMAX>
 __global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, const double *__restrict__ W,
                                             double alpha, double beta, double gamma, double *__restrict__ f,
@@ -55,28 +72,17 @@ __global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, c
   double mx[1] = {0.0};
   const int ops[1] = {R_MAX};
   if (i < P.Npx && j < P.Npy) {
-    double d;
-    if (in_reg(P.rMX, i) && in_reg(P.rMY, j)) {
-      // interior cell: regular rows of Mx and My, no boundary contribution
-      d = __ldg(P.hy + j) * reg_x(P.rMX, i, W, (long long)j * P.Nux) +
-          __ldg(P.hx + i) * reg_y(P.rMY, j, W + P.Nu, P.Nvx, i);
-    } else {
-      d = div_in(P, W, W + P.Nu, i, j);
-      if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
-      if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
-    }
-    d *= gamma;
+    const double d = div_cell(P, W, alpha, beta, gamma, i, j);
     f[(long long)j * P.Npx + i] = d;
     mx[0] = fabs(d);
   }
   if (WANTMAX) grid_reduce<1>(mx, ops, red);
 }
 
-__global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps P, const double *__restrict__ Wt,
-                                                const double *__restrict__ dp, double dt, double c,
-                                                double *__restrict__ Vo) {
-  const int i = blockIdx.x * BX + threadIdx.x;
-  const int j = blockIdx.y * BY + threadIdx.y;
+// V_out(i,j) = dt (Wt - c Om^-1 G dp) at the u and v points of (i,j)
+__device__ __forceinline__ void project_cell(const DevOps &P, const double *__restrict__ Wt,
+                                             const double *__restrict__ dp, double dt, double c,
+                                             double *__restrict__ Vo, int i, int j) {
   if (i < P.Nux && j < P.Nuy) {
     const long long idx = (long long)j * P.Nux + i;
     Vo[idx] = dt * (Wt[idx] - c * om_inv_u(P, i, j) * grad_x_fast(P, dp, i, j));
@@ -85,6 +91,12 @@ __global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps 
     const long long idx = P.Nu + (long long)j * P.Nvx + i;
     Vo[idx] = dt * (Wt[idx] - c * om_inv_v(P, i, j) * grad_y_fast(P, dp, i, j));
   }
+}
+
+__global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps P, const double *__restrict__ Wt,
+                                                const double *__restrict__ dp, double dt, double c,
+                                                double *__restrict__ Vo) {
+  project_cell(P, Wt, dp, dt, c, Vo, blockIdx.x * BX + threadIdx.x, blockIdx.y * BY + threadIdx.y);
 }
 
 __global__ void __launch_bounds__(256) k_correct(const __grid_constant__ DevOps P, const double *__restrict__ Vi,
@@ -143,6 +155,53 @@ __global__ void k_add(const double *__restrict__ x, double *__restrict__ y, long
     y[k] += x[k];
 }
 
+// --- ensembles ---------------------------------------------------------------------
+__device__ __forceinline__ void copy_ops(DevOps *dst, const DevOps *src) {
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  for (int k = tid; k < (int)(sizeof(DevOps) / 8); k += nt) ((long long *)dst)[k] = ((const long long *)src)[k];
+}
+
+__global__ void __launch_bounds__(256) k_div_ens(const EnsMemberD *__restrict__ mem, const int4 *__restrict__ tiles,
+                                                int mode, double alpha, double gamma) {
+  __shared__ __align__(16) DevOps sP;
+  const int4 t = tiles[blockIdx.x];
+  const EnsMemberD &M = mem[t.x];
+  copy_ops(&sP, &M.P);
+  __syncthreads();
+  const int i = t.y * BX + threadIdx.x, j = t.z * BY + threadIdx.y;
+  if (i < sP.Npx && j < sP.Npy)
+    M.f[(long long)j * sP.Npx + i] =
+        mode == 0 ? div_cell(sP, M.Wt, alpha, 0.0, gamma, i, j) : div_cell(sP, M.wres, 0.0, 0.0, 1.0, i, j);
+}
+
+__global__ void __launch_bounds__(256) k_project_ens(const EnsMemberD *__restrict__ mem,
+                                                    const int4 *__restrict__ tiles, double dt, double c, int from_p,
+                                                    int last) {
+  __shared__ __align__(16) DevOps sP;
+  const int4 t = tiles[blockIdx.x];
+  const EnsMemberD &M = mem[t.x];
+  copy_ops(&sP, &M.P);
+  __syncthreads();
+  project_cell(sP, M.Wt, from_p ? M.p : M.dp, dt, c, last ? M.V : M.Vs, t.y * BX + threadIdx.x,
+               t.z * BY + threadIdx.y);
+}
+
+__global__ void __launch_bounds__(256) k_stage_cached_ens(const EnsMemberD *__restrict__ mem,
+                                                         const int4 *__restrict__ tiles, double aii, double inv_dt) {
+  const int4 t = tiles[blockIdx.x];
+  const EnsMemberD &M = mem[t.x];
+  const int i = t.y * BX + threadIdx.x, j = t.z * BY + threadIdx.y;
+  const DevOps &P = M.P;
+  if (i < P.Nux && j < P.Nuy) {
+    const long long idx = (long long)j * P.Nux + i;
+    M.Wt[idx] = M.V[idx] * inv_dt + aii * M.kV[0][idx];
+  }
+  if (i < P.Nvx && j < P.Nvy) {
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    M.Wt[idx] = M.V[idx] * inv_dt + aii * M.kV[0][idx];
+  }
+}
+
 }  // namespace
 
 void launch_F(const DevOps &P, const double *V, const double *C, const double *p, double *F_out,
@@ -196,6 +255,31 @@ void launch_add(const double *x, double *y, long long n, cudaStream_t s) {
   if (b > 148 * 16) b = 148 * 16;
   if (b < 1) b = 1;
   k_add<<<(unsigned)b, 256, 0, s>>>(x, y, n);
+}
+
+}  // namespace ins2d
+
+namespace ins2d {
+
+void cell_tiles(const DevOps &P, int member, std::vector<int4> &out) {
+  const int nx = std::max(P.Npx, std::max(P.Nux, P.Nvx)), ny = std::max(P.Npy, std::max(P.Nuy, P.Nvy));
+  for (int by = 0; by < (ny + BY - 1) / BY; ++by)
+    for (int bx = 0; bx < (nx + BX - 1) / BX; ++bx) out.push_back(make_int4(member, bx, by, 0));
+}
+
+void launch_div_ens(const EnsMemberD *mem, const int4 *tiles, int n, int mode, double alpha, double gamma,
+                    cudaStream_t s) {
+  if (n > 0) k_div_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, mode, alpha, gamma);
+}
+
+void launch_project_ens(const EnsMemberD *mem, const int4 *tiles, int n, double dt, double c, int from_p, int last,
+                        cudaStream_t s) {
+  if (n > 0) k_project_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, dt, c, from_p, last);
+}
+
+void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, double aii, double inv_dt,
+                             cudaStream_t s) {
+  if (n > 0) k_stage_cached_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, aii, inv_dt);
 }
 
 }  // namespace ins2d

@@ -3,7 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "device.cuh"
+#include "mg.cuh"
 
 namespace ins2d {
 
@@ -62,6 +65,37 @@ void launch_stage_cached(const double *kV0, const double *Vn, double aii, double
 // y += x
 void launch_add(const double *x, double *y, long long n, cudaStream_t s);
 
+// --- ensembles: many independent member grids per launch -----------------------
+// Member descriptor in device memory: operator tables, state and work arrays.
+struct PcgWork;
+struct EnsMemberD;
+// Stage (mode 0) or additional-solve residual (mode 1) walker arguments shared
+// by all members (same Butcher tableau and dt).
+struct EnsWalk {
+  int mode, stage, store, use_vs, nprev, cache;
+  int kidx[kMaxStages];
+  double aprev[kMaxStages];
+  double aii, inv_dt;
+};
+// Host: the walker tiles {member, bx, by, 0} of one member, split into fast
+// (interior) and generic tiles.
+void walk_tiles(const DevOps &P, int member, std::vector<int4> &fast, std::vector<int4> &gen);
+void launch_walk_ens(const EnsMemberD *mem, const int4 *fast, int nfast, const int4 *gen, int ngen, const EnsWalk &w,
+                     bool fp32, cudaStream_t s);
+// Host: the 32x8 cell tiles {member, bx, by, 0} covering a member's u, v and p
+// index spaces.
+void cell_tiles(const DevOps &P, int member, std::vector<int4> &out);
+// f = (M Wt + alpha yM) gamma (mode 0, stage) or f = M wres (mode 1, residual)
+void launch_div_ens(const EnsMemberD *mem, const int4 *tiles, int n, int mode, double alpha, double gamma,
+                    cudaStream_t s);
+// V_out = dt (Wt - c Om^-1 G dp_src); dp_src = p (from_p) or dp; V_out = V
+// (last stage) or Vs
+void launch_project_ens(const EnsMemberD *mem, const int4 *tiles, int n, double dt, double c, int from_p, int last,
+                        cudaStream_t s);
+// Wt = V/dt + aii kV[0] (first stage from the cached residual)
+void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, double aii, double inv_dt,
+                             cudaStream_t s);
+
 // --- FFT Poisson (fft.cu) -------------------------------------------------------
 struct FftPlan {
   int Nx = 0, Ny = 0, logx = -1, logy = -1;  // log2 when a power of two, else -1
@@ -93,11 +127,40 @@ void pcg_init(const DevOps &P, const PcgWork &W, const double *f, double tol, lo
 void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s);
 void pcg_finish(const DevOps &P, const PcgWork &W, double *dp, bool accumulate, cudaStream_t s);
 int pcg_blocks(const DevOps &P);
+// Multi-block PCG with the multigrid preconditioner: k_init + one V-cycle,
+// then n iterations of SpMV, update, V-cycle, r'z, p update (mg.cu launches).
+void pcg_init_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double tol, long long maxit,
+                 cudaStream_t s);
+void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, cudaStream_t s);
+
+struct EnsMemberD {
+  DevOps P;
+  double *V, *p, *Vs, *Wt, *kV[kMaxStages], *f, *dp, *wres;
+  PcgWork W;
+  const MgD *mg;  // device copy of the member's hierarchy, or null (Jacobi)
+};
+// per-member solve statistics, accumulated over a run
+struct EnsStats {
+  long long n_solves, iters_total, iters_max;
+  double norm1_max;
+  int status, pad;
+};
+// Poisson solves of all members in one persistent launch: each thread block
+// takes the next member of `order` from a device queue and runs the whole
+// PCG (pcg_block_body).  which = 0: f -> dp; which = 1: p += solve(f)
+// (additional solve).  queue: two zeroed counters, left zeroed on exit.
+void launch_pcg_members(const EnsMemberD *mem, const int *order, int n, int which, double tol2, long long maxit,
+                        unsigned *queue, EnsStats *stats, int threads, int blocks, cudaStream_t s);
 // Small grids: the whole solve in one thread block (dp written or accumulated
 // when converged; status/iterations in W.sc)
 constexpr long long kPcgBlockMaxCells = 16384;
 bool pcg_use_block(const DevOps &P);
 void pcg_solve_block(const DevOps &P, const PcgWork &W, const double *f, double *dp, double tol, long long maxit,
                      bool accumulate, cudaStream_t s);
+// Same with a multigrid V-cycle as the preconditioner (mg.cuh); one thread
+// block, for grids up to kPcgBlockMgMaxCells cells.
+constexpr long long kPcgBlockMgMaxCells = 65536;
+void pcg_solve_block_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double *dp, double tol,
+                        long long maxit, bool accumulate, cudaStream_t s);
 
 }  // namespace ins2d

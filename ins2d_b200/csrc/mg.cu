@@ -1,0 +1,159 @@
+// Device side of the multigrid preconditioner (see mg.cuh): upload of the
+// level hierarchy built by mg_host.cpp, the per-line factors (one thread per
+// line), and the multi-block V-cycle launches.
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "mg.cuh"
+#include "mg_host.hpp"
+
+static_assert(ins2d::kMgMaxLevels == ins2d::kMgMaxLevelsHost && ins2d::kMgCoarseMax == ins2d::kMgCoarseMaxHost,
+              "host and device multigrid limits");
+
+namespace ins2d {
+
+namespace {
+
+__global__ void k_factor_x(MgLevelD L) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < L.ny) mg_factor_xline(L, j);
+}
+__global__ void k_factor_y(MgLevelD L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < L.nx) mg_factor_yline(L, i);
+}
+
+constexpr int kLineThreads = 128;
+constexpr int kTailThreads = 512;
+constexpr long long kTailMaxCells = 16384;
+
+__device__ __forceinline__ bool is_done(const int *done) { return done && *(volatile const int *)done; }
+
+__global__ void __launch_bounds__(kLineThreads) k_mg_xline(const MgLevelD L, const double *__restrict__ b,
+                                                           const double *__restrict__ xold, double *__restrict__ xnew,
+                                                           double omega, const int *done) {
+  if (is_done(done)) return;
+  mg_xline(L, b, xold, xnew, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+__global__ void __launch_bounds__(kLineThreads) k_mg_yline(const MgLevelD L, const double *__restrict__ b,
+                                                           const double *__restrict__ xold, double *__restrict__ xnew,
+                                                           double omega, const int *done) {
+  if (is_done(done)) return;
+  mg_yline(L, b, xold, xnew, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+__global__ void __launch_bounds__(256) k_mg_restrict(const MgLevelD F, const MgLevelD C, const double *__restrict__ b,
+                                                     const double *__restrict__ x, double *__restrict__ bc,
+                                                     const int *done) {
+  if (is_done(done)) return;
+  mg_restrict(F, C, b, x, bc, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+__global__ void __launch_bounds__(256) k_mg_prolong(const MgLevelD F, const MgLevelD C, double *__restrict__ x,
+                                                    const double *__restrict__ xc, double alpha, const int *done) {
+  if (is_done(done)) return;
+  mg_prolong(F, C, x, xc, alpha, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+__global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_constant__ MgD M, int l0,
+                                                            const double *__restrict__ b0, const int *done) {
+  if (is_done(done)) return;
+  mg_vcycle_block(M, b0, l0);
+}
+
+unsigned blocks_for(long long n, int t) {
+  long long b = (n + t - 1) / t;
+  if (b > 148LL * 32) b = 148LL * 32;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+int mg_tail_level(const MgD &M) {
+  for (int l = 0; l < M.nlev; ++l)
+    if ((long long)M.L[l].nx * M.L[l].ny <= kTailMaxCells) return l;
+  return M.nlev - 1;
+}
+
+void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStream_t s) {
+  const int lt = mg_tail_level(M);
+  for (int l = 0; l < lt; ++l) {
+    const MgLevelD &L = M.L[l];
+    const double *b = (l == 0) ? r0 : L.b;
+    k_mg_xline<<<blocks_for(L.ny, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x, M.omega, done);
+    k_mg_yline<<<blocks_for(L.nx, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t, M.omega, done);
+    const MgLevelD &C = M.L[l + 1];
+    k_mg_restrict<<<blocks_for((long long)C.nx * C.ny, 256), 256, 0, s>>>(L, C, b, L.t, C.b, done);
+  }
+  k_mg_tail<<<1, kTailThreads, 0, s>>>(M, lt, lt == 0 ? r0 : M.L[lt].b, done);
+  for (int l = lt - 1; l >= 0; --l) {
+    const MgLevelD &L = M.L[l];
+    const double *b = (l == 0) ? r0 : L.b;
+    const MgLevelD &C = M.L[l + 1];
+    k_mg_prolong<<<blocks_for((long long)L.nx * L.ny, 256), 256, 0, s>>>(L, C, L.t,
+                                                                         (l + 1 == M.nlev - 1) ? C.x : C.t,
+                                                                         M.alpha, done);
+    k_mg_yline<<<blocks_for(L.nx, kLineThreads), kLineThreads, 0, s>>>(L, b, L.t, L.x, M.omega, done);
+    k_mg_xline<<<blocks_for(L.ny, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t, M.omega, done);
+  }
+}
+
+void mg_setup_device(const std::vector<MgHostLevel> &lv, MgD &M, const std::function<double *(size_t)> &alloc,
+                     cudaStream_t s) {
+  M.nlev = (int)lv.size();
+  M.omega = 0.8;
+  M.alpha = 2.0;
+  auto up = [&](const std::vector<double> &v) {
+    double *d = alloc(v.size());
+    if (cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      throw std::runtime_error("multigrid: upload failed");
+    return d;
+  };
+  for (int l = 0; l < M.nlev; ++l) {
+    const MgHostLevel &H = lv[l];
+    MgLevelD &D = M.L[l];
+    D = MgLevelD{};
+    D.nx = H.nx;
+    D.ny = H.ny;
+    D.perx = H.perx;
+    D.pery = H.pery;
+    D.cx = H.cx;
+    D.cy = H.cy;
+    D.xm = up(H.xm);
+    D.x0 = up(H.x0);
+    D.xp = up(H.xp);
+    D.hx = up(H.hx);
+    D.ym = up(H.ym);
+    D.y0 = up(H.y0);
+    D.yp = up(H.yp);
+    D.hy = up(H.hy);
+    const size_t n = (size_t)H.nx * H.ny;
+    D.fxc = alloc(n);
+    D.fxi = alloc(n);
+    D.fyc = alloc(n);
+    D.fyi = alloc(n);
+    if (H.perx) {
+      D.zx = alloc(n);
+      D.gx = alloc(H.ny);
+      D.kx = alloc(H.ny);
+    }
+    if (H.pery) {
+      D.zy = alloc(n);
+      D.gy = alloc(H.nx);
+      D.ky = alloc(H.nx);
+    }
+    D.b = (l > 0) ? alloc(n) : nullptr;
+    D.x = alloc(n);
+    D.t = alloc(n);
+    k_factor_x<<<(H.ny + 127) / 128, 128, 0, s>>>(D);
+    k_factor_y<<<(H.nx + 127) / 128, 128, 0, s>>>(D);
+  }
+  const MgHostLevel &Cst = lv.back();
+  M.ncoarse = Cst.nx * Cst.ny;
+  M.cinv = up(mg_pinv(mg_dense(Cst), M.ncoarse));
+  if (cudaGetLastError() != cudaSuccess) throw std::runtime_error("multigrid: factor kernels failed");
+}
+
+}  // namespace ins2d

@@ -1,0 +1,412 @@
+// Multigrid V-cycle used as the preconditioner of the pressure PCG.
+//
+// The pressure matrix of the reference, A = M Om^-1 G (operator_divergence.m:208),
+// is separable: A = -(diag(hy) (x) TX + TY (x) diag(hx)) with TX, TY 1D
+// tridiagonal operators (periodic wraps included).  Coarse levels are the
+// Galerkin products P' A P for piecewise-constant aggregation of 2x2 (or 2x1)
+// cells, which keep the same separable form: TXc = Px' TX Px and the weights
+// summed over the aggregate (hxc = Px' hx).  So every level is described by
+// O(nx + ny) numbers: per row i of the 1D x operator its entries at i-1, i,
+// i+1 (xm, x0, xp) and per row j of the y operator (ym, y0, yp), with the
+// 5-point couplings
+//   W = -hy_j xm_i, E = -hy_j xp_i, S = -hx_i ym_j, N = -hx_i yp_j,
+//   C = -(hy_j x0_i + hx_i y0_j).
+// Smoother: alternating line relaxation (block Jacobi over x-lines, then over
+// y-lines, damped by omega), which stays robust on the strongly stretched
+// grids of the channel and cavity cases where point Jacobi stalls.  The
+// post-smoother applies the two sweeps in the reverse order, so the V-cycle
+// is a symmetric operator (as the preconditioner of CG must be).  The
+// coarsest level (<= kMgCoarseMax cells) is solved with a dense
+// pseudo-inverse, so singular (all-Neumann or periodic) problems are handled.
+// The coarse correction is scaled by alpha (over-correction of unsmoothed
+// aggregation).
+//
+// Line solves: each thread owns one line and runs the Thomas algorithm with
+// per-cell factors computed once at set-up; periodic lines use the
+// Sherman-Morrison form (T = T' + u v') with z = T'^-1 u stored per cell.
+//
+// The phase functions take (first line/cell, stride) so the same code runs
+// inside one thread block (small grids, ensembles: one block per solve) and
+// across a grid of blocks (large grids: one launch per phase).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <functional>
+#include <vector>
+
+namespace ins2d {
+
+constexpr int kMgMaxLevels = 20;
+constexpr int kMgCoarseMax = 64;
+
+struct MgLevelD {
+  int nx, ny, perx, pery;
+  int cx, cy;  // aggregation factors to the next level (1 or 2)
+  const double *xm, *x0, *xp, *hx;  // nx
+  const double *ym, *y0, *yp, *hy;  // ny
+  // line factors per cell: x-lines (fxc = c', fxi = 1/pivot), y-lines
+  double *fxc, *fxi, *fyc, *fyi;
+  // periodic lines: z = T'^-1 u per cell; per line g = a0/gamma, k = 1/(1 + v'z)
+  double *zx, *zy, *gx, *kx, *gy, *ky;
+  // vectors: right-hand side, iterate and its relaxed copy
+  double *b, *x, *t;
+};
+
+struct MgD {
+  int nlev;
+  int ncoarse;         // cells of the coarsest level
+  const double *cinv;  // ncoarse x ncoarse pseudo-inverse of the coarsest matrix
+  double omega, alpha;
+  MgLevelD L[kMgMaxLevels];
+};
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int mg_wrap_lo(int i, int n, int per) { return i > 0 ? i - 1 : (per ? n - 1 : 0); }
+__device__ __forceinline__ int mg_wrap_hi(int i, int n, int per) { return i < n - 1 ? i + 1 : (per ? 0 : n - 1); }
+
+// (A x)(i,j) at one cell of level L
+__device__ __forceinline__ double mg_apply(const MgLevelD &L, const double *__restrict__ x, int i, int j) {
+  const int nx = L.nx;
+  const double hx = L.hx[i], hy = L.hy[j];
+  const int im = mg_wrap_lo(i, nx, L.perx), ip = mg_wrap_hi(i, nx, L.perx);
+  const int jm = mg_wrap_lo(j, L.ny, L.pery), jp = mg_wrap_hi(j, L.ny, L.pery);
+  const long long r = (long long)j * nx;
+  return -(hy * (L.xm[i] * x[r + im] + L.x0[i] * x[r + i] + L.xp[i] * x[r + ip]) +
+           hx * (L.ym[j] * x[(long long)jm * nx + i] + L.y0[j] * x[r + i] + L.yp[j] * x[(long long)jp * nx + i]));
+}
+
+// Factors of the x-line of row j: T = tridiag(a, b, c), a_i = W(i,j),
+// b_i = C(i,j), c_i = E(i,j) (cyclic: corners a_0 and c_{n-1}).
+__device__ inline void mg_factor_xline(const MgLevelD &L, int j) {
+  const int n = L.nx;
+  const double hy = L.hy[j], y0 = L.y0[j];
+  const long long r = (long long)j * n;
+  auto A = [&](int i) { return -hy * L.xm[i]; };
+  auto B = [&](int i) { return -(hy * L.x0[i] + L.hx[i] * y0); };
+  auto C = [&](int i) { return -hy * L.xp[i]; };
+  const bool cyc = L.perx && n >= 3;
+  const double gamma = -B(0);
+  double cp = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double bi = B(i);
+    if (cyc && i == 0) bi -= gamma;
+    if (cyc && i == n - 1) bi -= C(n - 1) * A(0) / gamma;
+    const double ai = (i > 0) ? A(i) : 0.0;
+    const double inv = 1.0 / (bi - ai * cp);
+    cp = (i < n - 1) ? C(i) * inv : 0.0;
+    L.fxi[r + i] = inv;
+    L.fxc[r + i] = cp;
+  }
+  if (cyc) {
+    // z = T'^-1 u, u = (gamma, 0, ..., 0, c_{n-1})
+    double d = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double ui = (i == 0) ? gamma : (i == n - 1 ? C(n - 1) : 0.0);
+      const double ai = (i > 0) ? A(i) : 0.0;
+      d = (ui - ai * d) * L.fxi[r + i];
+      L.zx[r + i] = d;
+    }
+    double z = 0.0;
+    for (int i = n - 1; i >= 0; --i) {
+      z = L.zx[r + i] - L.fxc[r + i] * z;
+      L.zx[r + i] = z;
+    }
+    const double g = A(0) / gamma;
+    L.gx[j] = g;
+    L.kx[j] = 1.0 / (1.0 + L.zx[r] + g * L.zx[r + n - 1]);
+  }
+}
+
+__device__ inline void mg_factor_yline(const MgLevelD &L, int i) {
+  const int n = L.ny, nx = L.nx;
+  const double hx = L.hx[i], x0 = L.x0[i];
+  auto A = [&](int j) { return -hx * L.ym[j]; };
+  auto B = [&](int j) { return -(L.hy[j] * x0 + hx * L.y0[j]); };
+  auto C = [&](int j) { return -hx * L.yp[j]; };
+  const bool cyc = L.pery && n >= 3;
+  const double gamma = -B(0);
+  double cp = 0.0;
+  for (int j = 0; j < n; ++j) {
+    double bj = B(j);
+    if (cyc && j == 0) bj -= gamma;
+    if (cyc && j == n - 1) bj -= C(n - 1) * A(0) / gamma;
+    const double aj = (j > 0) ? A(j) : 0.0;
+    const double inv = 1.0 / (bj - aj * cp);
+    cp = (j < n - 1) ? C(j) * inv : 0.0;
+    const long long k = (long long)j * nx + i;
+    L.fyi[k] = inv;
+    L.fyc[k] = cp;
+  }
+  if (cyc) {
+    double d = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double uj = (j == 0) ? gamma : (j == n - 1 ? C(n - 1) : 0.0);
+      const double aj = (j > 0) ? A(j) : 0.0;
+      const long long k = (long long)j * nx + i;
+      d = (uj - aj * d) * L.fyi[k];
+      L.zy[k] = d;
+    }
+    double z = 0.0;
+    for (int j = n - 1; j >= 0; --j) {
+      const long long k = (long long)j * nx + i;
+      z = L.zy[k] - L.fyc[k] * z;
+      L.zy[k] = z;
+    }
+    const double g = A(0) / gamma;
+    L.gy[i] = g;
+    L.ky[i] = 1.0 / (1.0 + L.zy[i] + g * L.zy[(long long)(n - 1) * nx + i]);
+  }
+}
+
+// Line relaxation along a line of n cells: cell q of the line is at
+// base + q*st (st = 1 for x-lines, nx for y-lines); the couplings across the
+// line to the neighbouring lines (lo, hi: offsets of the neighbour cells)
+// enter the right-hand side with the old iterate:
+//   xnew = (1-omega) xold + omega T^-1 (b - X xold),   xold == nullptr: zero.
+// The loads of a chunk of kMgChunk cells are issued before its recurrence
+// steps, so the dependent Thomas chain pays one memory latency per chunk.
+#ifndef INS2D_MG_CHUNK
+#define INS2D_MG_CHUNK 8
+#endif
+#ifndef INS2D_MG_NOINLINE
+#define INS2D_MG_NOINLINE 1
+#endif
+#if INS2D_MG_NOINLINE
+#define MG_LINE_ATTR __noinline__
+#else
+#define MG_LINE_ATTR __forceinline__
+#endif
+constexpr int kMgChunk = INS2D_MG_CHUNK;
+
+struct MgLine {
+  long long base, st, lo, hi;  // cell q at base + q*st; neighbours at +lo, +hi
+  int n;
+  const double *cross_w;       // per cell of the line: weight of the cross couplings (hx or hy)
+  double cm, cp;               // cross-coupling entries (ym/yp or xm/xp) of this line
+  const double *am;            // per cell: entry at q-1 of the line operator (xm or ym)
+  double ascale;               // the line's weight (hy or hx)
+  const double *fi, *fc;       // Thomas factors
+  const double *z;             // periodic lines: T'^-1 u
+  double g, k;                 // periodic lines: v'/(1+v'z) terms
+  bool cyc;
+};
+
+// (The descriptor is taken by value and its fields are copied into
+// registers: stores through xnew cannot alias them.)
+static __device__ MG_LINE_ATTR void mg_line(const MgLine ln, const double *__restrict__ b,
+                                            const double *__restrict__ xold, double *__restrict__ xnew,
+                                            double omega) {
+  const int n = ln.n;
+  const long long base = ln.base, st = ln.st, lo = ln.lo, hi = ln.hi;
+  const double *__restrict__ cw = ln.cross_w;
+  const double *__restrict__ am = ln.am;
+  const double *__restrict__ fi_ = ln.fi;
+  const double *__restrict__ fc_ = ln.fc;
+  const double cm = ln.cm, cp = ln.cp, as = ln.ascale;
+  const bool cyc = ln.cyc;
+  const bool hasold = xold != nullptr;
+  double d = 0.0;
+  for (int q0 = 0; q0 < n; q0 += kMgChunk) {
+    double rhs[kMgChunk], a[kMgChunk], fi[kMgChunk];
+#pragma unroll
+    for (int u = 0; u < kMgChunk; ++u) {
+      const int q = q0 + u;
+      if (q < n) {
+        const long long k = base + q * st;
+        double v = b[k];
+        if (hasold) v += cw[q] * (cm * xold[k + lo] + cp * xold[k + hi]);
+        rhs[u] = v;
+        a[u] = (q > 0) ? -as * am[q] : 0.0;
+        fi[u] = fi_[k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kMgChunk; ++u) {
+      const int q = q0 + u;
+      if (q < n) {
+        d = (rhs[u] - a[u] * d) * fi[u];
+        xnew[base + q * st] = d;
+      }
+    }
+  }
+  double xn = 0.0;
+  for (int q1 = n - 1; q1 >= 0; q1 -= kMgChunk) {
+    double dd[kMgChunk], fc[kMgChunk], xo[kMgChunk];
+#pragma unroll
+    for (int u = 0; u < kMgChunk; ++u) {
+      const int q = q1 - u;
+      if (q >= 0) {
+        const long long k = base + q * st;
+        dd[u] = xnew[k];
+        fc[u] = fc_[k];
+        xo[u] = (hasold && !cyc) ? xold[k] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kMgChunk; ++u) {
+      const int q = q1 - u;
+      if (q >= 0) {
+        xn = dd[u] - fc[u] * xn;
+        const long long k = base + q * st;
+        if (cyc)
+          xnew[k] = xn;
+        else
+          xnew[k] = hasold ? (1.0 - omega) * xo[u] + omega * xn : omega * xn;
+      }
+    }
+  }
+  if (cyc) {
+    const double *__restrict__ z = ln.z;
+    const double s = (xnew[base] + ln.g * xnew[base + (long long)(n - 1) * st]) * ln.k;
+    for (int q = 0; q < n; ++q) {
+      const long long k = base + q * st;
+      const double v = xnew[k] - s * z[k];
+      xnew[k] = hasold ? (1.0 - omega) * xold[k] + omega * v : omega * v;
+    }
+  }
+}
+
+// x-line relaxation of rows j0, j0+js, ...
+__device__ inline void mg_xline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
+                                double *__restrict__ xnew, double omega, int j0, int js) {
+  const int nx = L.nx, ny = L.ny;
+  for (int j = j0; j < ny; j += js) {
+    MgLine ln;
+    ln.base = (long long)j * nx;
+    ln.st = 1;
+    ln.lo = (long long)(mg_wrap_lo(j, ny, L.pery) - j) * nx;
+    ln.hi = (long long)(mg_wrap_hi(j, ny, L.pery) - j) * nx;
+    ln.n = nx;
+    ln.cross_w = L.hx;
+    ln.cm = L.ym[j];
+    ln.cp = L.yp[j];
+    ln.am = L.xm;
+    ln.ascale = L.hy[j];
+    ln.fi = L.fxi;
+    ln.fc = L.fxc;
+    ln.cyc = L.perx && nx >= 3;
+    ln.z = L.zx;
+    ln.g = ln.cyc ? L.gx[j] : 0.0;
+    ln.k = ln.cyc ? L.kx[j] : 0.0;
+    mg_line(ln, b, xold, xnew, omega);
+  }
+}
+
+// y-line relaxation of columns i0, i0+is, ... (coalesced across threads)
+__device__ inline void mg_yline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
+                                double *__restrict__ xnew, double omega, int i0, int is) {
+  const int nx = L.nx, ny = L.ny;
+  for (int i = i0; i < nx; i += is) {
+    MgLine ln;
+    ln.base = i;
+    ln.st = nx;
+    ln.lo = mg_wrap_lo(i, nx, L.perx) - i;
+    ln.hi = mg_wrap_hi(i, nx, L.perx) - i;
+    ln.n = ny;
+    ln.cross_w = L.hy;
+    ln.cm = L.xm[i];
+    ln.cp = L.xp[i];
+    ln.am = L.ym;
+    ln.ascale = L.hx[i];
+    ln.fi = L.fyi;
+    ln.fc = L.fyc;
+    ln.cyc = L.pery && ny >= 3;
+    ln.z = L.zy;
+    ln.g = ln.cyc ? L.gy[i] : 0.0;
+    ln.k = ln.cyc ? L.ky[i] : 0.0;
+    mg_line(ln, b, xold, xnew, omega);
+  }
+}
+
+// bc = P' (b - A x) over the coarse cells k0, k0+ks, ...
+__device__ inline void mg_restrict(const MgLevelD &F, const MgLevelD &Cl, const double *__restrict__ b,
+                                   const double *__restrict__ x, double *__restrict__ bc, long long k0, long long ks) {
+  const long long nc = (long long)Cl.nx * Cl.ny;
+  for (long long k = k0; k < nc; k += ks) {
+    const int I = (int)(k % Cl.nx), J = (int)(k / Cl.nx);
+    double s = 0.0;
+    for (int dj = 0; dj < F.cy; ++dj) {
+      const int j = J * F.cy + dj;
+      if (j >= F.ny) break;
+      for (int di = 0; di < F.cx; ++di) {
+        const int i = I * F.cx + di;
+        if (i >= F.nx) break;
+        s += b[(long long)j * F.nx + i] - mg_apply(F, x, i, j);
+      }
+    }
+    bc[k] = s;
+  }
+}
+
+// x += alpha * P xc over the fine cells k0, k0+ks, ...
+__device__ inline void mg_prolong(const MgLevelD &F, const MgLevelD &Cl, double *__restrict__ x,
+                                  const double *__restrict__ xc, double alpha, long long k0, long long ks) {
+  const long long n = (long long)F.nx * F.ny;
+  for (long long k = k0; k < n; k += ks) {
+    const int i = (int)(k % F.nx), j = (int)(k / F.nx);
+    x[k] += alpha * xc[(long long)(j / F.cy) * Cl.nx + i / F.cx];
+  }
+}
+
+// x = Cinv b at the coarsest level (rows k0, k0+ks, ...)
+__device__ inline void mg_coarse(const MgD &M, const double *__restrict__ b, double *__restrict__ x, int k0, int ks) {
+  const int n = M.ncoarse;
+  for (int r = k0; r < n; r += ks) {
+    double s = 0.0;
+    for (int c = 0; c < n; ++c) s += M.cinv[(long long)r * n + c] * b[c];
+    x[r] = s;
+  }
+}
+
+// Result location of a V-cycle at level l: the relaxed copy t (levels above
+// the coarsest) or x (the coarsest).
+__device__ __forceinline__ double *mg_result(const MgD &M, int l) {
+  return (l == M.nlev - 1) ? M.L[l].x : M.L[l].t;
+}
+
+// One V-cycle inside a thread block from level l0 down to the coarsest and
+// back: z = B b with b = b0 the right-hand side of level l0; the result is at
+// mg_result(M, l0).  All threads of the block must call it.
+__device__ inline void mg_vcycle_block(const MgD &M, const double *__restrict__ b0, int l0 = 0) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int nl = M.nlev;
+  for (int l = l0; l < nl - 1; ++l) {
+    const MgLevelD &L = M.L[l];
+    const double *b = (l == l0) ? b0 : L.b;
+    mg_xline(L, b, nullptr, L.x, M.omega, tid, nt);
+    __syncthreads();
+    mg_yline(L, b, L.x, L.t, M.omega, tid, nt);
+    __syncthreads();
+    mg_restrict(L, M.L[l + 1], b, L.t, M.L[l + 1].b, tid, nt);
+    __syncthreads();
+  }
+  mg_coarse(M, (l0 == nl - 1) ? b0 : M.L[nl - 1].b, M.L[nl - 1].x, tid, nt);
+  __syncthreads();
+  for (int l = nl - 2; l >= l0; --l) {
+    const MgLevelD &L = M.L[l];
+    const double *b = (l == l0) ? b0 : L.b;
+    mg_prolong(L, M.L[l + 1], L.t, mg_result(M, l + 1), M.alpha, tid, nt);
+    __syncthreads();
+    mg_yline(L, b, L.t, L.x, M.omega, tid, nt);
+    __syncthreads();
+    mg_xline(L, b, L.x, L.t, M.omega, tid, nt);
+    __syncthreads();
+  }
+}
+
+// Multi-block V-cycle (mg.cu): one launch per phase on the levels above
+// mg_tail_level(M), one thread block for the rest.  Every kernel returns at
+// once when *done is set (the PCG has converged), so whole iterations can be
+// queued ahead.
+int mg_tail_level(const MgD &M);
+// Allocates (through alloc, in doubles) and fills the device hierarchy of the
+// host levels (mg_host.hpp); the factor kernels run on stream s.
+struct MgHostLevel;
+void mg_setup_device(const std::vector<MgHostLevel> &lv, MgD &M, const std::function<double *(size_t)> &alloc,
+                     cudaStream_t s);
+inline double *mg_result_host(const MgD &M, int l) { return (l == M.nlev - 1) ? M.L[l].x : M.L[l].t; }
+void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStream_t s);
+
+}  // namespace ins2d

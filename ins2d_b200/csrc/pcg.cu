@@ -21,6 +21,7 @@
 // iterations.
 #include "ins2d.h"
 #include "kernels.cuh"
+#include "mg.cuh"
 #include "reduce.cuh"
 
 namespace ins2d {
@@ -103,6 +104,9 @@ __global__ void __launch_bounds__(256) k_spmv(const __grid_constant__ DevOps P, 
   }
 }
 
+// MG = true: the preconditioned residual is not known yet (the V-cycle runs
+// after this kernel), so r'z and beta come from k_rz_mg.
+template <bool MG>
 __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P, const PcgWork W) {
   if (*(volatile int *)&W.sc->done) return;
   const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
@@ -116,7 +120,7 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P
     W.x[k] = x;
     W.r[k] = r;
     q[0] = r * r;
-    q[1] = r * (r / lap_diag(P, i, j));
+    q[1] = MG ? 0.0 : r * (r / lap_diag(P, i, j));
     q[2] = x;
     q[3] = x;
     q[4] = fabs(r);
@@ -137,10 +141,48 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P
     } else if (s->it >= s->maxit) {
       s->status = INS2D_ENOTCONV;
       s->done = 1;
-    } else {
+    } else if (!MG) {
       s->beta = out[1] / s->rz;
       s->rz = out[1];
     }
+  }
+}
+
+// r'z with z = the V-cycle's result; init: p = z and rz = r'z (first
+// iteration), else beta = r'z_new / r'z_old.
+__global__ void __launch_bounds__(256) k_rz_mg(const __grid_constant__ DevOps P, const PcgWork W,
+                                               const double *__restrict__ z, int init) {
+  if (*(volatile int *)&W.sc->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  double q[1] = {0.0};
+  const int ops[1] = {R_SUM};
+  if (i < P.Npx && j < P.Npy) {
+    const long long k = (long long)j * P.Npx + i;
+    q[0] = W.r[k] * z[k];
+    if (init) W.p[k] = z[k];
+  }
+  double out[1];
+  if (grid_reduce<1>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    if (!isfinite(out[0])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    } else if (init) {
+      s->rz = out[0];
+    } else {
+      s->beta = out[0] / s->rz;
+      s->rz = out[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_pupdate_mg(const __grid_constant__ DevOps P, const PcgWork W,
+                                                    const double *__restrict__ z) {
+  if (*(volatile int *)&W.sc->done) return;
+  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+  if (i < P.Npx && j < P.Npy) {
+    const long long k = (long long)j * P.Npx + i;
+    W.p[k] = z[k] + W.sc->beta * W.p[k];
   }
 }
 
@@ -183,26 +225,32 @@ __device__ void block_reduce(double (&v)[NQ], const int (&ops)[NQ], double (*sh)
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_constant__ DevOps P, const PcgWork W,
-                                                               const double *__restrict__ f, double *__restrict__ dp,
-                                                               double tol2, long long maxit, int accumulate) {
-  __shared__ double sh[kBlockThreads / 32][5];
+// The whole solve by one thread block.  MG = false: Jacobi preconditioner
+// (z = r / diag A); MG = true: one multigrid V-cycle per application
+// (mg.cuh).  Results go to out (the PcgScalars of this solve).
+template <bool MG>
+__device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, const double *__restrict__ f,
+                               double *__restrict__ dp, double tol2, long long maxit, int accumulate,
+                               PcgScalars *out, double (*sh)[5]) {
   const int Npx = P.Npx;
   const long long Np = P.Np;
   const int tid = threadIdx.x, nt = blockDim.x;
   double *__restrict__ x = W.x, *__restrict__ r = W.r, *__restrict__ p = W.p, *__restrict__ q = W.q;
+  const double *z = MG ? mg_result(*M, 0) : nullptr;
   // init (cg.F:207-229 with x_in = 0)
   double a3[3] = {0.0, 0.0, 0.0};
   const int op3[3] = {R_SUM, R_SUM, R_MAX};
   for (long long k = tid; k < Np; k += nt) {
     const int i = (int)(k % Npx), j = (int)(k / Npx);
     const double fv = f[k];
-    const double z = fv / lap_diag(P, i, j);
     x[k] = 0.0;
     r[k] = fv;
-    p[k] = z;
+    if (!MG) {
+      const double zv = fv / lap_diag(P, i, j);
+      p[k] = zv;
+      a3[1] += fv * zv;
+    }
     a3[0] += fv * fv;
-    a3[1] += fv * z;
     a3[2] = fmax(a3[2], fabs(fv));
   }
   block_reduce<3>(a3, op3, (double(*)[3])sh);
@@ -212,11 +260,25 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_con
   long long it = 0;
   int status = 0;
   bool done = (a3[2] < 1e-14 || rr0 <= tol2);  // pressure_poisson.m:33-38, cg.F:222-227
-  if (!isfinite(rr0) || !isfinite(rz)) {
+  if (!isfinite(rr0)) {
     status = INS2D_ENONFINITE;
     done = true;
   }
   const int op1[1] = {R_SUM};
+  if (MG && !done) {
+    mg_vcycle_block(*M, r);
+    double a1[1] = {0.0};
+    for (long long k = tid; k < Np; k += nt) {
+      p[k] = z[k];
+      a1[0] += r[k] * z[k];
+    }
+    block_reduce<1>(a1, op1, (double(*)[1])sh);
+    rz = a1[0];
+  }
+  if (!isfinite(rz)) {
+    status = INS2D_ENONFINITE;
+    done = true;
+  }
   const int op5[5] = {R_SUM, R_SUM, R_MAX, R_MIN, R_MAX};
   while (!done) {
     double a1[1] = {0.0};
@@ -245,7 +307,7 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_con
       x[k] = xv;
       r[k] = rv;
       a5[0] += rv * rv;
-      a5[1] += rv * (rv / lap_diag(P, i, j));
+      if (!MG) a5[1] += rv * (rv / lap_diag(P, i, j));
       a5[2] = fmax(a5[2], xv);
       a5[3] = fmin(a5[3], xv);
       a5[4] = fmax(a5[4], fabs(rv));
@@ -256,7 +318,7 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_con
     maxx = a5[2];
     minx = a5[3];
     maxres = a5[4];
-    if (!isfinite(rr) || !isfinite(a5[1])) {
+    if (!isfinite(rr)) {
       status = INS2D_ENONFINITE;
       break;
     }
@@ -265,28 +327,113 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_con
       status = INS2D_ENOTCONV;
       break;
     }
-    const double beta = a5[1] / rz;
-    rz = a5[1];
+    double rz_new = a5[1];
+    if (MG) {
+      mg_vcycle_block(*M, r);
+      double b1[1] = {0.0};
+      for (long long k = tid; k < Np; k += nt) b1[0] += r[k] * z[k];
+      block_reduce<1>(b1, op1, (double(*)[1])sh);
+      rz_new = b1[0];
+    }
+    if (!isfinite(rz_new)) {
+      status = INS2D_ENONFINITE;
+      break;
+    }
+    const double beta = rz_new / rz;
+    rz = rz_new;
     for (long long k = tid; k < Np; k += nt) {
       const int i = (int)(k % Npx), j = (int)(k / Npx);
-      p[k] = r[k] / lap_diag(P, i, j) + beta * p[k];
+      const double zv = MG ? z[k] : r[k] / lap_diag(P, i, j);
+      p[k] = zv + beta * p[k];
     }
     __syncthreads();
   }
   if (status == 0)
     for (long long k = tid; k < Np; k += nt) dp[k] = accumulate ? dp[k] + x[k] : x[k];
   if (tid == 0) {
-    PcgScalars *s = W.sc;
-    s->rr0 = rr0;
-    s->rr = rr;
-    s->it = it;
-    s->maxx = maxx;
-    s->minx = minx;
-    s->maxres = maxres;
-    s->status = status;
-    s->done = 1;
-    s->tol2 = tol2;
-    s->maxit = maxit;
+    out->rr0 = rr0;
+    out->rr = rr;
+    out->it = it;
+    out->maxx = maxx;
+    out->minx = minx;
+    out->maxres = maxres;
+    out->status = status;
+    out->done = 1;
+    out->tol2 = tol2;
+    out->maxit = maxit;
+  }
+}
+
+__global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_constant__ DevOps P, const PcgWork W,
+                                                               const double *__restrict__ f, double *__restrict__ dp,
+                                                               double tol2, long long maxit, int accumulate) {
+  __shared__ double sh[kBlockThreads / 32][5];
+  pcg_block_body<false>(P, nullptr, W, f, dp, tol2, maxit, accumulate, W.sc, sh);
+}
+
+// multigrid variant: 512 threads (the chunked line solves need ~128 registers)
+#ifndef INS2D_MG_THREADS
+#define INS2D_MG_THREADS 512
+#endif
+constexpr int kBlockThreadsMg = INS2D_MG_THREADS;
+__global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_block_mg(const __grid_constant__ DevOps P,
+                                                                  const __grid_constant__ MgD M, const PcgWork W,
+                                                                  const double *__restrict__ f,
+                                                                  double *__restrict__ dp, double tol2,
+                                                                  long long maxit, int accumulate) {
+  __shared__ double sh[kBlockThreads / 32][5];
+  pcg_block_body<true>(P, &M, W, f, dp, tol2, maxit, accumulate, W.sc, sh);
+}
+
+// Ensemble solves: a persistent launch whose blocks take members from a
+// queue (largest first) and run the whole PCG of each.
+__global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_members(const EnsMemberD *__restrict__ mem,
+                                                                  const int *__restrict__ order, int n, int which,
+                                                                  double tol2, long long maxit,
+                                                                  unsigned *queue, EnsStats *stats) {
+  __shared__ __align__(16) DevOps sP;
+  __shared__ __align__(16) MgD sM;
+  __shared__ double sh[kBlockThreads / 32][5];
+  __shared__ int s_k;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (;;) {
+    if (tid == 0) s_k = (int)atomicAdd(&queue[0], 1u);
+    __syncthreads();
+    const int k = s_k;
+    if (k >= n) break;
+    const int m = order[k];
+    const EnsMemberD &E = mem[m];
+    for (int w = tid; w < (int)(sizeof(DevOps) / 8); w += nt) ((long long *)&sP)[w] = ((const long long *)&E.P)[w];
+    const bool mg = E.mg != nullptr;
+    if (mg)
+      for (int w = tid; w < (int)(sizeof(MgD) / 8); w += nt) ((long long *)&sM)[w] = ((const long long *)E.mg)[w];
+    __syncthreads();
+    double *dst = which ? E.p : E.dp;
+    if (mg)
+      pcg_block_body<true>(sP, &sM, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh);
+    else
+      pcg_block_body<false>(sP, nullptr, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh);
+    __syncthreads();
+    if (tid == 0) {
+      const PcgScalars &o = *E.W.sc;
+      EnsStats &st = stats[m];
+      st.n_solves += 1;
+      st.iters_total += o.it;
+      st.iters_max = o.it > st.iters_max ? o.it : st.iters_max;
+      const double n1 = sqrt(o.rr);
+      st.norm1_max = n1 > st.norm1_max ? n1 : st.norm1_max;
+      if (o.status != 0 && st.status == 0) st.status = o.status;
+    }
+    __syncthreads();  // s_k and the shared descriptors are reused
+  }
+  if (tid == 0) {
+    __threadfence();
+    const unsigned d = atomicAdd(&queue[1], 1u);
+    if (d == gridDim.x - 1) {  // last block out: reset the queue for the next launch
+      queue[0] = 0;
+      queue[1] = 0;
+      __threadfence();
+    }
   }
 }
 
@@ -297,6 +444,11 @@ bool pcg_use_block(const DevOps &P) { return P.Np <= kPcgBlockMaxCells; }
 void pcg_solve_block(const DevOps &P, const PcgWork &W, const double *f, double *dp, double tol, long long maxit,
                      bool accumulate, cudaStream_t s) {
   k_pcg_block<<<1, kBlockThreads, 0, s>>>(P, W, f, dp, tol * tol, maxit, accumulate ? 1 : 0);
+}
+
+void pcg_solve_block_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double *dp, double tol,
+                        long long maxit, bool accumulate, cudaStream_t s) {
+  k_pcg_block_mg<<<1, kBlockThreadsMg, 0, s>>>(P, M, W, f, dp, tol * tol, maxit, accumulate ? 1 : 0);
 }
 
 int pcg_blocks(const DevOps &P) {
@@ -312,8 +464,27 @@ void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
   const dim3 g = pgrid(P), b(BX, BY);
   for (int it = 0; it < n; ++it) {
     k_spmv<<<g, b, 0, s>>>(P, W);
-    k_update<<<g, b, 0, s>>>(P, W);
+    k_update<false><<<g, b, 0, s>>>(P, W);
     k_pupdate<<<g, b, 0, s>>>(P, W);
+  }
+}
+
+void pcg_init_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double tol, long long maxit,
+                 cudaStream_t s) {
+  k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
+  mg_vcycle_launch(M, W.r, &W.sc->done, s);
+  k_rz_mg<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, mg_result_host(M, 0), 1);
+}
+
+void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, cudaStream_t s) {
+  const dim3 g = pgrid(P), b(BX, BY);
+  const double *z = mg_result_host(M, 0);
+  for (int it = 0; it < n; ++it) {
+    k_spmv<<<g, b, 0, s>>>(P, W);
+    k_update<true><<<g, b, 0, s>>>(P, W);
+    mg_vcycle_launch(M, W.r, &W.sc->done, s);
+    k_rz_mg<<<g, b, 0, s>>>(P, W, z, 0);
+    k_pupdate_mg<<<g, b, 0, s>>>(P, W, z);
   }
 }
 
@@ -322,6 +493,16 @@ void pcg_finish(const DevOps &P, const PcgWork &W, double *dp, bool accumulate, 
   long long blocks = (n + 255) / 256;
   if (blocks > 148 * 16) blocks = 148 * 16;
   k_copy_out<<<(unsigned)blocks, 256, 0, s>>>(W.x, dp, n, accumulate ? 1 : 0);
+}
+
+}  // namespace ins2d
+
+namespace ins2d {
+
+void launch_pcg_members(const EnsMemberD *mem, const int *order, int n, int which, double tol2, long long maxit,
+                        unsigned *queue, EnsStats *stats, int threads, int blocks, cudaStream_t s) {
+  if (n <= 0) return;
+  k_pcg_members<<<blocks, threads, 0, s>>>(mem, order, n, which, tol2, maxit, queue, stats);
 }
 
 }  // namespace ins2d

@@ -498,10 +498,9 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
   }
 }
 
+// one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
 template <typename S>
-__global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_fast(const __grid_constant__ DevOps P, const double *__restrict__ V,
-                                                      const __grid_constant__ Epi e) {
-  const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
+__device__ __forceinline__ void tile_fast(const DevOps &P, const double *__restrict__ V, const Epi &e, int bx, int by) {
   const int i = bx * WX + threadIdx.x;
   const int j0 = by * RUN, j1 = j0 + RUN;
   const double *u = V, *v = V + P.Nu;
@@ -510,6 +509,23 @@ __global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_fast(const __g
   else
     fast_v<S>(P, u, v, e, i, j0, j1);
 }
+template <typename S>
+__device__ __forceinline__ void tile_generic(const DevOps &P, const double *__restrict__ V, const Epi &e, int bx,
+                                             int by) {
+  const int i = bx * WX + threadIdx.x;
+  const int j0 = by * RUN, j1 = j0 + RUN;
+  const double *u = V, *v = V + P.Nu;
+  if (threadIdx.y == 0)
+    walk_u<S>(P, u, v, e, i, j0, j1);
+  else
+    walk_v<S>(P, u, v, e, i, j0, j1);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_fast(const __grid_constant__ DevOps P, const double *__restrict__ V,
+                                                      const __grid_constant__ Epi e) {
+  tile_fast<S>(P, V, e, P.fbx0 + blockIdx.x, P.fby0 + blockIdx.y);
+}
 
 template <typename S>
 __global__ void __launch_bounds__(WX * 2) k_walk(const __grid_constant__ DevOps P, const double *__restrict__ V,
@@ -517,13 +533,67 @@ __global__ void __launch_bounds__(WX * 2) k_walk(const __grid_constant__ DevOps 
   if ((int)blockIdx.x >= P.fbx0 && (int)blockIdx.x < P.fbx1 && (int)blockIdx.y >= P.fby0 &&
       (int)blockIdx.y < P.fby1)
     return;  // interior tile: handled by k_walk_fast
-  const int i = blockIdx.x * WX + threadIdx.x;
-  const int j0 = blockIdx.y * RUN, j1 = j0 + RUN;
-  const double *u = V, *v = V + P.Nu;
-  if (threadIdx.y == 0)
-    walk_u<S>(P, u, v, e, i, j0, j1);
+  tile_generic<S>(P, V, e, blockIdx.x, blockIdx.y);
+}
+
+// --- ensembles: one launch over the tiles of all member grids ------------------
+// The member's descriptor is copied to shared memory; the stage's pointers
+// come from the member's arrays.
+__device__ __forceinline__ void copy_words(void *dst, const void *src, int bytes) {
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
+  for (int k = tid; k < bytes / 8; k += nt) ((long long *)dst)[k] = ((const long long *)src)[k];
+}
+
+__device__ __forceinline__ const double *ens_epi(const EnsMemberD &M, const EnsWalk &w, Epi &e) {
+  e = Epi{};
+  e.mode = w.mode;
+  if (w.mode == 0) {
+    e.Vn = M.V;
+    e.kV = w.store ? M.kV[w.stage] : nullptr;
+    for (int q = 0; q < w.nprev; ++q) {
+      e.kprev[q] = M.kV[w.kidx[q]];
+      e.aprev[q] = w.aprev[q];
+    }
+    e.nprev = w.nprev;
+    e.aii = w.aii;
+    e.inv_dt = w.inv_dt;
+    e.Wt = M.Wt;
+    return w.use_vs ? M.Vs : M.V;
+  }
+  e.p = M.p;
+  e.w = M.wres;
+  e.kV_next = w.cache ? M.kV[0] : nullptr;
+  return M.V;
+}
+
+template <typename S, bool FAST>
+__device__ __forceinline__ void walk_ens_body(const EnsMemberD *__restrict__ mem, const int4 *__restrict__ work,
+                                              const EnsWalk &w) {
+  __shared__ __align__(16) DevOps sP;
+  __shared__ __align__(16) Epi sE;
+  __shared__ const double *sV;
+  const int4 it = work[blockIdx.x];
+  const EnsMemberD &M = mem[it.x];
+  copy_words(&sP, &M.P, (int)sizeof(DevOps));
+  if (threadIdx.x == 0 && threadIdx.y == 0) sV = ens_epi(M, w, sE);
+  __syncthreads();
+  if (FAST)
+    tile_fast<S>(sP, sV, sE, it.y, it.z);
   else
-    walk_v<S>(P, u, v, e, i, j0, j1);
+    tile_generic<S>(sP, sV, sE, it.y, it.z);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_ens_fast(const EnsMemberD *__restrict__ mem,
+                                                                          const int4 *__restrict__ work,
+                                                                          const __grid_constant__ EnsWalk w) {
+  walk_ens_body<S, true>(mem, work, w);
+}
+template <typename S>
+__global__ void __launch_bounds__(WX * 2) k_walk_ens_gen(const EnsMemberD *__restrict__ mem,
+                                                         const int4 *__restrict__ work,
+                                                         const __grid_constant__ EnsWalk w) {
+  walk_ens_body<S, false>(mem, work, w);
 }
 
 void launch_walk(const DevOps &P, const double *V, const Epi &e, bool fp32, cudaStream_t s) {
@@ -577,6 +647,33 @@ void walker_rectangle(DevOps &P) {
   P.fbx1 = bx1;
   P.fby0 = by0;
   P.fby1 = by1;
+}
+
+void walk_tiles(const DevOps &P, int member, std::vector<int4> &fast, std::vector<int4> &gen) {
+  const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
+  const int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  const int nbx = (nx + WX - 1) / WX, nby = (ny + RUN - 1) / RUN;
+  for (int by = 0; by < nby; ++by)
+    for (int bx = 0; bx < nbx; ++bx) {
+      const bool f = bx >= P.fbx0 && bx < P.fbx1 && by >= P.fby0 && by < P.fby1;
+      (f ? fast : gen).push_back(make_int4(member, bx, by, 0));
+    }
+}
+
+void launch_walk_ens(const EnsMemberD *mem, const int4 *fast, int nfast, const int4 *gen, int ngen, const EnsWalk &w,
+                     bool fp32, cudaStream_t s) {
+  if (nfast > 0) {
+    if (fp32)
+      k_walk_ens_fast<float><<<nfast, dim3(WX, 2), 0, s>>>(mem, fast, w);
+    else
+      k_walk_ens_fast<double><<<nfast, dim3(WX, 2), 0, s>>>(mem, fast, w);
+  }
+  if (ngen > 0) {
+    if (fp32)
+      k_walk_ens_gen<float><<<ngen, dim3(WX, 2), 0, s>>>(mem, gen, w);
+    else
+      k_walk_ens_gen<double><<<ngen, dim3(WX, 2), 0, s>>>(mem, gen, w);
+  }
 }
 
 void launch_stage(const DevOps &P, const StageArgs &a, bool fp32, cudaStream_t s) {

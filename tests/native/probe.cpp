@@ -51,3 +51,39 @@ extern "C" int probe_table(void *h, const char *name, int *nrows, int *ncols, co
   *b2 = t->b2.data();
   return 0;
 }
+
+// --- multigrid hierarchy (mg_host.cpp) ---------------------------------------
+#include <vector>
+
+#include "mg_host.hpp"
+
+struct ProbeMg {
+  std::vector<MgHostLevel> lv;
+  std::vector<double> pinv;
+};
+
+extern "C" void *probe_mg_build(void *h) {
+  ProbeMg *m = new ProbeMg();
+  try {
+    m->lv = mg_build_levels(*(HostOps *)h);
+    const MgHostLevel &c = m->lv.back();
+    m->pinv = mg_pinv(mg_dense(c), c.nx * c.ny);
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    delete m;
+    return nullptr;
+  }
+  return m;
+}
+extern "C" void probe_mg_free(void *m) { delete (ProbeMg *)m; }
+extern "C" int probe_mg_nlev(void *m) { return (int)((ProbeMg *)m)->lv.size(); }
+// dims = {nx, ny, perx, pery, cx, cy}; vec: 0..7 = xm, x0, xp, hx, ym, y0, yp, hy
+extern "C" int probe_mg_level(void *m, int l, int *dims, int which, const double **v) {
+  const MgHostLevel &L = ((ProbeMg *)m)->lv.at(l);
+  dims[0] = L.nx; dims[1] = L.ny; dims[2] = L.perx; dims[3] = L.pery; dims[4] = L.cx; dims[5] = L.cy;
+  const std::vector<double> *all[8] = {&L.xm, &L.x0, &L.xp, &L.hx, &L.ym, &L.y0, &L.yp, &L.hy};
+  if (which < 0 || which > 7) return 1;
+  *v = all[which]->data();
+  return 0;
+}
+extern "C" const double *probe_mg_pinv(void *m) { return ((ProbeMg *)m)->pinv.data(); }

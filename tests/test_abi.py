@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _declared():
     with open(os.path.join(ROOT, "include", "ins2d.h")) as fh:
         txt = fh.read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(ins2d_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int32_t|const char \*|ins2d_ctx \*)\s*(ins2d_\w+)\s*\(", txt, re.M)))
 
 
 def test_header_declares_entry_points():

@@ -1,0 +1,68 @@
+"""Ensembles (ins2d_ens_*): members of different grids, boundary conditions
+and Re advanced together must reproduce each member's own single-context
+run (the batched launches use the same per-cell arithmetic; the PCG solves
+agree to the solver tolerance)."""
+import numpy as np
+import pytest
+
+from ins2d_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(seed, n, sizes, stretch=1.05):
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        nx, ny = (int(v) for v in rng.choice(sizes, 2))
+        U = float(rng.uniform(0.5, 1.5))
+        Re = float(rng.uniform(100.0, 5000.0))
+        if m % 2 == 0:
+            x = cases.tanh_grid(nx, 0.0, 1.0, stretch)
+            y = cases.tanh_grid(ny, 0.0, 1.0, stretch)
+            out.append(dict(x=x, y=y, BC=cases.BC_CAVITY, Re=Re, uBC=cases.lid_uBC(U, 1.0)))
+        else:
+            x = cases.tanh_grid(nx, 0.0, 4.0, stretch)
+            y = cases.tanh_grid(ny, -0.5, 0.5, stretch)
+            out.append(dict(x=x, y=y, BC=cases.BC_CHANNEL, Re=Re,
+                            uBC=cases.channel_uBC(lambda yy, U=U: U * (1 - 4 * np.asarray(yy) ** 2))))
+    for kw in out:
+        kw.update(poisson=4, CG_acc=1e-12, CG_maxit=20000, RK="RK44")
+    return out
+
+
+@pytest.mark.parametrize("seed,n,sizes", [(4, 6, [24, 32, 40, 64]), (5, 9, [16, 48, 96, 130])])
+def test_ensemble_matches_single_runs(seed, n, sizes):
+    import ins2d_b200
+    members = _members(seed, n, sizes)
+    ens = ins2d_b200.Ensemble(members)
+    singles, states = [], []
+    for m, kw in enumerate(members):
+        o = ins2d_b200.Options(**kw)
+        V0 = np.zeros(o.NV)
+        p0 = o.pressure_additional_solve(V0, np.zeros(o.Np), 0.0)
+        ens.set_state(m, V0, p0)
+        singles.append(o)
+        states.append((V0, p0))
+    dt, nsteps = 2e-3, 6
+    stats = ens.time_ERK(0.0, dt, nsteps)
+    shape = ens.solve_shape()
+    assert shape["threads"] in (256, 512) and shape["blocks"] >= 1
+    for m, o in enumerate(singles):
+        V, p = o.time_ERK(*states[m], 0.0, dt, nsteps=nsteps)
+        Ve, pe = ens.get_state(m)
+        scale = max(np.max(np.abs(V)), 1e-30)
+        assert np.max(np.abs(Ve - V)) <= 1e-10 * scale, m
+        assert np.max(np.abs(pe - p)) <= 1e-8 * max(np.max(np.abs(p)), 1e-30), m
+        assert stats[m]["n_solves"] == 4 * nsteps  # 3 stage solves + 1 additional per RK4 step
+        assert stats[m]["iters_max"] <= 60
+        # the member context still serves the single-flow API on the ensemble's state
+        assert ens.member(m).check_conservation(Ve, nsteps * dt)[0] < 1e-10
+
+
+def test_ensemble_rejects_mixed_settings():
+    import ins2d_b200
+    members = _members(1, 2, [16, 24])
+    members[1]["CG_acc"] = 1e-6
+    with pytest.raises(ins2d_b200.Ins2dError):
+        ins2d_b200.Ensemble(members)

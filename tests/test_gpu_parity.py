@@ -193,3 +193,35 @@ def test_erk_fft_large_grid():
     Vg, pg = m.time_ERK(V0, np.zeros(g.Np), 0.0, 1e-4, nsteps=3)
     assert _rel(Vg, V) < 1e-12
     assert _rel(pg - pg.mean(), p - p.mean()) < 1e-10
+
+
+@pytest.mark.parametrize("combo", ["cavity", "channel", "periodic", "per_y_open", "open_x"])
+@pytest.mark.parametrize("shape", [(24, 20), (301, 257)])
+@pytest.mark.parametrize("precond", ["mg", "jacobi"])
+def test_pcg_preconditioners(combo, shape, precond):
+    """Multigrid and Jacobi preconditioned CG reach the stated tolerance and
+    agree with the oracle's direct solve, one thread block (24x20) and
+    multi-block (301x257) paths; multigrid needs few iterations on stretched
+    grids."""
+    nx, ny = shape
+    bc = BC_COMBOS[combo]
+    perx, pery = bc["u"]["left"] == "per", bc["v"]["low"] == "per"
+    x = grid_uniform(nx, 0.0, 1.7) if perx else grid_stretched(nx, 0.0, 1.7)
+    y = grid_uniform(ny, -0.5, 0.5) if pery else grid_stretched(ny, -0.5, 0.5, beta=1.2)
+    if precond == "jacobi" and nx > 100 and combo != "periodic":
+        pytest.skip("Jacobi-preconditioned CG on the large stretched grid takes too many iterations for a test")
+    o = R.make_options(x, y, bc, poisson=1)
+    m = _ins2d().Options(x, y, bc, poisson=4, CG_acc=1e-11, CG_maxit=50000, precond=precond)
+    rng = np.random.default_rng(nx + ny)
+    V = rng.standard_normal(o.grid.NV)
+    f = o.discretization.M @ V + o.discretization.yM
+    dp, st = m.pressure_poisson(f, return_stats=True)
+    A = o.discretization.A
+    res = np.linalg.norm(A @ dp - f) / np.linalg.norm(f)
+    assert res <= 2e-11
+    if precond == "mg":
+        assert st["iters"] <= 40, st
+    dp_ref = R.pressure_poisson(f, 0.0, o)
+    if is_closed(bc):
+        dp, dp_ref = dp - dp.mean(), dp_ref - dp_ref.mean()
+    assert _rel(dp, dp_ref) < 1e-8
