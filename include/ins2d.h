@@ -260,9 +260,13 @@ int ins2d_ens_set_stream(ins2d_ens *e, void *stream);
 /* member state V (NV values), p (Np values) in or out */
 int ins2d_ens_set_state(ins2d_ens *e, int32_t m, const double *V, const double *p, int mem);
 int ins2d_ens_get_state(ins2d_ens *e, int32_t m, double *V, double *p, int mem);
+/* a member's own time step (dt > 0; 0 = the dt of ins2d_ens_erk_run), e.g. a
+ * member whose explicit stability limit is below the ensemble's dt */
+int ins2d_ens_set_member_dt(ins2d_ens *e, int32_t m, double dt);
 /* device pointers of a member's state (valid for the ensemble's lifetime) */
 int ins2d_ens_state_ptr(ins2d_ens *e, int32_t m, double **V, double **p);
-/* nsteps of time_ERK for every member with the same t, dt; stats: n entries
+/* nsteps of time_ERK for every member (time step dt, or the member's own);
+ * stats: n entries
  * (per member, accumulated over the run) or NULL.  A member whose solve fails
  * makes the call return that status, naming the member. */
 int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_step_stats *stats);

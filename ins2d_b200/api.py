@@ -111,7 +111,10 @@ class Options:
 
     def __init__(self, x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_add_solve=1, RK="RK44",
                  uBC=None, vBC=None, dudtBC=None, dvdtBC=None, pLe=0.0, pRi=0.0, pLo=0.0, pUp=0.0,
-                 precision="fp64", device=0, BC_unsteady=None, precond="default", _handle=None):
+                 precision="fp64", device=0, BC_unsteady=None, precond="default", _handle=None, **private):
+        bad = [k for k in private if not k.startswith("_")]
+        if bad:
+            raise TypeError(f"unexpected options: {bad}")  # keys starting with '_' are annotations of a case
         self._lib = _lib.load()
         self._owner = _handle is None
         self.x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
@@ -439,14 +442,19 @@ class Ensemble:
         Va, pa = _Arr(V, o.NV, "V"), _Arr(p, o.Np, "p")
         self._check(self._lib.ins2d_ens_set_state(self._e, m, Va.ptr, pa.ptr, Options._mem(Va, pa)))
 
+    def set_member_dt(self, m, dt):
+        """Give member m its own time step (0: the run's dt)."""
+        self._check(self._lib.ins2d_ens_set_member_dt(self._e, m, float(dt)))
+
     def get_state(self, m, V=None, p=None):
         """The member's (V, p), into the given host arrays when passed."""
         o = self.members[m]
         V = np.empty(o.NV) if V is None else V
         p = np.empty(o.Np) if p is None else p
         Va, pa = _Arr(V, o.NV, "V"), _Arr(p, o.Np, "p")
-        if Va.obj is not V or pa.obj is not p:
-            raise ValueError("get_state: output arrays must be contiguous float64")
+        for a, arr in ((Va, V), (pa, p)):
+            if not a.dev and (not isinstance(arr, np.ndarray) or a.ptr != arr.ctypes.data):
+                raise ValueError("get_state: output arrays must be contiguous float64")
         self._check(self._lib.ins2d_ens_get_state(self._e, m, Va.ptr, pa.ptr, Options._mem(Va, pa)))
         return V, p
 

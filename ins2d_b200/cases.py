@@ -59,31 +59,17 @@ def nonuniform_grid(deltaz, z_low, z_up, sz):
 
 
 def tanh_grid(N, a, b, stretch):
-    """Grid clustered towards both ends by a tanh map, with the largest ratio
-    of neighbouring cell widths equal to ``stretch`` (the reference has no
-    tanh stretching; this is the map the benchmark configurations name).
-    stretch = 1 gives the uniform grid."""
-    if stretch <= 1.0:
+    """Grid lines clustered towards both ends by the tanh map
+    z(s) = tanh(stretch * s) / tanh(stretch), s uniform in [-1, 1] (the
+    reference has no tanh stretching; this is the map the benchmark
+    configurations name, with ``stretch`` its parameter: 1.05 makes the
+    end cells about 2.6 times narrower than the middle ones).  stretch <= 0
+    gives the uniform grid."""
+    if stretch <= 0.0:
         return uniform_grid(N, a, b)
     s = np.linspace(-1.0, 1.0, N + 1)
-
-    def ratio(d):
-        z = np.tanh(d * s) / np.tanh(d)
-        h = np.diff(z)
-        with np.errstate(divide="ignore", invalid="ignore"):
-            r = np.maximum(h[1:] / h[:-1], h[:-1] / h[1:])
-        return np.inf if not np.all(np.isfinite(r)) else np.max(r)
-
-    lo, hi = 1e-6, 20.0
-    if ratio(hi) < stretch:
-        raise ValueError("stretch factor too large for this N")
-    for _ in range(200):
-        mid = 0.5 * (lo + hi)
-        if ratio(mid) < stretch:
-            lo = mid
-        else:
-            hi = mid
-    z = np.tanh(hi * s) / np.tanh(hi)
+    z = np.tanh(stretch * s) / np.tanh(stretch)
+    z[0], z[-1] = -1.0, 1.0
     return a + (b - a) * (z + 1) / 2
 
 

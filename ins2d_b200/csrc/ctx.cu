@@ -921,6 +921,8 @@ struct ins2d_ens {
   cudaStream_t own_stream = nullptr, stream = nullptr;
   std::vector<ins2d_ctx *> mem;
   std::vector<double *> V, p;  // member state (owned by the member contexts' allocations)
+  std::vector<double> dt_member;  // per-member time step (0: the run's dt)
+  double dt_uploaded = -1.0;
   std::string err;
   bool fp32 = false;
   double tol2 = 0.0;
@@ -939,7 +941,6 @@ struct ins2d_ens {
   int solve_threads = 0, solve_blocks = 0;
   double tuned_ms[2] = {0.0, 0.0};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  double graph_dt[2] = {0.0, 0.0};
 };
 
 namespace {
@@ -966,7 +967,7 @@ void ens_release_graphs(ins2d_ens *e) {
 }
 
 // descriptor table, work lists and member order (largest first)
-void ens_upload(ins2d_ens *e) {
+void ens_upload(ins2d_ens *e, double dt) {
   const int n = (int)e->mem.size();
   std::vector<EnsMemberD> h(n);
   std::vector<int4> fast, gen, cells;
@@ -975,6 +976,7 @@ void ens_upload(ins2d_ens *e) {
     EnsMemberD &d = h[m];
     d = EnsMemberD{};
     d.P = c->P;
+    d.dt = e->dt_member[m] > 0.0 ? e->dt_member[m] : dt;
     d.V = e->V[m];
     d.p = e->p[m];
     d.Vs = c->Vs;
@@ -1010,6 +1012,7 @@ void ens_upload(ins2d_ens *e) {
   e->n_gen = (int)gen.size();
   e->n_cells = (int)cells.size();
   e->uploaded = true;
+  e->dt_uploaded = dt;
 }
 
 int sm_count(int device) {
@@ -1023,13 +1026,14 @@ void ens_solve(ins2d_ens *e, int which) {
                      e->solve_threads, e->solve_blocks, e->stream);
 }
 
-// one time step of every member (time_ERK.m with steady boundary conditions)
-void ens_step(ins2d_ens *e, double dt, bool k0_cached) {
+// one time step of every member (time_ERK.m with steady boundary conditions;
+// each member's dt is in its descriptor)
+void ens_step(ins2d_ens *e, bool k0_cached) {
   const ins2d_ctx *c0 = e->mem[0];
   const int s = c0->s;
   for (int i = 0; i < s; ++i) {
     if (i == 0 && k0_cached) {
-      launch_stage_cached_ens(e->d_mem, e->d_cells, e->n_cells, c0->A[0][0], 1.0 / dt, e->stream);
+      launch_stage_cached_ens(e->d_mem, e->d_cells, e->n_cells, c0->A[0][0], e->stream);
     } else {
       EnsWalk w{};
       w.mode = 0;
@@ -1043,22 +1047,20 @@ void ens_step(ins2d_ens *e, double dt, bool k0_cached) {
           ++w.nprev;
         }
       w.aii = c0->A[i][i];
-      w.inv_dt = 1.0 / dt;
       launch_walk_ens(e->d_mem, e->d_fast, e->n_fast, e->d_gen, e->n_gen, w, e->fp32, e->stream);
     }
     if (i > 0) {
-      launch_div_ens(e->d_mem, e->d_cells, e->n_cells, 0, 1.0 / dt, 1.0 / c0->c[i], e->stream);
+      launch_div_ens(e->d_mem, e->d_cells, e->n_cells, 0, 1.0 / c0->c[i], e->stream);
       ens_solve(e, 0);
     }
-    launch_project_ens(e->d_mem, e->d_cells, e->n_cells, dt, c0->c[i], i == 0 ? 1 : 0, i == s - 1 ? 1 : 0,
-                       e->stream);
+    launch_project_ens(e->d_mem, e->d_cells, e->n_cells, c0->c[i], i == 0 ? 1 : 0, i == s - 1 ? 1 : 0, e->stream);
   }
   // additional pressure solve; its residual is the next step's first stage
   EnsWalk w{};
   w.mode = 1;
   w.cache = 1;
   launch_walk_ens(e->d_mem, e->d_fast, e->n_fast, e->d_gen, e->n_gen, w, e->fp32, e->stream);
-  launch_div_ens(e->d_mem, e->d_cells, e->n_cells, 1, 0.0, 1.0, e->stream);
+  launch_div_ens(e->d_mem, e->d_cells, e->n_cells, 1, 1.0, e->stream);
   ens_solve(e, 1);
 }
 
@@ -1172,6 +1174,7 @@ int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_des
           CK(cudaMemcpy(dm, &c->mg, sizeof(MgD), cudaMemcpyHostToDevice));
         }
         e->d_mg.push_back(dm);
+        e->dt_member.push_back(0.0);
       }
       CK(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking));
       e->stream = e->own_stream;
@@ -1247,6 +1250,13 @@ int ins2d_ens_get_state(ins2d_ens *e, int32_t m, double *V, double *p, int mem) 
   ENS_END
 }
 
+int ins2d_ens_set_member_dt(ins2d_ens *e, int32_t m, double dt) {
+  if (!e || m < 0 || m >= (int32_t)e->mem.size() || !(dt >= 0.0)) return INS2D_EINVAL;
+  e->dt_member[m] = dt;
+  e->uploaded = false;
+  return INS2D_OK;
+}
+
 int ins2d_ens_state_ptr(ins2d_ens *e, int32_t m, double **V, double **p) {
   if (!e || m < 0 || m >= (int32_t)e->mem.size() || !V || !p) return INS2D_EINVAL;
   *V = e->V[m];
@@ -1259,7 +1269,7 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
   (void)t;  // steady boundary conditions: the step does not depend on t
   if (nsteps < 0 || !(dt > 0)) return ens_fail(e, INS2D_EINVAL, "erk_run: bad argument");
   const int n = (int)e->mem.size();
-  if (!e->uploaded) ens_upload(e);
+  if (!e->uploaded || e->dt_uploaded != dt) ens_upload(e, dt);
   CK(cudaMemsetAsync(e->d_stats, 0, n * sizeof(EnsStats), e->stream));
   for (int k = 0; k < nsteps; ++k) {
     const int g = k > 0 ? 1 : 0;  // graph 1: first stage from the cached residual
@@ -1270,7 +1280,7 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
       // statistics are kept
       e->solve_threads = 512;
       e->solve_blocks = std::min(n, sm_count(e->device));
-      ens_step(e, dt, g == 1);
+      ens_step(e, g == 1);
       std::vector<EnsStats> keep(n);
       CK(cudaMemcpyAsync(keep.data(), e->d_stats, n * sizeof(EnsStats), cudaMemcpyDeviceToHost, e->stream));
       CK(cudaStreamSynchronize(e->stream));
@@ -1279,19 +1289,18 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
       CK(cudaStreamSynchronize(e->stream));
       continue;
     }
-    if (!e->graph[g] || e->graph_dt[g] != dt) {
+    if (!e->graph[g]) {
       if (e->graph[g]) {
         cudaGraphExecDestroy(e->graph[g]);
         e->graph[g] = nullptr;
       }
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-      ens_step(e, dt, g == 1);
+      ens_step(e, g == 1);
       CK(cudaStreamEndCapture(e->stream, &gr));
       cudaError_t ie = cudaGraphInstantiate(&e->graph[g], gr, 0);
       cudaGraphDestroy(gr);
       CK(ie);
-      e->graph_dt[g] = dt;
     }
     CK(cudaGraphLaunch(e->graph[g], e->stream));
   }

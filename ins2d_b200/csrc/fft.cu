@@ -26,7 +26,7 @@ namespace {
 #define INS2D_FFT_COLS_MINB 1
 #endif
 #ifndef INS2D_FFT_COLS_BUDGET
-#define INS2D_FFT_COLS_BUDGET 72  // KB of shared memory per column block
+#define INS2D_FFT_COLS_BUDGET 80  // KB of shared memory per column block (two 2048-point columns)
 #endif
 #ifndef INS2D_FFT_COLS_G
 #define INS2D_FFT_COLS_G 2

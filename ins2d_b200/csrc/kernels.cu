@@ -162,7 +162,7 @@ __device__ __forceinline__ void copy_ops(DevOps *dst, const DevOps *src) {
 }
 
 __global__ void __launch_bounds__(256) k_div_ens(const EnsMemberD *__restrict__ mem, const int4 *__restrict__ tiles,
-                                                int mode, double alpha, double gamma) {
+                                                int mode, double gamma) {
   __shared__ __align__(16) DevOps sP;
   const int4 t = tiles[blockIdx.x];
   const EnsMemberD &M = mem[t.x];
@@ -171,25 +171,26 @@ __global__ void __launch_bounds__(256) k_div_ens(const EnsMemberD *__restrict__ 
   const int i = t.y * BX + threadIdx.x, j = t.z * BY + threadIdx.y;
   if (i < sP.Npx && j < sP.Npy)
     M.f[(long long)j * sP.Npx + i] =
-        mode == 0 ? div_cell(sP, M.Wt, alpha, 0.0, gamma, i, j) : div_cell(sP, M.wres, 0.0, 0.0, 1.0, i, j);
+        mode == 0 ? div_cell(sP, M.Wt, 1.0 / M.dt, 0.0, gamma, i, j) : div_cell(sP, M.wres, 0.0, 0.0, 1.0, i, j);
 }
 
 __global__ void __launch_bounds__(256) k_project_ens(const EnsMemberD *__restrict__ mem,
-                                                    const int4 *__restrict__ tiles, double dt, double c, int from_p,
+                                                    const int4 *__restrict__ tiles, double c, int from_p,
                                                     int last) {
   __shared__ __align__(16) DevOps sP;
   const int4 t = tiles[blockIdx.x];
   const EnsMemberD &M = mem[t.x];
   copy_ops(&sP, &M.P);
   __syncthreads();
-  project_cell(sP, M.Wt, from_p ? M.p : M.dp, dt, c, last ? M.V : M.Vs, t.y * BX + threadIdx.x,
+  project_cell(sP, M.Wt, from_p ? M.p : M.dp, M.dt, c, last ? M.V : M.Vs, t.y * BX + threadIdx.x,
                t.z * BY + threadIdx.y);
 }
 
 __global__ void __launch_bounds__(256) k_stage_cached_ens(const EnsMemberD *__restrict__ mem,
-                                                         const int4 *__restrict__ tiles, double aii, double inv_dt) {
+                                                         const int4 *__restrict__ tiles, double aii) {
   const int4 t = tiles[blockIdx.x];
   const EnsMemberD &M = mem[t.x];
+  const double inv_dt = 1.0 / M.dt;
   const int i = t.y * BX + threadIdx.x, j = t.z * BY + threadIdx.y;
   const DevOps &P = M.P;
   if (i < P.Nux && j < P.Nuy) {
@@ -267,19 +268,17 @@ void cell_tiles(const DevOps &P, int member, std::vector<int4> &out) {
     for (int bx = 0; bx < (nx + BX - 1) / BX; ++bx) out.push_back(make_int4(member, bx, by, 0));
 }
 
-void launch_div_ens(const EnsMemberD *mem, const int4 *tiles, int n, int mode, double alpha, double gamma,
-                    cudaStream_t s) {
-  if (n > 0) k_div_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, mode, alpha, gamma);
+void launch_div_ens(const EnsMemberD *mem, const int4 *tiles, int n, int mode, double gamma, cudaStream_t s) {
+  if (n > 0) k_div_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, mode, gamma);
 }
 
-void launch_project_ens(const EnsMemberD *mem, const int4 *tiles, int n, double dt, double c, int from_p, int last,
+void launch_project_ens(const EnsMemberD *mem, const int4 *tiles, int n, double c, int from_p, int last,
                         cudaStream_t s) {
-  if (n > 0) k_project_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, dt, c, from_p, last);
+  if (n > 0) k_project_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, c, from_p, last);
 }
 
-void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, double aii, double inv_dt,
-                             cudaStream_t s) {
-  if (n > 0) k_stage_cached_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, aii, inv_dt);
+void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, double aii, cudaStream_t s) {
+  if (n > 0) k_stage_cached_ens<<<n, dim3(BX, BY), 0, s>>>(mem, tiles, aii);
 }
 
 }  // namespace ins2d

@@ -70,12 +70,12 @@ void launch_add(const double *x, double *y, long long n, cudaStream_t s);
 struct PcgWork;
 struct EnsMemberD;
 // Stage (mode 0) or additional-solve residual (mode 1) walker arguments shared
-// by all members (same Butcher tableau and dt).
+// by all members (same Butcher tableau; each member's dt is in its descriptor).
 struct EnsWalk {
   int mode, stage, store, use_vs, nprev, cache;
   int kidx[kMaxStages];
   double aprev[kMaxStages];
-  double aii, inv_dt;
+  double aii;
 };
 // Host: the walker tiles {member, bx, by, 0} of one member, split into fast
 // (interior) and generic tiles.
@@ -85,16 +85,14 @@ void launch_walk_ens(const EnsMemberD *mem, const int4 *fast, int nfast, const i
 // Host: the 32x8 cell tiles {member, bx, by, 0} covering a member's u, v and p
 // index spaces.
 void cell_tiles(const DevOps &P, int member, std::vector<int4> &out);
-// f = (M Wt + alpha yM) gamma (mode 0, stage) or f = M wres (mode 1, residual)
-void launch_div_ens(const EnsMemberD *mem, const int4 *tiles, int n, int mode, double alpha, double gamma,
-                    cudaStream_t s);
+// f = (M Wt + yM/dt) gamma (mode 0, stage) or f = M wres (mode 1, residual)
+void launch_div_ens(const EnsMemberD *mem, const int4 *tiles, int n, int mode, double gamma, cudaStream_t s);
 // V_out = dt (Wt - c Om^-1 G dp_src); dp_src = p (from_p) or dp; V_out = V
 // (last stage) or Vs
-void launch_project_ens(const EnsMemberD *mem, const int4 *tiles, int n, double dt, double c, int from_p, int last,
+void launch_project_ens(const EnsMemberD *mem, const int4 *tiles, int n, double c, int from_p, int last,
                         cudaStream_t s);
 // Wt = V/dt + aii kV[0] (first stage from the cached residual)
-void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, double aii, double inv_dt,
-                             cudaStream_t s);
+void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, double aii, cudaStream_t s);
 
 // --- FFT Poisson (fft.cu) -------------------------------------------------------
 struct FftPlan {
@@ -135,6 +133,7 @@ void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, c
 
 struct EnsMemberD {
   DevOps P;
+  double dt;  // this member's time step
   double *V, *p, *Vs, *Wt, *kV[kMaxStages], *f, *dp, *wres;
   PcgWork W;
   const MgD *mg;  // device copy of the member's hierarchy, or null (Jacobi)

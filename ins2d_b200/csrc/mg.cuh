@@ -360,6 +360,27 @@ __device__ inline void mg_coarse(const MgD &M, const double *__restrict__ b, dou
   }
 }
 
+// Optional per-phase clock counters (timing builds only: -DINS2D_MG_TIMING)
+#ifdef INS2D_MG_TIMING
+static __device__ unsigned long long g_mg_clk[128];
+#define MG_T0() long long _mg_t0 = clock64()
+#define MG_TICK(k)                                                        \
+  do {                                                                    \
+    if (threadIdx.x == 0) {                                               \
+      const long long _t1 = clock64();                                    \
+      atomicAdd(&g_mg_clk[(k) & 127], (unsigned long long)(_t1 - _mg_t0)); \
+      _mg_t0 = _t1;                                                       \
+    }                                                                     \
+  } while (0)
+#else
+#define MG_T0() \
+  do {          \
+  } while (0)
+#define MG_TICK(k) \
+  do {             \
+  } while (0)
+#endif
+
 // Result location of a V-cycle at level l: the relaxed copy t (levels above
 // the coarsest) or x (the coarsest).
 __device__ __forceinline__ double *mg_result(const MgD &M, int l) {
@@ -372,27 +393,35 @@ __device__ __forceinline__ double *mg_result(const MgD &M, int l) {
 __device__ inline void mg_vcycle_block(const MgD &M, const double *__restrict__ b0, int l0 = 0) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int nl = M.nlev;
+  MG_T0();
   for (int l = l0; l < nl - 1; ++l) {
     const MgLevelD &L = M.L[l];
     const double *b = (l == l0) ? b0 : L.b;
     mg_xline(L, b, nullptr, L.x, M.omega, tid, nt);
     __syncthreads();
+    MG_TICK(l * 8 + 0);
     mg_yline(L, b, L.x, L.t, M.omega, tid, nt);
     __syncthreads();
+    MG_TICK(l * 8 + 1);
     mg_restrict(L, M.L[l + 1], b, L.t, M.L[l + 1].b, tid, nt);
     __syncthreads();
+    MG_TICK(l * 8 + 2);
   }
   mg_coarse(M, (l0 == nl - 1) ? b0 : M.L[nl - 1].b, M.L[nl - 1].x, tid, nt);
   __syncthreads();
+  MG_TICK((nl - 1) * 8 + 3);
   for (int l = nl - 2; l >= l0; --l) {
     const MgLevelD &L = M.L[l];
     const double *b = (l == l0) ? b0 : L.b;
     mg_prolong(L, M.L[l + 1], L.t, mg_result(M, l + 1), M.alpha, tid, nt);
     __syncthreads();
+    MG_TICK(l * 8 + 4);
     mg_yline(L, b, L.t, L.x, M.omega, tid, nt);
     __syncthreads();
+    MG_TICK(l * 8 + 5);
     mg_xline(L, b, L.x, L.t, M.omega, tid, nt);
     __syncthreads();
+    MG_TICK(l * 8 + 6);
   }
 }
 

@@ -280,6 +280,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
     done = true;
   }
   const int op5[5] = {R_SUM, R_SUM, R_MAX, R_MIN, R_MAX};
+  MG_T0();
   while (!done) {
     double a1[1] = {0.0};
     for (long long k = tid; k < Np; k += nt) {
@@ -289,6 +290,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
       a1[0] += p[k] * aq;
     }
     block_reduce<1>(a1, op1, (double(*)[1])sh);
+    MG_TICK(120);
     const double pq = a1[0];
     if (!isfinite(pq)) {
       status = INS2D_ENONFINITE;
@@ -313,6 +315,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
       a5[4] = fmax(a5[4], fabs(rv));
     }
     block_reduce<5>(a5, op5, (double(*)[5])sh);
+    MG_TICK(121);
     ++it;
     rr = a5[0] / rr0;
     maxx = a5[2];
@@ -329,11 +332,14 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
     }
     double rz_new = a5[1];
     if (MG) {
+      MG_TICK(124);
       mg_vcycle_block(*M, r);
+      MG_TICK(125);
       double b1[1] = {0.0};
       for (long long k = tid; k < Np; k += nt) b1[0] += r[k] * z[k];
       block_reduce<1>(b1, op1, (double(*)[1])sh);
       rz_new = b1[0];
+      MG_TICK(122);
     }
     if (!isfinite(rz_new)) {
       status = INS2D_ENONFINITE;
@@ -347,6 +353,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
       p[k] = zv + beta * p[k];
     }
     __syncthreads();
+    MG_TICK(123);
   }
   if (status == 0)
     for (long long k = tid; k < Np; k += nt) dp[k] = accumulate ? dp[k] + x[k] : x[k];
@@ -445,6 +452,17 @@ void pcg_solve_block(const DevOps &P, const PcgWork &W, const double *f, double 
                      bool accumulate, cudaStream_t s) {
   k_pcg_block<<<1, kBlockThreads, 0, s>>>(P, W, f, dp, tol * tol, maxit, accumulate ? 1 : 0);
 }
+
+#ifdef INS2D_MG_TIMING
+extern "C" int ins2d_debug_mg_clocks(unsigned long long out[128], int reset) {
+  if (cudaMemcpyFromSymbol(out, g_mg_clk, sizeof(unsigned long long) * 128) != cudaSuccess) return 1;
+  if (reset) {
+    static const unsigned long long z[128] = {};
+    cudaMemcpyToSymbol(g_mg_clk, z, sizeof z);
+  }
+  return 0;
+}
+#endif
 
 void pcg_solve_block_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double *dp, double tol,
                         long long maxit, bool accumulate, cudaStream_t s) {

@@ -556,7 +556,7 @@ __device__ __forceinline__ const double *ens_epi(const EnsMemberD &M, const EnsW
     }
     e.nprev = w.nprev;
     e.aii = w.aii;
-    e.inv_dt = w.inv_dt;
+    e.inv_dt = 1.0 / M.dt;
     e.Wt = M.Wt;
     return w.use_vs ? M.Vs : M.V;
   }

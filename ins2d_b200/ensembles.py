@@ -36,8 +36,21 @@ def random_members(n, seed=4, sizes=(64, 96, 128, 192, 256), stretch=1.05, Re_ra
             kw = dict(x=x, y=y, BC=cases.BC_CHANNEL, Re=Re,
                       uBC=cases.channel_uBC(lambda yy, U=U: U * (1.0 - 4.0 * np.asarray(yy) ** 2)))
         kw.update(poisson=4, CG_acc=CG_acc, CG_maxit=CG_maxit, RK=RK, precision=precision)
+        kw["_U"] = U
         out.append(kw)
     return out
+
+
+def stable_dt(kw, U, safety=0.8):
+    """Explicit RK4 step limit of a member: the diffusive eigenvalue bound
+    (4/Re)(1/hx^2 + 1/hy^2) against RK4's real-axis reach 2.78 plus the
+    convective bound U(1/hx + 1/hy) against its imaginary-axis reach 2.83,
+    with the smallest cell widths."""
+    hx = np.min(np.diff(kw["x"]))
+    hy = np.min(np.diff(kw["y"]))
+    lam_d = 4.0 / kw["Re"] * (1.0 / hx ** 2 + 1.0 / hy ** 2)
+    lam_c = U * (1.0 / hx + 1.0 / hy)
+    return safety / (lam_d / 2.78 + lam_c / 2.83)
 
 
 def member_cost(kw):
