@@ -404,11 +404,34 @@ def run_ensemble(args, wl, rank, world, local_rank):
 
 
 def cpu_baseline(wl, budget_s=25.0, steps=None):
-    """The oracle port (scipy/numpy restatement of the reference algorithm)
-    timed on the host on a bounded sample: RK44 steps of the same workload."""
+    """The reference algorithm on the host cores, on a bounded sample (RK44
+    steps of the same workload).  Periodic FFT workloads: the OpenMP C
+    restatement oracle/erk_periodic.c on all host threads (checked against the
+    scipy restatement in tests/test_oracle_pins.py); other workloads: the
+    scipy/numpy restatement (single-threaded sparse matvecs, cg.F's DIC-PCG in
+    C)."""
     from oracle import ins2d_ref as R
     from ins2d_b200 import cases
     N, L = wl["N"], wl["L"]
+    rng = np.random.default_rng(0)
+    dt = wl.get("dt", 1e-4)
+    if wl.get("poisson") == 6 and wl["ic"] in ("turbulence", "tg"):
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        V = 0.1 * rng.standard_normal(2 * N * N)
+        p = np.zeros(N * N)
+        R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, 1, threads=threads)  # warm-up (page-in)
+        n = 0
+        t0 = time.perf_counter()
+        while True:
+            V, p = R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, 1, threads=threads)
+            n += 1
+            el = time.perf_counter() - t0
+            if (steps is not None and n >= steps) or (steps is None and (el > budget_s or n >= 50)):
+                break
+        return {"value": N * N * n / el, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                "sample": f"{n} RK44 step(s) of the {N}x{N} periodic workload with the OpenMP C restatement "
+                          f"of the reference algorithm (oracle/erk_periodic.c, FFT pressure solve), "
+                          f"{threads} threads; random initial velocity (timing sample)"}
     x = cases.uniform_grid(N, 0.0, L)
     bc = cases.BC_CAVITY if wl["ic"] == "rest" else cases.BC_PERIODIC
     uBC = cases.lid_uBC(1.0, L) if wl["ic"] == "rest" else None
@@ -418,7 +441,6 @@ def cpu_baseline(wl, budget_s=25.0, steps=None):
                        CG_maxit=100000, uBC=uBC, RK="RK44")
     setup_s = time.perf_counter() - t0
     g = o.grid
-    rng = np.random.default_rng(0)
     if wl["ic"] == "rest":
         V = np.zeros(g.NV)
     elif wl["ic"] == "tg":
@@ -426,7 +448,6 @@ def cpu_baseline(wl, budget_s=25.0, steps=None):
     else:
         V = R.initial_projection(0.1 * rng.standard_normal(g.NV), 0.0, o)
     p = np.zeros(g.Np)
-    dt = wl.get("dt", 1e-4)
     n = 0
     t0 = time.perf_counter()
     while True:
@@ -435,10 +456,33 @@ def cpu_baseline(wl, budget_s=25.0, steps=None):
         el = time.perf_counter() - t0
         if (steps is not None and n >= steps) or (steps is None and (el > budget_s or n >= 50)):
             break
-    cores = 1
-    return {"value": g.Npx * g.Npy * n / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+    return {"value": g.Npx * g.Npy * n / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
             "sample": f"{n} RK44 step(s) of the {N}x{N} workload with the scipy/numpy restatement "
-                      f"(sparse matvecs single-threaded; operator setup {setup_s:.1f}s excluded)"}
+                      f"(sparse matvecs single-threaded, cg.F's DIC-PCG in C; operator setup "
+                      f"{setup_s:.1f}s excluded)"}
+
+
+def ensemble_cpu_baseline(wl, nmembers=2, steps=2):
+    """The scipy restatement on a bounded sample of the ensemble: the first
+    members of the same seeded ensemble, a few RK44 steps each."""
+    from oracle import ins2d_ref as R
+    from ins2d_b200 import ensembles
+    members = ensembles.random_members(nmembers, seed=4, sizes=wl["sizes"], stretch=wl["stretch"],
+                                       CG_acc=wl["CG_acc"])
+    cells, el = 0, 0.0
+    for kw in members:
+        o = R.make_options(kw["x"], kw["y"], kw["BC"], Re=kw["Re"], poisson=4, CG_acc=kw["CG_acc"],
+                           CG_maxit=100000, uBC=kw["uBC"], RK="RK44")
+        V, p = np.zeros(o.grid.NV), np.zeros(o.grid.Np)
+        dt = min(wl["dt"], ensembles.stable_dt(kw, kw["_U"]))
+        t0 = time.perf_counter()
+        for n in range(steps):
+            V, p = R.time_ERK(V, p, n * dt, dt, o)
+        el += time.perf_counter() - t0
+        cells += o.grid.Npx * o.grid.Npy * steps
+    return {"value": cells / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} RK44 steps of each of the first {nmembers} members with the scipy/numpy "
+                      f"restatement (cg.F's DIC-PCG in C, single-threaded)"}
 
 
 def run_reference(args, wl, rank, world):
@@ -448,7 +492,10 @@ def run_reference(args, wl, rank, world):
     # a bounded sample: the step count is capped so the whole run takes minutes
     warm = min(args.warmup, 1)
     nsteps = min(steps, 3)
-    cb = cpu_baseline(wl, budget_s=1e9, steps=warm + nsteps)
+    if wl.get("kind") == "ensemble":
+        cb = ensemble_cpu_baseline(wl)
+    else:
+        cb = cpu_baseline(wl, budget_s=1e9, steps=warm + nsteps)
     res = {
         "impl": "reference", "metric": "cell-updates/s per RK4 step incl. Poisson solve", "value": cb["value"],
         "unit": "cell-updates/s", "n_gpus": world, "steps": nsteps, "warmup": warm, "higher_is_better": True,

@@ -270,10 +270,15 @@ int ins2d_ens_state_ptr(ins2d_ens *e, int32_t m, double **V, double **p);
  * (per member, accumulated over the run) or NULL.  A member whose solve fails
  * makes the call return that status, naming the member. */
 int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_step_stats *stats);
-/* launch shape of the member solves chosen by the tuner on the first run
- * (threads per member, resident blocks) and the tuner's timings (ms of one
- * solve phase with 512 and with 256 threads per member) */
-int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[2]);
+/* form of the member solves: -1 = chosen by the tuner on the first run
+ * (default), 0 = batched across members, 256 or 512 = persistent launch with
+ * that many threads per member */
+int ins2d_ens_set_solver(ins2d_ens *e, int32_t threads);
+/* form of the member solves chosen by the tuner on the first run: threads
+ * per member of the persistent solve (512 or 256; 0 = solves batched across
+ * members, one launch per phase), its resident blocks, and the tuner's
+ * timings (ms of one solve phase for 512, 256 threads and batched) */
+int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[3]);
 
 #ifdef __cplusplus
 }

@@ -27,7 +27,7 @@ EXPORTED = [
     "ins2d_profile", "ins2d_profile_read", "ins2d_fft_poisson_noalloc",
     "ins2d_ens_create", "ins2d_ens_destroy", "ins2d_ens_last_error", "ins2d_ens_size", "ins2d_ens_member",
     "ins2d_ens_set_stream", "ins2d_ens_set_state", "ins2d_ens_get_state", "ins2d_ens_state_ptr", "ins2d_ens_set_member_dt",
-    "ins2d_ens_erk_run", "ins2d_ens_solve_shape",
+    "ins2d_ens_erk_run", "ins2d_ens_set_solver", "ins2d_ens_solve_shape",
 ]
 PROF_FAMILIES = ["stage", "div", "poisson", "project", "residual", "other"]
 
@@ -128,6 +128,7 @@ def load():
         "ins2d_ens_state_ptr": (ctypes.c_int, [vp, ctypes.c_int32, P(vp), P(vp)]),
         "ins2d_ens_set_member_dt": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_double]),
         "ins2d_ens_erk_run": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32, P(StepStats)]),
+        "ins2d_ens_set_solver": (ctypes.c_int, [vp, ctypes.c_int32]),
         "ins2d_ens_solve_shape": (ctypes.c_int, [vp, P(ctypes.c_int32), P(ctypes.c_int32), P(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():

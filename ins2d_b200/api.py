@@ -474,11 +474,17 @@ class Ensemble:
         return [dict(n_solves=s.n_solves, iters_total=s.iters_total, iters_max=s.iters_max, norm1_max=s.norm1_max)
                 for s in st]
 
+    def set_solver(self, threads):
+        """-1: tuned on the first run; 0: batched across members; 256/512:
+        persistent launch with that many threads per member."""
+        self._check(self._lib.ins2d_ens_set_solver(self._e, int(threads)))
+
     def solve_shape(self):
         th, bl = ctypes.c_int32(), ctypes.c_int32()
-        ms = (ctypes.c_double * 2)()
+        ms = (ctypes.c_double * 3)()
         self._check(self._lib.ins2d_ens_solve_shape(self._e, ctypes.byref(th), ctypes.byref(bl), ms))
-        return dict(threads=th.value, blocks=bl.value, tuned_ms={512: ms[0], 256: ms[1]})
+        return dict(threads=th.value, blocks=bl.value, batched=th.value == 0,
+                    tuned_ms={"persistent512": ms[0], "persistent256": ms[1], "batched": ms[2]})
 
 
 def _describe(x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_add_solve=1, RK="RK44",

@@ -937,9 +937,20 @@ struct ins2d_ens {
   EnsStats *d_stats = nullptr;
   std::vector<void *> allocs;
   bool uploaded = false;
-  // launch shape of the member solves (autotuned) and the step graphs
+  // batched solver (ens_pcg.cu): member levels, work segments, CG scalars
+  bool can_batch = false;
+  EnsMgD mgd{};
+  EnsMgPlan plan{};
+  int2 *d_ctiles = nullptr;
+  int n_ctiles = 0;
+  EnsCg *d_cg = nullptr;
+  int *d_active = nullptr, *h_active = nullptr;
+  // launch shape of the member solves (autotuned: 512 or 256 threads per
+  // member in the persistent solve, or 0 = batched solve) and the step graphs
   int solve_threads = 0, solve_blocks = 0;
-  double tuned_ms[2] = {0.0, 0.0};
+  int forced = -1;  // -1: tune on the first run
+  bool tuned = false;
+  double tuned_ms[3] = {0.0, 0.0, 0.0};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
 };
 
@@ -964,6 +975,113 @@ void ens_release_graphs(ins2d_ens *e) {
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
+}
+
+// Work segments, member level tables and CG scalars of the batched solver.
+void ens_build_batch(ins2d_ens *e, const std::vector<int> &order) {
+  const int n = (int)e->mem.size();
+  std::vector<MgLevelD> lev((size_t)n * kMgMaxLevels);
+  std::vector<int> nlev(n), ncoarse(n);
+  std::vector<const double *> cinv(n);
+  int lmax = 0;
+  for (int m = 0; m < n; ++m) {
+    const MgD &M = e->mem[m]->mg;
+    for (int l = 0; l < M.nlev; ++l) lev[(size_t)m * kMgMaxLevels + l] = M.L[l];
+    nlev[m] = M.nlev;
+    ncoarse[m] = M.ncoarse;
+    cinv[m] = M.cinv;
+    lmax = std::max(lmax, M.nlev);
+  }
+  MgLevelD *d_lev = ens_alloc<MgLevelD>(e, lev.size());
+  int *d_nlev = ens_alloc<int>(e, n), *d_nco = ens_alloc<int>(e, n);
+  const double **d_ci = ens_alloc<const double *>(e, n);
+  CK(cudaMemcpy(d_lev, lev.data(), lev.size() * sizeof(MgLevelD), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_nlev, nlev.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_nco, ncoarse.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_ci, cinv.data(), n * sizeof(const double *), cudaMemcpyHostToDevice));
+  e->mgd = EnsMgD{d_lev, d_nlev, d_ci, d_nco};
+  // segments: members in solve order (largest first), counts per phase
+  auto make_seg = [&](auto count) {
+    std::vector<int> mm;
+    std::vector<long long> st{0};
+    for (int m : order) {
+      const long long c = count(m);
+      if (c <= 0) continue;
+      mm.push_back(m);
+      st.push_back(st.back() + c);
+    }
+    EnsSeg sg{};
+    sg.n = (int)mm.size();
+    sg.total = st.back();
+    if (sg.n > 0) {
+      int *dm = ens_alloc<int>(e, mm.size());
+      long long *ds = ens_alloc<long long>(e, st.size());
+      CK(cudaMemcpy(dm, mm.data(), mm.size() * sizeof(int), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(ds, st.data(), st.size() * sizeof(long long), cudaMemcpyHostToDevice));
+      sg.mem = dm;
+      sg.start = ds;
+    }
+    return sg;
+  };
+  EnsMgPlan &pl = e->plan;
+  pl.lmax = lmax;
+  for (int l = 0; l < lmax - 1; ++l) {
+    auto L = [&](int m) -> const MgLevelD & { return lev[(size_t)m * kMgMaxLevels + l]; };
+    auto C = [&](int m) -> const MgLevelD & { return lev[(size_t)m * kMgMaxLevels + l + 1]; };
+    pl.xl[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).ny : 0LL; });
+    pl.yl[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).nx : 0LL; });
+    pl.rs[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)C(m).nx * C(m).ny : 0LL; });
+    pl.pr[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).nx * L(m).ny : 0LL; });
+  }
+  pl.co = make_seg([&](int m) { return (long long)ncoarse[m]; });
+  std::vector<int2> ct;
+  for (int m : order)
+    for (long long k = 0; k < e->mem[m]->P.Np; k += 256) ct.push_back(make_int2(m, (int)k));
+  e->d_ctiles = ens_alloc<int2>(e, ct.size());
+  CK(cudaMemcpy(e->d_ctiles, ct.data(), ct.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  e->n_ctiles = (int)ct.size();
+  std::vector<EnsCg> cg(n);
+  for (int m = 0; m < n; ++m) {
+    cg[m] = EnsCg{};
+    cg[m].tol2 = e->tol2;
+    cg[m].maxit = e->maxit;
+  }
+  e->d_cg = ens_alloc<EnsCg>(e, n);
+  CK(cudaMemcpy(e->d_cg, cg.data(), n * sizeof(EnsCg), cudaMemcpyHostToDevice));
+  e->d_active = ens_alloc<int>(e, 1);
+  CK(cudaMallocHost((void **)&e->h_active, sizeof(int)));
+}
+
+// All members' Poisson solves, batched across members (one launch per phase;
+// the host checks every few iterations whether any member still iterates).
+void ens_solve_batched(ins2d_ens *e, int which) {
+  const int n = (int)e->mem.size();
+  const MgD &M0 = e->mem[0]->mg;
+  const double om = M0.omega, al = M0.alpha;
+  cudaStream_t s = e->stream;
+  ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 0, s);
+  ens_cg_scalar(e->d_cg, n, 0, nullptr, s);
+  ens_vcycle(e->d_mem, e->mgd, e->d_cg, e->plan, om, al, s);
+  ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 4, s);
+  ens_cg_scalar(e->d_cg, n, 1, nullptr, s);
+  const int chunk = 4;
+  for (long long done_it = 0;; done_it += chunk) {
+    for (int k = 0; k < chunk; ++k) {
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 1, s);
+      ens_cg_scalar(e->d_cg, n, 2, nullptr, s);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 2, s);
+      ens_cg_scalar(e->d_cg, n, 3, e->d_active, s);
+      ens_vcycle(e->d_mem, e->mgd, e->d_cg, e->plan, om, al, s);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 3, s);
+      ens_cg_scalar(e->d_cg, n, 4, nullptr, s);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 5, s);
+    }
+    CK(cudaMemcpyAsync(e->h_active, e->d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (*e->h_active == 0) break;
+    if (done_it > e->maxit + 2 * chunk) throw CudaError("ensemble PCG: members still active after CG_maxit");
+  }
+  ens_cg_finish(e->d_mem, e->d_ctiles, e->n_ctiles, e->d_cg, n, which, e->d_stats, s);
 }
 
 // descriptor table, work lists and member order (largest first)
@@ -1011,6 +1129,7 @@ void ens_upload(ins2d_ens *e, double dt) {
   e->n_fast = (int)fast.size();
   e->n_gen = (int)gen.size();
   e->n_cells = (int)cells.size();
+  if (e->can_batch && !e->d_cg) ens_build_batch(e, order);
   e->uploaded = true;
   e->dt_uploaded = dt;
 }
@@ -1022,6 +1141,10 @@ int sm_count(int device) {
 }
 
 void ens_solve(ins2d_ens *e, int which) {
+  if (e->solve_threads == 0 && e->can_batch) {
+    ens_solve_batched(e, which);
+    return;
+  }
   launch_pcg_members(e->d_mem, e->d_order, (int)e->mem.size(), which, e->tol2, e->maxit, e->d_queue, e->d_stats,
                      e->solve_threads, e->solve_blocks, e->stream);
 }
@@ -1069,15 +1192,16 @@ void ens_step(ins2d_ens *e, bool k0_cached) {
 // reductions) and keeps the fastest.
 void ens_autotune(ins2d_ens *e) {
   const int sms = sm_count(e->device), n = (int)e->mem.size();
-  const int cand[2] = {512, 256};
+  const int cand[3] = {512, 256, 0};  // 0: batched across members
+  const int ncand = e->can_batch ? 3 : 2;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
   int best = -1;
   float best_ms = 0.f;
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < ncand; ++k) {
     e->solve_threads = cand[k];
-    e->solve_blocks = std::min(n, sms * (512 / cand[k]));
+    e->solve_blocks = cand[k] ? std::min(n, sms * (512 / cand[k])) : 0;
     ens_solve(e, 0);  // warm-up
     CK(cudaEventRecord(a, e->stream));
     ens_solve(e, 0);
@@ -1094,7 +1218,7 @@ void ens_autotune(ins2d_ens *e) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   e->solve_threads = cand[best];
-  e->solve_blocks = std::min(n, sms * (512 / cand[best]));
+  e->solve_blocks = cand[best] ? std::min(n, sms * (512 / cand[best])) : 0;
 }
 
 #define ENS_BEGIN                 \
@@ -1176,6 +1300,8 @@ int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_des
         e->d_mg.push_back(dm);
         e->dt_member.push_back(0.0);
       }
+      e->can_batch = true;
+      for (ins2d_ctx *c : e->mem) e->can_batch = e->can_batch && c->use_mg;
       CK(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking));
       e->stream = e->own_stream;
       CK(cudaDeviceSynchronize());
@@ -1201,6 +1327,7 @@ int ins2d_ens_destroy(ins2d_ens *e) {
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   ens_release_graphs(e);
+  if (e->h_active) cudaFreeHost(e->h_active);
   for (void *p : e->allocs) cudaFree(p);
   for (ins2d_ctx *c : e->mem) ins2d_ctx_destroy(c);
   if (e->own_stream) cudaStreamDestroy(e->own_stream);
@@ -1273,7 +1400,7 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
   CK(cudaMemsetAsync(e->d_stats, 0, n * sizeof(EnsStats), e->stream));
   for (int k = 0; k < nsteps; ++k) {
     const int g = k > 0 ? 1 : 0;  // graph 1: first stage from the cached residual
-    if (e->solve_threads == 0) {
+    if (e->forced < 0 && !e->tuned) {
       // first use: one direct step, then tune the solve launch on the
       // right-hand side it left behind (re-solving it changes no state: the
       // tuner writes dp, which every stage overwrites); the step's
@@ -1285,8 +1412,13 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
       CK(cudaMemcpyAsync(keep.data(), e->d_stats, n * sizeof(EnsStats), cudaMemcpyDeviceToHost, e->stream));
       CK(cudaStreamSynchronize(e->stream));
       ens_autotune(e);
+      e->tuned = true;
       CK(cudaMemcpyAsync(e->d_stats, keep.data(), n * sizeof(EnsStats), cudaMemcpyHostToDevice, e->stream));
       CK(cudaStreamSynchronize(e->stream));
+      continue;
+    }
+    if (e->solve_threads == 0) {  // batched solves poll the host: no graph
+      ens_step(e, g == 1);
       continue;
     }
     if (!e->graph[g]) {
@@ -1326,14 +1458,27 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
   ENS_END
 }
 
-int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[2]) {
+int ins2d_ens_set_solver(ins2d_ens *e, int32_t threads) {
+  if (!e || !(threads == -1 || threads == 0 || threads == 256 || threads == 512)) return INS2D_EINVAL;
+  if (threads == 0 && !e->can_batch) return ens_fail(e, INS2D_EINVAL, "batched solves need the multigrid preconditioner");
+  e->forced = threads;
+  if (threads >= 0) {
+    e->solve_threads = threads;
+    e->solve_blocks = threads ? std::min((int)e->mem.size(), sm_count(e->device) * (512 / threads)) : 0;
+  } else {
+    e->solve_threads = 0;
+    e->solve_blocks = 0;
+  }
+  ens_release_graphs(e);
+  return INS2D_OK;
+}
+
+int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[3]) {
   if (!e) return INS2D_EINVAL;
   if (threads) *threads = e->solve_threads;
   if (blocks) *blocks = e->solve_blocks;
-  if (tuned_ms) {
-    tuned_ms[0] = e->tuned_ms[0];
-    tuned_ms[1] = e->tuned_ms[1];
-  }
+  if (tuned_ms)
+    for (int k = 0; k < 3; ++k) tuned_ms[k] = e->tuned_ms[k];
   return INS2D_OK;
 }
 

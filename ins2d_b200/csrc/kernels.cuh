@@ -144,6 +144,44 @@ struct EnsStats {
   double norm1_max;
   int status, pad;
 };
+// --- batched ensemble solves (ens_pcg.cu) ----------------------------------
+// per-member CG scalars and accumulators
+struct EnsCg {
+  double acc_pq, acc_rr, acc_rz, maxf;
+  double rz, rr0, rr, alpha, beta, tol2;
+  long long it, maxit;
+  int done, status;
+};
+// members' multigrid levels: lev[m * kMgMaxLevels + l]
+struct EnsMgD {
+  const MgLevelD *lev;
+  const int *nlev;
+  const double *const *cinv;
+  const int *ncoarse;
+};
+// work of one phase over members: member mem[s] owns global work indices
+// [start[s], start[s+1]); total = start[n]
+struct EnsSeg {
+  const int *mem;
+  const long long *start;
+  int n;
+  long long total;
+};
+struct EnsMgPlan {
+  int lmax = 0;
+  EnsSeg xl[kMgMaxLevels], yl[kMgMaxLevels], rs[kMgMaxLevels], pr[kMgMaxLevels];
+  EnsSeg co{};
+};
+void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const EnsMgPlan &pl, double omega,
+                double alpha, cudaStream_t s);
+// op 0 init (x = 0, r = f), 1 q = A p, 2 x/r update, 3 r'z, 4 r'z with p = z, 5 p update
+void ens_cg_vec(const EnsMemberD *mem, const EnsMgD &G, const int2 *tiles, int ntiles, EnsCg *cg, int op,
+                cudaStream_t s);
+// op 0 after init, 1 first r'z, 2 alpha, 3 convergence, 4 beta; *active = members still iterating
+void ens_cg_scalar(EnsCg *cg, int n, int op, int *active, cudaStream_t s);
+void ens_cg_finish(const EnsMemberD *mem, const int2 *tiles, int ntiles, EnsCg *cg, int n, int which,
+                   EnsStats *stats, cudaStream_t s);
+
 // Poisson solves of all members in one persistent launch: each thread block
 // takes the next member of `order` from a device queue and runs the whole
 // PCG (pcg_block_body).  which = 0: f -> dp; which = 1: p += solve(f)

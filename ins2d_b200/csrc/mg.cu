@@ -82,8 +82,10 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
   for (int l = 0; l < lt; ++l) {
     const MgLevelD &L = M.L[l];
     const double *b = (l == 0) ? r0 : L.b;
-    k_mg_xline<<<blocks_for(L.ny, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x, M.omega, done);
-    k_mg_yline<<<blocks_for(L.nx, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t, M.omega, done);
+    k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x,
+                                                                                                  M.omega, done);
+    k_mg_yline<<<blocks_for((long long)L.nx * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
+                                                                                                  M.omega, done);
     const MgLevelD &C = M.L[l + 1];
     k_mg_restrict<<<blocks_for((long long)C.nx * C.ny, 256), 256, 0, s>>>(L, C, b, L.t, C.b, done);
   }
@@ -95,8 +97,10 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     k_mg_prolong<<<blocks_for((long long)L.nx * L.ny, 256), 256, 0, s>>>(L, C, L.t,
                                                                          (l + 1 == M.nlev - 1) ? C.x : C.t,
                                                                          M.alpha, done);
-    k_mg_yline<<<blocks_for(L.nx, kLineThreads), kLineThreads, 0, s>>>(L, b, L.t, L.x, M.omega, done);
-    k_mg_xline<<<blocks_for(L.ny, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t, M.omega, done);
+    k_mg_yline<<<blocks_for((long long)L.nx * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.t, L.x,
+                                                                                                  M.omega, done);
+    k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
+                                                                                                  M.omega, done);
   }
 }
 

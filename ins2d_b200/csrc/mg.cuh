@@ -268,57 +268,150 @@ static __device__ MG_LINE_ATTR void mg_line(const MgLine ln, const double *__res
   }
 }
 
-// x-line relaxation of rows j0, j0+js, ...
-__device__ inline void mg_xline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
-                                double *__restrict__ xnew, double omega, int j0, int js) {
+__device__ __forceinline__ MgLine mg_make_xline(const MgLevelD &L, int j) {
   const int nx = L.nx, ny = L.ny;
-  for (int j = j0; j < ny; j += js) {
-    MgLine ln;
-    ln.base = (long long)j * nx;
-    ln.st = 1;
-    ln.lo = (long long)(mg_wrap_lo(j, ny, L.pery) - j) * nx;
-    ln.hi = (long long)(mg_wrap_hi(j, ny, L.pery) - j) * nx;
-    ln.n = nx;
-    ln.cross_w = L.hx;
-    ln.cm = L.ym[j];
-    ln.cp = L.yp[j];
-    ln.am = L.xm;
-    ln.ascale = L.hy[j];
-    ln.fi = L.fxi;
-    ln.fc = L.fxc;
-    ln.cyc = L.perx && nx >= 3;
-    ln.z = L.zx;
-    ln.g = ln.cyc ? L.gx[j] : 0.0;
-    ln.k = ln.cyc ? L.kx[j] : 0.0;
-    mg_line(ln, b, xold, xnew, omega);
+  MgLine ln;
+  ln.base = (long long)j * nx;
+  ln.st = 1;
+  ln.lo = (long long)(mg_wrap_lo(j, ny, L.pery) - j) * nx;
+  ln.hi = (long long)(mg_wrap_hi(j, ny, L.pery) - j) * nx;
+  ln.n = nx;
+  ln.cross_w = L.hx;
+  ln.cm = L.ym[j];
+  ln.cp = L.yp[j];
+  ln.am = L.xm;
+  ln.ascale = L.hy[j];
+  ln.fi = L.fxi;
+  ln.fc = L.fxc;
+  ln.cyc = L.perx && nx >= 3;
+  ln.z = L.zx;
+  ln.g = ln.cyc ? L.gx[j] : 0.0;
+  ln.k = ln.cyc ? L.kx[j] : 0.0;
+  return ln;
+}
+__device__ __forceinline__ MgLine mg_make_yline(const MgLevelD &L, int i) {
+  const int nx = L.nx, ny = L.ny;
+  MgLine ln;
+  ln.base = i;
+  ln.st = nx;
+  ln.lo = mg_wrap_lo(i, nx, L.perx) - i;
+  ln.hi = mg_wrap_hi(i, nx, L.perx) - i;
+  ln.n = ny;
+  ln.cross_w = L.hy;
+  ln.cm = L.xm[i];
+  ln.cp = L.xp[i];
+  ln.am = L.ym;
+  ln.ascale = L.hx[i];
+  ln.fi = L.fyi;
+  ln.fc = L.fyc;
+  ln.cyc = L.pery && ny >= 3;
+  ln.z = L.zy;
+  ln.g = ln.cyc ? L.gy[i] : 0.0;
+  ln.k = ln.cyc ? L.ky[i] : 0.0;
+  return ln;
+}
+
+// One line solved by a whole warp: the Thomas recurrences are first-order
+// linear (forward d_q = al_q d_{q-1} + be_q with al = -a/pivot, be = rhs/pivot;
+// backward x_q = -c'_q x_{q+1} + d_q), so each chunk of 32 cells is one
+// warp-wide scan of affine maps (5 shuffle steps) carried from chunk to chunk.
+// The dependent chain is n/32 chunk steps instead of n cell steps, and the
+// loads of a chunk are coalesced along x-lines.  All 32 lanes must call it.
+static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const double *__restrict__ b,
+                                                    const double *__restrict__ xold, double *__restrict__ xnew,
+                                                    double omega) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int n = ln.n;
+  const long long base = ln.base, st = ln.st;
+  const bool hasold = xold != nullptr, cyc = ln.cyc;
+  double carry = 0.0;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int q = c0 + lane;
+    const long long k = base + (long long)q * st;
+    double A = 1.0, B = 0.0;
+    if (q < n) {
+      double rhs = b[k];
+      if (hasold) rhs += ln.cross_w[q] * (ln.cm * xold[k + ln.lo] + ln.cp * xold[k + ln.hi]);
+      const double f = ln.fi[k];
+      A = (q > 0) ? (ln.ascale * ln.am[q]) * f : 0.0;
+      B = rhs * f;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double Ap = __shfl_up_sync(FULL, A, off), Bp = __shfl_up_sync(FULL, B, off);
+      if (lane >= off) {
+        B = A * Bp + B;
+        A = A * Ap;
+      }
+    }
+    const double d = A * carry + B;
+    if (q < n) xnew[k] = d;
+    carry = __shfl_sync(FULL, d, 31);
+  }
+  carry = 0.0;
+  for (int c0 = ((n - 1) >> 5) << 5; c0 >= 0; c0 -= 32) {
+    const int q = c0 + lane;
+    const long long k = base + (long long)q * st;
+    double A = 1.0, B = 0.0;
+    if (q < n) {
+      A = -ln.fc[k];
+      B = xnew[k];
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double An = __shfl_down_sync(FULL, A, off), Bn = __shfl_down_sync(FULL, B, off);
+      if (lane + off < 32) {
+        B = A * Bn + B;
+        A = A * An;
+      }
+    }
+    const double x = A * carry + B;
+    carry = __shfl_sync(FULL, x, 0);
+    if (q < n) {
+      if (cyc)
+        xnew[k] = x;
+      else
+        xnew[k] = hasold ? (1.0 - omega) * xold[k] + omega * x : omega * x;
+    }
+  }
+  if (cyc) {
+    __syncwarp();
+    const double s = (xnew[base] + ln.g * xnew[base + (long long)(n - 1) * st]) * ln.k;
+    __syncwarp();
+    for (int q = lane; q < n; q += 32) {
+      const long long k = base + (long long)q * st;
+      const double v = xnew[k] - s * ln.z[k];
+      xnew[k] = hasold ? (1.0 - omega) * xold[k] + omega * v : omega * v;
+    }
   }
 }
 
-// y-line relaxation of columns i0, i0+is, ... (coalesced across threads)
+// Line relaxations: x-lines are the rows, y-lines the columns of a level.
+// With INS2D_MG_WARP_LINES (default) a warp solves each line (first = warp
+// index, step = warps); otherwise a thread (first = thread index, step =
+// threads).
+#ifndef INS2D_MG_WARP_LINES
+#define INS2D_MG_WARP_LINES 1
+#endif
+__device__ inline void mg_xline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
+                                double *__restrict__ xnew, double omega, int j0, int js) {
+#if INS2D_MG_WARP_LINES
+  for (int j = j0 >> 5; j < L.ny; j += (js + 31) >> 5) mg_line_warp(mg_make_xline(L, j), b, xold, xnew, omega);
+#else
+  for (int j = j0; j < L.ny; j += js) mg_line(mg_make_xline(L, j), b, xold, xnew, omega);
+#endif
+}
 __device__ inline void mg_yline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
                                 double *__restrict__ xnew, double omega, int i0, int is) {
-  const int nx = L.nx, ny = L.ny;
-  for (int i = i0; i < nx; i += is) {
-    MgLine ln;
-    ln.base = i;
-    ln.st = nx;
-    ln.lo = mg_wrap_lo(i, nx, L.perx) - i;
-    ln.hi = mg_wrap_hi(i, nx, L.perx) - i;
-    ln.n = ny;
-    ln.cross_w = L.hy;
-    ln.cm = L.xm[i];
-    ln.cp = L.xp[i];
-    ln.am = L.ym;
-    ln.ascale = L.hx[i];
-    ln.fi = L.fyi;
-    ln.fc = L.fyc;
-    ln.cyc = L.pery && ny >= 3;
-    ln.z = L.zy;
-    ln.g = ln.cyc ? L.gy[i] : 0.0;
-    ln.k = ln.cyc ? L.ky[i] : 0.0;
-    mg_line(ln, b, xold, xnew, omega);
-  }
+#if INS2D_MG_WARP_LINES
+  for (int i = i0 >> 5; i < L.nx; i += (is + 31) >> 5) mg_line_warp(mg_make_yline(L, i), b, xold, xnew, omega);
+#else
+  for (int i = i0; i < L.nx; i += is) mg_line(mg_make_yline(L, i), b, xold, xnew, omega);
+#endif
 }
+// lines per launch thread: 32 with warp lines, else 1
+constexpr int kMgLineThreads = INS2D_MG_WARP_LINES ? 32 : 1;
 
 // bc = P' (b - A x) over the coarse cells k0, k0+ks, ...
 __device__ inline void mg_restrict(const MgLevelD &F, const MgLevelD &Cl, const double *__restrict__ b,

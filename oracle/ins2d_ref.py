@@ -851,6 +851,40 @@ class CGNotConverged(RuntimeError):
     pass
 
 
+def erk_periodic_c(V, p, Nx, Ny, Lx, Ly, Re, dt, nsteps, RK="RK44", threads=0):
+    """oracle/erk_periodic.c: the same explicit RK steps as time_ERK for a
+    uniform, doubly periodic grid with the FFT pressure solve, matrix-free and
+    OpenMP-parallel (threads = 0: all).  V (2 Nx Ny) and p (Nx Ny) are
+    returned as new arrays."""
+    lib = _cg_lib()
+    if not hasattr(lib, "_erk_ready"):
+        lib.oracle_erk_periodic.restype = ctypes.c_int
+        lib.oracle_erk_periodic.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_int]
+        lib.oracle_max_threads.restype = ctypes.c_int
+        lib._erk_ready = True
+    A, b, c = getRKmethod(RK)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    V = np.array(V, dtype=np.float64)
+    p = np.array(p, dtype=np.float64)
+    rc = lib.oracle_erk_periodic(Nx, Ny, Lx, Ly, Re, len(b), A.ctypes.data, b.ctypes.data, c.ctypes.data, dt,
+                                 nsteps, V.ctypes.data, p.ctypes.data, threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_erk_periodic failed ({rc})")
+    return V, p
+
+
+def oracle_threads():
+    """Threads the OpenMP restatement uses by default."""
+    erk = _cg_lib()
+    erk.oracle_max_threads.restype = ctypes.c_int
+    return int(erk.oracle_max_threads())
+
+
 def lower_diagonals(A):
     """The storage cg.F / cg_matlab.m use: [B,d]=spdiags(A), the main and lower
     diagonals in order of distance (cg_matlab.m:30-34,

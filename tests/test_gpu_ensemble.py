@@ -32,10 +32,14 @@ def _members(seed, n, sizes, stretch=1.05):
 
 
 @pytest.mark.parametrize("seed,n,sizes", [(4, 6, [24, 32, 40, 64]), (5, 9, [16, 48, 96, 130])])
-def test_ensemble_matches_single_runs(seed, n, sizes):
+@pytest.mark.parametrize("solver", [-1, 0, 512])
+def test_ensemble_matches_single_runs(seed, n, sizes, solver):
+    """solver -1: tuned form; 0: solves batched across members; 512:
+    persistent member solve."""
     import ins2d_b200
     members = _members(seed, n, sizes)
     ens = ins2d_b200.Ensemble(members)
+    ens.set_solver(solver)
     singles, states = [], []
     for m, kw in enumerate(members):
         o = ins2d_b200.Options(**kw)
@@ -47,7 +51,9 @@ def test_ensemble_matches_single_runs(seed, n, sizes):
     dt, nsteps = 2e-3, 6
     stats = ens.time_ERK(0.0, dt, nsteps)
     shape = ens.solve_shape()
-    assert shape["threads"] in (256, 512) and shape["blocks"] >= 1
+    assert shape["threads"] in (0, 256, 512)
+    if solver >= 0:
+        assert shape["threads"] == solver
     for m, o in enumerate(singles):
         V, p = o.time_ERK(*states[m], 0.0, dt, nsteps=nsteps)
         Ve, pe = ens.get_state(m)
