@@ -262,6 +262,27 @@ def run_ours(args, wl, rank, world, local_rank):
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
                 "bytes_per_launch": bpc * cells, "launch_ms": round(launch_ms, 5),
                 "family_ms_per_step": {k: round(v / nprof, 4) for k, v in fam_ms.items()}}
+    # accuracy of this run: kinetic energy drift and divergence; for the FP32
+    # stencil workload also the deviation from the FP64 path over the same steps
+    total_steps = args.warmup + args.steps + nprof
+    acc = None
+    if rank == 0:
+        c0 = opts.check_conservation(torch.tensor(V0, dtype=torch.float64, device="cuda"), 0.0)
+        c1 = opts.check_conservation(Vd, t)
+        acc = {"steps": total_steps, "k0": c0[3], "k": c1[3],
+               "energy_change_rel": (c1[3] - c0[3]) / c0[3] if c0[3] != 0 else None, "maxdiv": c1[0]}
+        if wl["precision"] == "fp32":
+            ref_wl = dict(wl, precision="fp64")
+            o64, V64_0, _ = setup_case(ref_wl, device=local_rank)
+            o64.set_stream(stream.cuda_stream)
+            V64 = torch.tensor(V64_0, dtype=torch.float64, device="cuda")
+            p64 = o64.pressure_additional_solve(V64, torch.zeros(o64.Np, dtype=torch.float64, device="cuda"), 0.0)
+            o64.time_ERK(V64, p64, 0.0, dt, nsteps=args.warmup + args.steps)
+            o64.time_ERK(V64, p64, 0.0, dt, nsteps=nprof)
+            k64 = o64.check_conservation(V64, t)[3]
+            acc.update({"fp64_k": k64, "energy_vs_fp64_rel": abs(c1[3] - k64) / k64,
+                        "velocity_l2_vs_fp64_rel": float(torch.linalg.norm(Vd - V64) / torch.linalg.norm(V64))})
+            o64.close()
     # CPU baseline on rank 0 only at N=1
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -281,6 +302,7 @@ def run_ours(args, wl, rank, world, local_rank):
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,
+        "accuracy": acc,
         "clocks": clk,
     }
     if rank == 0:

@@ -262,6 +262,26 @@ __global__ void __launch_bounds__(128) k_emg_line(const EnsMemberD *__restrict__
 #endif
 }
 
+// y-lines in groups of 32 columns, one thread block per (member, group);
+// kind 1: x -> t, 2: t -> x
+constexpr int kColThreadsEns = 256;
+__global__ void __launch_bounds__(kColThreadsEns) k_emg_ycols(const EnsMemberD *__restrict__ mem, const EnsMgD G,
+                                                              const EnsCg *__restrict__ cg, EnsSeg S, int l, int kind,
+                                                              double omega) {
+  __shared__ double ysh[2 * kColThreadsEns];
+  const long long g = blockIdx.x;
+  const int s = seg_find(S.start, S.n, g);
+  const int m = S.mem[s];
+  if (cg[m].done) return;
+  const int grp = (int)(g - S.start[s]);
+  const MgLevelD &L = lev(G, m, l);
+  const double *b = level_rhs(mem, G, m, l);
+  if (kind == 1)
+    mg_ycols_block(L, b, L.x, L.t, omega, grp * 32, ysh);
+  else
+    mg_ycols_block(L, b, L.t, L.x, omega, grp * 32, ysh);
+}
+
 // kind 0: restriction into level l+1; 1: prolongation into level l;
 // 2: coarsest-level product
 __global__ void __launch_bounds__(256) k_emg_cells(const EnsMemberD *__restrict__ mem, const EnsMgD G,
@@ -297,16 +317,16 @@ unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const EnsMgPlan &pl, double omega,
                 double alpha, cudaStream_t s) {
   for (int l = 0; l < pl.lmax - 1; ++l) {
-    const EnsSeg &X = pl.xl[l], &Y = pl.yl[l], &R = pl.rs[l];
+    const EnsSeg &X = pl.xl[l], &Y = pl.yg[l], &R = pl.rs[l];
     if (X.total) k_emg_line<<<nblk(X.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, X, l, 0, omega);
-    if (Y.total) k_emg_line<<<nblk(Y.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, Y, l, 1, omega);
+    if (Y.total) k_emg_ycols<<<(unsigned)Y.total, kColThreadsEns, 0, s>>>(mem, G, cg, Y, l, 1, omega);
     if (R.total) k_emg_cells<<<nblk(R.total, 256), 256, 0, s>>>(mem, G, cg, R, l, 0, alpha);
   }
   if (pl.co.total) k_emg_cells<<<nblk(pl.co.total, 256), 256, 0, s>>>(mem, G, cg, pl.co, 0, 2, alpha);
   for (int l = pl.lmax - 2; l >= 0; --l) {
-    const EnsSeg &X = pl.xl[l], &Y = pl.yl[l], &P = pl.pr[l];
+    const EnsSeg &X = pl.xl[l], &Y = pl.yg[l], &P = pl.pr[l];
     if (P.total) k_emg_cells<<<nblk(P.total, 256), 256, 0, s>>>(mem, G, cg, P, l, 1, alpha);
-    if (Y.total) k_emg_line<<<nblk(Y.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, Y, l, 2, omega);
+    if (Y.total) k_emg_ycols<<<(unsigned)Y.total, kColThreadsEns, 0, s>>>(mem, G, cg, Y, l, 2, omega);
     if (X.total) k_emg_line<<<nblk(X.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, X, l, 3, omega);
   }
 }

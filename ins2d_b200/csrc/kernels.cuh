@@ -170,6 +170,7 @@ struct EnsSeg {
 struct EnsMgPlan {
   int lmax = 0;
   EnsSeg xl[kMgMaxLevels], yl[kMgMaxLevels], rs[kMgMaxLevels], pr[kMgMaxLevels];
+  EnsSeg yg[kMgMaxLevels];  // groups of 32 columns (one thread block each)
   EnsSeg co{};
 };
 void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const EnsMgPlan &pl, double omega,

@@ -59,8 +59,19 @@ __global__ void __launch_bounds__(256) k_mg_prolong(const MgLevelD F, const MgLe
 }
 __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_constant__ MgD M, int l0,
                                                             const double *__restrict__ b0, const int *done) {
+  __shared__ double ysh[2 * kTailThreads];
   if (is_done(done)) return;
-  mg_vcycle_block(M, b0, l0);
+  mg_vcycle_block(M, b0, l0, ysh);
+}
+
+// y-lines of 32 columns per block (kColThreads threads: one segment of rows per warp)
+constexpr int kColThreads = 1024;
+__global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, const double *__restrict__ b,
+                                                          const double *__restrict__ xold, double *__restrict__ xnew,
+                                                          double omega, const int *done) {
+  __shared__ double ysh[2 * kColThreads];
+  if (is_done(done)) return;
+  mg_ycols_block(L, b, xold, xnew, omega, blockIdx.x * 32, ysh);
 }
 
 unsigned blocks_for(long long n, int t) {
@@ -84,8 +95,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     const double *b = (l == 0) ? r0 : L.b;
     k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x,
                                                                                                   M.omega, done);
-    k_mg_yline<<<blocks_for((long long)L.nx * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
-                                                                                                  M.omega, done);
+    k_mg_ycols<<<(L.nx + 31) / 32, kColThreads, 0, s>>>(L, b, L.x, L.t, M.omega, done);
     const MgLevelD &C = M.L[l + 1];
     k_mg_restrict<<<blocks_for((long long)C.nx * C.ny, 256), 256, 0, s>>>(L, C, b, L.t, C.b, done);
   }
@@ -97,8 +107,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     k_mg_prolong<<<blocks_for((long long)L.nx * L.ny, 256), 256, 0, s>>>(L, C, L.t,
                                                                          (l + 1 == M.nlev - 1) ? C.x : C.t,
                                                                          M.alpha, done);
-    k_mg_yline<<<blocks_for((long long)L.nx * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.t, L.x,
-                                                                                                  M.omega, done);
+    k_mg_ycols<<<(L.nx + 31) / 32, kColThreads, 0, s>>>(L, b, L.t, L.x, M.omega, done);
     k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
                                                                                                   M.omega, done);
   }

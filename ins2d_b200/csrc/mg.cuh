@@ -413,6 +413,125 @@ __device__ inline void mg_yline(const MgLevelD &L, const double *__restrict__ b,
 // lines per launch thread: 32 with warp lines, else 1
 constexpr int kMgLineThreads = INS2D_MG_WARP_LINES ? 32 : 1;
 
+// y-lines (columns) i0 .. i0+31 of a level solved by a whole thread block:
+// lane = column (loads coalesced along rows), warp w = a segment of rows.
+// Each thread first composes the affine maps of the Thomas recurrences over
+// its segment, the segments' composites are chained through shared memory
+// (sh: 2 x warps x 32 doubles), then each thread re-walks its segment.  The
+// dependent chain per thread is about 4 n / warps + 2 warps steps.  All
+// threads of the block must call it.
+__device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restrict__ b,
+                                      const double *__restrict__ xold, double *__restrict__ xnew, double omega,
+                                      int i0, double *sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const int nx = L.nx, n = L.ny;
+  const int i = i0 + lane;
+  const bool col = i < nx;
+  const int m = (n + W - 1) / W;
+  const int j0 = min(n, w * m), j1 = min(n, j0 + m);
+  const bool hasold = xold != nullptr, cyc = L.pery && n >= 3;
+  double hx = 0.0, xmv = 0.0, xpv = 0.0;
+  int im = 0, ip = 0;
+  if (col) {
+    hx = L.hx[i];
+    xmv = L.xm[i];
+    xpv = L.xp[i];
+    im = mg_wrap_lo(i, nx, L.perx);
+    ip = mg_wrap_hi(i, nx, L.perx);
+  }
+  auto fwd = [&](int j, double &al, double &be) {
+    const long long k = (long long)j * nx + i;
+    double rhs = b[k];
+    if (hasold) rhs += L.hy[j] * (xmv * xold[(long long)j * nx + im] + xpv * xold[(long long)j * nx + ip]);
+    const double f = L.fyi[k];
+    al = (j > 0) ? (hx * L.ym[j]) * f : 0.0;
+    be = rhs * f;
+  };
+  // forward pass 1: composite of the segment, d_{j1-1} = A d_{j0-1} + B
+  double A = 1.0, B = 0.0;
+  if (col)
+    for (int j = j0; j < j1; ++j) {
+      double al, be;
+      fwd(j, al, be);
+      B = al * B + be;
+      A = al * A;
+    }
+  double *sA = sh, *sB = sh + W * 32;
+  sA[w * 32 + lane] = A;
+  sB[w * 32 + lane] = B;
+  __syncthreads();
+  if (w == 0) {
+    double d = 0.0;
+    for (int q = 0; q < W; ++q) {
+      const double Aq = sA[q * 32 + lane], Bq = sB[q * 32 + lane];
+      sA[q * 32 + lane] = d;  // value entering segment q
+      d = Aq * d + Bq;
+    }
+  }
+  __syncthreads();
+  double d = sA[w * 32 + lane];
+  __syncthreads();
+  if (col)
+    for (int j = j0; j < j1; ++j) {
+      double al, be;
+      fwd(j, al, be);
+      d = al * d + be;
+      xnew[(long long)j * nx + i] = d;
+    }
+  // backward pass 1: x_{j0} = A x_{j1} + B over the segment
+  A = 1.0;
+  B = 0.0;
+  if (col)
+    for (int j = j1 - 1; j >= j0; --j) {
+      const long long k = (long long)j * nx + i;
+      const double ga = -L.fyc[k];
+      B = ga * B + xnew[k];
+      A = ga * A;
+    }
+  sA[w * 32 + lane] = A;
+  sB[w * 32 + lane] = B;
+  __syncthreads();
+  if (w == 0) {
+    double x = 0.0;
+    for (int q = W - 1; q >= 0; --q) {
+      const double Aq = sA[q * 32 + lane], Bq = sB[q * 32 + lane];
+      sA[q * 32 + lane] = x;  // value above segment q
+      x = Aq * x + Bq;
+    }
+  }
+  __syncthreads();
+  double x = sA[w * 32 + lane];
+  __syncthreads();
+  if (col)
+    for (int j = j1 - 1; j >= j0; --j) {
+      const long long k = (long long)j * nx + i;
+      x = -L.fyc[k] * x + xnew[k];
+      xnew[k] = cyc ? x : (hasold ? (1.0 - omega) * xold[k] + omega * x : omega * x);
+    }
+  if (cyc) {
+    __syncthreads();
+    if (col) {
+      const double s = (xnew[i] + L.gy[i] * xnew[(long long)(n - 1) * nx + i]) * L.ky[i];
+      for (int j = j0; j < j1; ++j) {
+        const long long k = (long long)j * nx + i;
+        const double v = xnew[k] - s * L.zy[k];
+        xnew[k] = hasold ? (1.0 - omega) * xold[k] + omega * v : omega * v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// all y-lines of a level by one thread block (groups of 32 columns)
+__device__ inline void mg_yline_block(const MgLevelD &L, const double *__restrict__ b,
+                                      const double *__restrict__ xold, double *__restrict__ xnew, double omega,
+                                      double *sh) {
+  for (int i0 = 0; i0 < L.nx; i0 += 32) {
+    mg_ycols_block(L, b, xold, xnew, omega, i0, sh);
+    __syncthreads();
+  }
+}
+
 // bc = P' (b - A x) over the coarse cells k0, k0+ks, ...
 __device__ inline void mg_restrict(const MgLevelD &F, const MgLevelD &Cl, const double *__restrict__ b,
                                    const double *__restrict__ x, double *__restrict__ bc, long long k0, long long ks) {
@@ -482,8 +601,9 @@ __device__ __forceinline__ double *mg_result(const MgD &M, int l) {
 
 // One V-cycle inside a thread block from level l0 down to the coarsest and
 // back: z = B b with b = b0 the right-hand side of level l0; the result is at
-// mg_result(M, l0).  All threads of the block must call it.
-__device__ inline void mg_vcycle_block(const MgD &M, const double *__restrict__ b0, int l0 = 0) {
+// mg_result(M, l0).  ysh: shared memory of 2 x 32 x (block warps) doubles for
+// the column solves.  All threads of the block must call it.
+__device__ inline void mg_vcycle_block(const MgD &M, const double *__restrict__ b0, int l0, double *ysh) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int nl = M.nlev;
   MG_T0();
@@ -493,8 +613,7 @@ __device__ inline void mg_vcycle_block(const MgD &M, const double *__restrict__ 
     mg_xline(L, b, nullptr, L.x, M.omega, tid, nt);
     __syncthreads();
     MG_TICK(l * 8 + 0);
-    mg_yline(L, b, L.x, L.t, M.omega, tid, nt);
-    __syncthreads();
+    mg_yline_block(L, b, L.x, L.t, M.omega, ysh);
     MG_TICK(l * 8 + 1);
     mg_restrict(L, M.L[l + 1], b, L.t, M.L[l + 1].b, tid, nt);
     __syncthreads();
@@ -509,8 +628,7 @@ __device__ inline void mg_vcycle_block(const MgD &M, const double *__restrict__ 
     mg_prolong(L, M.L[l + 1], L.t, mg_result(M, l + 1), M.alpha, tid, nt);
     __syncthreads();
     MG_TICK(l * 8 + 4);
-    mg_yline(L, b, L.t, L.x, M.omega, tid, nt);
-    __syncthreads();
+    mg_yline_block(L, b, L.t, L.x, M.omega, ysh);
     MG_TICK(l * 8 + 5);
     mg_xline(L, b, L.x, L.t, M.omega, tid, nt);
     __syncthreads();

@@ -231,7 +231,7 @@ __device__ void block_reduce(double (&v)[NQ], const int (&ops)[NQ], double (*sh)
 template <bool MG>
 __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, const double *__restrict__ f,
                                double *__restrict__ dp, double tol2, long long maxit, int accumulate,
-                               PcgScalars *out, double (*sh)[5]) {
+                               PcgScalars *out, double (*sh)[5], double *ysh) {
   const int Npx = P.Npx;
   const long long Np = P.Np;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -266,7 +266,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
   }
   const int op1[1] = {R_SUM};
   if (MG && !done) {
-    mg_vcycle_block(*M, r);
+    mg_vcycle_block(*M, r, 0, ysh);
     double a1[1] = {0.0};
     for (long long k = tid; k < Np; k += nt) {
       p[k] = z[k];
@@ -333,7 +333,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
     double rz_new = a5[1];
     if (MG) {
       MG_TICK(124);
-      mg_vcycle_block(*M, r);
+      mg_vcycle_block(*M, r, 0, ysh);
       MG_TICK(125);
       double b1[1] = {0.0};
       for (long long k = tid; k < Np; k += nt) b1[0] += r[k] * z[k];
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_con
                                                                const double *__restrict__ f, double *__restrict__ dp,
                                                                double tol2, long long maxit, int accumulate) {
   __shared__ double sh[kBlockThreads / 32][5];
-  pcg_block_body<false>(P, nullptr, W, f, dp, tol2, maxit, accumulate, W.sc, sh);
+  pcg_block_body<false>(P, nullptr, W, f, dp, tol2, maxit, accumulate, W.sc, sh, nullptr);
 }
 
 // multigrid variant: 512 threads (the chunked line solves need ~128 registers)
@@ -389,7 +389,8 @@ __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_block_mg(const __gri
                                                                   double *__restrict__ dp, double tol2,
                                                                   long long maxit, int accumulate) {
   __shared__ double sh[kBlockThreads / 32][5];
-  pcg_block_body<true>(P, &M, W, f, dp, tol2, maxit, accumulate, W.sc, sh);
+  __shared__ double ysh[2 * kBlockThreadsMg];
+  pcg_block_body<true>(P, &M, W, f, dp, tol2, maxit, accumulate, W.sc, sh, ysh);
 }
 
 // Ensemble solves: a persistent launch whose blocks take members from a
@@ -401,6 +402,7 @@ __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_members(const EnsMem
   __shared__ __align__(16) DevOps sP;
   __shared__ __align__(16) MgD sM;
   __shared__ double sh[kBlockThreads / 32][5];
+  __shared__ double ysh[2 * kBlockThreadsMg];
   __shared__ int s_k;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (;;) {
@@ -417,9 +419,9 @@ __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_members(const EnsMem
     __syncthreads();
     double *dst = which ? E.p : E.dp;
     if (mg)
-      pcg_block_body<true>(sP, &sM, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh);
+      pcg_block_body<true>(sP, &sM, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh, ysh);
     else
-      pcg_block_body<false>(sP, nullptr, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh);
+      pcg_block_body<false>(sP, nullptr, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh, ysh);
     __syncthreads();
     if (tid == 0) {
       const PcgScalars &o = *E.W.sc;
