@@ -53,23 +53,28 @@ WORKLOADS = {
                         "members sharded over ranks longest-first"),
 }
 
-# algorithmic DRAM bytes per cell (FP64) of one launch of each kernel family
-# (each array read or written once per launch)
-def family_bytes_per_cell(fam, rk_stats):
-    if fam == "stage":
-        # V_i (16) + Vn (16) + Wt (16) + stored kV (16 on 3 of 4 RK44 stages)
-        # + earlier kV read on the last stage (48 on 1 of 4)
-        return 48 + (3 * 16 + 48) / 4.0
-    if fam == "div":
-        return 16 + 8
-    if fam == "project":
-        return 16 + 8 + 16
-    if fam == "residual":
-        return 16 + 8 + 16
-    if fam == "poisson_fft":
-        # rows r2c: 8 in + 8 out (half spectrum of complex), columns: 16, rows c2r: 8 + 8
-        return 48.0
-    return None
+# Algorithmic DRAM bytes per pressure cell (FP64) of one launch of each kernel
+# family, averaged over the family's launches in an RK44 step with steady
+# boundary conditions (each array read or written once per launch):
+#   stage:    first stage from the cached residual (kV0, Vn in; Wt out: 48),
+#             stages 2-3 (V_s, Vn in; Wt, kV out: 64 each), stage 4 (V_s, Vn,
+#             three earlier kV in; Wt out: 96)            -> 272 / 4 launches
+#   residual: V, p in; w, kV_next out                      -> 56
+#   project:  Wt, dp in; V out                             -> 40
+#   poisson_fft: rows with the divergence fused in (W in 16, half spectrum out
+#             8), columns (8 + 8), rows back (8 in, dp out 8; + 8 for the
+#             accumulating additional solve)               -> (3*56 + 64) / 4
+FAMILY_BYTES = {"stage": 272 / 4.0, "residual": 56.0, "project": 40.0, "poisson_fft": (3 * 56 + 64) / 4.0,
+                "div": 24.0}
+# per RK44 step: all launches of the families above
+STEP_BYTES = 272 + 56 + 4 * 40 + (3 * 56 + 64)
+# the same step in the reference's operator decomposition (fused stage + divergence
+# 88, projection 40, FFT solve 64 per stage, additional solve 40 + solve)
+STEP_BYTES_REFERENCE_DECOMPOSITION = 808
+
+
+def family_bytes_per_cell(fam, rk_stats=None):
+    return FAMILY_BYTES.get(fam)
 
 
 def load_peaks():
@@ -258,10 +263,27 @@ def run_ours(args, wl, rank, world, local_rank):
                     traffic = json.load(fh).get(args.workload, {}).get(fkey)
             except Exception:
                 traffic = None
+        per_family = {}
+        for k, (fms, nl) in fam.items():
+            kk = "poisson_fft" if (k == "poisson" and wl["poisson"] == 6) else k
+            b = family_bytes_per_cell(kk)
+            if b is None or nl == 0 or fms <= 0:
+                continue
+            lms = fms / (nprof * 4) if k == "poisson" else fms / nl
+            gbs = b * cells / (lms / 1e3) / 1e9
+            per_family[kk] = {"ms_per_launch": round(lms, 5), "bytes_per_cell": b, "achieved_gbs": round(gbs, 1),
+                              "frac": round(gbs / peak, 4)}
+        step_ms = ms_max / args.steps
         roof = {"bound": "hbm", "kernel": fkey, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
                 "bytes_per_launch": bpc * cells, "launch_ms": round(launch_ms, 5),
-                "family_ms_per_step": {k: round(v / nprof, 4) for k, v in fam_ms.items()}}
+                "family_ms_per_step": {k: round(v / nprof, 4) for k, v in fam_ms.items()},
+                "families": per_family,
+                "step": {"bytes_per_cell": STEP_BYTES, "achieved_gbs": round(STEP_BYTES * cells / step_ms / 1e6, 1),
+                         "frac": round(STEP_BYTES * cells / step_ms / 1e6 / peak, 4),
+                         "bytes_per_cell_reference_decomposition": STEP_BYTES_REFERENCE_DECOMPOSITION,
+                         "frac_reference_decomposition":
+                             round(STEP_BYTES_REFERENCE_DECOMPOSITION * cells / step_ms / 1e6 / peak, 4)}}
     # accuracy of this run: kinetic energy drift and divergence; for the FP32
     # stencil workload also the deviation from the FP64 path over the same steps
     total_steps = args.warmup + args.steps + nprof

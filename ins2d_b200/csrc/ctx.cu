@@ -289,6 +289,26 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
   return INS2D_OK;
 }
 
+// dp = pressure_poisson(f) with f = (M W + alpha yM + beta ydM) gamma: on the
+// FFT path the divergence is computed inside the first transform pass;
+// otherwise by its own kernel before the solve.
+int solve_div(ins2d_ctx *c, const double *W, double alpha, double beta, double gamma, double *dp, bool accumulate,
+              ins2d_solve_stats *st) {
+  if (c->poisson == INS2D_POISSON_FFT && fft_fuses_div(c->fft)) {
+    if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
+    Prof pr(c, INS2D_PROF_POISSON, 3);
+    launch_fft_poisson_div(c->P, c->fft, W, alpha, beta, gamma, dp, accumulate, c->stream);
+    CK(cudaGetLastError());
+    return INS2D_OK;
+  }
+  {
+    Prof pr(c, INS2D_PROF_DIV, 1);
+    launch_div(c->P, W, alpha, beta, gamma, c->f, false, c->red, c->stream);
+  }
+  CK(cudaGetLastError());
+  return solve(c, c->f, dp, accumulate, st);
+}
+
 void stats_add(ins2d_step_stats *s, const ins2d_solve_stats &o) {
   if (!s) return;
   s->n_solves += 1;
@@ -316,12 +336,7 @@ int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_s
     Prof pr(c, INS2D_PROF_RESIDUAL, 1);
     launch_residual(c->P, V, p, c->wres, kV_next, c->fp32, c->stream);
   }
-  {
-    Prof pr(c, INS2D_PROF_DIV, 1);
-    launch_div(c->P, c->wres, 0.0, c->bcd.bc_unsteady ? 1.0 : 0.0, 1.0, c->f, false, c->red, c->stream);
-  }
-  CK(cudaGetLastError());
-  return solve(c, c->f, p, true, st);
+  return solve_div(c, c->wres, 0.0, c->bcd.bc_unsteady ? 1.0 : 0.0, 1.0, p, true, st);
 }
 
 // [V,p] = time_ERK(V,p,T,t,dt,options) on device pointers, in place.
@@ -364,12 +379,8 @@ int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step
     }
     if (c->bcd.bc_unsteady || i > 0) {
       // f = (M*(Vn/dt + Vtemp) + yM/dt)/c_i   (time_ERK.m:117)
-      {
-        Prof pr(c, INS2D_PROF_DIV, 1);
-        launch_div(P, c->Wt, 1.0 / dt, 0.0, 1.0 / c->c[i], c->f, false, c->red, c->stream);
-      }
       ins2d_solve_stats st;
-      rc = solve(c, c->f, c->dp, false, &st);
+      rc = solve_div(c, c->Wt, 1.0 / dt, 0.0, 1.0 / c->c[i], c->dp, false, &st);
       if (rc) return rc;
       stats_add(stats, st);
       dpp = c->dp;
@@ -952,6 +963,7 @@ struct ins2d_ens {
   bool tuned = false;
   double tuned_ms[3] = {0.0, 0.0, 0.0};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t chunk_graph = nullptr;  // a chunk of batched PCG iterations
 };
 
 namespace {
@@ -975,6 +987,10 @@ void ens_release_graphs(ins2d_ens *e) {
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
+  if (e->chunk_graph) {
+    cudaGraphExecDestroy(e->chunk_graph);
+    e->chunk_graph = nullptr;
+  }
 }
 
 // Work segments, member level tables and CG scalars of the batched solver.
@@ -1066,7 +1082,7 @@ void ens_solve_batched(ins2d_ens *e, int which) {
   ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 4, s);
   ens_cg_scalar(e->d_cg, n, 1, nullptr, s);
   const int chunk = 4;
-  for (long long done_it = 0;; done_it += chunk) {
+  auto iterations = [&]() {
     for (int k = 0; k < chunk; ++k) {
       ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 1, s);
       ens_cg_scalar(e->d_cg, n, 2, nullptr, s);
@@ -1077,6 +1093,20 @@ void ens_solve_batched(ins2d_ens *e, int which) {
       ens_cg_scalar(e->d_cg, n, 4, nullptr, s);
       ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 5, s);
     }
+  };
+  // the chunk of iterations is one CUDA graph (its launches depend only on
+  // the ensemble's device tables), replayed until no member iterates
+  if (!e->chunk_graph) {
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    iterations();
+    CK(cudaStreamEndCapture(s, &gr));
+    cudaError_t ie = cudaGraphInstantiate(&e->chunk_graph, gr, 0);
+    cudaGraphDestroy(gr);
+    CK(ie);
+  }
+  for (long long done_it = 0;; done_it += chunk) {
+    CK(cudaGraphLaunch(e->chunk_graph, s));
     CK(cudaMemcpyAsync(e->h_active, e->d_active, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*e->h_active == 0) break;

@@ -25,6 +25,9 @@ namespace {
 #ifndef INS2D_FFT_COLS_MINB
 #define INS2D_FFT_COLS_MINB 1
 #endif
+#ifndef INS2D_FFT_ROWS_MINB
+#define INS2D_FFT_ROWS_MINB 1
+#endif
 #ifndef INS2D_FFT_COLS_BUDGET
 #define INS2D_FFT_COLS_BUDGET 80  // KB of shared memory per column block (two 2048-point columns)
 #endif
@@ -373,8 +376,14 @@ __device__ void dit_range(double2 *a, int G, int n, int logn, const double2 *tw,
 
 // rows j0, j1 -> half spectra (forward DIF; bit-reversed result read back
 // during the Hermitian split)
-__global__ void __launch_bounds__(kThreads) k_rows_r2c_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
-                                                         const double *__restrict__ f, double2 *__restrict__ spec) {
+// DIV: the rows are not read from f but computed on the fly as the
+// divergence (M W + alpha yM + beta ydM) * gamma of the velocity-sized W
+// (time_ERK.m:117, pressure_additional_solve.m:11-13), fusing that kernel in.
+template <bool DIV>
+__global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_r2c_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
+                                                         const double *__restrict__ f, double2 *__restrict__ spec,
+                                                         const __grid_constant__ DevOps P, double alpha, double beta,
+                                                         double gamma) {
   extern __shared__ double2 sm[];
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
   const bool has1 = j1 < Ny;
@@ -383,7 +392,13 @@ __global__ void __launch_bounds__(kThreads) k_rows_r2c_f(int Nx, int Ny, int L, 
   for (int k = threadIdx.x; k < per; k += blockDim.x) {
     double2 x[8];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = make_double2(__ldg(r0 + k + m * per), has1 ? __ldg(r1 + k + m * per) : 0.0);
+    for (int m = 0; m < 8; ++m) {
+      if (DIV)
+        x[m] = make_double2(div_cell(P, f, alpha, beta, gamma, k + m * per, j0),
+                            has1 ? div_cell(P, f, alpha, beta, gamma, k + m * per, j1) : 0.0);
+      else
+        x[m] = make_double2(__ldg(r0 + k + m * per), has1 ? __ldg(r1 + k + m * per) : 0.0);
+    }
     group_dif(x, 3, k, per, L - 2, L, tw, false);
 #pragma unroll
     for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
@@ -466,7 +481,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
 
 // half spectra of rows j0, j1 -> real rows (inverse DIF, bit-reversed result
 // read back in natural order)
-__global__ void __launch_bounds__(kThreads) k_rows_c2r_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
+__global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_c2r_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
                                                          const double2 *__restrict__ spec, double *__restrict__ out,
                                                          int accumulate, const unsigned long long *__restrict__ maxbits) {
   extern __shared__ double2 sm[];
@@ -545,7 +560,8 @@ bool fft_supported(int Nx, int Ny) {
 // Opt the transform kernels in to large dynamic shared memory on the current
 // device (called once per context).
 void fft_prepare() {
-  cudaFuncSetAttribute(k_rows_r2c_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_rows_r2c_f<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_rows_r2c_f<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_cols_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_rows_c2r_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -553,8 +569,9 @@ void fft_prepare() {
   cudaFuncSetAttribute(k_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
-void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
-                        cudaStream_t s) {
+namespace {
+void fft_passes(const DevOps &P, const FftPlan &plan, const double *src, bool div, double alpha, double beta,
+                double gamma, double *dp, bool accumulate, cudaStream_t s) {
   const int Nx = plan.Nx, Ny = plan.Ny;
   const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
   const int G = cols_group(Ny, plan.logy >= 0);
@@ -563,10 +580,13 @@ void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, d
   const int H = Nx / 2 + 1;
   cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
   const bool fx = plan.logx >= 6, fy = plan.logy >= 6;  // fused-pass kernels
-  if (fx)
-    k_rows_r2c_f<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, f, plan.spec);
+  if (fx && div)
+    k_rows_r2c_f<true><<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec, P, alpha, beta,
+                                                    gamma);
+  else if (fx)
+    k_rows_r2c_f<false><<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec, P, 0.0, 0.0, 0.0);
   else
-    k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, f, plan.spec);
+    k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
   if (fy)
     k_cols_f<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
                                                     plan.spec, (unsigned long long *)plan.maxabs);
@@ -579,6 +599,19 @@ void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, d
   else
     k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
                                             (const unsigned long long *)plan.maxabs);
+}
+}  // namespace
+
+void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
+                        cudaStream_t s) {
+  fft_passes(P, plan, f, false, 0.0, 0.0, 0.0, dp, accumulate, s);
+}
+
+bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= 6; }
+
+void launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha, double beta,
+                            double gamma, double *dp, bool accumulate, cudaStream_t s) {
+  fft_passes(P, plan, W, true, alpha, beta, gamma, dp, accumulate, s);
 }
 
 }  // namespace ins2d

@@ -47,22 +47,6 @@ __global__ void __launch_bounds__(256) k_F(const __grid_constant__ DevOps P, con
   grid_reduce<1>(mx, ops, red);
 }
 
-// f(i,j) = (M W + alpha yM + beta ydM)(i,j) * gamma
-__device__ __forceinline__ double div_cell(const DevOps &P, const double *__restrict__ W, double alpha, double beta,
-                                           double gamma, int i, int j) {
-  double d;
-  if (in_reg(P.rMX, i) && in_reg(P.rMY, j)) {
-    // interior cell: regular rows of Mx and My, no boundary contribution
-    d = __ldg(P.hy + j) * reg_x(P.rMX, i, W, (long long)j * P.Nux) +
-        __ldg(P.hx + i) * reg_y(P.rMY, j, W + P.Nu, P.Nvx, i);
-  } else {
-    d = div_in(P, W, W + P.Nu, i, j);
-    if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
-    if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
-  }
-  return d * gamma;
-}
-
 template <bool WANTMAX>
 __global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, const double *__restrict__ W,
                                             double alpha, double beta, double gamma, double *__restrict__ f,

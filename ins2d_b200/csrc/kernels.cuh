@@ -106,6 +106,11 @@ bool fft_supported(int Nx, int Ny);
 // accumulate.  Returns 0 (dp untouched / zero) when max|fhat| < 1e-14 (:21-32).
 void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
                         cudaStream_t s);
+// Same with the right-hand side f = (M W + alpha yM + beta ydM) gamma computed
+// inside the first pass (only when fft_fuses_div(plan): power-of-two rows >= 64).
+bool fft_fuses_div(const FftPlan &plan);
+void launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha, double beta,
+                            double gamma, double *dp, bool accumulate, cudaStream_t s);
 
 // --- PCG (pcg.cu) ---------------------------------------------------------------
 struct PcgScalars {

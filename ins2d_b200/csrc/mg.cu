@@ -40,12 +40,6 @@ __global__ void __launch_bounds__(kLineThreads) k_mg_xline(const MgLevelD L, con
   if (is_done(done)) return;
   mg_xline(L, b, xold, xnew, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
-__global__ void __launch_bounds__(kLineThreads) k_mg_yline(const MgLevelD L, const double *__restrict__ b,
-                                                           const double *__restrict__ xold, double *__restrict__ xnew,
-                                                           double omega, const int *done) {
-  if (is_done(done)) return;
-  mg_yline(L, b, xold, xnew, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
-}
 __global__ void __launch_bounds__(256) k_mg_restrict(const MgLevelD F, const MgLevelD C, const double *__restrict__ b,
                                                      const double *__restrict__ x, double *__restrict__ bc,
                                                      const int *done) {

@@ -326,6 +326,7 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
   const long long base = ln.base, st = ln.st;
   const bool hasold = xold != nullptr, cyc = ln.cyc;
   double carry = 0.0;
+#pragma unroll 2
   for (int c0 = 0; c0 < n; c0 += 32) {
     const int q = c0 + lane;
     const long long k = base + (long long)q * st;
@@ -350,6 +351,7 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
     carry = __shfl_sync(FULL, d, 31);
   }
   carry = 0.0;
+#pragma unroll 2
   for (int c0 = ((n - 1) >> 5) << 5; c0 >= 0; c0 -= 32) {
     const int q = c0 + lane;
     const long long k = base + (long long)q * st;
@@ -410,6 +412,10 @@ __device__ inline void mg_yline(const MgLevelD &L, const double *__restrict__ b,
   for (int i = i0; i < L.nx; i += is) mg_line(mg_make_yline(L, i), b, xold, xnew, omega);
 #endif
 }
+#ifndef INS2D_MG_UNROLL
+#define INS2D_MG_UNROLL 4
+#endif
+constexpr int kMgUnroll = INS2D_MG_UNROLL;  // unrolling of the column segment walks
 // lines per launch thread: 32 with warp lines, else 1
 constexpr int kMgLineThreads = INS2D_MG_WARP_LINES ? 32 : 1;
 
@@ -450,6 +456,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   // forward pass 1: composite of the segment, d_{j1-1} = A d_{j0-1} + B
   double A = 1.0, B = 0.0;
   if (col)
+#pragma unroll kMgUnroll
     for (int j = j0; j < j1; ++j) {
       double al, be;
       fwd(j, al, be);
@@ -472,6 +479,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   double d = sA[w * 32 + lane];
   __syncthreads();
   if (col)
+#pragma unroll kMgUnroll
     for (int j = j0; j < j1; ++j) {
       double al, be;
       fwd(j, al, be);
@@ -482,6 +490,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   A = 1.0;
   B = 0.0;
   if (col)
+#pragma unroll kMgUnroll
     for (int j = j1 - 1; j >= j0; --j) {
       const long long k = (long long)j * nx + i;
       const double ga = -L.fyc[k];
@@ -503,6 +512,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   double x = sA[w * 32 + lane];
   __syncthreads();
   if (col)
+#pragma unroll kMgUnroll
     for (int j = j1 - 1; j >= j0; --j) {
       const long long k = (long long)j * nx + i;
       x = -L.fyc[k] * x + xnew[k];
