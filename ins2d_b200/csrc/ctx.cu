@@ -993,6 +993,9 @@ void ens_release_graphs(ins2d_ens *e) {
   }
 }
 
+#ifndef INS2D_ENS_TAIL_LEVEL
+#define INS2D_ENS_TAIL_LEVEL 2
+#endif
 // Work segments, member level tables and CG scalars of the batched solver.
 void ens_build_batch(ins2d_ens *e, const std::vector<int> &order) {
   const int n = (int)e->mem.size();
@@ -1051,6 +1054,12 @@ void ens_build_batch(ins2d_ens *e, const std::vector<int> &order) {
     pl.pr[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).nx * L(m).ny : 0LL; });
   }
   pl.co = make_seg([&](int m) { return (long long)ncoarse[m]; });
+  // levels from INS2D_ENS_TAIL_LEVEL down run in one block per member
+  pl.ltail = std::min(INS2D_ENS_TAIL_LEVEL, std::max(lmax - 1, 0));
+  const MgD **d_mgs = ens_alloc<const MgD *>(e, n);
+  std::vector<const MgD *> hm(e->d_mg.begin(), e->d_mg.end());
+  CK(cudaMemcpy(d_mgs, hm.data(), n * sizeof(const MgD *), cudaMemcpyHostToDevice));
+  pl.mgs = d_mgs;
   std::vector<int2> ct;
   for (int m : order)
     for (long long k = 0; k < e->mem[m]->P.Np; k += 256) ct.push_back(make_int2(m, (int)k));

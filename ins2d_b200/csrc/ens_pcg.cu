@@ -310,20 +310,41 @@ __global__ void __launch_bounds__(256) k_emg_cells(const EnsMemberD *__restrict_
   }
 }
 
+// The coarse part of the V-cycle (levels >= ltail, a few thousand cells per
+// member at most) for all members at once: one thread block per member runs
+// the single-block V-cycle from its level ltail down and back.
+constexpr int kTailThreadsEns = 256;
+__global__ void __launch_bounds__(kTailThreadsEns) k_emg_tail(const EnsMemberD *__restrict__ mem,
+                                                             const MgD *const *__restrict__ mgs,
+                                                             const EnsCg *__restrict__ cg, int ltail) {
+  __shared__ __align__(16) MgD sM;
+  __shared__ double ysh[2 * kTailThreadsEns];
+  const int m = blockIdx.x;
+  if (cg[m].done) return;
+  const MgD *src = mgs[m];
+  for (int w = threadIdx.x; w < (int)(sizeof(MgD) / 8); w += blockDim.x)
+    ((long long *)&sM)[w] = ((const long long *)src)[w];
+  __syncthreads();
+  const int l0 = min(ltail, sM.nlev - 1);
+  const double *b0 = (l0 == 0) ? mem[m].W.r : sM.L[l0].b;
+  mg_vcycle_block(sM, b0, l0, ysh);
+}
+
 unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
 
 void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const EnsMgPlan &pl, double omega,
                 double alpha, cudaStream_t s) {
-  for (int l = 0; l < pl.lmax - 1; ++l) {
+  const int lb = pl.ltail;  // batched levels 0 .. lb-1
+  for (int l = 0; l < lb; ++l) {
     const EnsSeg &X = pl.xl[l], &Y = pl.yg[l], &R = pl.rs[l];
     if (X.total) k_emg_line<<<nblk(X.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, X, l, 0, omega);
     if (Y.total) k_emg_ycols<<<(unsigned)Y.total, kColThreadsEns, 0, s>>>(mem, G, cg, Y, l, 1, omega);
     if (R.total) k_emg_cells<<<nblk(R.total, 256), 256, 0, s>>>(mem, G, cg, R, l, 0, alpha);
   }
-  if (pl.co.total) k_emg_cells<<<nblk(pl.co.total, 256), 256, 0, s>>>(mem, G, cg, pl.co, 0, 2, alpha);
-  for (int l = pl.lmax - 2; l >= 0; --l) {
+  k_emg_tail<<<pl.co.n, kTailThreadsEns, 0, s>>>(mem, pl.mgs, cg, lb);
+  for (int l = lb - 1; l >= 0; --l) {
     const EnsSeg &X = pl.xl[l], &Y = pl.yg[l], &P = pl.pr[l];
     if (P.total) k_emg_cells<<<nblk(P.total, 256), 256, 0, s>>>(mem, G, cg, P, l, 1, alpha);
     if (Y.total) k_emg_ycols<<<(unsigned)Y.total, kColThreadsEns, 0, s>>>(mem, G, cg, Y, l, 2, omega);

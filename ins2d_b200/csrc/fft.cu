@@ -26,7 +26,7 @@ namespace {
 #define INS2D_FFT_COLS_MINB 1
 #endif
 #ifndef INS2D_FFT_ROWS_MINB
-#define INS2D_FFT_ROWS_MINB 1
+#define INS2D_FFT_ROWS_MINB 4
 #endif
 #ifndef INS2D_FFT_COLS_BUDGET
 #define INS2D_FFT_COLS_BUDGET 80  // KB of shared memory per column block (two 2048-point columns)

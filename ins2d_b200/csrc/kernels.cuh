@@ -174,6 +174,8 @@ struct EnsSeg {
 };
 struct EnsMgPlan {
   int lmax = 0;
+  int ltail = 0;              // levels >= ltail: one thread block per member (k_emg_tail)
+  const MgD *const *mgs = nullptr;  // device: each member's hierarchy
   EnsSeg xl[kMgMaxLevels], yl[kMgMaxLevels], rs[kMgMaxLevels], pr[kMgMaxLevels];
   EnsSeg yg[kMgMaxLevels];  // groups of 32 columns (one thread block each)
   EnsSeg co{};

@@ -68,6 +68,14 @@ __global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, cons
   mg_ycols_block(L, b, xold, xnew, omega, blockIdx.x * 32, ysh);
 }
 
+// warps per column block: one segment of about 16 rows each, at most 32
+int col_threads(int ny) {
+  int w = ny / 16;
+  if (w < 1) w = 1;
+  if (w > kColThreads / 32) w = kColThreads / 32;
+  return 32 * w;
+}
+
 unsigned blocks_for(long long n, int t) {
   long long b = (n + t - 1) / t;
   if (b > 148LL * 32) b = 148LL * 32;
@@ -89,7 +97,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     const double *b = (l == 0) ? r0 : L.b;
     k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x,
                                                                                                   M.omega, done);
-    k_mg_ycols<<<(L.nx + 31) / 32, kColThreads, 0, s>>>(L, b, L.x, L.t, M.omega, done);
+    k_mg_ycols<<<(L.nx + 31) / 32, col_threads(L.ny), 0, s>>>(L, b, L.x, L.t, M.omega, done);
     const MgLevelD &C = M.L[l + 1];
     k_mg_restrict<<<blocks_for((long long)C.nx * C.ny, 256), 256, 0, s>>>(L, C, b, L.t, C.b, done);
   }
@@ -101,7 +109,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     k_mg_prolong<<<blocks_for((long long)L.nx * L.ny, 256), 256, 0, s>>>(L, C, L.t,
                                                                          (l + 1 == M.nlev - 1) ? C.x : C.t,
                                                                          M.alpha, done);
-    k_mg_ycols<<<(L.nx + 31) / 32, kColThreads, 0, s>>>(L, b, L.t, L.x, M.omega, done);
+    k_mg_ycols<<<(L.nx + 31) / 32, col_threads(L.ny), 0, s>>>(L, b, L.t, L.x, M.omega, done);
     k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
                                                                                                   M.omega, done);
   }
