@@ -41,7 +41,12 @@ WORKLOADS = {
     "turb2048_fp32": dict(N=2048, L=1.0, Re=2000.0, poisson=6, precision="fp32", ic="turbulence",
                           desc="decaying 2D turbulence 2048x2048, FP32 stencils + FP64 Poisson/projection"),
     "turb2048_pcg": dict(N=2048, L=1.0, Re=2000.0, poisson=4, precision="fp64", ic="turbulence", CG_acc=1e-10,
-                         desc="decaying 2D turbulence 2048x2048, PCG Poisson to 1e-10, FP64"),
+                         compare_plain=True,
+                         desc="decaying 2D turbulence 2048x2048, PCG Poisson to 1e-10 (multigrid-preconditioned), FP64"),
+    "turb2048_pcg_fp32": dict(N=2048, L=1.0, Re=2000.0, poisson=4, precision="fp32", ic="turbulence", CG_acc=1e-10,
+                              compare_plain=True,
+                              desc="decaying 2D turbulence 2048x2048, FP32 stencils, multigrid-preconditioned PCG "
+                                   "to 1e-10, FP64 Poisson/projection"),
     "tg512": dict(N=512, L=2 * math.pi, Re=1e100, poisson=6, precision="fp64", ic="tg", dt=1e-3,
                   desc="inviscid Taylor-Green 512x512 periodic [0,2pi]^2, RK44 dt=1e-3, FFT Poisson, FP64"),
     "ldc64": dict(N=64, L=1.0, Re=1000.0, poisson=4, precision="fp64", ic="rest", dt=1e-3, CG_acc=1e-12,
@@ -145,7 +150,8 @@ def setup_case(wl, device=0):
         bc = cases.BC_PERIODIC
         uBC = None
     opts = ins2d_b200.Options(x, x.copy(), bc, Re=wl["Re"], poisson=wl["poisson"], CG_acc=wl.get("CG_acc", 1e-12),
-                              CG_maxit=50000, uBC=uBC, RK="RK44", precision=wl["precision"], device=device)
+                              CG_maxit=50000, uBC=uBC, RK="RK44", precision=wl["precision"], device=device,
+                              precond=wl.get("precond", "default"))
     if wl["ic"] == "turbulence":
         V = cases.decaying_turbulence_ic(opts, k0=10.0, seed=2048)
         dt = cases.cfl_dt(opts, V, 0.5)
@@ -305,6 +311,26 @@ def run_ours(args, wl, rank, world, local_rank):
             acc.update({"fp64_k": k64, "energy_vs_fp64_rel": abs(c1[3] - k64) / k64,
                         "velocity_l2_vs_fp64_rel": float(torch.linalg.norm(Vd - V64) / torch.linalg.norm(V64))})
             o64.close()
+    # the plain FP64 PCG (Jacobi preconditioner) on the same case, same
+    # tolerance: one timed step after one warm-up step
+    plain = None
+    if rank == 0 and wl.get("compare_plain"):
+        pwl = dict(wl, precision="fp64", precond="jacobi")
+        op, Vp0, _ = setup_case(pwl, device=local_rank)
+        op.set_stream(stream.cuda_stream)
+        Vp = torch.tensor(Vp0, dtype=torch.float64, device="cuda")
+        pp = op.pressure_additional_solve(Vp, torch.zeros(op.Np, dtype=torch.float64, device="cuda"), 0.0)
+        op.time_ERK(Vp, pp, 0.0, dt, nsteps=1)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _, _, pst = op.time_ERK(Vp, pp, dt, dt, nsteps=1, return_stats=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1)
+        plain = {"precond": "jacobi", "dtype": "f64", "ms_per_step": pms,
+                 "cg_iters_per_solve": pst["iters_total"] / max(pst["n_solves"], 1),
+                 "value": cells / (pms / 1e3), "speedup_of_this_run": (cells / (pms / 1e3)) and value / (cells / (pms / 1e3))}
+        op.close()
     # CPU baseline on rank 0 only at N=1
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -325,6 +351,7 @@ def run_ours(args, wl, rank, world, local_rank):
         "roofline": roof,
         "cpu_baseline": cpu,
         "accuracy": acc,
+        "plain_pcg": plain,
         "clocks": clk,
     }
     if rank == 0:

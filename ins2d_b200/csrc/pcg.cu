@@ -148,44 +148,6 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P
   }
 }
 
-// r'z with z = the V-cycle's result; init: p = z and rz = r'z (first
-// iteration), else beta = r'z_new / r'z_old.
-__global__ void __launch_bounds__(256) k_rz_mg(const __grid_constant__ DevOps P, const PcgWork W,
-                                               const double *__restrict__ z, int init) {
-  if (*(volatile int *)&W.sc->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-  double q[1] = {0.0};
-  const int ops[1] = {R_SUM};
-  if (i < P.Npx && j < P.Npy) {
-    const long long k = (long long)j * P.Npx + i;
-    q[0] = W.r[k] * z[k];
-    if (init) W.p[k] = z[k];
-  }
-  double out[1];
-  if (grid_reduce<1>(q, ops, red_of(W), out)) {
-    PcgScalars *s = W.sc;
-    if (!isfinite(out[0])) {
-      s->status = INS2D_ENONFINITE;
-      s->done = 1;
-    } else if (init) {
-      s->rz = out[0];
-    } else {
-      s->beta = out[0] / s->rz;
-      s->rz = out[0];
-    }
-  }
-}
-
-__global__ void __launch_bounds__(256) k_pupdate_mg(const __grid_constant__ DevOps P, const PcgWork W,
-                                                    const double *__restrict__ z) {
-  if (*(volatile int *)&W.sc->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-  if (i < P.Npx && j < P.Npy) {
-    const long long k = (long long)j * P.Npx + i;
-    W.p[k] = z[k] + W.sc->beta * W.p[k];
-  }
-}
-
 __global__ void __launch_bounds__(256) k_pupdate(const __grid_constant__ DevOps P, const PcgWork W) {
   if (*(volatile int *)&W.sc->done) return;
   const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
@@ -393,6 +355,104 @@ __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_block_mg(const __gri
   pcg_block_body<true>(P, &M, W, f, dp, tol2, maxit, accumulate, W.sc, sh, ysh);
 }
 
+// Grid-stride CG kernels of the multigrid path for large grids: the SpMV uses
+// the 3-point 1D rows of the hierarchy's level 0 (the same operator as A,
+// without table indirection), and each thread handles many cells, so the
+// block partials of the reductions stay few.
+constexpr int kVecThreads = 256;
+__global__ void __launch_bounds__(kVecThreads) k_spmv_g(const MgLevelD L0, const PcgWork W, long long n) {
+  if (*(volatile int *)&W.sc->done) return;
+  double q[1] = {0.0};
+  const int ops[1] = {R_SUM};
+  const int nx = L0.nx;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % nx), j = (int)(k / nx);
+    const double aq = mg_apply(L0, W.p, i, j);
+    W.q[k] = aq;
+    q[0] += W.p[k] * aq;
+  }
+  double out[1];
+  if (grid_reduce<1>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    s->pq = out[0];
+    if (!isfinite(out[0])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    } else if (out[0] == 0.0) {
+      s->status = INS2D_EBREAKDOWN;
+      s->done = 1;
+    } else {
+      s->alpha = s->rz / out[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_update_g(const PcgWork W, long long n) {
+  if (*(volatile int *)&W.sc->done) return;
+  const double alpha = W.sc->alpha;
+  double q[4] = {0.0, -DBL_MAX, DBL_MAX, 0.0};
+  const int ops[4] = {R_SUM, R_MAX, R_MIN, R_MAX};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double x = W.x[k] + alpha * W.p[k];
+    const double r = W.r[k] - alpha * W.q[k];
+    W.x[k] = x;
+    W.r[k] = r;
+    q[0] += r * r;
+    q[1] = fmax(q[1], x);
+    q[2] = fmin(q[2], x);
+    q[3] = fmax(q[3], fabs(r));
+  }
+  double out[4];
+  if (grid_reduce<4>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    s->it += 1;
+    s->rr = out[0] / s->rr0;
+    s->maxx = out[1];
+    s->minx = out[2];
+    s->maxres = out[3];
+    if (!isfinite(s->rr)) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    } else if (s->rr <= s->tol2) {
+      s->done = 1;
+    } else if (s->it >= s->maxit) {
+      s->status = INS2D_ENOTCONV;
+      s->done = 1;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_rz_g(const PcgWork W, const double *__restrict__ z, long long n,
+                                                      int init) {
+  if (*(volatile int *)&W.sc->done) return;
+  double q[1] = {0.0};
+  const int ops[1] = {R_SUM};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    q[0] += W.r[k] * z[k];
+    if (init) W.p[k] = z[k];
+  }
+  double out[1];
+  if (grid_reduce<1>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    if (!isfinite(out[0])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    } else if (init) {
+      s->rz = out[0];
+    } else {
+      s->beta = out[0] / s->rz;
+      s->rz = out[0];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) k_pupdate_g(const PcgWork W, const double *__restrict__ z, long long n) {
+  if (*(volatile int *)&W.sc->done) return;
+  const double beta = W.sc->beta;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    W.p[k] = z[k] + beta * W.p[k];
+}
+
 // Ensemble solves: a persistent launch whose blocks take members from a
 // queue (largest first) and run the whole PCG of each.
 __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_members(const EnsMemberD *__restrict__ mem,
@@ -489,22 +549,33 @@ void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
   }
 }
 
+namespace {
+// blocks of the grid-stride kernels: at most 8 per SM and at most the
+// reduction scratch's capacity
+unsigned vec_blocks(const DevOps &P, const PcgWork &W) {
+  long long b = (P.Np + kVecThreads - 1) / kVecThreads;
+  if (b > 148LL * 8) b = 148LL * 8;
+  if (b > W.blocks) b = W.blocks;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+}  // namespace
+
 void pcg_init_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double tol, long long maxit,
                  cudaStream_t s) {
   k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
   mg_vcycle_launch(M, W.r, &W.sc->done, s);
-  k_rz_mg<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, mg_result_host(M, 0), 1);
+  k_rz_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(W, mg_result_host(M, 0), P.Np, 1);
 }
 
 void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, cudaStream_t s) {
-  const dim3 g = pgrid(P), b(BX, BY);
+  const unsigned g = vec_blocks(P, W);
   const double *z = mg_result_host(M, 0);
   for (int it = 0; it < n; ++it) {
-    k_spmv<<<g, b, 0, s>>>(P, W);
-    k_update<true><<<g, b, 0, s>>>(P, W);
+    k_spmv_g<<<g, kVecThreads, 0, s>>>(M.L[0], W, P.Np);
+    k_update_g<<<g, kVecThreads, 0, s>>>(W, P.Np);
     mg_vcycle_launch(M, W.r, &W.sc->done, s);
-    k_rz_mg<<<g, b, 0, s>>>(P, W, z, 0);
-    k_pupdate_mg<<<g, b, 0, s>>>(P, W, z);
+    k_rz_g<<<g, kVecThreads, 0, s>>>(W, z, P.Np, 0);
+    k_pupdate_g<<<g, kVecThreads, 0, s>>>(W, z, P.Np);
   }
 }
 
