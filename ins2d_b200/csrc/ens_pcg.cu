@@ -243,7 +243,7 @@ __global__ void k_ecg_stats(EnsCg *__restrict__ cg, int n, EnsStats *__restrict_
 __global__ void __launch_bounds__(128) k_emg_line(const EnsMemberD *__restrict__ mem, const EnsMgD G,
                                                   const EnsCg *__restrict__ cg, EnsSeg S, int l, int kind,
                                                   double omega) {
-  const long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / kMgLineThreads;  // line of this warp / thread
+  const long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / kMgLineThreads;  // line of this warp
   if (g >= S.total) return;
   const int s = seg_find(S.start, S.n, g);
   const int m = S.mem[s];
@@ -255,11 +255,7 @@ __global__ void __launch_bounds__(128) k_emg_line(const EnsMemberD *__restrict__
   const MgLine ln = xl ? mg_make_xline(L, line) : mg_make_yline(L, line);
   const double *xold = kind == 0 ? nullptr : (kind == 2 ? L.t : L.x);
   double *xnew = (kind == 0 || kind == 2) ? L.x : L.t;
-#if INS2D_MG_WARP_LINES
   mg_line_warp(ln, b, xold, xnew, omega);
-#else
-  mg_line(ln, b, xold, xnew, omega);
-#endif
 }
 
 // y-lines in groups of 32 columns, one thread block per (member, group);

@@ -21,9 +21,11 @@
 // The coarse correction is scaled by alpha (over-correction of unsmoothed
 // aggregation).
 //
-// Line solves: each thread owns one line and runs the Thomas algorithm with
-// per-cell factors computed once at set-up; periodic lines use the
-// Sherman-Morrison form (T = T' + u v') with z = T'^-1 u stored per cell.
+// Line solves use per-cell Thomas factors computed once at set-up (periodic
+// lines in the Sherman-Morrison form T = T' + u v', z = T'^-1 u stored per
+// cell).  The Thomas recurrences are first-order linear, so a row is solved
+// by a warp as a scan of affine maps (mg_line_warp) and 32 columns by a thread
+// block whose warps compose segments of rows (mg_ycols_block).
 //
 // The phase functions take (first line/cell, stride) so the same code runs
 // inside one thread block (small grids, ensembles: one block per solve) and
@@ -160,26 +162,10 @@ __device__ inline void mg_factor_yline(const MgLevelD &L, int i) {
   }
 }
 
-// Line relaxation along a line of n cells: cell q of the line is at
-// base + q*st (st = 1 for x-lines, nx for y-lines); the couplings across the
-// line to the neighbouring lines (lo, hi: offsets of the neighbour cells)
-// enter the right-hand side with the old iterate:
+// One line of a level: cell q at base + q*st (st = 1 for x-lines, nx for
+// y-lines); the couplings to the neighbouring lines (at +lo, +hi) enter the
+// right-hand side with the old iterate:
 //   xnew = (1-omega) xold + omega T^-1 (b - X xold),   xold == nullptr: zero.
-// The loads of a chunk of kMgChunk cells are issued before its recurrence
-// steps, so the dependent Thomas chain pays one memory latency per chunk.
-#ifndef INS2D_MG_CHUNK
-#define INS2D_MG_CHUNK 8
-#endif
-#ifndef INS2D_MG_NOINLINE
-#define INS2D_MG_NOINLINE 1
-#endif
-#if INS2D_MG_NOINLINE
-#define MG_LINE_ATTR __noinline__
-#else
-#define MG_LINE_ATTR __forceinline__
-#endif
-constexpr int kMgChunk = INS2D_MG_CHUNK;
-
 struct MgLine {
   long long base, st, lo, hi;  // cell q at base + q*st; neighbours at +lo, +hi
   int n;
@@ -192,81 +178,6 @@ struct MgLine {
   double g, k;                 // periodic lines: v'/(1+v'z) terms
   bool cyc;
 };
-
-// (The descriptor is taken by value and its fields are copied into
-// registers: stores through xnew cannot alias them.)
-static __device__ MG_LINE_ATTR void mg_line(const MgLine ln, const double *__restrict__ b,
-                                            const double *__restrict__ xold, double *__restrict__ xnew,
-                                            double omega) {
-  const int n = ln.n;
-  const long long base = ln.base, st = ln.st, lo = ln.lo, hi = ln.hi;
-  const double *__restrict__ cw = ln.cross_w;
-  const double *__restrict__ am = ln.am;
-  const double *__restrict__ fi_ = ln.fi;
-  const double *__restrict__ fc_ = ln.fc;
-  const double cm = ln.cm, cp = ln.cp, as = ln.ascale;
-  const bool cyc = ln.cyc;
-  const bool hasold = xold != nullptr;
-  double d = 0.0;
-  for (int q0 = 0; q0 < n; q0 += kMgChunk) {
-    double rhs[kMgChunk], a[kMgChunk], fi[kMgChunk];
-#pragma unroll
-    for (int u = 0; u < kMgChunk; ++u) {
-      const int q = q0 + u;
-      if (q < n) {
-        const long long k = base + q * st;
-        double v = b[k];
-        if (hasold) v += cw[q] * (cm * xold[k + lo] + cp * xold[k + hi]);
-        rhs[u] = v;
-        a[u] = (q > 0) ? -as * am[q] : 0.0;
-        fi[u] = fi_[k];
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kMgChunk; ++u) {
-      const int q = q0 + u;
-      if (q < n) {
-        d = (rhs[u] - a[u] * d) * fi[u];
-        xnew[base + q * st] = d;
-      }
-    }
-  }
-  double xn = 0.0;
-  for (int q1 = n - 1; q1 >= 0; q1 -= kMgChunk) {
-    double dd[kMgChunk], fc[kMgChunk], xo[kMgChunk];
-#pragma unroll
-    for (int u = 0; u < kMgChunk; ++u) {
-      const int q = q1 - u;
-      if (q >= 0) {
-        const long long k = base + q * st;
-        dd[u] = xnew[k];
-        fc[u] = fc_[k];
-        xo[u] = (hasold && !cyc) ? xold[k] : 0.0;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kMgChunk; ++u) {
-      const int q = q1 - u;
-      if (q >= 0) {
-        xn = dd[u] - fc[u] * xn;
-        const long long k = base + q * st;
-        if (cyc)
-          xnew[k] = xn;
-        else
-          xnew[k] = hasold ? (1.0 - omega) * xo[u] + omega * xn : omega * xn;
-      }
-    }
-  }
-  if (cyc) {
-    const double *__restrict__ z = ln.z;
-    const double s = (xnew[base] + ln.g * xnew[base + (long long)(n - 1) * st]) * ln.k;
-    for (int q = 0; q < n; ++q) {
-      const long long k = base + q * st;
-      const double v = xnew[k] - s * z[k];
-      xnew[k] = hasold ? (1.0 - omega) * xold[k] + omega * v : omega * v;
-    }
-  }
-}
 
 __device__ __forceinline__ MgLine mg_make_xline(const MgLevelD &L, int j) {
   const int nx = L.nx, ny = L.ny;
@@ -389,35 +300,19 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
   }
 }
 
-// Line relaxations: x-lines are the rows, y-lines the columns of a level.
-// With INS2D_MG_WARP_LINES (default) a warp solves each line (first = warp
-// index, step = warps); otherwise a thread (first = thread index, step =
-// threads).
-#ifndef INS2D_MG_WARP_LINES
-#define INS2D_MG_WARP_LINES 1
-#endif
+// x-line relaxations: a warp per row (first = warp index j0 >> 5, step =
+// warps (js + 31) >> 5 when called with thread indices)
 __device__ inline void mg_xline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
                                 double *__restrict__ xnew, double omega, int j0, int js) {
-#if INS2D_MG_WARP_LINES
   for (int j = j0 >> 5; j < L.ny; j += (js + 31) >> 5) mg_line_warp(mg_make_xline(L, j), b, xold, xnew, omega);
-#else
-  for (int j = j0; j < L.ny; j += js) mg_line(mg_make_xline(L, j), b, xold, xnew, omega);
-#endif
 }
-__device__ inline void mg_yline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
-                                double *__restrict__ xnew, double omega, int i0, int is) {
-#if INS2D_MG_WARP_LINES
-  for (int i = i0 >> 5; i < L.nx; i += (is + 31) >> 5) mg_line_warp(mg_make_yline(L, i), b, xold, xnew, omega);
-#else
-  for (int i = i0; i < L.nx; i += is) mg_line(mg_make_yline(L, i), b, xold, xnew, omega);
-#endif
-}
+// threads per line of the warp solves
+constexpr int kMgLineThreads = 32;
+
 #ifndef INS2D_MG_UNROLL
 #define INS2D_MG_UNROLL 4
 #endif
 constexpr int kMgUnroll = INS2D_MG_UNROLL;  // unrolling of the column segment walks
-// lines per launch thread: 32 with warp lines, else 1
-constexpr int kMgLineThreads = INS2D_MG_WARP_LINES ? 32 : 1;
 
 // y-lines (columns) i0 .. i0+31 of a level solved by a whole thread block:
 // lane = column (loads coalesced along rows), warp w = a segment of rows.

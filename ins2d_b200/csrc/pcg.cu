@@ -104,9 +104,6 @@ __global__ void __launch_bounds__(256) k_spmv(const __grid_constant__ DevOps P, 
   }
 }
 
-// MG = true: the preconditioned residual is not known yet (the V-cycle runs
-// after this kernel), so r'z and beta come from k_rz_mg.
-template <bool MG>
 __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P, const PcgWork W) {
   if (*(volatile int *)&W.sc->done) return;
   const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
@@ -120,7 +117,7 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P
     W.x[k] = x;
     W.r[k] = r;
     q[0] = r * r;
-    q[1] = MG ? 0.0 : r * (r / lap_diag(P, i, j));
+    q[1] = r * (r / lap_diag(P, i, j));
     q[2] = x;
     q[3] = x;
     q[4] = fabs(r);
@@ -141,7 +138,7 @@ __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P
     } else if (s->it >= s->maxit) {
       s->status = INS2D_ENOTCONV;
       s->done = 1;
-    } else if (!MG) {
+    } else {
       s->beta = out[1] / s->rz;
       s->rz = out[1];
     }
@@ -544,7 +541,7 @@ void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
   const dim3 g = pgrid(P), b(BX, BY);
   for (int it = 0; it < n; ++it) {
     k_spmv<<<g, b, 0, s>>>(P, W);
-    k_update<false><<<g, b, 0, s>>>(P, W);
+    k_update<<<g, b, 0, s>>>(P, W);
     k_pupdate<<<g, b, 0, s>>>(P, W);
   }
 }
