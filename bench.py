@@ -11,12 +11,14 @@ working set of a step (about 0.5 GB of FP64 fields, 32 MiB each) is larger
 than the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload turb2048|turb2048_fp32|tg512|ldc64|turb2048_pcg]
+                  [--workload turb2048|turb2048_fp32|turb2048_pcg|turb2048_pcg_fp32|tg512|ldc64|ens256]
+                  [--members M]
 
 --impl reference times the reference algorithm's CPU restatement (the oracle
 port; the MATLAB reference itself cannot run here) on the host cores.
-Multi-GPU (torchrun): one independent replica of the workload per rank
-(weak scaling, no data-path collective), time = max over ranks.
+Multi-GPU (torchrun): single-grid workloads run one independent replica per
+rank (weak scaling, no data-path collective); the ensemble workload splits
+its members over the ranks (strong scaling); time = max over ranks.
 """
 import argparse
 import json

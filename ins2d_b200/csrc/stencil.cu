@@ -299,6 +299,41 @@ __device__ __forceinline__ S rw(const double *w, int r) {
   return S(__ldg(w + r));
 }
 
+// y-direction weights and metrics of one tile's rows, staged in shared
+// memory once per block (faces j0..j0+RUN, rows j0..j0+RUN-1): the walkers
+// read them per row without a global-memory round trip.
+struct YRows {
+  double auy0[RUN + 1], auy1[RUN + 1], suy0[RUN + 1], suy1[RUN + 1], ivy0[RUN + 1], ivy1[RUN + 1];
+  double avy0[RUN + 1], avy1[RUN + 1], svy0[RUN + 1], svy1[RUN + 1];
+  double hy[RUN], rhy[RUN], iuy0[RUN], iuy1[RUN], gyi[RUN], rgyi[RUN];
+};
+
+__device__ __forceinline__ void stage_yrows(const DevOps &P, int j0, YRows &Y) {
+  const int t = threadIdx.x + blockDim.x * threadIdx.y;
+  if (t <= RUN) {
+    const int r = j0 + t;
+    Y.auy0[t] = __ldg(P.rAUY.w0 + r);
+    Y.auy1[t] = __ldg(P.rAUY.w1 + r);
+    Y.suy0[t] = __ldg(P.rSUY.w0 + r);
+    Y.suy1[t] = __ldg(P.rSUY.w1 + r);
+    Y.ivy0[t] = __ldg(P.rIVY.w0 + r);
+    Y.ivy1[t] = __ldg(P.rIVY.w1 + r);
+    Y.avy0[t] = __ldg(P.rAVY.w0 + r);
+    Y.avy1[t] = __ldg(P.rAVY.w1 + r);
+    Y.svy0[t] = __ldg(P.rSVY.w0 + r);
+    Y.svy1[t] = __ldg(P.rSVY.w1 + r);
+  }
+  if (t < RUN) {
+    const int j = j0 + t;
+    Y.hy[t] = __ldg(P.hy + j);
+    Y.rhy[t] = __ldg(P.rhy + j);
+    Y.iuy0[t] = __ldg(P.rIUY.w0 + j);
+    Y.iuy1[t] = __ldg(P.rIUY.w1 + j);
+    Y.gyi[t] = __ldg(P.gyi + j);
+    Y.rgyi[t] = __ldg(P.rgyi + j);
+  }
+}
+
 // Raw loads of one row of the u walker: the x-face values of row j, the
 // field values of the y-face j+1 and the epilogue input; issued one row ahead
 // of their use so each warp keeps two rows of loads in flight.
@@ -310,7 +345,7 @@ struct URaw {
 
 template <typename S>
 __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
-                       int i, int j0, int j1) {
+                       int i, int j0, int j1, const YRows &Y) {
   const S ire = S(P.invRe);
   // columns (modulo the row length for periodic wraps)
   const int cA0 = wrapn(i + P.rAUX.s, P.rAUX.n), cA1 = wrapn(cA0 + 1, P.rAUX.n), cA2 = wrapn(cA1 + 1, P.rAUX.n);
@@ -343,9 +378,10 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
     }
   };
   auto face = [&](int r, const URaw<S> &q, S &uy, S &sy, S &vf) {
-    uy = rw<S>(P.rAUY.w0, r) * q.f0 + rw<S>(P.rAUY.w1, r) * q.f1;
-    sy = rw<S>(P.rSUY.w0, r) * q.f0 + rw<S>(P.rSUY.w1, r) * q.f1;
-    vf = rw<S>(P.rIVY.w0, r) * (iv0 * q.va0 + iv1 * q.va1) + rw<S>(P.rIVY.w1, r) * (iv0 * q.vb0 + iv1 * q.vb1);
+    const int y = r - j0;
+    uy = S(Y.auy0[y]) * q.f0 + S(Y.auy1[y]) * q.f1;
+    sy = S(Y.suy0[y]) * q.f0 + S(Y.suy1[y]) * q.f1;
+    vf = S(Y.ivy0[y]) * (iv0 * q.va0 + iv1 * q.va1) + S(Y.ivy1[y]) * (iv0 * q.vb0 + iv1 * q.vb1);
   };
   auto load_row = [&](int j, URaw<S> &q) {
     const double *row = u + (long long)j * Nux;
@@ -371,14 +407,14 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
     face(j + 1, cur, uy1, sy1, vf1);
     const S uxl = a00 * cur.um + a01 * cur.u0, uxr = a10 * cur.u0 + a11 * cur.up;
     const S sxl = s00 * cur.um + s01 * cur.u0, sxr = s10 * cur.u0 + s11 * cur.up;
-    const double hyd = __ldg(P.hy + j);
+    const double hyd = Y.hy[j - j0];
     const S hy = S(hyd);
     const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
     const S duvdy = vf1 * uy1 - vf0 * uy0;
     const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
     const double R = (double)(-(du2dx + duvdy) + d2u);
     const long long idx = (long long)j * Nux + i;
-    const double oi = __ldg(P.rhy + j) * rgx;
+    const double oi = Y.rhy[j - j0] * rgx;
     if (e.mode == 0) {
       const double k = oi * R;
       if (e.kV) e.kV[idx] = k;
@@ -406,7 +442,7 @@ struct VRaw {
 
 template <typename S>
 __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
-                       int i, int j0, int j1) {
+                       int i, int j0, int j1, const YRows &Y) {
   const S ire = S(P.invRe);
   const int cV0 = wrapn(i + P.rAVX.s, P.rAVX.n), cV1 = wrapn(cV0 + 1, P.rAVX.n), cV2 = wrapn(cV1 + 1, P.rAVX.n);
   const int cU0 = wrapn(i + P.rIUX.s, P.rIUX.n), cU1 = wrapn(cU0 + 1, P.rIUX.n), cU2 = wrapn(cU1 + 1, P.rIUX.n);
@@ -428,8 +464,9 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
     q.f1 = twoVy ? S(__ldg(v + (long long)wrapn(ra + 1, P.rAVY.n) * Nvx + i)) : S(0);
   };
   auto face = [&](int r, const VRaw<S> &q, S &vy, S &sy) {
-    vy = rw<S>(P.rAVY.w0, r) * q.f0 + rw<S>(P.rAVY.w1, r) * q.f1;
-    sy = rw<S>(P.rSVY.w0, r) * q.f0 + rw<S>(P.rSVY.w1, r) * q.f1;
+    const int y = r - j0;
+    vy = S(Y.avy0[y]) * q.f0 + S(Y.avy1[y]) * q.f1;
+    sy = S(Y.svy0[y]) * q.f0 + S(Y.svy1[y]) * q.f1;
   };
   auto load_row = [&](int j, VRaw<S> &q) {
     const double *row = v + (long long)j * Nvx;
@@ -471,15 +508,15 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
     // ubar at vx faces i, i+1: IUY row j times IUX rows i, i+1
     const S la = wu00 * cur.ua0 + wu01 * cur.ua1, ra = wu10 * cur.ua1 + wu11 * cur.ua2;
     const S lb = wu00 * cur.ub0 + wu01 * cur.ub1, rb = wu10 * cur.ub1 + wu11 * cur.ub2;
-    const S wy0 = rw<S>(P.rIUY.w0, j), wy1 = rw<S>(P.rIUY.w1, j);
+    const S wy0 = S(Y.iuy0[j - j0]), wy1 = S(Y.iuy1[j - j0]);
     const S ufl = wy0 * la + wy1 * lb, ufr = wy0 * ra + wy1 * rb;
     const S duvdx = ufr * vxr - ufl * vxl;
     const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
-    const double gyd = __ldg(P.gyi + j);
+    const double gyd = Y.gyi[j - j0];
     const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
     const double R = (double)(-(duvdx + dv2dy) + d2v);
     const long long idx = P.Nu + (long long)j * Nvx + i;
-    const double oi = __ldg(P.rgyi + j) * rhx;
+    const double oi = Y.rgyi[j - j0] * rhx;
     if (e.mode == 0) {
       const double k = oi * R;
       if (e.kV) e.kV[idx] = k;
@@ -501,13 +538,16 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
 // one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
 template <typename S>
 __device__ __forceinline__ void tile_fast(const DevOps &P, const double *__restrict__ V, const Epi &e, int bx, int by) {
+  __shared__ YRows Y;
   const int i = bx * WX + threadIdx.x;
   const int j0 = by * RUN, j1 = j0 + RUN;
   const double *u = V, *v = V + P.Nu;
+  stage_yrows(P, j0, Y);
+  __syncthreads();
   if (threadIdx.y == 0)
-    fast_u<S>(P, u, v, e, i, j0, j1);
+    fast_u<S>(P, u, v, e, i, j0, j1, Y);
   else
-    fast_v<S>(P, u, v, e, i, j0, j1);
+    fast_v<S>(P, u, v, e, i, j0, j1, Y);
 }
 template <typename S>
 __device__ __forceinline__ void tile_generic(const DevOps &P, const double *__restrict__ V, const Epi &e, int bx,

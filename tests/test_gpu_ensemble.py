@@ -66,9 +66,21 @@ def test_ensemble_matches_single_runs(seed, n, sizes, solver):
         assert ens.member(m).check_conservation(Ve, nsteps * dt)[0] < 1e-10
 
 
-def test_ensemble_rejects_mixed_settings():
+def test_ensemble_rejects_unsupported_members():
+    """Mixed solver settings, unsteady boundary conditions and the FFT solver
+    are refused with EINVAL (no member is advanced)."""
     import ins2d_b200
     members = _members(1, 2, [16, 24])
     members[1]["CG_acc"] = 1e-6
-    with pytest.raises(ins2d_b200.Ins2dError):
+    with pytest.raises(ins2d_b200.Ins2dError) as ei:
         ins2d_b200.Ensemble(members)
+    assert ei.value.status == 1
+    members = _members(1, 2, [16, 24])
+    members[0]["BC"] = dict(members[0]["BC"], BC_unsteady=1)
+    with pytest.raises(ins2d_b200.Ins2dError) as ei:
+        ins2d_b200.Ensemble(members)
+    assert ei.value.status == 1
+    x = cases.uniform_grid(16, 0.0, 1.0)
+    with pytest.raises(ins2d_b200.Ins2dError) as ei:
+        ins2d_b200.Ensemble([dict(x=x, y=x.copy(), BC=cases.BC_PERIODIC, Re=100.0, poisson=6)])
+    assert ei.value.status == 1
