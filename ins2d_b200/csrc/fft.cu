@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
     for (int m = 0; m < 8; ++m) {
       const int J = brev(8 * k + m, L);
       const double2 F = x[m];
-      lmax = fmax(lmax, sqrt(F.x * F.x + F.y * F.y));
+      lmax = fmax(lmax, F.x * F.x + F.y * F.y);  // squared; one square root per block
       const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + I) + __ldg(ay + J));
       const double r = -1.0 / lam;
       x[m] = make_double2(F.x * r, F.y * r);
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
   if (threadIdx.x == 0) {
     double mm = wmax[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mm = fmax(mm, wmax[w]);
-    atomicMax(maxbits, (unsigned long long)__double_as_longlong(mm));
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(sqrt(mm)));
   }
 }
 

@@ -305,7 +305,7 @@ __device__ __forceinline__ S rw(const double *w, int r) {
 struct YRows {
   double auy0[RUN + 1], auy1[RUN + 1], suy0[RUN + 1], suy1[RUN + 1], ivy0[RUN + 1], ivy1[RUN + 1];
   double avy0[RUN + 1], avy1[RUN + 1], svy0[RUN + 1], svy1[RUN + 1];
-  double hy[RUN], rhy[RUN], iuy0[RUN], iuy1[RUN], gyi[RUN], rgyi[RUN];
+  double hy[RUN], rhy[RUN], iuy0[RUN], iuy1[RUN], gyi[RUN], rgyi[RUN], myt0[RUN], myt1[RUN];
 };
 
 __device__ __forceinline__ void stage_yrows(const DevOps &P, int j0, YRows &Y) {
@@ -331,6 +331,8 @@ __device__ __forceinline__ void stage_yrows(const DevOps &P, int j0, YRows &Y) {
     Y.iuy1[t] = __ldg(P.rIUY.w1 + j);
     Y.gyi[t] = __ldg(P.gyi + j);
     Y.rgyi[t] = __ldg(P.rgyi + j);
+    Y.myt0[t] = __ldg(P.rMYT.w0 + j);
+    Y.myt1[t] = __ldg(P.rMYT.w1 + j);
   }
 }
 
@@ -525,7 +527,11 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
       vt += e.aii * k;
       e.Wt[idx] = cur.ep * e.inv_dt + vt;
     } else {
-      const double g = -hxd * reg_y(P.rMYT, j, e.p, P.Npx, i);
+      // (G p)_v = -hx MYT p with the row's weights from shared memory
+      const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
+      double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
+      if (P.rMYT.two) gy += Y.myt1[j - j0] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
+      const double g = -hxd * gy;
       e.w[idx] = oi * (R - g);
       if (e.kV_next) e.kV_next[idx] = oi * R;
     }
