@@ -84,3 +84,23 @@ def test_ensemble_rejects_unsupported_members():
     with pytest.raises(ins2d_b200.Ins2dError) as ei:
         ins2d_b200.Ensemble([dict(x=x, y=x.copy(), BC=cases.BC_PERIODIC, Re=100.0, poisson=6)])
     assert ei.value.status == 1
+
+
+def test_ensemble_reports_failing_member():
+    """A member whose state holds a NaN makes the run return ENONFINITE naming
+    that member; the other members are still advanced."""
+    import ins2d_b200
+    members = _members(3, 3, [24, 32])
+    ens = ins2d_b200.Ensemble(members)
+    ens.set_solver(0)
+    for m in range(3):
+        o = ens.member(m)
+        V = np.zeros(o.NV)
+        if m == 1:
+            V[5] = np.nan
+        ens.set_state(m, V, np.zeros(o.Np))
+    with pytest.raises(ins2d_b200.Ins2dError) as ei:
+        ens.time_ERK(0.0, 1e-3, 1)
+    assert ei.value.status == 4 and "member 1" in str(ei.value)
+    V0, _ = ens.get_state(0)
+    assert np.all(np.isfinite(V0)) and np.max(np.abs(V0)) > 0.0

@@ -225,3 +225,20 @@ def test_pcg_preconditioners(combo, shape, precond):
     if is_closed(bc):
         dp, dp_ref = dp - dp.mean(), dp_ref - dp_ref.mean()
     assert _rel(dp, dp_ref) < 1e-8
+
+
+@pytest.mark.parametrize("poisson,precond", [(4, "mg"), (4, "jacobi")])
+def test_nonfinite_rhs_reports_error(poisson, precond):
+    """A NaN in the right-hand side ends the solve with INS2D_ENONFINITE (the
+    device path reports it as a status; no fault, the context stays usable)."""
+    o, _ = _pair("cavity", False, nx=24, ny=20)
+    m = _ins2d().Options(o.grid.x, o.grid.y, BC_COMBOS["cavity"], Re=45.0, poisson=poisson, CG_acc=1e-12,
+                         precond=precond)
+    f = o.discretization.M @ np.random.default_rng(1).standard_normal(o.grid.NV) + o.discretization.yM
+    bad = f.copy()
+    bad[7] = np.nan
+    with pytest.raises(_ins2d().Ins2dError) as ei:
+        m.pressure_poisson(bad)
+    assert ei.value.status == 4  # INS2D_ENONFINITE
+    dp = m.pressure_poisson(f)  # the context still works
+    assert np.linalg.norm(o.discretization.A @ dp - f) <= 2e-12 * np.linalg.norm(f)
