@@ -222,7 +222,7 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
  * pressure_poisson.m:92-104 with its early return -- for device arrays f, dp
  * on the current device and a cudaStream_t stream (NULL = default stream).
  * Allocates nothing: the scratch lives in one static device array of
- * about 8.5 MB that every GPU loading the library keeps until exit.
+ * about 8.8 MB that every GPU loading the library keeps until exit.
  * Limits: 2 <= Nx, Ny <= INS2D_NOALLOC_MAX_N, Nx*Ny <= INS2D_NOALLOC_MAX_CELLS,
  * and sizes the FFT path supports; other sizes return INS2D_EINVAL.
  * The first call on a device looks up the array's device address and sets

@@ -578,18 +578,9 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
       F.Ny = H.Ny;
       F.logx = is_pow2(H.Nx) ? (int)std::lround(std::log2((double)H.Nx)) : -1;
       F.logy = is_pow2(H.Ny) ? (int)std::lround(std::log2((double)H.Ny)) : -1;
-      auto tw = [&](int n) {
-        std::vector<double> v(2 * (size_t)n);
-        for (int k = 0; k < n; ++k) {
-          const double ang = 2.0 * M_PI * (double)k / (double)n;
-          v[2 * k] = std::cos(ang);
-          v[2 * k + 1] = -std::sin(ang);
-        }
-        return v;
-      };
-      auto tx = tw(H.Nx), ty = tw(H.Ny);
-      F.twx = dalloc<double2>(c, H.Nx);
-      F.twy = dalloc<double2>(c, H.Ny);
+      const std::vector<double> tx = fft_twiddle_table(H.Nx), ty = fft_twiddle_table(H.Ny);
+      F.twx = dalloc<double2>(c, 2 * (size_t)H.Nx);
+      F.twy = dalloc<double2>(c, 2 * (size_t)H.Ny);
       CK(cudaMemcpy(F.twx, tx.data(), tx.size() * sizeof(double), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(F.twy, ty.data(), ty.size() * sizeof(double), cudaMemcpyHostToDevice));
       F.spec = dalloc<double2>(c, (size_t)(H.Nx / 2 + 1) * H.Ny);

@@ -13,6 +13,9 @@
 //     inverse FFT (scaled 1/Nx).
 // Power-of-two lengths use radix-2 DIT/DIF with a twiddle table; other
 // lengths use a shared-memory DFT (O(N^2), small grids).
+#include <cmath>
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace ins2d {
@@ -48,10 +51,17 @@ __device__ __forceinline__ double2 twid(const double2 *tw, int k, bool inv) {
 }
 __device__ __forceinline__ int brev(int k, int logn) { return (int)(__brev((unsigned)k) >> (32 - logn)); }
 
-// Shared-memory layout: one padding slot after every 8 complex values keeps
-// strided butterfly accesses free of bank conflicts.
-__device__ __forceinline__ int pd(int i) { return i + (i >> 3); }
-__host__ __device__ __forceinline__ int padded(int n) { return n + (n >> 3) + 1; }
+// Shared-memory layout: complex value i sits at i + i/8 + i/64 + i/512 +
+// i/4096.  A 16-byte access is served eight lanes at a time, so the eight
+// lanes must fall on distinct 16-byte bank groups (slot mod 8): the i/8 term
+// does that for the strided butterfly accesses, the others for the
+// bit-reversed readouts (eight lanes 2^(L-3) apart).  Line strides are 4 mod 8,
+// so two lines interleaved in one warp (column blocks) use disjoint groups.
+__host__ __device__ __forceinline__ int pd(int i) { return i + (i >> 3) + (i >> 6) + (i >> 9) + (i >> 12); }
+__host__ __device__ __forceinline__ int padded(int n) {
+  const int p = pd(n - 1) + 1;
+  return p + ((4 - p) & 7);
+}
 
 // In-place radix-2 decimation in time on G lines of length n (input in
 // bit-reversed order, output natural), three stages per pass: each thread
@@ -292,33 +302,81 @@ __global__ void __launch_bounds__(kThreads) k_rows_c2r(int Nx, int Ny, int logx,
 // ---------------------------------------------------------------------------
 // Register groups of up to three radix-2 stages on 8 values x[m] at positions
 // base + m*h (h = half size of the smallest stage of the group, k = base mod h).
-__device__ __forceinline__ void group_dif(double2 (&x)[8], int ns, int k, int h, int s_lo, int logn,
-                                          const double2 *tw, bool inv) {
+// The stage with half size hh*h multiplies by W_{2 hh h}^(k + j h), j < hh,
+// = W_{2 hh h}^k * W_{2 hh}^j: the first factor is a power of the group's top
+// twiddle W_{R h}^k (R = 2^ns values; read once from the pyramid table, whose
+// level of length Lt holds W_Lt^k, k < Lt/2, at Lt/2 + k, so lanes with
+// consecutive k read consecutive entries), the second one of the eighth roots
+// of unity, applied as adds and one scaling.
+
+// a * W_{2 hh}^j (conjugate root when inv), j < hh <= 4
+__device__ __forceinline__ double2 rot(double2 a, int hh, int j, bool inv) {
+  constexpr double r = 0.70710678118654752440;  // 1/sqrt(2)
+  if (j == 0) return a;
+  if (2 * j == hh) return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);  // +i / -i
+  if (j == 1)  // (1 + i)/sqrt(2) / (1 - i)/sqrt(2)
+    return inv ? make_double2((a.x - a.y) * r, (a.x + a.y) * r) : make_double2((a.x + a.y) * r, (a.y - a.x) * r);
+  // j == 3: (-1 + i)/sqrt(2) / (-1 - i)/sqrt(2)
+  return inv ? make_double2(-(a.x + a.y) * r, (a.x - a.y) * r) : make_double2((a.y - a.x) * r, -(a.x + a.y) * r);
+}
+__device__ __forceinline__ double2 csq(double2 a) { return make_double2(a.x * a.x - a.y * a.y, 2.0 * a.x * a.y); }
+
+// base twiddles W_{2^(st+1) h}^k of the group's stages st = 0, 1, 2
+__device__ __forceinline__ void group_twiddles(int ns, int k, int h, const double2 *pyr, bool inv, double2 &w0,
+                                               double2 &w1, double2 &w2) {
+  double2 wt = __ldg(pyr + (((1 << ns) * h) >> 1) + k);
+  if (inv) wt.y = -wt.y;
+  if (ns == 3) {
+    w2 = wt;
+    w1 = csq(w2);
+    w0 = csq(w1);
+  } else if (ns == 2) {
+    w1 = w2 = wt;
+    w0 = csq(w1);
+  } else {
+    w0 = w1 = w2 = wt;
+  }
+}
+
+// UNIT: k = 0, h = 1 (all twiddles are roots of unity of order <= 8)
+template <bool UNIT>
+__device__ __forceinline__ void group_dif(double2 (&x)[8], int ns, int k, int h, const double2 *pyr, bool inv) {
+  double2 w0 = make_double2(1.0, 0.0), w1 = w0, w2 = w0;
+  if (!UNIT) group_twiddles(ns, k, h, pyr, inv, w0, w1, w2);
 #pragma unroll
   for (int st = 2; st >= 0; --st) {
     if (st >= ns) continue;
-    const int hh = 1 << st, sh = logn - (s_lo + st);
+    const int hh = 1 << st;
+    double2 tw[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j < hh) tw[j] = rot(st == 2 ? w2 : (st == 1 ? w1 : w0), hh, j, inv);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       if ((m & (2 * hh - 1)) >= hh || m + hh >= (1 << ns)) continue;
-      const int off = k + (m & (hh - 1)) * h;
       const double2 x0 = x[m], x1 = x[m + hh];
+      const double2 d = make_double2(x0.x - x1.x, x0.y - x1.y);
       x[m] = make_double2(x0.x + x1.x, x0.y + x1.y);
-      x[m + hh] = cmul(make_double2(x0.x - x1.x, x0.y - x1.y), twid(tw, off << sh, inv));
+      x[m + hh] = UNIT ? rot(d, hh, m & (hh - 1), inv) : cmul(d, tw[m & (hh - 1)]);
     }
   }
 }
-__device__ __forceinline__ void group_dit(double2 (&x)[8], int ns, int k, int h, int s0, int logn,
-                                          const double2 *tw, bool inv) {
+template <bool UNIT>
+__device__ __forceinline__ void group_dit(double2 (&x)[8], int ns, int k, int h, const double2 *pyr, bool inv) {
+  double2 w0 = make_double2(1.0, 0.0), w1 = w0, w2 = w0;
+  if (!UNIT) group_twiddles(ns, k, h, pyr, inv, w0, w1, w2);
 #pragma unroll
   for (int st = 0; st < 3; ++st) {
     if (st >= ns) break;
-    const int hh = 1 << st, sh = logn - (s0 + st + 1);
+    const int hh = 1 << st;
+    double2 tw[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (j < hh) tw[j] = rot(st == 2 ? w2 : (st == 1 ? w1 : w0), hh, j, inv);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       if ((m & (2 * hh - 1)) >= hh || m + hh >= (1 << ns)) continue;
-      const int off = k + (m & (hh - 1)) * h;
-      const double2 y = cmul(twid(tw, off << sh, inv), x[m + hh]);
+      const double2 y = UNIT ? rot(x[m + hh], hh, m & (hh - 1), inv) : cmul(tw[m & (hh - 1)], x[m + hh]);
       x[m + hh] = make_double2(x[m].x - y.x, x[m].y - y.y);
       x[m] = make_double2(x[m].x + y.x, x[m].y + y.y);
     }
@@ -327,7 +385,7 @@ __device__ __forceinline__ void group_dit(double2 (&x)[8], int ns, int k, int h,
 
 // Shared-memory passes over stages s_top down to s_bot (DIF) / s_bot up to
 // s_top (DIT), three stages per pass.
-__device__ void dif_range(double2 *a, int G, int n, int logn, const double2 *tw, bool inv, int s_top, int s_bot) {
+__device__ void dif_range(double2 *a, int G, int n, const double2 *pyr, bool inv, int s_top, int s_bot) {
   const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
   for (int s_hi = s_top; s_hi >= s_bot; s_hi -= 3) {
     const int ns = min(3, s_hi - s_bot + 1), s_lo = s_hi - ns + 1;
@@ -341,7 +399,7 @@ __device__ void dif_range(double2 *a, int G, int n, int logn, const double2 *tw,
 #pragma unroll
       for (int m = 0; m < 8; ++m)
         if (m < R) x[m] = L[pd(base + m * h)];
-      group_dif(x, ns, k, h, s_lo, logn, tw, inv);
+      group_dif<false>(x, ns, k, h, pyr, inv);
 #pragma unroll
       for (int m = 0; m < 8; ++m)
         if (m < R) L[pd(base + m * h)] = x[m];
@@ -349,7 +407,7 @@ __device__ void dif_range(double2 *a, int G, int n, int logn, const double2 *tw,
     __syncthreads();
   }
 }
-__device__ void dit_range(double2 *a, int G, int n, int logn, const double2 *tw, bool inv, int s_bot, int s_top) {
+__device__ void dit_range(double2 *a, int G, int n, const double2 *pyr, bool inv, int s_bot, int s_top) {
   const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
   for (int s0 = s_bot - 1; s0 < s_top; s0 += 3) {
     const int ns = min(3, s_top - s0), R = 1 << ns, h = 1 << s0, per = n >> ns;
@@ -362,7 +420,7 @@ __device__ void dit_range(double2 *a, int G, int n, int logn, const double2 *tw,
 #pragma unroll
       for (int m = 0; m < 8; ++m)
         if (m < R) x[m] = L[pd(base + m * h)];
-      group_dit(x, ns, k, h, s0, logn, tw, inv);
+      group_dit<false>(x, ns, k, h, pyr, inv);
 #pragma unroll
       for (int m = 0; m < 8; ++m)
         if (m < R) L[pd(base + m * h)] = x[m];
@@ -372,7 +430,8 @@ __device__ void dit_range(double2 *a, int G, int n, int logn, const double2 *tw,
 }
 
 // --- power-of-two lengths >= 64: first and last radix-8 passes fused with
-// the global loads/stores, no permutation passes --------------------------------
+// the global loads/stores, no permutation passes; tw is the table of
+// fft_twiddle_table (the pyramid at tw + N) ----------------------------------
 
 // rows j0, j1 -> half spectra (forward DIF; bit-reversed result read back
 // during the Hermitian split)
@@ -385,6 +444,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_r2c_f(in
                                                          const __grid_constant__ DevOps P, double alpha, double beta,
                                                          double gamma) {
   extern __shared__ double2 sm[];
+  const double2 *pyr = tw + Nx;
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
   const bool has1 = j1 < Ny;
   const int H = Nx / 2 + 1, per = Nx >> 3;
@@ -399,12 +459,12 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_r2c_f(in
       else
         x[m] = make_double2(__ldg(r0 + k + m * per), has1 ? __ldg(r1 + k + m * per) : 0.0);
     }
-    group_dif(x, 3, k, per, L - 2, L, tw, false);
+    group_dif<false>(x, 3, k, per, pyr, false);
 #pragma unroll
     for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
   }
   __syncthreads();
-  dif_range(sm, 1, Nx, L, tw, false, L - 3, 1);
+  dif_range(sm, 1, Nx, pyr, false, L - 3, 1);
   for (int I = threadIdx.x; I < H; I += blockDim.x) {
     const double2 z = sm[pd(brev(I, L))], m = sm[pd(brev((Nx - I) & (Nx - 1), L))];
     spec[(size_t)j0 * H + I] = make_double2(0.5 * (z.x + m.x), 0.5 * (z.y - m.y));
@@ -420,6 +480,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
                                                      unsigned long long *__restrict__ maxbits) {
   extern __shared__ double2 sm[];
   __shared__ double wmax[kThreads / 32];
+  const double2 *pyr = tw + Ny;
   const int H = Nx / 2 + 1, per = Ny >> 3, ld = padded(Ny);
   const int c0 = blockIdx.x * G;
   const int g_here = min(G, H - c0);
@@ -428,12 +489,12 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
     double2 x[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) x[m] = spec[(size_t)(k + m * per) * H + c0 + line];
-    group_dif(x, 3, k, per, L - 2, L, tw, false);
+    group_dif<false>(x, 3, k, per, pyr, false);
 #pragma unroll
     for (int m = 0; m < 8; ++m) sm[(size_t)line * ld + pd(k + m * per)] = x[m];
   }
   __syncthreads();
-  dif_range(sm, g_here, Ny, L, tw, false, L - 3, 4);
+  dif_range(sm, g_here, Ny, pyr, false, L - 3, 4);
   double lmax = 0.0;
   for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
     const int line = gidx / per, k = gidx - line * per;
@@ -442,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
     double2 x[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) x[m] = Ls[pd(8 * k + m)];
-    group_dif(x, 3, 0, 1, 1, L, tw, false);
+    group_dif<true>(x, 3, 0, 1, pyr, false);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int J = brev(8 * k + m, L);
@@ -452,19 +513,19 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
       const double r = -1.0 / lam;
       x[m] = make_double2(F.x * r, F.y * r);
     }
-    group_dit(x, 3, 0, 1, 0, L, tw, true);
+    group_dit<true>(x, 3, 0, 1, pyr, true);
 #pragma unroll
     for (int m = 0; m < 8; ++m) Ls[pd(8 * k + m)] = x[m];
   }
   __syncthreads();
-  dit_range(sm, g_here, Ny, L, tw, true, 4, L - 3);
+  dit_range(sm, g_here, Ny, pyr, true, 4, L - 3);
   const double sc = 1.0 / Ny;
   for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
     const int k = gidx / g_here, line = gidx - k * g_here;
     double2 x[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) x[m] = sm[(size_t)line * ld + pd(k + m * per)];
-    group_dit(x, 3, k, per, L - 3, L, tw, true);
+    group_dit<false>(x, 3, k, per, pyr, true);
 #pragma unroll
     for (int m = 0; m < 8; ++m)
       spec[(size_t)(k + m * per) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
@@ -497,6 +558,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_c2r_f(in
       }
     return;
   }
+  const double2 *pyr = tw + Nx;
   const double2 *s0 = spec + (size_t)j0 * H, *s1 = spec + (size_t)j1 * H;
   for (int k = threadIdx.x; k < per; k += blockDim.x) {
     double2 x[8];
@@ -515,12 +577,12 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_c2r_f(in
       }
       x[m] = make_double2(g0.x - g1.y, g0.y + g1.x);
     }
-    group_dif(x, 3, k, per, L - 2, L, tw, true);
+    group_dif<false>(x, 3, k, per, pyr, true);
 #pragma unroll
     for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
   }
   __syncthreads();
-  dif_range(sm, 1, Nx, L, tw, true, L - 3, 1);
+  dif_range(sm, 1, Nx, pyr, true, L - 3, 1);
   const double sc = 1.0 / Nx;
   for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
     const double2 w = sm[pd(brev(k, L))];
@@ -551,6 +613,23 @@ int cols_group(int Ny, bool pow2) {
 }
 
 }  // namespace
+
+std::vector<double> fft_twiddle_table(int n) {
+  std::vector<double> v(4 * (size_t)n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const double ang = 2.0 * M_PI * (double)k / (double)n;
+    v[2 * k] = std::cos(ang);
+    v[2 * k + 1] = -std::sin(ang);
+  }
+  if (ilog2_exact(n) >= 0)
+    for (int Lt = 2; Lt <= n; Lt *= 2)
+      for (int k = 0; k < Lt / 2; ++k) {
+        const double ang = 2.0 * M_PI * (double)k / (double)Lt;
+        v[2 * ((size_t)n + Lt / 2 + k)] = std::cos(ang);
+        v[2 * ((size_t)n + Lt / 2 + k) + 1] = -std::sin(ang);
+      }
+  return v;
+}
 
 bool fft_supported(int Nx, int Ny) {
   auto ok = [](int n) { return n >= 2 && ((ilog2_exact(n) >= 0 && n <= kMaxPow2) || n <= kMaxGeneric); };

@@ -97,11 +97,15 @@ void launch_stage_cached_ens(const EnsMemberD *mem, const int4 *tiles, int n, do
 // --- FFT Poisson (fft.cu) -------------------------------------------------------
 struct FftPlan {
   int Nx = 0, Ny = 0, logx = -1, logy = -1;  // log2 when a power of two, else -1
-  double2 *twx = nullptr, *twy = nullptr;    // twiddles e^{-2 pi i k/N}
+  double2 *twx = nullptr, *twy = nullptr;    // 2N entries each: fft_twiddle_table(N)
   double2 *spec = nullptr;                   // (Nx/2+1) x Ny complex spectrum
   double *maxabs = nullptr;                  // max |fhat| of the last solve
 };
 bool fft_supported(int Nx, int Ny);
+// Twiddles of a length-n transform as 2n complex values (4n doubles): entries
+// [0, n) hold e^{-2 pi i k/n}; for power-of-two n, entry n + Lt/2 + k holds
+// e^{-2 pi i k/Lt} for every power of two 2 <= Lt <= n and k < Lt/2.
+std::vector<double> fft_twiddle_table(int n);
 // dp = real(ifft2(-fft2(f)./Ahat)) (pressure_poisson.m:92-104); dp += result when
 // accumulate.  Returns 0 (dp untouched / zero) when max|fhat| < 1e-14 (:21-32).
 void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,

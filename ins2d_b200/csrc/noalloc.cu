@@ -28,10 +28,11 @@ namespace {
 constexpr int kMaxN = INS2D_NOALLOC_MAX_N;
 constexpr long long kMaxCells = INS2D_NOALLOC_MAX_CELLS;
 // layout in double2 units: spectrum ((Nx/2+1)*Ny <= kMaxCells/2 + kMaxN),
-// twiddles x and y (<= kMaxN each), symbol factors x and y (<= kMaxN doubles
-// each = kMaxN/2 double2), max|fhat| (one double, padded to a double2)
+// twiddle tables x and y (2N <= 2 kMaxN each), symbol factors x and y
+// (<= kMaxN doubles each = kMaxN/2 double2), max|fhat| (one double, padded to
+// a double2)
 constexpr size_t kSpec = (size_t)(kMaxCells / 2 + kMaxN);
-constexpr size_t kTotal = kSpec + 2 * (size_t)kMaxN + (size_t)kMaxN + 1;
+constexpr size_t kTotal = kSpec + 4 * (size_t)kMaxN + (size_t)kMaxN + 1;
 
 static __device__ __align__(256) double2 g_scratch[kTotal];
 
@@ -70,29 +71,24 @@ extern "C" int ins2d_fft_poisson_noalloc(const double *f, double *dp, int32_t Nx
     base = g_scratch_addr[dev];
   }
   cudaStream_t s = (cudaStream_t)stream;
-  // twiddles e^{-2 pi i k/N} and the symbol factors (1/dx^2) sin^2(I pi/Nx),
+  // twiddle tables and the symbol factors (1/dx^2) sin^2(I pi/Nx),
   // (1/dy^2) sin^2(J pi/Ny) of operator_divergence.m:283, as in the context path
-  std::vector<double> tx(2 * (size_t)Nx), ty(2 * (size_t)Ny), ax((size_t)Nx), ay((size_t)Ny);
+  const std::vector<double> tx = fft_twiddle_table(Nx), ty = fft_twiddle_table(Ny);
+  std::vector<double> ax((size_t)Nx), ay((size_t)Ny);
   for (int k = 0; k < Nx; ++k) {
-    const double a = 2.0 * M_PI * (double)k / (double)Nx;
-    tx[2 * k] = std::cos(a);
-    tx[2 * k + 1] = -std::sin(a);
     const double sn = std::sin((double)k * M_PI / Nx);
     ax[k] = (1.0 / (dx * dx)) * (sn * sn);
   }
   for (int k = 0; k < Ny; ++k) {
-    const double a = 2.0 * M_PI * (double)k / (double)Ny;
-    ty[2 * k] = std::cos(a);
-    ty[2 * k + 1] = -std::sin(a);
     const double sn = std::sin((double)k * M_PI / Ny);
     ay[k] = (1.0 / (dy * dy)) * (sn * sn);
   }
   double2 *spec = base;
   double2 *twx = base + kSpec;
-  double2 *twy = twx + kMaxN;
-  double *axd = (double *)(twy + kMaxN);  // kMaxN doubles
-  double *ayd = axd + kMaxN;              // kMaxN doubles
-  double *maxabs = (double *)(base + kSpec + 3 * (size_t)kMaxN);
+  double2 *twy = twx + 2 * (size_t)kMaxN;
+  double *axd = (double *)(twy + 2 * (size_t)kMaxN);  // kMaxN doubles
+  double *ayd = axd + kMaxN;                           // kMaxN doubles
+  double *maxabs = (double *)(base + kSpec + 5 * (size_t)kMaxN);
   if (cudaMemcpyAsync(twx, tx.data(), tx.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(twy, ty.data(), ty.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
       cudaMemcpyAsync(axd, ax.data(), ax.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||

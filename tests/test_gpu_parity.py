@@ -70,7 +70,8 @@ def test_F_divergence_laplacian(combo, stretch):
         assert abs(a - b) <= 1e-12 * max(abs(b), 1.0)
 
 
-@pytest.mark.parametrize("nx,ny", [(16, 8), (40, 40), (64, 32), (12, 10), (128, 128)])
+@pytest.mark.parametrize("nx,ny", [(16, 8), (40, 40), (64, 32), (12, 10), (128, 128), (1024, 512), (2048, 2048),
+                                   (8192, 64), (64, 8192), (4096, 32)])
 def test_fft_poisson(nx, ny):
     x = grid_uniform(nx, 0.0, 2 * np.pi)
     y = grid_uniform(ny, 0.0, 3.0)
