@@ -14,6 +14,7 @@
 // Power-of-two lengths use radix-2 DIT/DIF with a twiddle table; other
 // lengths use a shared-memory DFT (O(N^2), small grids).
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "kernels.cuh"
@@ -383,126 +384,181 @@ __device__ __forceinline__ void group_dit(double2 (&x)[8], int ns, int k, int h,
   }
 }
 
-// Shared-memory passes over stages s_top down to s_bot (DIF) / s_bot up to
-// s_top (DIT), three stages per pass.
-__device__ void dif_range(double2 *a, int G, int n, const double2 *pyr, bool inv, int s_top, int s_bot) {
-  const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
-  for (int s_hi = s_top; s_hi >= s_bot; s_hi -= 3) {
-    const int ns = min(3, s_hi - s_bot + 1), s_lo = s_hi - ns + 1;
-    const int R = 1 << ns, h = 1 << (s_lo - 1), per = n >> ns;
-    for (int g = t; g < G * per; g += nt) {
-      const int line = g / per, gg = g - line * per;
-      const int k = gg & (h - 1), blk = gg >> (s_lo - 1);
-      const int base = blk * R * h + k;
-      double2 *L = a + (size_t)line * ld;
-      double2 x[8];
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-        if (m < R) x[m] = L[pd(base + m * h)];
-      group_dif<false>(x, ns, k, h, pyr, inv);
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-        if (m < R) L[pd(base + m * h)] = x[m];
-    }
-    __syncthreads();
-  }
+// --- power-of-two lengths 2^L, 6 <= L <= 13: every shape a compile-time
+// constant; the first and last radix-8 passes fused with the global loads and
+// stores, no permutation passes; tw is the table of fft_twiddle_table (the
+// pyramid at tw + 2^L) ---------------------------------------------------------
+
+// Slot of complex value i in a line of length 2^L: the general layout above,
+// or for L >= 9 the cheaper i + i/8 + i/2^(L-3), conflict-free for the same
+// accesses at those lengths (the last term spreads the bit-reversed readouts,
+// whose eight lanes lie 2^(L-3) apart).
+template <int L>
+__host__ __device__ constexpr int pdl(int i) {
+  return L >= 9 ? i + (i >> 3) + (i >> (L - 3)) : i + (i >> 3) + (i >> 6) + (i >> 9) + (i >> 12);
 }
-__device__ void dit_range(double2 *a, int G, int n, const double2 *pyr, bool inv, int s_bot, int s_top) {
-  const int t = threadIdx.x, nt = blockDim.x, ld = padded(n);
-  for (int s0 = s_bot - 1; s0 < s_top; s0 += 3) {
-    const int ns = min(3, s_top - s0), R = 1 << ns, h = 1 << s0, per = n >> ns;
-    for (int g = t; g < G * per; g += nt) {
-      const int line = g / per, gg = g - line * per;
-      const int k = gg & (h - 1), blk = gg >> s0;
-      const int base = blk * R * h + k;
-      double2 *L = a + (size_t)line * ld;
-      double2 x[8];
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-        if (m < R) x[m] = L[pd(base + m * h)];
-      group_dit<false>(x, ns, k, h, pyr, inv);
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-        if (m < R) L[pd(base + m * h)] = x[m];
-    }
-    __syncthreads();
-  }
+template <int L>
+__host__ __device__ constexpr int paddedl() {
+  return (pdl<L>((1 << L) - 1) + 1) + ((4 - (pdl<L>((1 << L) - 1) + 1)) & 7);
+}
+// spectrum columns per column block: two 2048-point columns (32-byte row
+// segments) in the shared-memory budget, more for short columns
+template <int L>
+constexpr int cols_per_block() {
+  constexpr int per = paddedl<L>() * 16;
+  constexpr int g = (INS2D_FFT_COLS_BUDGET * 1024) / per;
+  constexpr int g8 = g > 8 ? 8 : (g < 1 ? 1 : g);
+  return (L >= 10 && g8 > INS2D_FFT_COLS_G) ? INS2D_FFT_COLS_G : g8;
 }
 
-// --- power-of-two lengths >= 64: first and last radix-8 passes fused with
-// the global loads/stores, no permutation passes; tw is the table of
-// fft_twiddle_table (the pyramid at tw + N) ----------------------------------
+// DIF passes over stages S_HI down to S_BOT (three per pass) on the first
+// `lines` of G lines of stride ld
+template <int L, int S_HI, int S_BOT, int G>
+__device__ __forceinline__ void dif_passes(double2 *a, int ld, int lines, const double2 *pyr, bool inv) {
+  if constexpr (S_HI >= S_BOT) {
+    constexpr int NS = (S_HI - S_BOT + 1) < 3 ? (S_HI - S_BOT + 1) : 3;
+    constexpr int S_LO = S_HI - NS + 1, R = 1 << NS, H = 1 << (S_LO - 1), PER = (1 << L) >> NS;
+    const unsigned lim = (G > 1 ? lines : 1) * PER;
+    for (unsigned g = threadIdx.x; g < lim; g += kThreads) {
+      const int line = (int)(g / PER), gg = (int)(g % PER);
+      const int k = gg & (H - 1), blk = gg >> (S_LO - 1);
+      const int base = blk * R * H + k;
+      double2 *Lp = a + line * ld;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < R; ++m) x[m] = Lp[pdl<L>(base + m * H)];
+      group_dif<false>(x, NS, k, H, pyr, inv);
+#pragma unroll
+      for (int m = 0; m < R; ++m) Lp[pdl<L>(base + m * H)] = x[m];
+    }
+    __syncthreads();
+    dif_passes<L, S_HI - 3, S_BOT, G>(a, ld, lines, pyr, inv);
+  }
+}
+// DIT passes over stages S0 + 1 up to S_TOP (three per pass)
+template <int L, int S0, int S_TOP, int G>
+__device__ __forceinline__ void dit_passes(double2 *a, int ld, int lines, const double2 *pyr, bool inv) {
+  if constexpr (S0 < S_TOP) {
+    constexpr int NS = (S_TOP - S0) < 3 ? (S_TOP - S0) : 3;
+    constexpr int R = 1 << NS, H = 1 << S0, PER = (1 << L) >> NS;
+    const unsigned lim = (G > 1 ? lines : 1) * PER;
+    for (unsigned g = threadIdx.x; g < lim; g += kThreads) {
+      const int line = (int)(g / PER), gg = (int)(g % PER);
+      const int k = gg & (H - 1), blk = gg >> S0;
+      const int base = blk * R * H + k;
+      double2 *Lp = a + line * ld;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < R; ++m) x[m] = Lp[pdl<L>(base + m * H)];
+      group_dit<false>(x, NS, k, H, pyr, inv);
+#pragma unroll
+      for (int m = 0; m < R; ++m) Lp[pdl<L>(base + m * H)] = x[m];
+    }
+    __syncthreads();
+    dit_passes<L, S0 + 3, S_TOP, G>(a, ld, lines, pyr, inv);
+  }
+}
 
 // rows j0, j1 -> half spectra (forward DIF; bit-reversed result read back
 // during the Hermitian split)
 // DIV: the rows are not read from f but computed on the fly as the
 // divergence (M W + alpha yM + beta ydM) * gamma of the velocity-sized W
 // (time_ERK.m:117, pressure_additional_solve.m:11-13), fusing that kernel in.
-template <bool DIV>
-__global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_r2c_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
-                                                         const double *__restrict__ f, double2 *__restrict__ spec,
-                                                         const __grid_constant__ DevOps P, double alpha, double beta,
-                                                         double gamma) {
+// fastdiv: every cell is a regular two-point row of Mx and My (the periodic
+// grids this solver takes): the row weights of j0, j1 and the three v rows
+// they share are set up once, the column weights once per column.
+template <int L, bool DIV>
+__global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
+    k_rows_r2c_t(int Ny, const double2 *__restrict__ tw, const double *__restrict__ f, double2 *__restrict__ spec,
+                 const __grid_constant__ DevOps P, double alpha, double beta, double gamma, int fastdiv) {
+  constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
   extern __shared__ double2 sm[];
-  const double2 *pyr = tw + Nx;
+  const double2 *pyr = tw + N;
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
   const bool has1 = j1 < Ny;
-  const int H = Nx / 2 + 1, per = Nx >> 3;
-  const double *r0 = f + (size_t)j0 * Nx, *r1 = f + (size_t)j1 * Nx;
-  for (int k = threadIdx.x; k < per; k += blockDim.x) {
-    double2 x[8];
+  if (DIV && fastdiv) {
+    const double *u = f, *v = f + P.Nu;
+    const double hy0 = __ldg(P.hy + j0), hy1 = has1 ? __ldg(P.hy + j1) : 0.0;
+    const double m00 = __ldg(P.rMY.w0 + j0), m01 = __ldg(P.rMY.w1 + j0);
+    const double m10 = has1 ? __ldg(P.rMY.w0 + j1) : 0.0, m11 = has1 ? __ldg(P.rMY.w1 + j1) : 0.0;
+    const int r0 = wrapn(j0 + P.rMY.s, P.rMY.n), r1 = wrapn(r0 + 1, P.rMY.n), r2 = wrapn(r1 + 1, P.rMY.n);
+    const double *ua = u + (long long)j0 * P.Nux, *ub = u + (long long)(has1 ? j1 : j0) * P.Nux;
+    const double *va = v + (long long)r0 * P.Nvx, *vb = v + (long long)r1 * P.Nvx, *vc = v + (long long)r2 * P.Nvx;
+    for (int k = threadIdx.x; k < PER; k += kThreads) {
+      double2 x[8];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      if (DIV)
-        x[m] = make_double2(div_cell(P, f, alpha, beta, gamma, k + m * per, j0),
-                            has1 ? div_cell(P, f, alpha, beta, gamma, k + m * per, j1) : 0.0);
-      else
-        x[m] = make_double2(__ldg(r0 + k + m * per), has1 ? __ldg(r1 + k + m * per) : 0.0);
+      for (int m = 0; m < 8; ++m) {
+        const int i = k + m * PER;
+        const double w0 = __ldg(P.rMX.w0 + i), w1 = __ldg(P.rMX.w1 + i), hx = __ldg(P.hx + i);
+        const int c0 = wrapn(i + P.rMX.s, P.rMX.n), c1 = wrapn(c0 + 1, P.rMX.n);
+        const double vb_i = __ldg(vb + i);
+        const double d0 = hy0 * (w0 * __ldg(ua + c0) + w1 * __ldg(ua + c1)) + hx * (m00 * __ldg(va + i) + m01 * vb_i);
+        const double d1 = hy1 * (w0 * __ldg(ub + c0) + w1 * __ldg(ub + c1)) + hx * (m10 * vb_i + m11 * __ldg(vc + i));
+        x[m] = make_double2(d0 * gamma, has1 ? d1 * gamma : 0.0);
+      }
+      group_dif<false>(x, 3, k, PER, pyr, false);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) sm[pdl<L>(k + m * PER)] = x[m];
     }
-    group_dif<false>(x, 3, k, per, pyr, false);
+  } else {
+    const double *r0 = f + (size_t)j0 * N, *r1 = f + (size_t)j1 * N;
+    for (int k = threadIdx.x; k < PER; k += kThreads) {
+      double2 x[8];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
+      for (int m = 0; m < 8; ++m) {
+        if (DIV)
+          x[m] = make_double2(div_cell(P, f, alpha, beta, gamma, k + m * PER, j0),
+                              has1 ? div_cell(P, f, alpha, beta, gamma, k + m * PER, j1) : 0.0);
+        else
+          x[m] = make_double2(__ldg(r0 + k + m * PER), has1 ? __ldg(r1 + k + m * PER) : 0.0);
+      }
+      group_dif<false>(x, 3, k, PER, pyr, false);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) sm[pdl<L>(k + m * PER)] = x[m];
+    }
   }
   __syncthreads();
-  dif_range(sm, 1, Nx, pyr, false, L - 3, 1);
-  for (int I = threadIdx.x; I < H; I += blockDim.x) {
-    const double2 z = sm[pd(brev(I, L))], m = sm[pd(brev((Nx - I) & (Nx - 1), L))];
+  dif_passes<L, L - 3, 1, 1>(sm, 0, 1, pyr, false);
+  for (int I = threadIdx.x; I < H; I += kThreads) {
+    const double2 z = sm[pdl<L>(brev(I, L))], m = sm[pdl<L>(brev((N - I) & (N - 1), L))];
     spec[(size_t)j0 * H + I] = make_double2(0.5 * (z.x + m.x), 0.5 * (z.y - m.y));
     if (has1) spec[(size_t)j1 * H + I] = make_double2(0.5 * (z.y + m.y), 0.5 * (m.x - z.x));
   }
 }
 
-// G spectrum columns: forward DIF, -1/Ahat scaling fused with the last DIF and
-// first DIT passes, inverse DIT; max |fhat| reduction
-__global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx, int Ny, int L, int G, const double2 *__restrict__ tw,
-                                                     const double *__restrict__ ax, const double *__restrict__ ay,
-                                                     double dxdy, double2 *__restrict__ spec,
-                                                     unsigned long long *__restrict__ maxbits) {
+// G spectrum columns of length 2^L: forward DIF, -1/Ahat scaling fused with
+// the last DIF and first DIT passes, inverse DIT; max |fhat| reduction
+template <int L, int G>
+__global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
+    k_cols_t(int Nx, const double2 *__restrict__ tw, const double *__restrict__ ax, const double *__restrict__ ay,
+             double dxdy, double2 *__restrict__ spec, unsigned long long *__restrict__ maxbits) {
+  constexpr int N = 1 << L, PER = N >> 3, LD = paddedl<L>();
   extern __shared__ double2 sm[];
   __shared__ double wmax[kThreads / 32];
-  const double2 *pyr = tw + Ny;
-  const int H = Nx / 2 + 1, per = Ny >> 3, ld = padded(Ny);
+  const double2 *pyr = tw + N;
+  const int H = Nx / 2 + 1;
   const int c0 = blockIdx.x * G;
   const int g_here = min(G, H - c0);
-  for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
-    const int k = gidx / g_here, line = gidx - k * g_here;
+  for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
+    const int k = (int)(gidx / G), line = (int)(gidx % G);
+    if (line >= g_here) continue;
     double2 x[8];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = spec[(size_t)(k + m * per) * H + c0 + line];
-    group_dif<false>(x, 3, k, per, pyr, false);
+    for (int m = 0; m < 8; ++m) x[m] = spec[(size_t)(k + m * PER) * H + c0 + line];
+    group_dif<false>(x, 3, k, PER, pyr, false);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) sm[(size_t)line * ld + pd(k + m * per)] = x[m];
+    for (int m = 0; m < 8; ++m) sm[line * LD + pdl<L>(k + m * PER)] = x[m];
   }
   __syncthreads();
-  dif_range(sm, g_here, Ny, pyr, false, L - 3, 4);
+  dif_passes<L, L - 3, 4, G>(sm, LD, g_here, pyr, false);
   double lmax = 0.0;
-  for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
-    const int line = gidx / per, k = gidx - line * per;
-    double2 *Ls = sm + (size_t)line * ld;
+  for (unsigned gidx = threadIdx.x; gidx < g_here * PER; gidx += kThreads) {
+    const int line = (int)(gidx / PER), k = (int)(gidx % PER);
+    double2 *Ls = sm + line * LD;
     const int I = c0 + line;
     double2 x[8];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = Ls[pd(8 * k + m)];
+    for (int m = 0; m < 8; ++m) x[m] = Ls[pdl<L>(8 * k + m)];
     group_dif<true>(x, 3, 0, 1, pyr, false);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
@@ -515,86 +571,103 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB) k_cols_f(int Nx
     }
     group_dit<true>(x, 3, 0, 1, pyr, true);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) Ls[pd(8 * k + m)] = x[m];
+    for (int m = 0; m < 8; ++m) Ls[pdl<L>(8 * k + m)] = x[m];
   }
   __syncthreads();
-  dit_range(sm, g_here, Ny, pyr, true, 4, L - 3);
-  const double sc = 1.0 / Ny;
-  for (int gidx = threadIdx.x; gidx < g_here * per; gidx += blockDim.x) {
-    const int k = gidx / g_here, line = gidx - k * g_here;
+  dit_passes<L, 3, L - 3, G>(sm, LD, g_here, pyr, true);
+  const double sc = 1.0 / N;
+  for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
+    const int k = (int)(gidx / G), line = (int)(gidx % G);
+    if (line >= g_here) continue;
     double2 x[8];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = sm[(size_t)line * ld + pd(k + m * per)];
-    group_dit<false>(x, 3, k, per, pyr, true);
+    for (int m = 0; m < 8; ++m) x[m] = sm[line * LD + pdl<L>(k + m * PER)];
+    group_dit<false>(x, 3, k, PER, pyr, true);
 #pragma unroll
     for (int m = 0; m < 8; ++m)
-      spec[(size_t)(k + m * per) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
+      spec[(size_t)(k + m * PER) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
   }
   for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, off));
   if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
   __syncthreads();
   if (threadIdx.x == 0) {
     double mm = wmax[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mm = fmax(mm, wmax[w]);
+    for (int w = 1; w < kThreads / 32; ++w) mm = fmax(mm, wmax[w]);
     atomicMax(maxbits, (unsigned long long)__double_as_longlong(sqrt(mm)));
   }
 }
 
 // half spectra of rows j0, j1 -> real rows (inverse DIF, bit-reversed result
 // read back in natural order)
-__global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB) k_rows_c2r_f(int Nx, int Ny, int L, const double2 *__restrict__ tw,
-                                                         const double2 *__restrict__ spec, double *__restrict__ out,
-                                                         int accumulate, const unsigned long long *__restrict__ maxbits) {
+template <int L>
+__global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
+    k_rows_c2r_t(int Ny, const double2 *__restrict__ tw, const double2 *__restrict__ spec, double *__restrict__ out,
+                 int accumulate, const unsigned long long *__restrict__ maxbits) {
+  constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
   extern __shared__ double2 sm[];
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
   const bool has1 = j1 < Ny;
-  const int H = Nx / 2 + 1, per = Nx >> 3;
   const double mx = __longlong_as_double((long long)*maxbits);
   if (mx < 1e-14) {  // pressure_poisson.m:21-32: dp stays zero
     if (!accumulate)
-      for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
-        out[(size_t)j0 * Nx + k] = 0.0;
-        if (has1) out[(size_t)j1 * Nx + k] = 0.0;
+      for (int k = threadIdx.x; k < N; k += kThreads) {
+        out[(size_t)j0 * N + k] = 0.0;
+        if (has1) out[(size_t)j1 * N + k] = 0.0;
       }
     return;
   }
-  const double2 *pyr = tw + Nx;
+  const double2 *pyr = tw + N;
   const double2 *s0 = spec + (size_t)j0 * H, *s1 = spec + (size_t)j1 * H;
-  for (int k = threadIdx.x; k < per; k += blockDim.x) {
+  for (int k = threadIdx.x; k < PER; k += kThreads) {
     double2 x[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
-      const int q = k + m * per;
+      const int q = k + m * PER;
       double2 g0, g1;
       if (q < H) {
         g0 = s0[q];
         g1 = has1 ? s1[q] : make_double2(0.0, 0.0);
       } else {
-        const double2 a = s0[Nx - q];
-        const double2 b = has1 ? s1[Nx - q] : make_double2(0.0, 0.0);
+        const double2 a = s0[N - q];
+        const double2 b = has1 ? s1[N - q] : make_double2(0.0, 0.0);
         g0 = make_double2(a.x, -a.y);
         g1 = make_double2(b.x, -b.y);
       }
       x[m] = make_double2(g0.x - g1.y, g0.y + g1.x);
     }
-    group_dif<false>(x, 3, k, per, pyr, true);
+    group_dif<false>(x, 3, k, PER, pyr, true);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) sm[pd(k + m * per)] = x[m];
+    for (int m = 0; m < 8; ++m) sm[pdl<L>(k + m * PER)] = x[m];
   }
   __syncthreads();
-  dif_range(sm, 1, Nx, pyr, true, L - 3, 1);
-  const double sc = 1.0 / Nx;
-  for (int k = threadIdx.x; k < Nx; k += blockDim.x) {
-    const double2 w = sm[pd(brev(k, L))];
+  dif_passes<L, L - 3, 1, 1>(sm, 0, 1, pyr, true);
+  const double sc = 1.0 / N;
+  for (int k = threadIdx.x; k < N; k += kThreads) {
+    const double2 w = sm[pdl<L>(brev(k, L))];
     if (accumulate) {
-      out[(size_t)j0 * Nx + k] += w.x * sc;
-      if (has1) out[(size_t)j1 * Nx + k] += w.y * sc;
+      out[(size_t)j0 * N + k] += w.x * sc;
+      if (has1) out[(size_t)j1 * N + k] += w.y * sc;
     } else {
-      out[(size_t)j0 * Nx + k] = w.x * sc;
-      if (has1) out[(size_t)j1 * Nx + k] = w.y * sc;
+      out[(size_t)j0 * N + k] = w.x * sc;
+      if (has1) out[(size_t)j1 * N + k] = w.y * sc;
     }
   }
 }
+
+// calls f(std::integral_constant<int, L>) for the runtime l in [LO, 13]
+template <int L, typename Fn>
+bool with_log2(int l, Fn &&fn) {
+  if constexpr (L > 13) {
+    return false;
+  } else {
+    if (l == L) {
+      fn(std::integral_constant<int, L>{});
+      return true;
+    }
+    return with_log2<L + 1>(l, fn);
+  }
+}
+constexpr int kFusedMinLog = 6;
 
 int ilog2_exact(int n) {
   int l = 0;
@@ -639,10 +712,15 @@ bool fft_supported(int Nx, int Ny) {
 // Opt the transform kernels in to large dynamic shared memory on the current
 // device (called once per context).
 void fft_prepare() {
-  cudaFuncSetAttribute(k_rows_r2c_f<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_rows_r2c_f<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_cols_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_rows_c2r_f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  for (int l = kFusedMinLog; l <= 13; ++l)
+    with_log2<kFusedMinLog>(l, [](auto c) {
+      constexpr int L = decltype(c)::value;
+      cudaFuncSetAttribute(k_rows_r2c_t<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      cudaFuncSetAttribute(k_rows_r2c_t<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      cudaFuncSetAttribute(k_cols_t<L, cols_per_block<L>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           200 * 1024);
+      cudaFuncSetAttribute(k_rows_c2r_t<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    });
   cudaFuncSetAttribute(k_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -652,32 +730,43 @@ namespace {
 void fft_passes(const DevOps &P, const FftPlan &plan, const double *src, bool div, double alpha, double beta,
                 double gamma, double *dp, bool accumulate, cudaStream_t s) {
   const int Nx = plan.Nx, Ny = plan.Ny;
-  const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
-  const int G = cols_group(Ny, plan.logy >= 0);
-  const size_t smy = (size_t)G * padded(Ny) * sizeof(double2) * (plan.logy >= 0 ? 1 : 2);
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
   cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
-  const bool fx = plan.logx >= 6, fy = plan.logy >= 6;  // fused-pass kernels
-  if (fx && div)
-    k_rows_r2c_f<true><<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec, P, alpha, beta,
-                                                    gamma);
-  else if (fx)
-    k_rows_r2c_f<false><<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec, P, 0.0, 0.0, 0.0);
-  else
-    k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
-  if (fy)
-    k_cols_f<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
-                                                    plan.spec, (unsigned long long *)plan.maxabs);
-  else
+  unsigned long long *maxbits = (unsigned long long *)plan.maxabs;
+  // rows, real -> half spectrum
+  const int fastdiv = P.rMX.lo <= 0 && P.rMX.hi >= Nx && P.rMY.lo <= 0 && P.rMY.hi >= Ny && P.rMX.two && P.rMY.two;
+  const bool fx = with_log2<kFusedMinLog>(plan.logx, [&](auto c) {
+    constexpr int L = decltype(c)::value;
+    const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
+    if (div)
+      k_rows_r2c_t<L, true><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, plan.spec, P, alpha, beta, gamma, fastdiv);
+    else
+      k_rows_r2c_t<L, false><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, plan.spec, P, 0.0, 0.0, 0.0, 0);
+  });
+  const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
+  if (!fx) k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
+  // columns: forward, scaling, inverse
+  const bool fy = with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
+    constexpr int L = decltype(c)::value, G = cols_per_block<L>();
+    const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
+    k_cols_t<L, G><<<(H + G - 1) / G, kThreads, sm, s>>>(Nx, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy, plan.spec,
+                                                         maxbits);
+  });
+  if (!fy) {
+    const int G = cols_group(Ny, plan.logy >= 0);
+    const size_t smy = (size_t)G * padded(Ny) * sizeof(double2) * (plan.logy >= 0 ? 1 : 2);
     k_cols<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
-                                                  plan.spec, (unsigned long long *)plan.maxabs);
-  if (fx)
-    k_rows_c2r_f<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
-                                              (const unsigned long long *)plan.maxabs);
-  else
-    k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
-                                            (const unsigned long long *)plan.maxabs);
+                                                  plan.spec, maxbits);
+  }
+  // rows, half spectrum -> real
+  const bool fx2 = with_log2<kFusedMinLog>(plan.logx, [&](auto c) {
+    constexpr int L = decltype(c)::value;
+    const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
+    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, plan.spec, dp, accumulate ? 1 : 0, maxbits);
+  });
+  if (!fx2)
+    k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0, maxbits);
 }
 }  // namespace
 
@@ -686,7 +775,7 @@ void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, d
   fft_passes(P, plan, f, false, 0.0, 0.0, 0.0, dp, accumulate, s);
 }
 
-bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= 6; }
+bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= kFusedMinLog && plan.logx <= 13; }
 
 void launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha, double beta,
                             double gamma, double *dp, bool accumulate, cudaStream_t s) {
