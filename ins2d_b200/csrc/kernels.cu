@@ -77,10 +77,20 @@ __device__ __forceinline__ void project_cell(const DevOps &P, const double *__re
   }
 }
 
+// Each thread projects kProjRows rows (BY apart) of one column, so a warp
+// has that many independent rows of loads in flight and the column's x
+// weights are read once.
+#ifndef INS2D_PROJ_ROWS
+#define INS2D_PROJ_ROWS 4
+#endif
+constexpr int kProjRows = INS2D_PROJ_ROWS;
 __global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps P, const double *__restrict__ Wt,
                                                 const double *__restrict__ dp, double dt, double c,
                                                 double *__restrict__ Vo) {
-  project_cell(P, Wt, dp, dt, c, Vo, blockIdx.x * BX + threadIdx.x, blockIdx.y * BY + threadIdx.y);
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j0 = blockIdx.y * (BY * kProjRows) + threadIdx.y;
+#pragma unroll
+  for (int r = 0; r < kProjRows; ++r) project_cell(P, Wt, dp, dt, c, Vo, i, j0 + r * BY);
 }
 
 __global__ void __launch_bounds__(256) k_correct(const __grid_constant__ DevOps P, const double *__restrict__ Vi,
@@ -209,7 +219,8 @@ void launch_div(const DevOps &P, const double *W, double alpha, double beta, dou
 
 void launch_project(const DevOps &P, const double *Wt, const double *dp, double dt, double c, double *V_out,
                     cudaStream_t s) {
-  dim3 g = grid_for(P.Nux > P.Nvx ? P.Nux : P.Nvx, P.Nuy > P.Nvy ? P.Nuy : P.Nvy);
+  const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project<<<g, dim3(BX, BY), 0, s>>>(P, Wt, dp, dt, c, V_out);
 }
 
