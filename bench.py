@@ -53,6 +53,15 @@ WORKLOADS = {
                   desc="inviscid Taylor-Green 512x512 periodic [0,2pi]^2, RK44 dt=1e-3, FFT Poisson, FP64"),
     "ldc64": dict(N=64, L=1.0, Re=1000.0, poisson=4, precision="fp64", ic="rest", dt=1e-3, CG_acc=1e-12,
                   desc="lid-driven cavity 64x64, Re=1000, RK44 dt=1e-3, PCG to 1e-12, FP64"),
+    "bfs1024": dict(N=1024, ic="bfs", Re=800.0, poisson=4, precision="fp64", dt=1e-3, CG_acc=1e-10,
+                    desc="backward-facing step 1024x1024, x in [0,30], y in [-0.5,0.5], tanh-stretched 1.02, "
+                         "inflow u=24y(0.5-y) for y>=0, outflow p=0, Re=800, RK44 dt=1e-3, multigrid PCG to "
+                         "1e-10, FP64"),
+    "bfs1024_learned": dict(N=1024, ic="bfs", Re=800.0, poisson=4, precision="fp64", dt=1e-3, CG_acc=1e-10,
+                            learned=dict(record_steps=24, pairs=120, train_steps=300, batch=4, lr=2e-3, seed=0),
+                            desc="backward-facing step 1024x1024 (as bfs1024) with the learned initial guess: "
+                                 "a 6-layer 32-channel BF16 CNN trained on the GPU on the (f, dp) pairs of the "
+                                 "first steps' solves; multigrid PCG to the same 1e-10"),
     "ens256": dict(kind="ensemble", n=256, sizes=(64, 96, 128, 192, 256), stretch=1.05, dt=5e-4, CG_acc=1e-10,
                    poisson=4, precision="fp64",
                    desc="ensemble of 256 cavity/channel flows, tanh-stretched 1.05, nx,ny in {64..256}, "
@@ -140,9 +149,26 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def bfs_profile(y):
+    """inflow above the step (y >= 0): u = 24 y (0.5 - y)"""
+    y = np.asarray(y, dtype=np.float64)
+    return np.where(y >= 0.0, 24.0 * y * (0.5 - y), 0.0)
+
+
 def setup_case(wl, device=0):
     import ins2d_b200
     from ins2d_b200 import cases
+    if wl["ic"] == "bfs":
+        N = wl["N"]
+        x = cases.tanh_grid(N, 0.0, 30.0, 1.02)
+        y = cases.tanh_grid(N, -0.5, 0.5, 1.02)
+        opts = ins2d_b200.Options(x, y, cases.BC_CHANNEL, Re=wl["Re"], poisson=wl["poisson"],
+                                  CG_acc=wl.get("CG_acc", 1e-10), CG_maxit=50000, uBC=cases.channel_uBC(bfs_profile),
+                                  RK="RK44", precision=wl["precision"], device=device,
+                                  precond=wl.get("precond", "default"))
+        V = np.r_[bfs_profile(opts.yu), np.zeros(opts.Nv)]
+        V = opts.initial_projection(V, 0.0)
+        return opts, V, wl["dt"]
     N, L = wl["N"], wl["L"]
     x = cases.uniform_grid(N, 0.0, L)
     if wl["ic"] == "rest":
@@ -166,6 +192,50 @@ def setup_case(wl, device=0):
     return opts, V, dt
 
 
+def setup_learned(opts, lw, Vd, pd, t, dt, stream, device):
+    """Records the (f, dp) pairs of the first steps' PCG solves, trains the
+    network on them on the GPU and attaches it as the initial guess.  Returns
+    the time reached and a description of the training."""
+    import torch
+    from ins2d_b200 import learned
+    f_buf, p_buf = learned.record_pairs(opts, lw["pairs"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, _, rst = opts.time_ERK(Vd, pd, t, dt, nsteps=lw["record_steps"], return_stats=True)
+    torch.cuda.synchronize()
+    rec_s = time.perf_counter() - t0
+    t += lw["record_steps"] * dt
+    n = learned.recorded_pairs(opts)
+    learned.stop_recording(opts)
+    inp, tgt = learned.prepare_pairs(opts, f_buf[:n], p_buf[:n])
+    del f_buf, p_buf
+    torch.cuda.empty_cache()
+    net = learned.ConvNet(device=device, seed=lw.get("seed", 0))
+    net.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = learned.train(net, inp, tgt, steps=lw["train_steps"], batch=lw["batch"], lr=lw["lr"],
+                           seed=lw.get("seed", 0))
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del inp, tgt
+    torch.cuda.empty_cache()
+    learned.attach(opts, net)
+    info = {"pairs": n, "record_steps": lw["record_steps"], "record_s": round(rec_s, 3),
+            "record_cg_iters_per_solve": rst["iters_total"] / max(rst["n_solves"], 1),
+            "train_steps": lw["train_steps"], "batch": lw["batch"], "train_s": round(train_s, 3),
+            "loss_rel_first": float(np.mean(losses[:5])), "loss_rel_last": float(np.mean(losses[-10:]))}
+    return t, info, net
+
+
+def load_tensor_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured bf16 burst (MEASURED_PEAKS.json)"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def run_ours(args, wl, rank, world, local_rank):
     import torch
     import ins2d_b200
@@ -182,6 +252,11 @@ def run_ours(args, wl, rank, world, local_rank):
     pd = torch.zeros(opts.Np, dtype=torch.float64, device="cuda")
     pd = opts.pressure_additional_solve(Vd, pd, 0.0)  # p_initial (input_check.m:126-128)
     t = 0.0
+    lw = wl.get("learned")
+    learned_info = None
+    if lw:
+        t, learned_info, net = setup_learned(opts, lw, Vd, pd, t, dt, stream, local_rank)
+    state0 = (Vd.clone(), pd.clone(), t) if lw else None
     # warm-up
     _, _, st = opts.time_ERK(Vd, pd, t, dt, nsteps=args.warmup, return_stats=True)
     t += args.warmup * dt
@@ -333,6 +408,44 @@ def run_ours(args, wl, rank, world, local_rank):
                  "cg_iters_per_solve": pst["iters_total"] / max(pst["n_solves"], 1),
                  "value": cells / (pms / 1e3), "speedup_of_this_run": (cells / (pms / 1e3)) and value / (cells / (pms / 1e3))}
         op.close()
+    # the learned guess's effect: the same steps from the same state without
+    # the network (multigrid PCG from zero), and the network's own forward time
+    if lw:
+        from ins2d_b200 import learned
+        tc = state0[2]
+        learned.attach(opts, None)
+        Vc, pc = state0[0].clone(), state0[1].clone()
+        opts.time_ERK(Vc, pc, tc, dt, nsteps=args.warmup)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _, _, wst = opts.time_ERK(Vc, pc, tc + args.warmup * dt, dt, nsteps=args.steps, return_stats=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wms = e0.elapsed_time(e1)
+        learned_info["without"] = {"ms_per_step": wms / args.steps, "value": cells * args.steps / (wms / 1e3),
+                                   "cg_iters_per_solve": wst["iters_total"] / max(wst["n_solves"], 1)}
+        learned_info["with"] = {"ms_per_step": ms_max / args.steps, "value": value,
+                                "cg_iters_per_solve": st["iters_total"] / max(st["n_solves"], 1)}
+        learned_info["speedup"] = learned_info["without"]["ms_per_step"] / learned_info["with"]["ms_per_step"]
+        # forward pass of the network on one field of the grid (tensor-core layers)
+        x_in = torch.randn(1, opts.Npy, opts.Npx, dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            net.forward(x_in)
+        nrep = 10
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(nrep):
+            net.forward(x_in)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fms = e0.elapsed_time(e1) / nrep
+        flops = 2 * 9 * (1 * 32 + 4 * 32 * 32 + 32 * 1) * cells
+        tpk = load_tensor_peak()
+        learned_info["forward"] = {"ms": round(fms, 4), "flops": flops, "achieved_tflops": round(flops / fms / 1e9, 2),
+                                   "peak_tflops": tpk[0], "peak_kind": tpk[1],
+                                   "frac": round(flops / fms / 1e9 / tpk[0], 4),
+                                   "note": "ms includes the host synchronisation of each ins2d_cnn_forward call"}
+        del net
     # CPU baseline on rank 0 only at N=1
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -354,6 +467,7 @@ def run_ours(args, wl, rank, world, local_rank):
         "cpu_baseline": cpu,
         "accuracy": acc,
         "plain_pcg": plain,
+        "learned": learned_info,
         "clocks": clk,
     }
     if rank == 0:
@@ -485,6 +599,8 @@ def cpu_baseline(wl, budget_s=25.0, steps=None):
     C)."""
     from oracle import ins2d_ref as R
     from ins2d_b200 import cases
+    if wl["ic"] == "bfs":
+        return bfs_cpu_baseline(wl, budget_s, steps)
     N, L = wl["N"], wl["L"]
     rng = np.random.default_rng(0)
     dt = wl.get("dt", 1e-4)
@@ -533,6 +649,37 @@ def cpu_baseline(wl, budget_s=25.0, steps=None):
             "sample": f"{n} RK44 step(s) of the {N}x{N} workload with the scipy/numpy restatement "
                       f"(sparse matvecs single-threaded, cg.F's DIC-PCG in C; operator setup "
                       f"{setup_s:.1f}s excluded)"}
+
+
+def bfs_cpu_baseline(wl, budget_s=25.0, steps=None, n_sample=128):
+    """The scipy restatement (single-threaded sparse matvecs, cg.F's DIC-PCG
+    in C) on a bounded sample of the backward-facing-step workload: the same
+    case on a 128x128 grid (the 1024x1024 grid's DIC-PCG takes minutes per
+    step on one core), from the projected inflow profile."""
+    from oracle import ins2d_ref as R
+    from ins2d_b200 import cases
+    x = cases.tanh_grid(n_sample, 0.0, 30.0, 1.02)
+    y = cases.tanh_grid(n_sample, -0.5, 0.5, 1.02)
+    t0 = time.perf_counter()
+    o = R.make_options(x, y, cases.BC_CHANNEL, Re=wl["Re"], poisson=4, CG_acc=wl.get("CG_acc", 1e-10),
+                       CG_maxit=100000, uBC=cases.channel_uBC(bfs_profile), RK="RK44")
+    setup_s = time.perf_counter() - t0
+    g = o.grid
+    V = R.initial_projection(np.r_[bfs_profile(g.yu), np.zeros(g.Nv)], 0.0, o)
+    p = np.zeros(g.Np)
+    dt = wl["dt"]
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        V, p = R.time_ERK(V, p, n * dt, dt, o)
+        n += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and n >= steps) or (steps is None and (el > budget_s or n >= 50)):
+            break
+    return {"value": g.Npx * g.Npy * n / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{n} RK44 step(s) of the backward-facing step on a {n_sample}x{n_sample} grid (the "
+                      f"{wl['N']}x{wl['N']} workload's case at a size the single-threaded scipy restatement "
+                      f"finishes in seconds; operator setup {setup_s:.1f}s excluded)"}
 
 
 def ensemble_cpu_baseline(wl, nmembers=2, steps=2):

@@ -280,6 +280,55 @@ int ins2d_ens_set_solver(ins2d_ens *e, int32_t threads);
  * timings (ms of one solve phase for 512, 256 threads and batched) */
 int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks, double tuned_ms[3]);
 
+/* --- learned initial guess of the PCG ---------------------------------------
+ * No counterpart in the reference: its solves start from zero
+ * (pressure_poisson.m:61-70, cg.F:207-229 with x_in = 0).  A small
+ * convolutional network (six 3x3 convolutions, 1 -> 32 -> 32 -> 32 -> 32 -> 32
+ * -> 1 channels, ReLU between, no biases, zero padding; BF16 tensor-core
+ * layers accumulating in FP32) maps the Jacobi-scaled right-hand side to an
+ * approximation of the solution.  The PCG starts from that guess (scaled by
+ * the Rayleigh-Ritz factor (x0'f)/(x0'A x0)) and still stops on the
+ * reference's rule ||r|| <= CG_acc ||f||, so a solution changes only within
+ * the tolerance.  Parameters (INS2D_CNN_NPARAM floats): W1 [32][9],
+ * W2..W5 [32][9][32] ([out][tap][in]), W6 [9][32]; tap t = (dy+1)*3 + (dx+1).
+ * Inputs, targets and outputs of the network are fp32 device arrays of B
+ * fields of H x W (x fastest). */
+#define INS2D_CNN_NPARAM 37440
+typedef struct ins2d_cnn ins2d_cnn;
+/* He-normal weights from the seed; out_scale 1 */
+int ins2d_cnn_create(int32_t device, uint64_t seed, ins2d_cnn **out);
+int ins2d_cnn_destroy(ins2d_cnn *net);
+const char *ins2d_cnn_last_error(const ins2d_cnn *net);
+int ins2d_cnn_set_stream(ins2d_cnn *net, void *stream);
+/* host copies of the FP32 master weights (w may be NULL) and the output scale */
+int ins2d_cnn_get_params(ins2d_cnn *net, float *w, float *out_scale);
+int ins2d_cnn_set_params(ins2d_cnn *net, const float *w, float out_scale);
+/* y = out_scale * net(in) */
+int ins2d_cnn_forward(ins2d_cnn *net, const float *in, float *y, int32_t B, int32_t H, int32_t W);
+/* loss = mean((net(in) - tgt)^2) and its gradient (host array of
+ * INS2D_CNN_NPARAM floats, may be NULL); no update */
+int ins2d_cnn_loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int32_t B, int32_t H, int32_t W,
+                        double *loss, float *grad);
+/* one Adam step (beta 0.9/0.999, eps 1e-8) on that loss */
+int ins2d_cnn_train_step(ins2d_cnn *net, const float *in, const float *tgt, int32_t B, int32_t H, int32_t W,
+                         float lr, double *loss);
+/* Training pairs of a context's grid: for npairs right-hand sides f and
+ * solutions p (device, Np each, one after another) writes the network input
+ * in = (f / diag A) / s and target tgt = (p - center * mean(p)) / s, with
+ * s = rms(f / diag A) per pair (fp32 device arrays, Np each). */
+int ins2d_cnn_prepare_pairs(ins2d_ctx *ctx, const double *f, const double *p, int32_t npairs, int32_t center,
+                            float *in, float *tgt);
+/* attach (net != NULL) or detach the learned initial guess of ctx's PCG
+ * solves (poisson 1-5; the FFT path is direct and ignores it).  The context
+ * borrows the network: keep it alive while attached. */
+int ins2d_set_learned_guess(ins2d_ctx *ctx, ins2d_cnn *net);
+/* Recording of the solver's own (f, dp) pairs: each later PCG solve without
+ * a learned guess copies its right-hand side and solution into the device
+ * buffers f_buf, p_buf (capacity pairs of Np doubles) until they are full;
+ * capacity 0 stops recording.  ins2d_recorded_pairs gives the count. */
+int ins2d_record_pairs(ins2d_ctx *ctx, double *f_buf, double *p_buf, int32_t capacity);
+int32_t ins2d_recorded_pairs(const ins2d_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "cnn.cuh"
 #include "ins2d.h"
 #include "kernels.cuh"
 #include "setup.hpp"
@@ -79,6 +80,12 @@ struct ins2d_ctx {
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
   StepGraph step_graph[2];
+  // learned initial guess of the PCG (borrowed network) and its work arrays
+  ins2d_cnn *cnn = nullptr;
+  double *lg_x0 = nullptr, *lg_q = nullptr, *lg_r0 = nullptr, *lg_red = nullptr;
+  // recording of (f, dp) pairs of the plain PCG solves
+  double *rec_f = nullptr, *rec_p = nullptr;
+  int rec_cap = 0, rec_n = 0;
 };
 
 namespace {
@@ -220,21 +227,15 @@ void setup_rk(ins2d_ctx *c) {
 
 // ---------------------------------------------------------------------------
 // Poisson solve: dp = pressure_poisson(f) (or dp += ... when accumulate)
-int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st) {
-  if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
-  if (c->poisson == INS2D_POISSON_FFT) {
-    Prof pr(c, INS2D_PROF_POISSON, 3);
-    launch_fft_poisson(c->P, c->fft, f, dp, accumulate, c->stream);
-    CK(cudaGetLastError());
-    return INS2D_OK;
-  }
+// PCG to the relative residual tol (cg.F's rule ||r|| <= tol ||f||)
+int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st, double tol) {
   const bool block = c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P);
   Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
   if (block) {
     if (c->use_mg)
-      pcg_solve_block_mg(c->P, c->mg, c->pcg, f, dp, c->opts.CG_acc, c->opts.CG_maxit, accumulate, c->stream);
+      pcg_solve_block_mg(c->P, c->mg, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
     else
-      pcg_solve_block(c->P, c->pcg, f, dp, c->opts.CG_acc, c->opts.CG_maxit, accumulate, c->stream);
+      pcg_solve_block(c->P, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -255,9 +256,9 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
     return INS2D_OK;
   }
   if (c->use_mg)
-    pcg_init_mg(c->P, c->mg, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
+    pcg_init_mg(c->P, c->mg, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
   else
-    pcg_init(c->P, c->pcg, f, c->opts.CG_acc, c->opts.CG_maxit, c->stream);
+    pcg_init(c->P, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
   CK(cudaGetLastError());
   int chunk = c->use_mg ? 2 : 4;
   long long launched = 0;
@@ -296,6 +297,69 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
   c->launches[INS2D_PROF_POISSON] += 1;
   CK(cudaGetLastError());
   return INS2D_OK;
+}
+
+// PCG from the learned initial guess: x0 = a * net(f) with the Rayleigh-Ritz
+// factor a = (x0'f)/(x0'A x0) (the best multiple of the network's output in
+// the energy norm), then CG on A e = r0 = f - A x0 to ||r|| <= CG_acc ||f||
+// (the inner tolerance is rescaled to ||r0||), dp = x0 + e.  Right-hand
+// sides with max|f| < 1e-14 take the plain path (pressure_poisson.m:33-38).
+int solve_learned(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st) {
+  const long long n = c->P.Np;
+  const double tol = c->opts.CG_acc;
+  double d[4], rd[2];
+  {
+    Prof pr(c, INS2D_PROF_POISSON, 13);
+    cnn::guess(c->cnn, c->P, f, c->lg_x0, c->stream);
+    launch_lap(c->P, c->lg_x0, c->lg_q, c->stream);
+    CK(cudaGetLastError());
+    cnn::dots(n, c->lg_x0, f, c->lg_q, c->lg_red, d, c->stream);
+  }
+  if (!(d[3] >= 1e-14) || !std::isfinite(d[0]) || !std::isfinite(d[1]) || d[1] == 0.0)
+    return solve_pcg(c, f, dp, accumulate, st, tol);
+  {
+    Prof pr(c, INS2D_PROF_POISSON, 2);
+    cnn::residual(n, f, c->lg_q, d[0] / d[1], c->lg_x0, c->lg_r0, c->lg_red, rd, c->stream);
+  }
+  const double ff = d[2], rr0 = rd[0];
+  if (rr0 <= tol * tol * ff || rd[1] < 1e-14) {
+    Prof pr(c, INS2D_PROF_POISSON, 1);
+    if (accumulate)
+      launch_add(c->lg_x0, dp, n, c->stream);
+    else
+      CK(cudaMemcpyAsync(dp, c->lg_x0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaGetLastError());
+    if (st) *st = ins2d_solve_stats{0, std::sqrt(rr0 / ff), 0.0};
+    return INS2D_OK;
+  }
+  const double scale = std::sqrt(rr0 / ff);
+  int rc = solve_pcg(c, c->lg_r0, dp, accumulate, st, tol / scale);
+  if (rc) return rc;
+  if (st) st->norm1 *= scale;
+  Prof pr(c, INS2D_PROF_POISSON, 1);
+  launch_add(c->lg_x0, dp, n, c->stream);
+  CK(cudaGetLastError());
+  return INS2D_OK;
+}
+
+int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st) {
+  if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
+  if (c->poisson == INS2D_POISSON_FFT) {
+    Prof pr(c, INS2D_PROF_POISSON, 3);
+    launch_fft_poisson(c->P, c->fft, f, dp, accumulate, c->stream);
+    CK(cudaGetLastError());
+    return INS2D_OK;
+  }
+  if (c->cnn) return solve_learned(c, f, dp, accumulate, st);
+  int rc = solve_pcg(c, f, dp, accumulate, st, c->opts.CG_acc);
+  if (rc == INS2D_OK && c->rec_n < c->rec_cap) {
+    // the solution stays in the PCG iterate x after the solve
+    const size_t nb = (size_t)c->P.Np * sizeof(double);
+    CK(cudaMemcpyAsync(c->rec_f + (size_t)c->rec_n * c->P.Np, f, nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->rec_p + (size_t)c->rec_n * c->P.Np, c->pcg.x, nb, cudaMemcpyDeviceToDevice, c->stream));
+    c->rec_n += 1;
+  }
+  return rc;
 }
 
 // dp = pressure_poisson(f) with f = (M W + alpha yM + beta ydM) gamma: on the
@@ -436,6 +500,9 @@ int check_mem(ins2d_ctx *c, int mem) {
 #define API_END                                                  \
   }                                                              \
   catch (const CudaError &e) {                                   \
+    return fail(ctx, INS2D_ECUDA, e.what());                     \
+  }                                                              \
+  catch (const cnn::CudaError &e) {                              \
     return fail(ctx, INS2D_ECUDA, e.what());                     \
   }                                                              \
   catch (const std::bad_alloc &) {                               \
@@ -955,6 +1022,53 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
   return INS2D_OK;
   API_END
 }
+
+
+int ins2d_cnn_prepare_pairs(ins2d_ctx *ctx, const double *f, const double *p, int32_t npairs, int32_t center,
+                            float *in, float *tgt) {
+  API_BEGIN
+  if (npairs < 0 || (npairs > 0 && (!f || !p || !in || !tgt)))
+    return fail(ctx, INS2D_EINVAL, "cnn_prepare_pairs: null argument or negative count");
+  const long long Np = ctx->P.Np;
+  if (!ctx->lg_red) ctx->lg_red = dalloc<double>(ctx, cnn::red_doubles());
+  for (int32_t k = 0; k < npairs; ++k)
+    cnn::prepare(ctx->P, f + k * Np, p + k * Np, center ? 1 : 0, in + k * Np, tgt + k * Np, ctx->lg_red,
+                 ctx->stream);
+  CK(cudaStreamSynchronize(ctx->stream));
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_set_learned_guess(ins2d_ctx *ctx, ins2d_cnn *net) {
+  API_BEGIN
+  if (net && net->device != ctx->device)
+    return fail(ctx, INS2D_EINVAL, "set_learned_guess: network and context on different devices");
+  if (net && !ctx->lg_x0) {
+    const size_t Np = (size_t)ctx->P.Np;
+    ctx->lg_x0 = dalloc<double>(ctx, Np);
+    ctx->lg_q = dalloc<double>(ctx, Np);
+    ctx->lg_r0 = dalloc<double>(ctx, Np);
+    if (!ctx->lg_red) ctx->lg_red = dalloc<double>(ctx, cnn::red_doubles());
+  }
+  if (net) cnn::reserve(net, ctx->P.Np);
+  ctx->cnn = net;
+  return INS2D_OK;
+  API_END
+}
+
+int ins2d_record_pairs(ins2d_ctx *ctx, double *f_buf, double *p_buf, int32_t capacity) {
+  API_BEGIN
+  if (capacity < 0 || (capacity > 0 && (!f_buf || !p_buf)))
+    return fail(ctx, INS2D_EINVAL, "record_pairs: null buffer or negative capacity");
+  ctx->rec_f = capacity ? f_buf : nullptr;
+  ctx->rec_p = capacity ? p_buf : nullptr;
+  ctx->rec_cap = capacity;
+  ctx->rec_n = 0;
+  return INS2D_OK;
+  API_END
+}
+
+int32_t ins2d_recorded_pairs(const ins2d_ctx *ctx) { return ctx ? ctx->rec_n : 0; }
 
 }  // extern "C"
 

@@ -1,0 +1,182 @@
+"""The learned initial guess of the pressure solve (include/ins2d.h,
+``ins2d_cnn_*``): a six-layer 3x3 convolutional network, trained on the GPU by
+the library's own BF16 tensor-core forward and backward kernels on
+(right-hand side, pressure) pairs recorded from the solver's own PCG solves.
+
+There is no counterpart in the reference, whose solves start from zero
+(pressure_poisson.m:61-70).  Attached to a context, the network's output
+(scaled by the Rayleigh-Ritz factor) is where PCG starts; CG still iterates
+to ||r|| <= CG_acc ||f||, so solutions change only within that tolerance.
+
+Device buffers here are torch CUDA tensors (plumbing); every computation runs
+in libins2d.so.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .api import Ins2dError
+
+NPARAM = _lib.CNN_NPARAM
+
+
+def _require_cuda(t, dtype, name):
+    import torch
+    if not (hasattr(t, "is_cuda") and t.is_cuda and t.dtype == dtype and t.is_contiguous()):
+        raise ValueError(f"{name}: need a contiguous CUDA tensor of {dtype}")
+    return t
+
+
+class ConvNet:
+    """The network (device-resident FP32 master weights, BF16 copies for the
+    tensor-core layers, Adam moments).  ``seed`` fixes the He-normal initial
+    weights."""
+
+    def __init__(self, device=0, seed=0):
+        self._lib = _lib.load()
+        self._h = ctypes.c_void_p()
+        self.device = int(device)
+        rc = self._lib.ins2d_cnn_create(self.device, ctypes.c_uint64(int(seed)), ctypes.byref(self._h))
+        if rc != 0:
+            raise Ins2dError(rc, "cnn_create failed")
+
+    def _check(self, rc):
+        if rc != 0:
+            m = self._lib.ins2d_cnn_last_error(self._h)
+            raise Ins2dError(rc, m.decode() if m else "")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ins2d_cnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream):
+        self._check(self._lib.ins2d_cnn_set_stream(self._h, ctypes.c_void_p(stream)))
+
+    def params(self):
+        """(FP32 weights as a numpy array of NPARAM, out_scale)."""
+        w = np.empty(NPARAM, dtype=np.float32)
+        sc = ctypes.c_float()
+        self._check(self._lib.ins2d_cnn_get_params(self._h, w.ctypes.data, ctypes.byref(sc)))
+        return w, float(sc.value)
+
+    def set_params(self, w=None, out_scale=1.0):
+        ptr = None
+        if w is not None:
+            w = np.ascontiguousarray(np.asarray(w, dtype=np.float32).ravel())
+            if w.size != NPARAM:
+                raise ValueError(f"need {NPARAM} weights")
+            ptr = w.ctypes.data
+        self._check(self._lib.ins2d_cnn_set_params(self._h, ptr, float(out_scale)))
+
+    def forward(self, inp):
+        """out_scale * net(inp) for a float32 CUDA tensor of shape (B, H, W)."""
+        import torch
+        _require_cuda(inp, torch.float32, "inp")
+        B, H, W = inp.shape
+        y = torch.empty_like(inp)
+        torch.cuda.synchronize(inp.device)
+        self._check(self._lib.ins2d_cnn_forward(self._h, inp.data_ptr(), y.data_ptr(), B, H, W))
+        return y
+
+    def loss_grad(self, inp, tgt):
+        """(mean squared error, gradient as a numpy float32 array); no update."""
+        import torch
+        _require_cuda(inp, torch.float32, "inp")
+        _require_cuda(tgt, torch.float32, "tgt")
+        B, H, W = inp.shape
+        g = np.empty(NPARAM, dtype=np.float32)
+        loss = ctypes.c_double()
+        torch.cuda.synchronize(inp.device)
+        self._check(self._lib.ins2d_cnn_loss_grad(self._h, inp.data_ptr(), tgt.data_ptr(), B, H, W,
+                                                  ctypes.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def train_step(self, inp, tgt, lr):
+        """One Adam step on the mean squared error; returns the loss before it."""
+        import torch
+        _require_cuda(inp, torch.float32, "inp")
+        _require_cuda(tgt, torch.float32, "tgt")
+        B, H, W = inp.shape
+        loss = ctypes.c_double()
+        self._check(self._lib.ins2d_cnn_train_step(self._h, inp.data_ptr(), tgt.data_ptr(), B, H, W, float(lr),
+                                                   ctypes.byref(loss)))
+        return loss.value
+
+
+def record_pairs(options, capacity):
+    """Starts recording the (f, dp) pairs of ``options``' next PCG solves into
+    new device buffers; returns them as (f_buf, p_buf), shape (capacity, Np)."""
+    import torch
+    dev = torch.device("cuda", options._desc[2].device)
+    f_buf = torch.zeros((capacity, options.Np), dtype=torch.float64, device=dev)
+    p_buf = torch.zeros((capacity, options.Np), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    options._check(options._lib.ins2d_record_pairs(options._ctx, f_buf.data_ptr(), p_buf.data_ptr(), int(capacity)))
+    options._rec = (f_buf, p_buf)
+    return f_buf, p_buf
+
+
+def recorded_pairs(options):
+    """Number of pairs recorded so far; stops recording when called with stop."""
+    return int(options._lib.ins2d_recorded_pairs(options._ctx))
+
+
+def stop_recording(options):
+    options._check(options._lib.ins2d_record_pairs(options._ctx, None, None, 0))
+
+
+def singular(options):
+    """True when A has the constant null space (no pressure boundary): the
+    targets are then centred (their mean is arbitrary)."""
+    return not any(options.BC[c][s] == "pres" for c in ("u", "v") for s in ("left", "right", "low", "up"))
+
+
+def prepare_pairs(options, f, p, n=None):
+    """Network inputs and targets (float32, shape (n, Npy, Npx)) from n
+    recorded pairs: in = (f / diag A) / s, tgt = (p - mean) / s, s = rms(f / diag A)."""
+    import torch
+    n = f.shape[0] if n is None else int(n)
+    inp = torch.empty((n, options.Npy, options.Npx), dtype=torch.float32, device=f.device)
+    tgt = torch.empty_like(inp)
+    torch.cuda.synchronize(f.device)
+    options._check(options._lib.ins2d_cnn_prepare_pairs(options._ctx, f.data_ptr(), p.data_ptr(), n,
+                                                        int(singular(options)), inp.data_ptr(), tgt.data_ptr()))
+    return inp, tgt
+
+
+def train(net, inp, tgt, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None):
+    """Adam on random mini-batches of the pairs (cosine-decayed learning
+    rate); sets out_scale to the targets' rms first.  Returns the losses."""
+    import torch
+    n = inp.shape[0]
+    w, _ = net.params()
+    scale = float(torch.sqrt(torch.mean(tgt.double() ** 2)).item()) or 1.0
+    net.set_params(w, scale)
+    gen = torch.Generator(device="cpu").manual_seed(int(seed))
+    lr_final = lr * 0.05 if lr_final is None else lr_final
+    losses = []
+    for k in range(int(steps)):
+        idx = torch.randint(0, n, (min(batch, n),), generator=gen).to(inp.device)
+        xb = inp.index_select(0, idx).contiguous()
+        yb = tgt.index_select(0, idx).contiguous()
+        rate = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(steps - 1, 1)))
+        losses.append(net.train_step(xb, yb, rate) / scale ** 2)
+    return losses
+
+
+def attach(options, net):
+    """Use ``net`` as the initial guess of ``options``' PCG solves (None detaches)."""
+    options._check(options._lib.ins2d_set_learned_guess(options._ctx, net.handle if net is not None else None))
+    options._net = net

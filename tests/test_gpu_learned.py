@@ -1,0 +1,147 @@
+"""The learned initial guess on the GPU, through the C-ABI (ins2d_cnn_*):
+forward pass and loss gradient of the BF16 tensor-core network against the
+CPU oracle (oracle/cnn_ref.py, which emulates the same rounding points),
+training on the solver's own (f, dp) pairs, and what the trained network
+gains over the PCG without it at an unchanged residual tolerance."""
+import numpy as np
+import pytest
+
+from oracle import cnn_ref as N
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _net(seed=5, scale=0.8):
+    from ins2d_b200.learned import ConvNet
+    net = ConvNet(device=0, seed=seed)
+    w = N.he_init(seed)
+    net.set_params(w, scale)
+    return net, w.astype(np.float64), scale
+
+
+def _inputs(seed, B, H, W):
+    torch = _torch()
+    rng = np.random.default_rng(seed)
+    inp = rng.standard_normal((B, H, W)).astype(np.float32)
+    tgt = rng.standard_normal((B, H, W)).astype(np.float32)
+    return inp, tgt, torch.from_numpy(inp).cuda(), torch.from_numpy(tgt).cuda()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+@pytest.mark.parametrize("shape", [(1, 8, 16), (2, 37, 29), (1, 70, 131)])
+def test_forward_matches_oracle(shape):
+    B, H, W = shape
+    net, w, scale = _net()
+    inp, _, ti, _ = _inputs(1, B, H, W)
+    y = net.forward(ti).cpu().numpy()
+    y_ref, _ = N.forward(w, scale, inp, bf16_mode=True)
+    assert _rel(y, y_ref) < 1e-4, _rel(y, y_ref)
+
+
+@pytest.mark.parametrize("shape", [(2, 37, 29), (1, 24, 48)])
+def test_loss_gradient_matches_oracle(shape):
+    B, H, W = shape
+    net, w, scale = _net(seed=7, scale=1.3)
+    inp, tgt, ti, tt = _inputs(2, B, H, W)
+    loss, g = net.loss_grad(ti, tt)
+    loss_ref, g_ref = N.loss_grad(w, scale, inp, tgt, bf16_mode=True)
+    assert abs(loss - loss_ref) / loss_ref < 1e-5
+    # every layer's gradient block
+    bounds = [0, N.OFF_WM] + [N.OFF_WM + (l + 1) * N.SZ_WM for l in range(N.NMID)] + [N.NPARAM]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        assert _rel(g[a:b], g_ref[a:b]) < 2e-3, (a, b, _rel(g[a:b], g_ref[a:b]))
+
+
+def test_invalid_arguments_rejected():
+    from ins2d_b200.api import Ins2dError
+    torch = _torch()
+    net, _, _ = _net()
+    host = torch.zeros((1, 8, 8), dtype=torch.float32)  # host memory
+    with pytest.raises((Ins2dError, ValueError)):
+        net.forward(host)
+    dev = torch.zeros((1, 8, 8), dtype=torch.float32, device="cuda")
+    with pytest.raises(Ins2dError):
+        net.train_step(dev, dev, -1.0)
+    with pytest.raises(Ins2dError):
+        net.set_params(None, 0.0)
+
+
+def _cavity(N_=48, precond="jacobi", tol=1e-10):
+    import ins2d_b200
+    from ins2d_b200 import cases
+    x = cases.tanh_grid(N_, 0.0, 1.0, 1.05)
+    return ins2d_b200.Options(x, x.copy(), cases.BC_CAVITY, Re=1000.0, poisson=4, CG_acc=tol, CG_maxit=100000,
+                              uBC=cases.lid_uBC(1.0, 1.0), precond=precond, device=0)
+
+
+def _record(m, steps, capacity):
+    from ins2d_b200 import learned
+    f_buf, p_buf = learned.record_pairs(m, capacity)
+    V = np.zeros(m.NV)
+    p = m.pressure_additional_solve(V, np.zeros(m.Np), 0.0)
+    V, p = m.time_ERK(V, p, 0.0, 2e-3, nsteps=steps)
+    n = learned.recorded_pairs(m)
+    learned.stop_recording(m)
+    return f_buf, p_buf, n
+
+
+def test_training_gains_over_plain_pcg():
+    """Pairs from the solver's own first steps (a stretched lid-driven cavity);
+    the network trained on the first 80% and judged on the held-out rest: the
+    same tolerance is reached in fewer Jacobi-PCG iterations from the learned
+    guess, and the solutions agree within the tolerance."""
+    from ins2d_b200 import learned
+    torch = _torch()
+    m = _cavity()
+    f_buf, p_buf, n = _record(m, 24, 160)
+    assert n >= 100
+    ntr = int(0.8 * n)
+    inp, tgt = learned.prepare_pairs(m, f_buf[:ntr], p_buf[:ntr])
+    net = learned.ConvNet(device=0, seed=11)
+    losses = learned.train(net, inp, tgt, steps=400, batch=8, lr=3e-3, seed=1)
+    assert np.mean(losses[-20:]) < 0.5 * np.mean(losses[:5]), (losses[:5], losses[-20:])
+    it_plain, it_learned, res = [], [], []
+    for k in range(ntr, n):
+        f = f_buf[k].contiguous()
+        learned.attach(m, None)
+        dp0, s0 = m.pressure_poisson(f, return_stats=True)
+        learned.attach(m, net)
+        dp1, s1 = m.pressure_poisson(f, return_stats=True)
+        it_plain.append(s0["iters"])
+        it_learned.append(s1["iters"])
+        assert s1["norm1"] <= 1e-10 * (1 + 1e-9)
+        fh = f.cpu().numpy()
+        r = fh - m.laplacian(dp1.cpu().numpy())
+        res.append(np.linalg.norm(r) / np.linalg.norm(fh))
+    learned.attach(m, None)
+    print(f"\nheld-out solves: plain Jacobi-PCG {np.mean(it_plain):.1f} iterations, "
+          f"learned guess {np.mean(it_learned):.1f}; max relative residual {max(res):.2e}")
+    assert max(res) < 2e-10
+    assert np.mean(it_learned) < 0.95 * np.mean(it_plain)
+
+
+def test_learned_guess_with_multigrid_and_time_steps():
+    """With the multigrid preconditioner and inside time steps the learned
+    guess leaves the flow unchanged within the solver tolerance."""
+    from ins2d_b200 import learned
+    m = _cavity(precond="mg", tol=1e-12)
+    f_buf, p_buf, n = _record(m, 6, 40)
+    inp, tgt = learned.prepare_pairs(m, f_buf[:n], p_buf[:n])
+    net = learned.ConvNet(device=0, seed=3)
+    learned.train(net, inp, tgt, steps=60, batch=4, lr=3e-3)
+    V = np.zeros(m.NV)
+    p = m.pressure_additional_solve(V, np.zeros(m.Np), 0.0)
+    V0, p0 = m.time_ERK(V, p, 0.0, 2e-3, nsteps=5)
+    learned.attach(m, net)
+    V1, p1 = m.time_ERK(V, p, 0.0, 2e-3, nsteps=5)
+    learned.attach(m, None)
+    assert _rel(V1, V0) < 1e-9
