@@ -300,11 +300,20 @@ int ins2d_cnn_create(int32_t device, uint64_t seed, ins2d_cnn **out);
 int ins2d_cnn_destroy(ins2d_cnn *net);
 const char *ins2d_cnn_last_error(const ins2d_cnn *net);
 int ins2d_cnn_set_stream(ins2d_cnn *net, void *stream);
+/* tensor-core instructions of the 32 -> 32 layers (forward and
+ * backward-data): tcgen05.mma with TMEM accumulators (default) or the
+ * warp-level mma.sync m16n8k16; both BF16 x BF16 -> FP32 */
+#define INS2D_CNN_PATH_TCGEN05 0
+#define INS2D_CNN_PATH_MMA_SYNC 1
+int ins2d_cnn_set_path(ins2d_cnn *net, int32_t path);
 /* host copies of the FP32 master weights (w may be NULL) and the output scale */
 int ins2d_cnn_get_params(ins2d_cnn *net, float *w, float *out_scale);
 int ins2d_cnn_set_params(ins2d_cnn *net, const float *w, float out_scale);
 /* y = out_scale * net(in) */
 int ins2d_cnn_forward(ins2d_cnn *net, const float *in, float *y, int32_t B, int32_t H, int32_t W);
+/* host copy of the BF16 output of layer 1..5 (NHWC, 32 channels per pixel)
+ * of the last forward pass over `pixels` = B*H*W pixels */
+int ins2d_cnn_get_activations(ins2d_cnn *net, int32_t layer, int64_t pixels, uint16_t *out);
 /* loss = mean((net(in) - tgt)^2) and its gradient (host array of
  * INS2D_CNN_NPARAM floats, may be NULL); no update */
 int ins2d_cnn_loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int32_t B, int32_t H, int32_t W,

@@ -28,12 +28,13 @@ EXPORTED = [
     "ins2d_ens_create", "ins2d_ens_destroy", "ins2d_ens_last_error", "ins2d_ens_size", "ins2d_ens_member",
     "ins2d_ens_set_stream", "ins2d_ens_set_state", "ins2d_ens_get_state", "ins2d_ens_state_ptr", "ins2d_ens_set_member_dt",
     "ins2d_ens_erk_run", "ins2d_ens_set_solver", "ins2d_ens_solve_shape",
-    "ins2d_cnn_create", "ins2d_cnn_destroy", "ins2d_cnn_last_error", "ins2d_cnn_set_stream",
-    "ins2d_cnn_get_params", "ins2d_cnn_set_params", "ins2d_cnn_forward", "ins2d_cnn_loss_grad",
+    "ins2d_cnn_create", "ins2d_cnn_destroy", "ins2d_cnn_last_error", "ins2d_cnn_set_stream", "ins2d_cnn_set_path",
+    "ins2d_cnn_get_params", "ins2d_cnn_set_params", "ins2d_cnn_get_activations", "ins2d_cnn_forward", "ins2d_cnn_loss_grad",
     "ins2d_cnn_train_step", "ins2d_cnn_prepare_pairs", "ins2d_set_learned_guess", "ins2d_record_pairs",
     "ins2d_recorded_pairs",
 ]
 CNN_NPARAM = 37440
+CNN_PATH_TCGEN05, CNN_PATH_MMA_SYNC = 0, 1
 PROF_FAMILIES = ["stage", "div", "poisson", "project", "residual", "other"]
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
@@ -139,8 +140,10 @@ def load():
         "ins2d_cnn_destroy": (ctypes.c_int, [vp]),
         "ins2d_cnn_last_error": (ctypes.c_char_p, [vp]),
         "ins2d_cnn_set_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_cnn_set_path": (ctypes.c_int, [vp, ctypes.c_int32]),
         "ins2d_cnn_get_params": (ctypes.c_int, [vp, vp, P(ctypes.c_float)]),
         "ins2d_cnn_set_params": (ctypes.c_int, [vp, vp, ctypes.c_float]),
+        "ins2d_cnn_get_activations": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int64, vp]),
         "ins2d_cnn_forward": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
         "ins2d_cnn_loss_grad": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                P(ctypes.c_double), vp]),

@@ -193,6 +193,177 @@ __global__ void __launch_bounds__(256) k_conv_mid(const bf16 *__restrict__ in, c
   }
 }
 
+// --- 32 -> 32 on the 5th-generation tensor cores (tcgen05, TMEM accumulators) --------
+// Persistent blocks of 256 threads, two per SM.  Per 128-pixel tile (16 x 8):
+// all threads gather the im2col tile A (128 pixels x 288 = 9 taps x 32
+// channels, BF16) into shared memory in the canonical K-major layout without
+// swizzle (8-row x 16-byte core matrices; core matrices adjacent in K are
+// kALbo bytes apart, 8-row groups 128 bytes apart); one thread issues the 18
+// MMAs of K = 16 (M = 128, N = 32, FP32 accumulators in 32 TMEM columns) and
+// commits them to an mbarrier; after the (bounded) wait, warp w reads TMEM
+// lanes 32 (w % 4) .. +31 (its pixels), columns 16 (w / 4) .. +15 (its
+// channels), applies ReLU (MODE 0) or the mask (MODE 1) and stores BF16.
+// The weights (B: 32 x 288, same layout, kBLbo) are loaded once per block.
+constexpr int kTcM = 128;
+constexpr int kALbo = (kTcM / 8) * 128;        // 2048: next 8 K-elements of A
+constexpr int kBLbo = (kC / 8) * 128;          // 512: next 8 K-elements of B
+constexpr int kABytes = (kK / 8) * kALbo;      // 73728
+constexpr int kBBytes = (kK / 8) * kBLbo;      // 18432
+// Dynamic shared memory: A, B, the mbarrier and the TMEM address slot, padded
+// so that every address the descriptors can form stays inside the block's
+// allocation.
+constexpr int kTcSmem = 106496;
+// kind::f16 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B
+// BF16 (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at
+// bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kC >> 3) << 17) |
+                            ((uint32_t)(kTcM >> 4) << 24);
+constexpr long long kTcWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// shared-memory matrix descriptor: start, leading (K) and stride (M/N) byte
+// offsets in 16-byte units, descriptor version 1 (bit 46), no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 2) k_conv_mid_tc(const bf16 *__restrict__ in, const bf16 *__restrict__ wt,
+                                                        const bf16 *__restrict__ mask, bf16 *__restrict__ out, int B,
+                                                        int H, int W, int tiles_x, int tiles_y,
+                                                        unsigned *__restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sA = smem;
+  uint8_t *sB = smem + kABytes;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kABytes + kBBytes);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kABytes + kBBytes + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // B: element (n = co, k) at (k / 8) * kBLbo + co * 16 + (k % 8) * 2
+  for (int i = tid; i < kC * (kK / 8); i += 256) {
+    const int co = i % kC, kc = i / kC;
+    *reinterpret_cast<uint4 *>(sB + kc * kBLbo + co * 16) = *reinterpret_cast<const uint4 *>(&wt[co * kK + kc * 8]);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                 "r"(kC)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  const uint32_t mb = smem_u32(mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mb), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t taddr = *tslot;
+  const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+  uint32_t phase = 0;
+  const long long per_field = (long long)tiles_x * tiles_y;
+  const long long ntiles = per_field * B;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int b = (int)(tile / per_field);
+    const int rem = (int)(tile % per_field);
+    const int x0 = (rem % tiles_x) * TW, y0 = (rem / tiles_x) * TH;
+    const long long fbase = (long long)b * H * W;
+    // A: element (m, k) at (k / 8) * kALbo + m * 16 + (k % 8) * 2, k = tap * 32 + ci
+    for (int i = tid; i < kTcM * (kK / 8); i += 256) {
+      const int m = i & (kTcM - 1), kc = i >> 7;
+      const int t = kc >> 2, c8 = kc & 3;
+      const int gx = x0 + (m & (TW - 1)) + t % 3 - 1, gy = y0 + (m >> 4) + t / 3 - 1;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gx >= 0 && gx < W && gy >= 0 && gy < H)
+        v = *reinterpret_cast<const uint4 *>(&in[(fbase + (long long)gy * W + gx) * kC + c8 * 8]);
+      *reinterpret_cast<uint4 *>(sA + kc * kALbo + m * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+      for (int ks = 0; ks < kK / 16; ++ks)
+        tc_mma(taddr, smem_desc(aBase + 2 * ks * kALbo, kALbo, 128), smem_desc(bBase + 2 * ks * kBLbo, kBLbo, 128),
+               kIdesc, ks > 0 ? 1u : 0u);
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
+                   : "memory");
+    }
+    bool ok = false;
+    for (long long it = 0; it < kTcWaitLimit && !ok; ++it) ok = mbar_try(mb, phase);
+    if (!__syncthreads_and(ok)) {
+      // give the MMAs a second bounded wait before the TMEM is freed
+      if (tid == 0) atomicExch(err, 1u);
+      for (long long it = 0; it < kTcWaitLimit && !ok; ++it) ok = mbar_try(mb, phase);
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    uint32_t r[16];
+    const int ch0 = 16 * (warp >> 2);
+    tmem_ld16(taddr + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)ch0, r);
+    const int m = 32 * (warp & 3) + lane;
+    const int gx = x0 + (m & (TW - 1)), gy = y0 + (m >> 4);
+    if (gx < W && gy < H) {
+      const long long pix = fbase + (long long)gy * W + gx;
+      float v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+      if (MODE == 0) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j], 0.0f);
+      } else {
+        const uint4 *mp = reinterpret_cast<const uint4 *>(&mask[pix * kC + ch0]);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          float mv[8];
+          unpack8(mp[q], mv);
+#pragma unroll
+          for (int e = 0; e < 8; ++e)
+            if (!(mv[e] > 0.0f)) v[q * 8 + e] = 0.0f;
+        }
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(&out[pix * kC + ch0]);
+      dst[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+      dst[1] = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]), pack2(v[14], v[15]));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(kC) : "memory");
+}
+
 // --- layer 6: 32 -> 1 ------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_conv_out(const bf16 *__restrict__ a5, const float *__restrict__ w6,
                                                   float scale, float *__restrict__ y, int B, int H, int W) {
@@ -531,6 +702,20 @@ __global__ void __launch_bounds__(256) k_resid(long long n, const double *__rest
   block_sum<2>(v, mx, part + 2 * blockIdx.x);
 }
 
+template <int MODE>
+void launch_mid(ins2d_cnn *net, const bf16 *in, const bf16 *wt, const bf16 *mask, bf16 *out, int B, int H, int W,
+                cudaStream_t s) {
+  const int tiles_x = (W + TW - 1) / TW, tiles_y = (H + TH - 1) / TH;
+  if (net->path == INS2D_CNN_PATH_TCGEN05) {
+    CK(cudaFuncSetAttribute(k_conv_mid_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    const long long nt = (long long)tiles_x * tiles_y * B;
+    const int grid = (int)std::min<long long>(nt, 2LL * net->sms);
+    k_conv_mid_tc<MODE><<<grid, 256, kTcSmem, s>>>(in, wt, mask, out, B, H, W, tiles_x, tiles_y, net->flag);
+  } else {
+    k_conv_mid<MODE><<<dim3(tiles_x, tiles_y, B), 256, 0, s>>>(in, wt, mask, out, H, W);
+  }
+}
+
 unsigned stride_blocks(long long n, int per_sm = 8) {
   long long b = (n + 255) / 256;
   const long long cap = std::min<long long>(148LL * per_sm, kRedBlocks);
@@ -546,6 +731,8 @@ void pack(ins2d_cnn *net, cudaStream_t s) {
 }
 
 }  // namespace
+
+void check(ins2d_cnn *net, cudaStream_t s);
 
 void reserve(ins2d_cnn *net, long long pixels) {
   if (pixels <= net->cap) return;
@@ -571,9 +758,8 @@ void forward(ins2d_cnn *net, const float *in, int B, int H, int W, cudaStream_t 
   pack(net, s);
   const unsigned gb = stride_blocks(n, 16);
   k_conv_in<<<gb, 256, 0, s>>>(in, net->w + kOffW1, net->act[0], B, H, W);
-  const dim3 grid((W + TW - 1) / TW, (H + TH - 1) / TH, B);
   for (int l = 0; l < kMid; ++l)
-    k_conv_mid<0><<<grid, 256, 0, s>>>(net->act[l], net->wf + l * kSzWm, nullptr, net->act[l + 1], H, W);
+    launch_mid<0>(net, net->act[l], net->wf + l * kSzWm, nullptr, net->act[l + 1], B, H, W, s);
   k_conv_out<<<gb, 256, 0, s>>>(net->act[4], net->w + kOffW6, net->out_scale, net->y, B, H, W);
   CK(cudaGetLastError());
 }
@@ -596,13 +782,12 @@ double loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int B, int H
   const int tiles_x = (W + TW - 1) / TW, tiles_y = (H + TH - 1) / TH;
   const long long ntiles = (long long)tiles_x * tiles_y * B;
   const int wb = (int)std::min<long long>(kWgBlocks, ntiles);
-  const dim3 grid(tiles_x, tiles_y, B);
   int cur = 0;
   for (int l = kMid - 1; l >= 0; --l) {
     // layer index l: input act[l], output act[l + 1], gradient dZ in dz[cur]
     k_wgrad_mid<<<wb, kK, 0, s>>>(net->dz[cur], net->act[l], net->partials, B, H, W, tiles_x, tiles_y);
     k_reduce_rows<<<(kSzWm + 255) / 256, 256, 0, s>>>(net->partials, wb, kSzWm, net->g + kOffWm + l * kSzWm, 0);
-    k_conv_mid<1><<<grid, 256, 0, s>>>(net->dz[cur], net->wb + l * kSzWm, net->act[l], net->dz[cur ^ 1], H, W);
+    launch_mid<1>(net, net->dz[cur], net->wb + l * kSzWm, net->act[l], net->dz[cur ^ 1], B, H, W, s);
     cur ^= 1;
   }
   // layer 1
@@ -612,7 +797,18 @@ double loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int B, int H
   double h = 0.0;
   CK(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  check(net, s);
   return h / (double)n;
+}
+
+void check(ins2d_cnn *net, cudaStream_t s) {
+  unsigned f = 0;
+  CK(cudaMemcpyAsync(&f, net->flag, sizeof f, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (f) {
+    CK(cudaMemsetAsync(net->flag, 0, sizeof(unsigned), s));
+    throw CudaError("cnn: a tensor-core wait gave up (tcgen05 MMA did not complete)");
+  }
 }
 
 void adam(ins2d_cnn *net, float lr, cudaStream_t s) {
@@ -746,6 +942,9 @@ int ins2d_cnn_create(int32_t device, uint64_t seed, ins2d_cnn **out) {
     if (cudaMalloc(&n->partials, (size_t)cnn::kWgBlocks * cnn::kSzWm * sizeof(float)) != cudaSuccess)
       throw std::bad_alloc();
     if (cudaMalloc(&n->red, cnn::red_doubles() * sizeof(double)) != cudaSuccess) throw std::bad_alloc();
+    if (cudaMalloc(&n->flag, sizeof(unsigned)) != cudaSuccess) throw std::bad_alloc();
+    CK(cudaMemset(n->flag, 0, sizeof(unsigned)));
+    CK(cudaDeviceGetAttribute(&n->sms, cudaDevAttrMultiProcessorCount, device));
     std::vector<float> w;
     init_weights(w, seed);
     CK(cudaMemcpy(n->w, w.data(), pb, cudaMemcpyHostToDevice));
@@ -770,6 +969,7 @@ int ins2d_cnn_destroy(ins2d_cnn *n) {
   cudaFree(n->wf);
   cudaFree(n->wb);
   cudaFree(n->red);
+  cudaFree(n->flag);
   for (auto *a : n->act) cudaFree(a);
   for (auto *a : n->dz) cudaFree(a);
   delete n;
@@ -781,6 +981,14 @@ const char *ins2d_cnn_last_error(const ins2d_cnn *n) { return n ? n->err.c_str()
 int ins2d_cnn_set_stream(ins2d_cnn *n, void *stream) {
   if (!n) return INS2D_EINVAL;
   n->stream = (cudaStream_t)stream;
+  return INS2D_OK;
+}
+
+int ins2d_cnn_set_path(ins2d_cnn *n, int32_t path) {
+  if (!n) return INS2D_EINVAL;
+  if (path != INS2D_CNN_PATH_TCGEN05 && path != INS2D_CNN_PATH_MMA_SYNC)
+    return cnn_fail(n, INS2D_EINVAL, "cnn_set_path: unknown tensor-core path");
+  n->path = path;
   return INS2D_OK;
 }
 
@@ -826,8 +1034,24 @@ int ins2d_cnn_forward(ins2d_cnn *n, const float *in, float *y, int32_t B, int32_
     cnn::forward(n, in, B, H, W, n->stream);
     CK(cudaMemcpyAsync(y, n->y, (size_t)B * H * W * sizeof(float), cudaMemcpyDeviceToDevice, n->stream));
     CK(cudaStreamSynchronize(n->stream));
+    cnn::check(n, n->stream);
   } catch (const std::bad_alloc &) {
     return cnn_fail(n, INS2D_ENOMEM, "cnn_forward: out of device memory");
+  } catch (const std::exception &e) {
+    return cnn_fail(n, INS2D_ECUDA, e.what());
+  }
+  return INS2D_OK;
+}
+
+int ins2d_cnn_get_activations(ins2d_cnn *n, int32_t layer, int64_t pixels, uint16_t *out) {
+  if (!n) return INS2D_EINVAL;
+  if (layer < 1 || layer > 5 || !out || pixels < 1 || pixels > n->cap)
+    return cnn_fail(n, INS2D_EINVAL, "cnn_get_activations: layer 1..5, pixels of the last forward pass");
+  try {
+    CK(cudaSetDevice(n->device));
+    CK(cudaMemcpyAsync(out, n->act[layer - 1], (size_t)pixels * cnn::kC * sizeof(uint16_t), cudaMemcpyDeviceToHost,
+                       n->stream));
+    CK(cudaStreamSynchronize(n->stream));
   } catch (const std::exception &e) {
     return cnn_fail(n, INS2D_ECUDA, e.what());
   }

@@ -17,6 +17,7 @@
 #include <string>
 
 #include "device.cuh"
+#include "ins2d.h"
 
 namespace ins2d {
 namespace cnn {
@@ -52,6 +53,9 @@ struct ins2d_cnn {
   float *partials = nullptr;             // weight-gradient partials
   int part_rows = 0;
   double *red = nullptr;                 // reduction scratch (partials + results)
+  unsigned *flag = nullptr;              // set by a tensor-core kernel whose wait gave up
+  int sms = 148;
+  int path = INS2D_CNN_PATH_TCGEN05;     // tensor-core instructions of the 32 -> 32 layers
 };
 
 namespace ins2d {
@@ -75,6 +79,8 @@ void forward(ins2d_cnn *net, const float *in, int B, int H, int W, cudaStream_t 
 void guess(ins2d_cnn *net, const DevOps &P, const double *f, double *x0, cudaStream_t s);
 // ensures the buffers hold `pixels` pixels (throws std::bad_alloc)
 void reserve(ins2d_cnn *net, long long pixels);
+// throws when a tensor-core kernel reported a wait that gave up (synchronises)
+void check(ins2d_cnn *net, cudaStream_t s);
 // reductions for the Rayleigh-Ritz scaling of the guess (results copied to
 // the host; synchronises the stream):
 //   d[0] = x.f, d[1] = x.q, d[2] = f.f, d[3] = max|f|

@@ -64,6 +64,12 @@ class ConvNet:
     def set_stream(self, stream):
         self._check(self._lib.ins2d_cnn_set_stream(self._h, ctypes.c_void_p(stream)))
 
+    def set_path(self, path):
+        """Tensor-core instructions of the 32 -> 32 layers: 'tcgen05' (default)
+        or 'mma_sync'."""
+        code = {"tcgen05": _lib.CNN_PATH_TCGEN05, "mma_sync": _lib.CNN_PATH_MMA_SYNC}[path]
+        self._check(self._lib.ins2d_cnn_set_path(self._h, code))
+
     def params(self):
         """(FP32 weights as a numpy array of NPARAM, out_scale)."""
         w = np.empty(NPARAM, dtype=np.float32)
@@ -89,6 +95,13 @@ class ConvNet:
         torch.cuda.synchronize(inp.device)
         self._check(self._lib.ins2d_cnn_forward(self._h, inp.data_ptr(), y.data_ptr(), B, H, W))
         return y
+
+    def activations(self, layer, pixels):
+        """BF16 output of layer 1..5 of the last forward pass, as float32
+        numpy values of shape (pixels, 32)."""
+        raw = np.empty((int(pixels), 32), dtype=np.uint16)
+        self._check(self._lib.ins2d_cnn_get_activations(self._h, int(layer), int(pixels), raw.ctypes.data))
+        return (raw.astype(np.uint32) << 16).view(np.float32)
 
     def loss_grad(self, inp, tgt):
         """(mean squared error, gradient as a numpy float32 array); no update."""

@@ -86,11 +86,40 @@ def forward(w, out_scale, inp, bf16_mode=True):
     return out_scale * y6, acts
 
 
-def loss_grad(w, out_scale, inp, tgt, bf16_mode=True):
-    """(loss, flat gradient) of mean((y - tgt)^2)."""
+def layer(w, l, a_prev, bf16_mode=True):
+    """Output of layer l (1..6) from the given input activations (teacher
+    forcing: the device's own inputs of that layer); layers 1..5 after ReLU
+    and rounding, layer 6 before out_scale."""
     rnd = bf16 if bf16_mode else (lambda a: np.asarray(a, dtype=np.float64))
     W1, Wm, W6 = split(w)
-    y, acts = forward(w, out_scale, inp, bf16_mode)
+    a_prev = np.asarray(a_prev, dtype=np.float64)
+    if l == 1:
+        Z = np.zeros(a_prev.shape + (C,))
+        for t, (dy, dx) in enumerate(_taps()):
+            Z += _shift(a_prev, dy, dx)[..., None] * W1[:, t][None, None, None, :]
+        return rnd(np.maximum(Z, 0.0))
+    if l == 6:
+        y6 = np.zeros(a_prev.shape[:3])
+        for t, (dy, dx) in enumerate(_taps()):
+            y6 += _shift(a_prev, dy, dx) @ W6[t]
+        return y6
+    Wl = rnd(Wm[l - 2]) if bf16_mode else Wm[l - 2]
+    Z = np.zeros_like(a_prev)
+    for t, (dy, dx) in enumerate(_taps()):
+        Z += _shift(a_prev, dy, dx) @ Wl[:, t, :].T
+    return rnd(np.maximum(Z, 0.0))
+
+
+def loss_grad(w, out_scale, inp, tgt, bf16_mode=True, acts=None):
+    """(loss, flat gradient) of mean((y - tgt)^2).  ``acts`` = [A1..A5] uses
+    given forward activations (the device's) instead of recomputing them."""
+    rnd = bf16 if bf16_mode else (lambda a: np.asarray(a, dtype=np.float64))
+    W1, Wm, W6 = split(w)
+    if acts is None:
+        y, acts = forward(w, out_scale, inp, bf16_mode)
+    else:
+        acts = [np.asarray(inp, dtype=np.float64)] + [np.asarray(a, dtype=np.float64) for a in acts]
+        y = out_scale * layer(w, 6, acts[5], bf16_mode)
     n = y.size
     d = y - np.asarray(tgt, dtype=np.float64)
     loss = float(np.sum(d * d) / n)

@@ -17,9 +17,10 @@ def _torch():
     return torch
 
 
-def _net(seed=5, scale=0.8):
+def _net(seed=5, scale=0.8, path="tcgen05"):
     from ins2d_b200.learned import ConvNet
     net = ConvNet(device=0, seed=seed)
+    net.set_path(path)
     w = N.he_init(seed)
     net.set_params(w, scale)
     return net, w.astype(np.float64), scale
@@ -37,28 +38,68 @@ def _rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
 
+def _check_layers(net, w, scale, inp, y):
+    """Teacher-forced check of every layer: the oracle's layer l from the
+    device's own input of that layer must equal the device's BF16 output,
+    except for rare one-ulp rounding flips (FP32 sums on the device, FP64 in
+    the oracle) and ReLU decisions at |Z| ~ 0."""
+    B, H, W = inp.shape
+    acts = [net.activations(l, B * H * W).reshape(B, H, W, 32) for l in range(1, 6)]
+    prev = inp
+    for l in range(1, 6):
+        ref = N.layer(w, l, prev)
+        got = acts[l - 1].astype(np.float64)
+        diff = np.abs(got - ref)
+        bad = diff > 2.0 ** -7 * np.maximum(np.abs(ref), np.abs(got)) + 1e-6 * np.max(np.abs(ref))
+        assert not bad.any(), (l, int(bad.sum()), float(diff.max()))
+        assert np.mean(got != ref) < 5e-3, (l, float(np.mean(got != ref)))
+        prev = got
+    y_ref = scale * N.layer(w, 6, prev)
+    assert _rel(y, y_ref) < 1e-5, _rel(y, y_ref)
+    return acts
+
+
+@pytest.mark.parametrize("path", ["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("shape", [(1, 8, 16), (2, 37, 29), (1, 70, 131)])
-def test_forward_matches_oracle(shape):
+def test_forward_matches_oracle(shape, path):
     B, H, W = shape
-    net, w, scale = _net()
+    net, w, scale = _net(path=path)
     inp, _, ti, _ = _inputs(1, B, H, W)
     y = net.forward(ti).cpu().numpy()
+    _check_layers(net, w, scale, inp, y)
+    # end to end, the rounding flips cascade: a looser bound
     y_ref, _ = N.forward(w, scale, inp, bf16_mode=True)
-    assert _rel(y, y_ref) < 1e-4, _rel(y, y_ref)
+    assert _rel(y, y_ref) < 3e-2, _rel(y, y_ref)
 
 
+@pytest.mark.parametrize("path", ["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("shape", [(2, 37, 29), (1, 24, 48)])
-def test_loss_gradient_matches_oracle(shape):
+def test_loss_gradient_matches_oracle(shape, path):
     B, H, W = shape
-    net, w, scale = _net(seed=7, scale=1.3)
+    net, w, scale = _net(seed=7, scale=1.3, path=path)
     inp, tgt, ti, tt = _inputs(2, B, H, W)
     loss, g = net.loss_grad(ti, tt)
-    loss_ref, g_ref = N.loss_grad(w, scale, inp, tgt, bf16_mode=True)
+    acts = [net.activations(l, B * H * W).reshape(B, H, W, 32) for l in range(1, 6)]
+    loss_ref, g_ref = N.loss_grad(w, scale, inp, tgt, bf16_mode=True, acts=acts)
     assert abs(loss - loss_ref) / loss_ref < 1e-5
-    # every layer's gradient block
+    # every layer's gradient block (the backward pass's BF16 rounding flips
+    # of dZ cascade like the forward's)
     bounds = [0, N.OFF_WM] + [N.OFF_WM + (l + 1) * N.SZ_WM for l in range(N.NMID)] + [N.NPARAM]
     for a, b in zip(bounds[:-1], bounds[1:]):
-        assert _rel(g[a:b], g_ref[a:b]) < 2e-3, (a, b, _rel(g[a:b], g_ref[a:b]))
+        assert _rel(g[a:b], g_ref[a:b]) < 1e-2, (a, b, _rel(g[a:b], g_ref[a:b]))
+    # the layer-6 gradient sees no rounding after the device's activations
+    assert _rel(g[N.OFF_W6:], g_ref[N.OFF_W6:]) < 1e-5
+
+
+def test_tensor_core_paths_agree_on_large_field():
+    """Both instruction paths on a field larger than the persistent grid
+    (several tiles per block) give the same network output."""
+    torch = _torch()
+    a, _, _ = _net(seed=9, path="tcgen05")
+    b, _, _ = _net(seed=9, path="mma_sync")
+    x = torch.randn(2, 301, 517, dtype=torch.float32, device="cuda")
+    ya, yb = a.forward(x), b.forward(x)
+    assert float(torch.linalg.norm(ya - yb) / torch.linalg.norm(yb)) < 1e-5
 
 
 def test_invalid_arguments_rejected():
