@@ -193,3 +193,36 @@ def attach(options, net):
     """Use ``net`` as the initial guess of ``options``' PCG solves (None detaches)."""
     options._check(options._lib.ins2d_set_learned_guess(options._ctx, net.handle if net is not None else None))
     options._net = net
+
+
+def _main():
+    """Times the network's forward pass on one random N x N field with CUDA
+    events (``python -m ins2d_b200.learned --forward 1024 --path tcgen05``)."""
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--forward", type=int, default=1024, help="field size N (N x N pixels)")
+    ap.add_argument("--batch", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--path", default="tcgen05", choices=["tcgen05", "mma_sync"])
+    a = ap.parse_args()
+    net = ConvNet(device=0, seed=0)
+    net.set_path(a.path)
+    x = torch.randn(a.batch, a.forward, a.forward, dtype=torch.float32, device="cuda")
+    net.forward(x)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.reps):
+        net.forward(x)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.reps
+    flops = 2 * 9 * (1 * 32 + 4 * 32 * 32 + 32 * 1) * a.batch * a.forward ** 2
+    print(json.dumps({"path": a.path, "pixels": a.batch * a.forward ** 2, "ms_per_forward": ms,
+                      "tflops": flops / ms / 1e9}))
+
+
+if __name__ == "__main__":
+    _main()
