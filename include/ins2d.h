@@ -331,6 +331,15 @@ int ins2d_cnn_prepare_pairs(ins2d_ctx *ctx, const double *f, const double *p, in
  * solves (poisson 1-5; the FFT path is direct and ignores it).  The context
  * borrows the network: keep it alive while attached. */
 int ins2d_set_learned_guess(ins2d_ctx *ctx, ins2d_cnn *net);
+/* role of the attached network: INS2D_LEARNED_GUESS (default: the PCG with
+ * the context's preconditioner starts from the network's guess) or
+ * INS2D_LEARNED_PRECOND (flexible CG, FCG(1), from the guess with the network
+ * as the preconditioner, z = M(r); after 200 iterations without convergence
+ * or on a breakdown the plain PCG finishes from the current iterate).  Both
+ * stop on ||r|| <= CG_acc ||f||. */
+#define INS2D_LEARNED_GUESS 0
+#define INS2D_LEARNED_PRECOND 1
+int ins2d_set_learned_mode(ins2d_ctx *ctx, int32_t mode);
 /* Recording of the solver's own (f, dp) pairs: each later PCG solve without
  * a learned guess copies its right-hand side and solution into the device
  * buffers f_buf, p_buf (capacity pairs of Np doubles) until they are full;

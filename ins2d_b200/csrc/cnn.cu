@@ -716,6 +716,56 @@ void launch_mid(ins2d_cnn *net, const bf16 *in, const bf16 *wt, const bf16 *mask
   }
 }
 
+// z = rms * y: the network output rescaled by the rms of its unscaled input
+// (stats[0] = sum of squares over n_stat cells), so z = M(r) is homogeneous
+// of degree one in r
+__global__ void k_widen_scaled(const float *__restrict__ y, double *__restrict__ x, long long n,
+                               const double *__restrict__ stats, double n_stat) {
+  const double s = sqrt(stats[0] / n_stat);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    x[k] = s * (double)y[k];
+}
+
+// flexible CG vector steps (each with its block partials)
+__global__ void __launch_bounds__(256) k_fcg_pq(long long n, const double *__restrict__ p,
+                                                const double *__restrict__ q, const double *__restrict__ r,
+                                                double *__restrict__ part) {
+  double v[2] = {0.0, 0.0};
+  const bool mx[2] = {false, false};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double pv = p[k];
+    v[0] += pv * q[k];
+    v[1] += pv * r[k];
+  }
+  block_sum<2>(v, mx, part + 2 * blockIdx.x);
+}
+__global__ void __launch_bounds__(256) k_fcg_update(long long n, double a, double *__restrict__ x,
+                                                    double *__restrict__ r, const double *__restrict__ p,
+                                                    const double *__restrict__ q, double *__restrict__ part) {
+  double v[2] = {0.0, 0.0};
+  const bool mx[2] = {false, true};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    x[k] += a * p[k];
+    const double rv = r[k] - a * q[k];
+    r[k] = rv;
+    v[0] += rv * rv;
+    v[1] = fmax(v[1], fabs(rv));
+  }
+  block_sum<2>(v, mx, part + 2 * blockIdx.x);
+}
+__global__ void __launch_bounds__(256) k_fcg_zq(long long n, const double *__restrict__ z,
+                                                const double *__restrict__ q, double *__restrict__ part) {
+  double v[1] = {0.0};
+  const bool mx[1] = {false};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    v[0] += z[k] * q[k];
+  block_sum<1>(v, mx, part + blockIdx.x);
+}
+__global__ void k_fcg_p(long long n, double b, const double *__restrict__ z, double *__restrict__ p) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    p[k] = z[k] + b * p[k];
+}
+
 unsigned stride_blocks(long long n, int per_sm = 8) {
   long long b = (n + 255) / 256;
   const long long cap = std::min<long long>(148LL * per_sm, kRedBlocks);
@@ -842,6 +892,58 @@ void guess(ins2d_cnn *net, const DevOps &P, const double *f, double *x0, cudaStr
   prepare(P, f, nullptr, 0, net->in1, nullptr, net->red, s);
   forward(net, net->in1, 1, P.Npy, P.Npx, s);
   k_widen<<<stride_blocks(P.Np), 256, 0, s>>>(net->y, x0, P.Np);
+  CK(cudaGetLastError());
+}
+
+void precond(ins2d_cnn *net, const DevOps &P, const double *r, double *z, cudaStream_t s) {
+  reserve(net, P.Np);
+  if (net->in1_cap < P.Np) {
+    cudaFree(net->in1);
+    net->in1 = nullptr;
+    net->in1_cap = 0;
+    if (cudaMalloc(&net->in1, P.Np * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
+    net->in1_cap = P.Np;
+  }
+  prepare(P, r, nullptr, 0, net->in1, nullptr, net->red, s);
+  forward(net, net->in1, 1, P.Npy, P.Npx, s);
+  k_widen_scaled<<<stride_blocks(P.Np), 256, 0, s>>>(net->y, z, P.Np, net->red + 4 * kRedBlocks, (double)P.Np);
+  CK(cudaGetLastError());
+}
+
+namespace {
+void finish_read(int nq, unsigned gb, int max_mask, double *red, double *d, cudaStream_t s) {
+  double *part = red, *res = red + 4 * kRedBlocks;
+  if (nq == 1)
+    k_finish<1><<<1, 256, 0, s>>>(part, (int)gb, max_mask, res);
+  else
+    k_finish<2><<<1, 256, 0, s>>>(part, (int)gb, max_mask, res);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(d, res, nq * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+}
+}  // namespace
+
+void fcg_pq(long long n, const double *p, const double *q, const double *r, double *red, double d[2],
+            cudaStream_t s) {
+  const unsigned gb = stride_blocks(n);
+  k_fcg_pq<<<gb, 256, 0, s>>>(n, p, q, r, red);
+  finish_read(2, gb, 0, red, d, s);
+}
+void fcg_update(long long n, double a, double *x, double *r, const double *p, const double *q, double *red,
+                double d[2], cudaStream_t s) {
+  const unsigned gb = stride_blocks(n);
+  k_fcg_update<<<gb, 256, 0, s>>>(n, a, x, r, p, q, red);
+  finish_read(2, gb, 2, red, d, s);
+}
+double fcg_zq(long long n, const double *z, const double *q, double *red, cudaStream_t s) {
+  const unsigned gb = stride_blocks(n);
+  k_fcg_zq<<<gb, 256, 0, s>>>(n, z, q, red);
+  double d = 0.0;
+  finish_read(1, gb, 0, red, &d, s);
+  return d;
+}
+void fcg_p(long long n, double b, const double *z, double *p, cudaStream_t s) {
+  k_fcg_p<<<stride_blocks(n), 256, 0, s>>>(n, b, z, p);
   CK(cudaGetLastError());
 }
 

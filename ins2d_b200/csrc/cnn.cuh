@@ -85,6 +85,17 @@ void check(ins2d_cnn *net, cudaStream_t s);
 // the host; synchronises the stream):
 //   d[0] = x.f, d[1] = x.q, d[2] = f.f, d[3] = max|f|
 void dots(long long n, const double *x, const double *f, const double *q, double *red, double d[4], cudaStream_t s);
+// z = M(r): the network applied to r (prepared like f), rescaled by the rms of
+// r / diag A so that M(c r) = c M(r) for c > 0
+void precond(ins2d_cnn *net, const DevOps &P, const double *r, double *z, cudaStream_t s);
+// flexible CG steps (each synchronises and returns its reductions):
+//   d = {p.q, p.r};  x += a p, r -= a q, d = {r.r, max|r|};  z.q;  p = z + b p
+void fcg_pq(long long n, const double *p, const double *q, const double *r, double *red, double d[2],
+            cudaStream_t s);
+void fcg_update(long long n, double a, double *x, double *r, const double *p, const double *q, double *red,
+                double d[2], cudaStream_t s);
+double fcg_zq(long long n, const double *z, const double *q, double *red, cudaStream_t s);
+void fcg_p(long long n, double b, const double *z, double *p, cudaStream_t s);
 //   r = f - a q, x *= a; d[0] = r.r, d[1] = max|r|
 void residual(long long n, const double *f, const double *q, double a, double *x, double *r, double *red,
               double d[2], cudaStream_t s);

@@ -82,7 +82,8 @@ struct ins2d_ctx {
   StepGraph step_graph[2];
   // learned initial guess of the PCG (borrowed network) and its work arrays
   ins2d_cnn *cnn = nullptr;
-  double *lg_x0 = nullptr, *lg_q = nullptr, *lg_r0 = nullptr, *lg_red = nullptr;
+  int lg_mode = INS2D_LEARNED_GUESS;
+  double *lg_x0 = nullptr, *lg_q = nullptr, *lg_r0 = nullptr, *lg_red = nullptr, *lg_p = nullptr, *lg_z = nullptr;
   // recording of (f, dp) pairs of the plain PCG solves
   double *rec_f = nullptr, *rec_p = nullptr;
   int rec_cap = 0, rec_n = 0;
@@ -304,6 +305,70 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
 // the energy norm), then CG on A e = r0 = f - A x0 to ||r|| <= CG_acc ||f||
 // (the inner tolerance is rescaled to ||r0||), dp = x0 + e.  Right-hand
 // sides with max|f| < 1e-14 take the plain path (pressure_poisson.m:33-38).
+// Flexible CG with the network as the preconditioner, from x = lg_x0 with
+// residual r = lg_r0 (FCG(1): each new direction z = M(r) is A-orthogonalised
+// against the previous one, beta = -(z'Ap)/(p'Ap), which keeps CG's short
+// recurrence meaningful for a nonlinear M).  Same stopping rule as cg.F.  If
+// it has not converged after kFcgMaxit iterations or breaks down, the plain
+// PCG finishes the solve from the current iterate.
+constexpr int kFcgMaxit = 200;
+int fcg_learned(ins2d_ctx *c, double *dp, bool accumulate, ins2d_solve_stats *st, double ff) {
+  const long long n = c->P.Np;
+  const double tol = c->opts.CG_acc;
+  double *x = c->lg_x0, *r = c->lg_r0, *q = c->lg_q, *p = c->lg_p, *z = c->lg_z;
+  const int maxit = std::min(c->opts.CG_maxit, kFcgMaxit);
+  bool conv = false;
+  double rr = 0.0;
+  int it = 0;
+  {
+    Prof pr(c, INS2D_PROF_POISSON, 12);
+    cnn::precond(c->cnn, c->P, r, z, c->stream);
+    CK(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  while (it < maxit) {
+    Prof pr(c, INS2D_PROF_POISSON, 20);
+    launch_lap(c->P, p, q, c->stream);
+    CK(cudaGetLastError());
+    double d[2], u[2];
+    cnn::fcg_pq(n, p, q, r, c->lg_red, d, c->stream);
+    if (!std::isfinite(d[0]) || !std::isfinite(d[1]) || d[0] == 0.0) break;
+    cnn::fcg_update(n, d[1] / d[0], x, r, p, q, c->lg_red, u, c->stream);
+    ++it;
+    rr = u[0];
+    if (!std::isfinite(rr)) return fail(c, INS2D_ENONFINITE, "FCG: non-finite residual");
+    if (rr <= tol * tol * ff || u[1] < 1e-300) {
+      conv = true;
+      break;
+    }
+    cnn::precond(c->cnn, c->P, r, z, c->stream);
+    cnn::fcg_p(n, -cnn::fcg_zq(n, z, q, c->lg_red, c->stream) / d[0], z, p, c->stream);
+  }
+  cnn::check(c->cnn, c->stream);
+  if (conv) {
+    Prof pr(c, INS2D_PROF_POISSON, 1);
+    if (accumulate)
+      launch_add(x, dp, n, c->stream);
+    else
+      CK(cudaMemcpyAsync(dp, x, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaGetLastError());
+    if (st) *st = ins2d_solve_stats{it, std::sqrt(rr / ff), 0.0};
+    return INS2D_OK;
+  }
+  double d[2];
+  cnn::fcg_pq(n, r, r, r, c->lg_red, d, c->stream);
+  const double scale = std::sqrt(d[0] / ff);
+  int rc = solve_pcg(c, r, dp, accumulate, st, tol / scale);
+  if (rc) return rc;
+  if (st) {
+    st->norm1 *= scale;
+    st->iters += it;
+  }
+  Prof pr(c, INS2D_PROF_POISSON, 1);
+  launch_add(x, dp, n, c->stream);
+  CK(cudaGetLastError());
+  return INS2D_OK;
+}
+
 int solve_learned(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st) {
   const long long n = c->P.Np;
   const double tol = c->opts.CG_acc;
@@ -332,6 +397,7 @@ int solve_learned(ins2d_ctx *c, const double *f, double *dp, bool accumulate, in
     if (st) *st = ins2d_solve_stats{0, std::sqrt(rr0 / ff), 0.0};
     return INS2D_OK;
   }
+  if (c->lg_mode == INS2D_LEARNED_PRECOND) return fcg_learned(c, dp, accumulate, st, ff);
   const double scale = std::sqrt(rr0 / ff);
   int rc = solve_pcg(c, c->lg_r0, dp, accumulate, st, tol / scale);
   if (rc) return rc;
@@ -1048,12 +1114,22 @@ int ins2d_set_learned_guess(ins2d_ctx *ctx, ins2d_cnn *net) {
     ctx->lg_x0 = dalloc<double>(ctx, Np);
     ctx->lg_q = dalloc<double>(ctx, Np);
     ctx->lg_r0 = dalloc<double>(ctx, Np);
+    ctx->lg_p = dalloc<double>(ctx, Np);
+    ctx->lg_z = dalloc<double>(ctx, Np);
     if (!ctx->lg_red) ctx->lg_red = dalloc<double>(ctx, cnn::red_doubles());
   }
   if (net) cnn::reserve(net, ctx->P.Np);
   ctx->cnn = net;
   return INS2D_OK;
   API_END
+}
+
+int ins2d_set_learned_mode(ins2d_ctx *ctx, int32_t mode) {
+  if (!ctx) return INS2D_EINVAL;
+  if (mode != INS2D_LEARNED_GUESS && mode != INS2D_LEARNED_PRECOND)
+    return fail(ctx, INS2D_EINVAL, "set_learned_mode: unknown mode");
+  ctx->lg_mode = mode;
+  return INS2D_OK;
 }
 
 int ins2d_record_pairs(ins2d_ctx *ctx, double *f_buf, double *p_buf, int32_t capacity) {

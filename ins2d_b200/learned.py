@@ -189,9 +189,13 @@ def train(net, inp, tgt, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None):
     return losses
 
 
-def attach(options, net):
-    """Use ``net`` as the initial guess of ``options``' PCG solves (None detaches)."""
+def attach(options, net, mode="guess"):
+    """Use ``net`` in ``options``' PCG solves (None detaches): mode 'guess'
+    starts the context's PCG from the network's guess; 'precond' runs a
+    flexible CG with the network as the preconditioner (plain PCG finishes
+    if it stalls)."""
     options._check(options._lib.ins2d_set_learned_guess(options._ctx, net.handle if net is not None else None))
+    options._check(options._lib.ins2d_set_learned_mode(options._ctx, {"guess": 0, "precond": 1}[mode]))
     options._net = net
 
 

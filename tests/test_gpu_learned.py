@@ -150,24 +150,27 @@ def test_training_gains_over_plain_pcg():
     net = learned.ConvNet(device=0, seed=11)
     losses = learned.train(net, inp, tgt, steps=400, batch=8, lr=3e-3, seed=1)
     assert np.mean(losses[-20:]) < 0.5 * np.mean(losses[:5]), (losses[:5], losses[-20:])
-    it_plain, it_learned, res = [], [], []
+    it_plain, it_learned, it_fcg, res = [], [], [], []
     for k in range(ntr, n):
         f = f_buf[k].contiguous()
+        fh = f.cpu().numpy()
         learned.attach(m, None)
         dp0, s0 = m.pressure_poisson(f, return_stats=True)
-        learned.attach(m, net)
-        dp1, s1 = m.pressure_poisson(f, return_stats=True)
         it_plain.append(s0["iters"])
-        it_learned.append(s1["iters"])
-        assert s1["norm1"] <= 1e-10 * (1 + 1e-9)
-        fh = f.cpu().numpy()
-        r = fh - m.laplacian(dp1.cpu().numpy())
-        res.append(np.linalg.norm(r) / np.linalg.norm(fh))
+        for mode, its in (("guess", it_learned), ("precond", it_fcg)):
+            learned.attach(m, net, mode)
+            dp1, s1 = m.pressure_poisson(f, return_stats=True)
+            its.append(s1["iters"])
+            assert s1["norm1"] <= 1e-10 * (1 + 1e-9)
+            r = fh - m.laplacian(dp1.cpu().numpy())
+            res.append(np.linalg.norm(r) / np.linalg.norm(fh))
     learned.attach(m, None)
     print(f"\nheld-out solves: plain Jacobi-PCG {np.mean(it_plain):.1f} iterations, "
-          f"learned guess {np.mean(it_learned):.1f}; max relative residual {max(res):.2e}")
+          f"from the learned guess {np.mean(it_learned):.1f}, flexible CG with the network as the "
+          f"preconditioner {np.mean(it_fcg):.1f}; max relative residual {max(res):.2e}")
     assert max(res) < 2e-10
     assert np.mean(it_learned) < 0.95 * np.mean(it_plain)
+    assert np.mean(it_fcg) < 0.5 * np.mean(it_plain)
 
 
 def test_learned_guess_with_multigrid_and_time_steps():
