@@ -49,6 +49,14 @@ WORKLOADS = {
                               compare_plain=True,
                               desc="decaying 2D turbulence 2048x2048, FP32 stencils, multigrid-preconditioned PCG "
                                    "to 1e-10, FP64 Poisson/projection"),
+    "turb2048_pcg_fp32_learned": dict(N=2048, L=1.0, Re=2000.0, poisson=4, precision="fp32", ic="turbulence",
+                                      CG_acc=1e-10, compare_plain=True,
+                                      learned=dict(record_steps=12, pairs=60, train_steps=200, batch=2, lr=2e-3,
+                                                   seed=0),
+                                      desc="decaying 2D turbulence 2048x2048, FP32 stencils, multigrid PCG to 1e-10 "
+                                           "started from the learned guess (CNN trained on the GPU on the first "
+                                           "steps' solves), FP64 Poisson/projection; against the plain FP64 "
+                                           "Jacobi-PCG at the same residual"),
     "tg512": dict(N=512, L=2 * math.pi, Re=1e100, poisson=6, precision="fp64", ic="tg", dt=1e-3,
                   desc="inviscid Taylor-Green 512x512 periodic [0,2pi]^2, RK44 dt=1e-3, FFT Poisson, FP64"),
     "ldc64": dict(N=64, L=1.0, Re=1000.0, poisson=4, precision="fp64", ic="rest", dt=1e-3, CG_acc=1e-12,
@@ -369,7 +377,7 @@ def run_ours(args, wl, rank, world, local_rank):
                              round(STEP_BYTES_REFERENCE_DECOMPOSITION * cells / step_ms / 1e6 / peak, 4)}}
     # accuracy of this run: kinetic energy drift and divergence; for the FP32
     # stencil workload also the deviation from the FP64 path over the same steps
-    total_steps = args.warmup + args.steps + nprof
+    total_steps = (lw["record_steps"] if lw else 0) + args.warmup + args.steps + nprof
     acc = None
     if rank == 0:
         c0 = opts.check_conservation(torch.tensor(V0, dtype=torch.float64, device="cuda"), 0.0)
@@ -382,7 +390,7 @@ def run_ours(args, wl, rank, world, local_rank):
             o64.set_stream(stream.cuda_stream)
             V64 = torch.tensor(V64_0, dtype=torch.float64, device="cuda")
             p64 = o64.pressure_additional_solve(V64, torch.zeros(o64.Np, dtype=torch.float64, device="cuda"), 0.0)
-            o64.time_ERK(V64, p64, 0.0, dt, nsteps=args.warmup + args.steps)
+            o64.time_ERK(V64, p64, 0.0, dt, nsteps=(lw["record_steps"] if lw else 0) + args.warmup + args.steps)
             o64.time_ERK(V64, p64, 0.0, dt, nsteps=nprof)
             k64 = o64.check_conservation(V64, t)[3]
             acc.update({"fp64_k": k64, "energy_vs_fp64_rel": abs(c1[3] - k64) / k64,
