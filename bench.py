@@ -222,8 +222,8 @@ def setup_learned(opts, lw, Vd, pd, t, dt, stream, device):
     net.set_stream(stream.cuda_stream)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    losses = learned.train(net, inp, tgt, steps=lw["train_steps"], batch=lw["batch"], lr=lw["lr"],
-                           seed=lw.get("seed", 0))
+    losses = learned.train(net, inp, None, steps=lw["train_steps"], batch=lw["batch"], lr=lw["lr"],
+                           seed=lw.get("seed", 0), options=opts)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     del inp, tgt

@@ -321,6 +321,17 @@ int ins2d_cnn_loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int32
 /* one Adam step (beta 0.9/0.999, eps 1e-8) on that loss */
 int ins2d_cnn_train_step(ins2d_cnn *net, const float *in, const float *tgt, int32_t B, int32_t H, int32_t W,
                          float lr, double *loss);
+/* The residual loss on a context's grid: mean((A y - diag(A) in)^2) with
+ * y = net(in) and A = M Om^-1 G the context's pressure operator (for inputs
+ * from ins2d_cnn_prepare_pairs, diag(A) in = f / s, so this is the scaled
+ * residual of y as a solution); it rewards what a local network can learn, an
+ * approximate inverse of A on the short wavelengths.  in: B fields of the
+ * context's Npy x Npx pressure grid.  loss_grad returns the loss and the
+ * gradient (host array, may be NULL); train_step takes one Adam step. */
+int ins2d_cnn_loss_grad_residual(ins2d_ctx *ctx, ins2d_cnn *net, const float *in, int32_t B, double *loss,
+                                 float *grad);
+int ins2d_cnn_train_step_residual(ins2d_ctx *ctx, ins2d_cnn *net, const float *in, int32_t B, float lr,
+                                  double *loss);
 /* Training pairs of a context's grid: for npairs right-hand sides f and
  * solutions p (device, Np each, one after another) writes the network input
  * in = (f / diag A) / s and target tgt = (p - center * mean(p)) / s, with

@@ -30,7 +30,7 @@ EXPORTED = [
     "ins2d_ens_erk_run", "ins2d_ens_set_solver", "ins2d_ens_solve_shape",
     "ins2d_cnn_create", "ins2d_cnn_destroy", "ins2d_cnn_last_error", "ins2d_cnn_set_stream", "ins2d_cnn_set_path",
     "ins2d_cnn_get_params", "ins2d_cnn_set_params", "ins2d_cnn_get_activations", "ins2d_cnn_forward", "ins2d_cnn_loss_grad",
-    "ins2d_cnn_train_step", "ins2d_cnn_prepare_pairs", "ins2d_set_learned_guess", "ins2d_set_learned_mode", "ins2d_record_pairs",
+    "ins2d_cnn_train_step", "ins2d_cnn_loss_grad_residual", "ins2d_cnn_train_step_residual", "ins2d_cnn_prepare_pairs", "ins2d_set_learned_guess", "ins2d_set_learned_mode", "ins2d_record_pairs",
     "ins2d_recorded_pairs",
 ]
 CNN_NPARAM = 37440
@@ -149,6 +149,9 @@ def load():
                                                P(ctypes.c_double), vp]),
         "ins2d_cnn_train_step": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_float, P(ctypes.c_double)]),
+        "ins2d_cnn_loss_grad_residual": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32, P(ctypes.c_double), vp]),
+        "ins2d_cnn_train_step_residual": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32, ctypes.c_float,
+                                                         P(ctypes.c_double)]),
         "ins2d_cnn_prepare_pairs": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32, ctypes.c_int32, vp, vp]),
         "ins2d_set_learned_guess": (ctypes.c_int, [vp, vp]),
         "ins2d_set_learned_mode": (ctypes.c_int, [vp, ctypes.c_int32]),

@@ -194,25 +194,33 @@ __global__ void __launch_bounds__(256) k_conv_mid(const bf16 *__restrict__ in, c
 }
 
 // --- 32 -> 32 on the 5th-generation tensor cores (tcgen05, TMEM accumulators) --------
-// Persistent blocks of 256 threads, two per SM.  Per 128-pixel tile (16 x 8):
-// all threads gather the im2col tile A (128 pixels x 288 = 9 taps x 32
-// channels, BF16) into shared memory in the canonical K-major layout without
-// swizzle (8-row x 16-byte core matrices; core matrices adjacent in K are
-// kALbo bytes apart, 8-row groups 128 bytes apart); one thread issues the 18
-// MMAs of K = 16 (M = 128, N = 32, FP32 accumulators in 32 TMEM columns) and
-// commits them to an mbarrier; after the (bounded) wait, warp w reads TMEM
-// lanes 32 (w % 4) .. +31 (its pixels), columns 16 (w / 4) .. +15 (its
-// channels), applies ReLU (MODE 0) or the mask (MODE 1) and stores BF16.
-// The weights (B: 32 x 288, same layout, kBLbo) are loaded once per block.
+// Persistent blocks of 256 threads, several per SM.  Per tile of 8 x 16
+// pixels (M = 128 rows, m = py * 8 + px): all threads stage the 10 x 18 halo
+// tile in shared memory as four channel planes (plane c8 holds channels
+// 8 c8 .. 8 c8 + 7 of every halo pixel, 16 bytes per pixel, rows of 10
+// pixels).  That is the canonical K-major layout without swizzle for every
+// tap at once: a core matrix is 8 consecutive pixels of one tile row (16
+// bytes apart), the next tile row is kTcSbo = 160 bytes further, the next 8
+// channels kTcLbo = 2880 bytes further, and tap (dy, dx) only moves the start
+// address by (dy * 10 + dx) * 16 bytes.  So the A operands of the 18 MMAs of
+// K = 16 (9 taps x 2 channel halves) are descriptors over one halo tile, with
+// no im2col copy.  One thread issues them (N = 32, FP32 accumulators in 32
+// TMEM columns) and commits to an mbarrier; after the (bounded) wait, warp w
+// reads TMEM lanes 32 (w % 4) .. +31 (its pixels), columns 16 (w / 4) .. +15
+// (its channels), applies ReLU (MODE 0) or the mask (MODE 1) and stores BF16.
+// The weights (B: 32 x 288; core matrices of 8 output channels, next 8 input
+// channels kBLbo bytes further) are loaded once per block.
 constexpr int kTcM = 128;
-constexpr int kALbo = (kTcM / 8) * 128;        // 2048: next 8 K-elements of A
+constexpr int kTcTW = 8, kTcTH = 16;           // tile: 8 pixels wide, 16 rows
+constexpr int kTcHW = kTcTW + 2, kTcHH = kTcTH + 2;
+constexpr int kTcSbo = kTcHW * 16;             // 160: next tile row
+constexpr int kTcLbo = kTcHH * kTcSbo;         // 2880: next 8 channels (plane)
+constexpr int kABytes = (kC / 8) * kTcLbo;     // 11520
 constexpr int kBLbo = (kC / 8) * 128;          // 512: next 8 K-elements of B
-constexpr int kABytes = (kK / 8) * kALbo;      // 73728
 constexpr int kBBytes = (kK / 8) * kBLbo;      // 18432
-// Dynamic shared memory: A, B, the mbarrier and the TMEM address slot, padded
-// so that every address the descriptors can form stays inside the block's
-// allocation.
-constexpr int kTcSmem = 106496;
+// Dynamic shared memory: A (halo planes), B, the mbarrier and the TMEM slot
+constexpr int kTcSmem = kABytes + kBBytes + 16;
+constexpr int kTcBlocksPerSm = 6;
 // kind::f16 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B
 // BF16 (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at
 // bits 24-28.
@@ -256,7 +264,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256, 2) k_conv_mid_tc(const bf16 *__restrict__ in, const bf16 *__restrict__ wt,
+__global__ void __launch_bounds__(256, kTcBlocksPerSm) k_conv_mid_tc(const bf16 *__restrict__ in, const bf16 *__restrict__ wt,
                                                         const bf16 *__restrict__ mask, bf16 *__restrict__ out, int B,
                                                         int H, int W, int tiles_x, int tiles_y,
                                                         unsigned *__restrict__ err) {
@@ -294,26 +302,28 @@ __global__ void __launch_bounds__(256, 2) k_conv_mid_tc(const bf16 *__restrict__
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int b = (int)(tile / per_field);
     const int rem = (int)(tile % per_field);
-    const int x0 = (rem % tiles_x) * TW, y0 = (rem / tiles_x) * TH;
+    const int x0 = (rem % tiles_x) * kTcTW, y0 = (rem / tiles_x) * kTcTH;
     const long long fbase = (long long)b * H * W;
-    // A: element (m, k) at (k / 8) * kALbo + m * 16 + (k % 8) * 2, k = tap * 32 + ci
-    for (int i = tid; i < kTcM * (kK / 8); i += 256) {
-      const int m = i & (kTcM - 1), kc = i >> 7;
-      const int t = kc >> 2, c8 = kc & 3;
-      const int gx = x0 + (m & (TW - 1)) + t % 3 - 1, gy = y0 + (m >> 4) + t / 3 - 1;
+    // halo planes: channels 8 c8 .. 8 c8 + 7 of halo pixel hp at c8 * kTcLbo + hp * 16
+    for (int i = tid; i < kTcHW * kTcHH * 4; i += 256) {
+      const int hp = i >> 2, c8 = i & 3;
+      const int gx = x0 - 1 + hp % kTcHW, gy = y0 - 1 + hp / kTcHW;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if (gx >= 0 && gx < W && gy >= 0 && gy < H)
         v = *reinterpret_cast<const uint4 *>(&in[(fbase + (long long)gy * W + gx) * kC + c8 * 8]);
-      *reinterpret_cast<uint4 *>(sA + kc * kALbo + m * 16) = v;
+      *reinterpret_cast<uint4 *>(sA + c8 * kTcLbo + hp * 16) = v;
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-      for (int ks = 0; ks < kK / 16; ++ks)
-        tc_mma(taddr, smem_desc(aBase + 2 * ks * kALbo, kALbo, 128), smem_desc(bBase + 2 * ks * kBLbo, kBLbo, 128),
-               kIdesc, ks > 0 ? 1u : 0u);
+      for (int ks = 0; ks < kK / 16; ++ks) {
+        const int t = ks >> 1, h = ks & 1;
+        const uint32_t a0 = aBase + 2 * h * kTcLbo + ((t / 3) * kTcHW + t % 3) * 16;
+        tc_mma(taddr, smem_desc(a0, kTcLbo, kTcSbo), smem_desc(bBase + 2 * ks * kBLbo, kBLbo, 128), kIdesc,
+               ks > 0 ? 1u : 0u);
+      }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mb)
                    : "memory");
     }
@@ -331,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) k_conv_mid_tc(const bf16 *__restrict__
     const int ch0 = 16 * (warp >> 2);
     tmem_ld16(taddr + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)ch0, r);
     const int m = 32 * (warp & 3) + lane;
-    const int gx = x0 + (m & (TW - 1)), gy = y0 + (m >> 4);
+    const int gx = x0 + (m & (kTcTW - 1)), gy = y0 + (m >> 3);
     if (gx < W && gy < H) {
       const long long pix = fbase + (long long)gy * W + gx;
       float v[16];
@@ -444,6 +454,49 @@ __global__ void __launch_bounds__(256) k_loss(const float *__restrict__ y, const
     v[0] += (double)d * d;
   }
   block_sum<1>(v, mx, part + blockIdx.x);
+}
+
+// The pressure Laplacian A = M Om^-1 G of a context (its 1D row tables, the
+// form of lap() in device.cuh) applied to one FP32 field
+__device__ __forceinline__ float lap_f(const DevOps &P, const float *__restrict__ f, int i, int j) {
+  const int32_t *cx = P.TX.c + kT * i;
+  const double *wx = P.TX.w + kT * i;
+  const int32_t *cy = P.TY.c + kT * j;
+  const double *wy = P.TY.w + kT * j;
+  const long long row = (long long)j * P.Npx;
+  const float sx = (float)__ldg(wx) * f[row + __ldg(cx)] + (float)__ldg(wx + 1) * f[row + __ldg(cx + 1)] +
+                   (float)__ldg(wx + 2) * f[row + __ldg(cx + 2)];
+  const float sy = (float)__ldg(wy) * f[(long long)__ldg(cy) * P.Npx + i] +
+                   (float)__ldg(wy + 1) * f[(long long)__ldg(cy + 1) * P.Npx + i] +
+                   (float)__ldg(wy + 2) * f[(long long)__ldg(cy + 2) * P.Npx + i];
+  return -((float)__ldg(P.hy + j) * sx + (float)__ldg(P.hx + i) * sy);
+}
+
+// residual loss, pass 1: d = A y - diag(A) in per field (in = f / (diag(A) s),
+// so diag(A) in = f / s); partial sums of d^2
+__global__ void __launch_bounds__(256) k_res_loss(const __grid_constant__ DevOps P, const float *__restrict__ y,
+                                                  const float *__restrict__ in, float *__restrict__ d, int B,
+                                                  double *__restrict__ part) {
+  double v[1] = {0.0};
+  const bool mx[1] = {false};
+  const long long n = (long long)B * P.Np;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const long long b = k / P.Np, kk = k % P.Np;
+    const int i = (int)(kk % P.Npx), j = (int)(kk / P.Npx);
+    const float dv = lap_f(P, y + b * P.Np, i, j) - (float)lap_diag(P, i, j) * in[k];
+    d[k] = dv;
+    v[0] += (double)dv * dv;
+  }
+  block_sum<1>(v, mx, part + blockIdx.x);
+}
+// pass 2: dy = g A d (A is symmetric)
+__global__ void __launch_bounds__(256) k_res_grad(const __grid_constant__ DevOps P, const float *__restrict__ d,
+                                                  float *__restrict__ dy, float g, int B) {
+  const long long n = (long long)B * P.Np;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const long long b = k / P.Np, kk = k % P.Np;
+    dy[k] = g * lap_f(P, d + b * P.Np, (int)(kk % P.Npx), (int)(kk / P.Npx));
+  }
 }
 
 // dZ5[p][ci] = (sum_t W6[t][ci] dy[p - t]) [A5[p][ci] > 0]
@@ -705,13 +758,13 @@ __global__ void __launch_bounds__(256) k_resid(long long n, const double *__rest
 template <int MODE>
 void launch_mid(ins2d_cnn *net, const bf16 *in, const bf16 *wt, const bf16 *mask, bf16 *out, int B, int H, int W,
                 cudaStream_t s) {
-  const int tiles_x = (W + TW - 1) / TW, tiles_y = (H + TH - 1) / TH;
   if (net->path == INS2D_CNN_PATH_TCGEN05) {
-    CK(cudaFuncSetAttribute(k_conv_mid_tc<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-    const long long nt = (long long)tiles_x * tiles_y * B;
-    const int grid = (int)std::min<long long>(nt, 2LL * net->sms);
-    k_conv_mid_tc<MODE><<<grid, 256, kTcSmem, s>>>(in, wt, mask, out, B, H, W, tiles_x, tiles_y, net->flag);
+    const int tx = (W + kTcTW - 1) / kTcTW, ty = (H + kTcTH - 1) / kTcTH;
+    const long long nt = (long long)tx * ty * B;
+    const int grid = (int)std::min<long long>(nt, (long long)kTcBlocksPerSm * net->sms);
+    k_conv_mid_tc<MODE><<<grid, 256, kTcSmem, s>>>(in, wt, mask, out, B, H, W, tx, ty, net->flag);
   } else {
+    const int tiles_x = (W + TW - 1) / TW, tiles_y = (H + TH - 1) / TH;
     k_conv_mid<MODE><<<dim3(tiles_x, tiles_y, B), 256, 0, s>>>(in, wt, mask, out, H, W);
   }
 }
@@ -790,7 +843,8 @@ void reserve(ins2d_cnn *net, long long pixels) {
   for (auto *&a : net->dz) cudaFree(a), a = nullptr;
   cudaFree(net->y);
   cudaFree(net->dy);
-  net->y = net->dy = nullptr;
+  cudaFree(net->dres);
+  net->y = net->dy = net->dres = nullptr;
   net->cap = 0;
   const size_t nb = (size_t)pixels * kC * sizeof(bf16);
   for (auto *&a : net->act)
@@ -799,6 +853,7 @@ void reserve(ins2d_cnn *net, long long pixels) {
     if (cudaMalloc(&a, nb) != cudaSuccess) throw std::bad_alloc();
   if (cudaMalloc(&net->y, pixels * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
   if (cudaMalloc(&net->dy, pixels * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
+  if (cudaMalloc(&net->dres, pixels * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
   net->cap = pixels;
 }
 
@@ -815,12 +870,19 @@ void forward(ins2d_cnn *net, const float *in, int B, int H, int W, cudaStream_t 
 }
 
 // loss (returned, after a stream synchronisation) and the gradient in net->g
-double loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int B, int H, int W, cudaStream_t s) {
+double loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int B, int H, int W, cudaStream_t s,
+                 const DevOps *P) {
   const long long n = (long long)B * H * W;
   forward(net, in, B, H, W, s);
   const unsigned gb = stride_blocks(n, 16);
   double *part = net->red, *res = net->red + 4 * kRedBlocks;
-  k_loss<<<gb, 256, 0, s>>>(net->y, tgt, net->dy, (float)(2.0 / (double)n) * net->out_scale, n, part);
+  const float g = (float)(2.0 / (double)n) * net->out_scale;
+  if (P) {
+    k_res_loss<<<gb, 256, 0, s>>>(*P, net->y, in, net->dres, B, part);
+    k_res_grad<<<gb, 256, 0, s>>>(*P, net->dres, net->dy, g, B);
+  } else {
+    k_loss<<<gb, 256, 0, s>>>(net->y, tgt, net->dy, g, n, part);
+  }
   k_finish<1><<<1, 256, 0, s>>>(part, (int)gb, 0, res);
   // layer 6
   k_bwd_out<<<gb, 256, 0, s>>>(net->dy, net->w + kOffW6, net->act[4], net->dz[0], B, H, W);
@@ -1067,7 +1129,7 @@ int ins2d_cnn_create(int32_t device, uint64_t seed, ins2d_cnn **out) {
 int ins2d_cnn_destroy(ins2d_cnn *n) {
   if (!n) return INS2D_OK;
   cudaSetDevice(n->device);
-  for (float *p : {n->w, n->g, n->m, n->v, n->y, n->dy, n->in1, n->partials}) cudaFree(p);
+  for (float *p : {n->w, n->g, n->m, n->v, n->y, n->dy, n->dres, n->in1, n->partials}) cudaFree(p);
   cudaFree(n->wf);
   cudaFree(n->wb);
   cudaFree(n->red);
@@ -1168,7 +1230,7 @@ int ins2d_cnn_loss_grad(ins2d_cnn *n, const float *in, const float *tgt, int32_t
   if (!tgt) return cnn_fail(n, INS2D_EINVAL, "cnn_loss_grad: null targets");
   try {
     CK(cudaSetDevice(n->device));
-    const double l = cnn::loss_grad(n, in, tgt, B, H, W, n->stream);
+    const double l = cnn::loss_grad(n, in, tgt, B, H, W, n->stream, nullptr);
     if (loss) *loss = l;
     if (grad) {
       CK(cudaMemcpyAsync(grad, n->g, cnn::kNParam * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
@@ -1191,7 +1253,7 @@ int ins2d_cnn_train_step(ins2d_cnn *n, const float *in, const float *tgt, int32_
   if (!(lr > 0.0f) || !std::isfinite(lr)) return cnn_fail(n, INS2D_EINVAL, "cnn_train_step: lr must be > 0");
   try {
     CK(cudaSetDevice(n->device));
-    const double l = cnn::loss_grad(n, in, tgt, B, H, W, n->stream);
+    const double l = cnn::loss_grad(n, in, tgt, B, H, W, n->stream, nullptr);
     if (!std::isfinite(l)) return cnn_fail(n, INS2D_ENONFINITE, "cnn_train_step: non-finite loss");
     cnn::adam(n, lr, n->stream);
     if (loss) *loss = l;

@@ -48,6 +48,7 @@ struct ins2d_cnn {
   __nv_bfloat16 *act[5] = {};            // post-ReLU activations of layers 1..5, NHWC
   __nv_bfloat16 *dz[2] = {};             // pre-activation gradients (ping-pong)
   float *y = nullptr, *dy = nullptr;     // output and its gradient
+  float *dres = nullptr;                 // residual A y - diag(A) in of the residual loss
   float *in1 = nullptr;                  // single-field input of the solver's guess
   long long in1_cap = 0;
   float *partials = nullptr;             // weight-gradient partials
@@ -75,6 +76,13 @@ void prepare(const DevOps &P, const double *f, const double *p, int center, floa
              cudaStream_t s);
 // forward pass over B fields of H x W (in: fp32 [B][H][W]); output in net->y
 void forward(ins2d_cnn *net, const float *in, int B, int H, int W, cudaStream_t s);
+// loss (after a stream synchronisation) and gradient in net->g.  P = null:
+// mean((y - tgt)^2); P = a context's operators: the residual loss
+// mean((A y - diag(A) in)^2) on that grid (tgt unused), gradient 2 A (.) / n.
+double loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int B, int H, int W, cudaStream_t s,
+                 const DevOps *P);
+// one Adam step from net->g
+void adam(ins2d_cnn *net, float lr, cudaStream_t s);
 // the solver's initial guess: x0 = network(prepare(f)) as fp64
 void guess(ins2d_cnn *net, const DevOps &P, const double *f, double *x0, cudaStream_t s);
 // ensures the buffers hold `pixels` pixels (throws std::bad_alloc)

@@ -1105,6 +1105,40 @@ int ins2d_cnn_prepare_pairs(ins2d_ctx *ctx, const double *f, const double *p, in
   API_END
 }
 
+namespace {
+int cnn_residual_call(ins2d_ctx *ctx, ins2d_cnn *net, const float *in, int32_t B, float lr, double *loss,
+                      float *grad) {
+  if (!net || !in || B < 1) return fail(ctx, INS2D_EINVAL, "cnn residual loss: null network/input or B < 1");
+  if (net->device != ctx->device) return fail(ctx, INS2D_EINVAL, "cnn residual loss: network on another device");
+  if ((long long)B * ctx->P.Np > (1LL << 26)) return fail(ctx, INS2D_EINVAL, "cnn residual loss: B*Np > 2^26");
+  if (lr < 0.0f || !std::isfinite(lr)) return fail(ctx, INS2D_EINVAL, "cnn residual loss: lr must be >= 0");
+  const double l = cnn::loss_grad(net, in, nullptr, B, ctx->P.Npy, ctx->P.Npx, net->stream, &ctx->P);
+  if (!std::isfinite(l)) return fail(ctx, INS2D_ENONFINITE, "cnn residual loss: non-finite loss");
+  if (loss) *loss = l;
+  if (grad) {
+    CK(cudaMemcpyAsync(grad, net->g, cnn::kNParam * sizeof(float), cudaMemcpyDeviceToHost, net->stream));
+    CK(cudaStreamSynchronize(net->stream));
+  }
+  if (lr > 0.0f) cnn::adam(net, lr, net->stream);
+  return INS2D_OK;
+}
+}  // namespace
+
+int ins2d_cnn_loss_grad_residual(ins2d_ctx *ctx, ins2d_cnn *net, const float *in, int32_t B, double *loss,
+                                 float *grad) {
+  API_BEGIN
+  return cnn_residual_call(ctx, net, in, B, 0.0f, loss, grad);
+  API_END
+}
+
+int ins2d_cnn_train_step_residual(ins2d_ctx *ctx, ins2d_cnn *net, const float *in, int32_t B, float lr,
+                                  double *loss) {
+  API_BEGIN
+  if (!(lr > 0.0f)) return fail(ctx, INS2D_EINVAL, "cnn_train_step_residual: lr must be > 0");
+  return cnn_residual_call(ctx, net, in, B, lr, loss, nullptr);
+  API_END
+}
+
 int ins2d_set_learned_guess(ins2d_ctx *ctx, ins2d_cnn *net) {
   API_BEGIN
   if (net && net->device != ctx->device)

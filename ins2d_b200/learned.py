@@ -116,6 +116,27 @@ class ConvNet:
                                                   ctypes.byref(loss), g.ctypes.data))
         return loss.value, g
 
+    def loss_grad_residual(self, options, inp):
+        """Residual loss mean((A net(inp) - diag(A) inp)^2) on ``options``'
+        grid and its gradient (numpy float32); no update."""
+        import torch
+        _require_cuda(inp, torch.float32, "inp")
+        g = np.empty(NPARAM, dtype=np.float32)
+        loss = ctypes.c_double()
+        torch.cuda.synchronize(inp.device)
+        options._check(self._lib.ins2d_cnn_loss_grad_residual(options._ctx, self._h, inp.data_ptr(), inp.shape[0],
+                                                              ctypes.byref(loss), g.ctypes.data))
+        return loss.value, g
+
+    def train_step_residual(self, options, inp, lr):
+        """One Adam step on the residual loss; returns the loss before it."""
+        import torch
+        _require_cuda(inp, torch.float32, "inp")
+        loss = ctypes.c_double()
+        options._check(self._lib.ins2d_cnn_train_step_residual(options._ctx, self._h, inp.data_ptr(), inp.shape[0],
+                                                               float(lr), ctypes.byref(loss)))
+        return loss.value
+
     def train_step(self, inp, tgt, lr):
         """One Adam step on the mean squared error; returns the loss before it."""
         import torch
@@ -169,24 +190,36 @@ def prepare_pairs(options, f, p, n=None):
     return inp, tgt
 
 
-def train(net, inp, tgt, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None):
+def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None, options=None):
     """Adam on random mini-batches of the pairs (cosine-decayed learning
-    rate); sets out_scale to the targets' rms first.  Returns the losses."""
+    rate).  With ``options`` the loss is the residual loss on its grid
+    (``tgt`` unused; out_scale first matched to the inputs' rms), else the
+    squared error against ``tgt`` (out_scale first set to the targets' rms).
+    Returns the losses relative to the first one."""
     import torch
     n = inp.shape[0]
     w, _ = net.params()
-    scale = float(torch.sqrt(torch.mean(tgt.double() ** 2)).item()) or 1.0
-    net.set_params(w, scale)
     gen = torch.Generator(device="cpu").manual_seed(int(seed))
+    if options is None:
+        scale = float(torch.sqrt(torch.mean(tgt.double() ** 2)).item()) or 1.0
+    else:
+        net.set_params(w, 1.0)
+        x0 = inp[: min(batch, n)].contiguous()
+        y0 = net.forward(x0)
+        scale = float(torch.sqrt(torch.mean(x0.double() ** 2) / torch.mean(y0.double() ** 2).clamp_min(1e-30)))
+    net.set_params(w, scale)
     lr_final = lr * 0.05 if lr_final is None else lr_final
     losses = []
     for k in range(int(steps)):
         idx = torch.randint(0, n, (min(batch, n),), generator=gen).to(inp.device)
         xb = inp.index_select(0, idx).contiguous()
-        yb = tgt.index_select(0, idx).contiguous()
         rate = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(steps - 1, 1)))
-        losses.append(net.train_step(xb, yb, rate) / scale ** 2)
-    return losses
+        if options is None:
+            yb = tgt.index_select(0, idx).contiguous()
+            losses.append(net.train_step(xb, yb, rate))
+        else:
+            losses.append(net.train_step_residual(options, xb, rate))
+    return [l / losses[0] for l in losses] if losses and losses[0] > 0 else losses
 
 
 def attach(options, net, mode="guess"):

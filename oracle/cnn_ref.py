@@ -110,9 +110,11 @@ def layer(w, l, a_prev, bf16_mode=True):
     return rnd(np.maximum(Z, 0.0))
 
 
-def loss_grad(w, out_scale, inp, tgt, bf16_mode=True, acts=None):
+def loss_grad(w, out_scale, inp, tgt, bf16_mode=True, acts=None, A=None):
     """(loss, flat gradient) of mean((y - tgt)^2).  ``acts`` = [A1..A5] uses
-    given forward activations (the device's) instead of recomputing them."""
+    given forward activations (the device's) instead of recomputing them.
+    With a sparse pressure operator ``A`` (Np x Np, x fastest) the loss is the
+    residual loss mean((A y - diag(A) inp)^2) per field instead (tgt unused)."""
     rnd = bf16 if bf16_mode else (lambda a: np.asarray(a, dtype=np.float64))
     W1, Wm, W6 = split(w)
     if acts is None:
@@ -121,9 +123,19 @@ def loss_grad(w, out_scale, inp, tgt, bf16_mode=True, acts=None):
         acts = [np.asarray(inp, dtype=np.float64)] + [np.asarray(a, dtype=np.float64) for a in acts]
         y = out_scale * layer(w, 6, acts[5], bf16_mode)
     n = y.size
-    d = y - np.asarray(tgt, dtype=np.float64)
-    loss = float(np.sum(d * d) / n)
-    dy6 = 2.0 * d / n * out_scale
+    if A is None:
+        d = y - np.asarray(tgt, dtype=np.float64)
+        loss = float(np.sum(d * d) / n)
+        dy6 = 2.0 * d / n * out_scale
+    else:
+        dg = A.diagonal()
+        x0 = np.asarray(inp, dtype=np.float64)
+        loss, dy6 = 0.0, np.zeros_like(y)
+        for b in range(y.shape[0]):
+            r = A @ y[b].ravel() - dg * x0[b].ravel()
+            loss += float(r @ r)
+            dy6[b] = (2.0 / n * out_scale) * (A @ r).reshape(y.shape[1:])
+        loss /= n
     taps = _taps()
     A5 = acts[5]
     gW6 = np.zeros_like(W6)

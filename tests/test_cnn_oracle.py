@@ -73,3 +73,32 @@ def test_positive_homogeneity():
     y1, _ = N.forward(w, 1.0, inp, bf16_mode=False)
     y2, _ = N.forward(w, 1.0, 3.0 * inp, bf16_mode=False)
     assert np.allclose(y2, 3.0 * y1, rtol=1e-12, atol=1e-12)
+
+
+def test_residual_loss_gradient_matches_finite_differences():
+    # the residual loss on a small stretched cavity's pressure operator
+    from oracle import ins2d_ref as R
+    from ins2d_b200 import cases
+    x = cases.tanh_grid(7, 0.0, 1.0, 1.05)
+    y = cases.tanh_grid(6, 0.0, 1.0, 1.05)
+    o = R.make_options(x, y, cases.BC_CAVITY, Re=100.0, poisson=4)
+    A = o.discretization.A
+    H, W = 6, 7
+    assert A.shape == (H * W, H * W)
+    w, inp, _ = _case(5, B=2, H=H, W=W)
+    scale = 0.9
+    loss, g = N.loss_grad(w, scale, inp, None, bf16_mode=False, A=A)
+    assert loss > 0
+    rng = np.random.default_rng(7)
+    idx = np.concatenate([rng.choice(N.OFF_WM, 4, replace=False),
+                          N.OFF_WM + rng.choice(N.OFF_W6 - N.OFF_WM, 8, replace=False),
+                          N.OFF_W6 + rng.choice(N.K, 4, replace=False)])
+    eps = 1e-6
+    gmax = np.max(np.abs(g))
+    for k in idx:
+        wp, wm = w.copy(), w.copy()
+        wp[k] += eps
+        wm[k] -= eps
+        fd = (N.loss_grad(wp, scale, inp, None, bf16_mode=False, A=A)[0] -
+              N.loss_grad(wm, scale, inp, None, bf16_mode=False, A=A)[0]) / (2 * eps)
+        assert abs(fd - g[k]) <= 1e-6 * gmax + 1e-5 * abs(g[k]), (k, fd, g[k])

@@ -91,6 +91,29 @@ def test_loss_gradient_matches_oracle(shape, path):
     assert _rel(g[N.OFF_W6:], g_ref[N.OFF_W6:]) < 1e-5
 
 
+@pytest.mark.parametrize("path", ["tcgen05", "mma_sync"])
+def test_residual_loss_gradient_matches_oracle(path):
+    """The residual loss on a context's grid (FP32 stencil of the context's
+    own operator tables) against the oracle with the oracle's sparse A."""
+    import ins2d_b200
+    from ins2d_b200 import cases
+    from oracle import ins2d_ref as R
+    x = cases.tanh_grid(29, 0.0, 1.0, 1.05)
+    y = cases.tanh_grid(21, 0.0, 1.0, 1.05)
+    m = ins2d_b200.Options(x, y, cases.BC_CAVITY, Re=100.0, poisson=4, device=0)
+    A = R.make_options(x, y, cases.BC_CAVITY, Re=100.0, poisson=4).discretization.A
+    net, w, scale = _net(seed=13, scale=0.7, path=path)
+    inp, _, ti, _ = _inputs(3, 2, m.Npy, m.Npx)
+    loss, g = net.loss_grad_residual(m, ti)
+    acts = [net.activations(l, ti.numel()).reshape(2, m.Npy, m.Npx, 32) for l in range(1, 6)]
+    loss_ref, g_ref = N.loss_grad(w, scale, inp, None, bf16_mode=True, acts=acts, A=A)
+    assert abs(loss - loss_ref) / loss_ref < 1e-4, (loss, loss_ref)
+    bounds = [0, N.OFF_WM] + [N.OFF_WM + (l + 1) * N.SZ_WM for l in range(N.NMID)] + [N.NPARAM]
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        assert _rel(g[a:b], g_ref[a:b]) < 1e-2, (a, b, _rel(g[a:b], g_ref[a:b]))
+    assert _rel(g[N.OFF_W6:], g_ref[N.OFF_W6:]) < 1e-4
+
+
 def test_tensor_core_paths_agree_on_large_field():
     """Both instruction paths on a field larger than the persistent grid
     (several tiles per block) give the same network output."""
@@ -138,8 +161,10 @@ def _record(m, steps, capacity):
 def test_training_gains_over_plain_pcg():
     """Pairs from the solver's own first steps (a stretched lid-driven cavity);
     the network trained on the first 80% and judged on the held-out rest: the
-    same tolerance is reached in fewer Jacobi-PCG iterations from the learned
-    guess, and the solutions agree within the tolerance."""
+    same tolerance is reached in fewer iterations than the Jacobi-PCG without
+    it -- from the learned guess, and (much fewer) with the network as the
+    preconditioner of a flexible CG -- and the solutions agree within the
+    tolerance."""
     from ins2d_b200 import learned
     torch = _torch()
     m = _cavity()
@@ -148,7 +173,7 @@ def test_training_gains_over_plain_pcg():
     ntr = int(0.8 * n)
     inp, tgt = learned.prepare_pairs(m, f_buf[:ntr], p_buf[:ntr])
     net = learned.ConvNet(device=0, seed=11)
-    losses = learned.train(net, inp, tgt, steps=400, batch=8, lr=3e-3, seed=1)
+    losses = learned.train(net, inp, None, steps=400, batch=8, lr=3e-3, seed=1, options=m)
     assert np.mean(losses[-20:]) < 0.5 * np.mean(losses[:5]), (losses[:5], losses[-20:])
     it_plain, it_learned, it_fcg, res = [], [], [], []
     for k in range(ntr, n):
@@ -181,7 +206,7 @@ def test_learned_guess_with_multigrid_and_time_steps():
     f_buf, p_buf, n = _record(m, 6, 40)
     inp, tgt = learned.prepare_pairs(m, f_buf[:n], p_buf[:n])
     net = learned.ConvNet(device=0, seed=3)
-    learned.train(net, inp, tgt, steps=60, batch=4, lr=3e-3)
+    learned.train(net, inp, None, steps=60, batch=4, lr=3e-3, options=m)
     V = np.zeros(m.NV)
     p = m.pressure_additional_solve(V, np.zeros(m.Np), 0.0)
     V0, p0 = m.time_ERK(V, p, 0.0, 2e-3, nsteps=5)
