@@ -63,8 +63,8 @@ WORKLOADS = {
                   desc="lid-driven cavity 64x64, Re=1000, RK44 dt=1e-3, PCG to 1e-12, FP64"),
     "bfs1024": dict(N=1024, ic="bfs", Re=800.0, poisson=4, precision="fp64", dt=1e-3, CG_acc=1e-10,
                     desc="backward-facing step 1024x1024, x in [0,30], y in [-0.5,0.5], tanh-stretched 1.02, "
-                         "inflow u=24y(0.5-y) for y>=0, outflow p=0, Re=800, RK44 dt=1e-3, multigrid PCG to "
-                         "1e-10, FP64"),
+                         "inflow u=24y(0.5-y) for y>=0, outflow p=0, Re=800, RK44 with dt = min(1e-3, 0.7 x the "
+                         "explicit stability limit on the smallest cells), multigrid PCG to 1e-10, FP64"),
     "bfs1024_learned": dict(N=1024, ic="bfs", Re=800.0, poisson=4, precision="fp64", dt=1e-3, CG_acc=1e-10,
                             learned=dict(record_steps=24, pairs=120, train_steps=300, batch=4, lr=2e-3, seed=0),
                             desc="backward-facing step 1024x1024 (as bfs1024) with the learned initial guess: "
@@ -163,6 +163,18 @@ def bfs_profile(y):
     return np.where(y >= 0.0, 24.0 * y * (0.5 - y), 0.0)
 
 
+def bfs_dt(x, y, Re, dt_max, umax=1.5, safety=0.7):
+    """The configuration's dt = 1e-3 is beyond explicit RK4's stability limit
+    on a 1024-cell unit height (diffusion: |lambda dt| = 4 dt (1/hx^2 + 1/hy^2)
+    / Re must stay below 2.78, convection: umax dt (1/hx + 1/hy) below 2.83),
+    so the step is the smaller of dt_max and 0.7 times those limits on the
+    smallest cells."""
+    hx, hy = float(np.min(np.diff(x))), float(np.min(np.diff(y)))
+    lim_d = 2.78 / (4.0 / Re * (1.0 / hx ** 2 + 1.0 / hy ** 2))
+    lim_c = 2.83 / (umax * (1.0 / hx + 1.0 / hy))
+    return min(dt_max, safety * min(lim_d, lim_c))
+
+
 def setup_case(wl, device=0):
     import ins2d_b200
     from ins2d_b200 import cases
@@ -176,7 +188,7 @@ def setup_case(wl, device=0):
                                   precond=wl.get("precond", "default"))
         V = np.r_[bfs_profile(opts.yu), np.zeros(opts.Nv)]
         V = opts.initial_projection(V, 0.0)
-        return opts, V, wl["dt"]
+        return opts, V, bfs_dt(x, y, wl["Re"], wl["dt"])
     N, L = wl["N"], wl["L"]
     x = cases.uniform_grid(N, 0.0, L)
     if wl["ic"] == "rest":
@@ -675,7 +687,7 @@ def bfs_cpu_baseline(wl, budget_s=25.0, steps=None, n_sample=128):
     g = o.grid
     V = R.initial_projection(np.r_[bfs_profile(g.yu), np.zeros(g.Nv)], 0.0, o)
     p = np.zeros(g.Np)
-    dt = wl["dt"]
+    dt = bfs_dt(x, y, wl["Re"], wl["dt"])
     n = 0
     t0 = time.perf_counter()
     while True:

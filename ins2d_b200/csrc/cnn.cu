@@ -215,12 +215,12 @@ constexpr int kTcTW = 8, kTcTH = 16;           // tile: 8 pixels wide, 16 rows
 constexpr int kTcHW = kTcTW + 2, kTcHH = kTcTH + 2;
 constexpr int kTcSbo = kTcHW * 16;             // 160: next tile row
 constexpr int kTcLbo = kTcHH * kTcSbo;         // 2880: next 8 channels (plane)
-constexpr int kABytes = (kC / 8) * kTcLbo;     // 11520
+constexpr int kABytes = (kC / 8) * kTcLbo;     // 11520 per halo buffer (two: double-buffered)
 constexpr int kBLbo = (kC / 8) * 128;          // 512: next 8 K-elements of B
 constexpr int kBBytes = (kK / 8) * kBLbo;      // 18432
 // Dynamic shared memory: A (halo planes), B, the mbarrier and the TMEM slot
-constexpr int kTcSmem = kABytes + kBBytes + 16;
-constexpr int kTcBlocksPerSm = 6;
+constexpr int kTcSmem = 2 * kABytes + kBBytes + 16;
+constexpr int kTcBlocksPerSm = 5;
 // kind::f16 instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B
 // BF16 (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at
 // bits 24-28.
@@ -243,6 +243,10 @@ __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, ui
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
       "l"(a), "l"(b), "r"(idesc), "r"(acc)
       : "memory");
+}
+// 16-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
   uint32_t done;
@@ -269,10 +273,10 @@ __global__ void __launch_bounds__(256, kTcBlocksPerSm) k_conv_mid_tc(const bf16 
                                                         int H, int W, int tiles_x, int tiles_y,
                                                         unsigned *__restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t *sA = smem;
-  uint8_t *sB = smem + kABytes;
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kABytes + kBBytes);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + kABytes + kBBytes + 8);
+  uint8_t *sA = smem;  // two halo buffers of kABytes
+  uint8_t *sB = smem + 2 * kABytes;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + 2 * kABytes + kBBytes);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + 2 * kABytes + kBBytes + 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // B: element (n = co, k) at (k / 8) * kBLbo + co * 16 + (k % 8) * 2
   for (int i = tid; i < kC * (kK / 8); i += 256) {
@@ -299,20 +303,34 @@ __global__ void __launch_bounds__(256, kTcBlocksPerSm) k_conv_mid_tc(const bf16 
   uint32_t phase = 0;
   const long long per_field = (long long)tiles_x * tiles_y;
   const long long ntiles = per_field * B;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  // halo planes of a tile into buffer buf: channels 8 c8 .. 8 c8 + 7 of halo
+  // pixel hp at c8 * kTcLbo + hp * 16 (zeros outside the field)
+  auto load_halo = [&](long long tl, int buf) {
+    const int bb = (int)(tl / per_field);
+    const int rm = (int)(tl % per_field);
+    const int hx0 = (rm % tiles_x) * kTcTW - 1, hy0 = (rm / tiles_x) * kTcTH - 1;
+    const long long fb = (long long)bb * H * W;
+    for (int i = tid; i < kTcHW * kTcHH * 4; i += 256) {
+      const int hp = i >> 2, c8 = i & 3;
+      const int gx = hx0 + hp % kTcHW, gy = hy0 + hp / kTcHW;
+      const bool inside = gx >= 0 && gx < W && gy >= 0 && gy < H;
+      const bf16 *src = inside ? &in[(fb + (long long)gy * W + gx) * kC + c8 * 8] : in;
+      cp_async16(aBase + buf * kABytes + c8 * kTcLbo + hp * 16, src, inside ? 16u : 0u);
+    }
+  };
+  if ((long long)blockIdx.x < ntiles) load_halo(blockIdx.x, 0);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  int it = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int buf = it & 1;
+    // the next tile's halo loads overlap this tile's MMAs and epilogue
+    if (tile + gridDim.x < ntiles) load_halo(tile + gridDim.x, buf ^ 1);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     const int b = (int)(tile / per_field);
     const int rem = (int)(tile % per_field);
     const int x0 = (rem % tiles_x) * kTcTW, y0 = (rem / tiles_x) * kTcTH;
     const long long fbase = (long long)b * H * W;
-    // halo planes: channels 8 c8 .. 8 c8 + 7 of halo pixel hp at c8 * kTcLbo + hp * 16
-    for (int i = tid; i < kTcHW * kTcHH * 4; i += 256) {
-      const int hp = i >> 2, c8 = i & 3;
-      const int gx = x0 - 1 + hp % kTcHW, gy = y0 - 1 + hp / kTcHW;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (gx >= 0 && gx < W && gy >= 0 && gy < H)
-        v = *reinterpret_cast<const uint4 *>(&in[(fbase + (long long)gy * W + gx) * kC + c8 * 8]);
-      *reinterpret_cast<uint4 *>(sA + c8 * kTcLbo + hp * 16) = v;
-    }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (tid == 0) {
@@ -320,7 +338,7 @@ __global__ void __launch_bounds__(256, kTcBlocksPerSm) k_conv_mid_tc(const bf16 
 #pragma unroll
       for (int ks = 0; ks < kK / 16; ++ks) {
         const int t = ks >> 1, h = ks & 1;
-        const uint32_t a0 = aBase + 2 * h * kTcLbo + ((t / 3) * kTcHW + t % 3) * 16;
+        const uint32_t a0 = aBase + buf * kABytes + 2 * h * kTcLbo + ((t / 3) * kTcHW + t % 3) * 16;
         tc_mma(taddr, smem_desc(a0, kTcLbo, kTcSbo), smem_desc(bBase + 2 * ks * kBLbo, kBLbo, 128), kIdesc,
                ks > 0 ? 1u : 0u);
       }
@@ -368,6 +386,7 @@ __global__ void __launch_bounds__(256, kTcBlocksPerSm) k_conv_mid_tc(const bf16 
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0)
@@ -721,9 +740,10 @@ __global__ void __launch_bounds__(256) k_prep_write(const __grid_constant__ DevO
   }
 }
 
-__global__ void k_widen(const float *__restrict__ y, double *__restrict__ x, long long n) {
+// second field of a pair = -first (the odd part of the network needs both)
+__global__ void k_negate(float *__restrict__ a, long long n) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-    x[k] = (double)y[k];
+    a[n + k] = -a[k];
 }
 
 __global__ void __launch_bounds__(256) k_dots(long long n, const double *__restrict__ x, const double *__restrict__ f,
@@ -772,11 +792,15 @@ void launch_mid(ins2d_cnn *net, const bf16 *in, const bf16 *wt, const bf16 *mask
 // z = rms * y: the network output rescaled by the rms of its unscaled input
 // (stats[0] = sum of squares over n_stat cells), so z = M(r) is homogeneous
 // of degree one in r
-__global__ void k_widen_scaled(const float *__restrict__ y, double *__restrict__ x, long long n,
-                               const double *__restrict__ stats, double n_stat) {
-  const double s = sqrt(stats[0] / n_stat);
+// x = s (y[k] - y[n + k]) / 2: the odd part of the network over the pair
+// (r, -r), rescaled by s = rms of the unscaled input (stats[0] = its sum of
+// squares over n_stat cells) when stats is given, so that the result is odd
+// and homogeneous of degree one in r
+__global__ void k_widen_odd(const float *__restrict__ y, double *__restrict__ x, long long n,
+                            const double *__restrict__ stats, double n_stat) {
+  const double s = stats ? sqrt(stats[0] / n_stat) : 1.0;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-    x[k] = s * (double)y[k];
+    x[k] = 0.5 * s * ((double)y[k] - (double)y[n + k]);
 }
 
 // flexible CG vector steps (each with its block partials)
@@ -942,34 +966,33 @@ void prepare(const DevOps &P, const double *f, const double *p, int center, floa
   CK(cudaGetLastError());
 }
 
-void guess(ins2d_cnn *net, const DevOps &P, const double *f, double *x0, cudaStream_t s) {
-  reserve(net, P.Np);
-  if (net->in1_cap < P.Np) {
+namespace {
+// the network's odd part applied to the prepared field v (f or r):
+// out = scaled (N(v) - N(-v)) / 2, one forward pass over the pair
+void apply_odd(ins2d_cnn *net, const DevOps &P, const double *v, double *out, bool rescale, cudaStream_t s) {
+  reserve(net, 2 * P.Np);
+  if (net->in1_cap < 2 * P.Np) {
     cudaFree(net->in1);
     net->in1 = nullptr;
     net->in1_cap = 0;
-    if (cudaMalloc(&net->in1, P.Np * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
-    net->in1_cap = P.Np;
+    if (cudaMalloc(&net->in1, 2 * P.Np * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
+    net->in1_cap = 2 * P.Np;
   }
-  prepare(P, f, nullptr, 0, net->in1, nullptr, net->red, s);
-  forward(net, net->in1, 1, P.Npy, P.Npx, s);
-  k_widen<<<stride_blocks(P.Np), 256, 0, s>>>(net->y, x0, P.Np);
+  prepare(P, v, nullptr, 0, net->in1, nullptr, net->red, s);
+  k_negate<<<stride_blocks(P.Np), 256, 0, s>>>(net->in1, P.Np);
+  forward(net, net->in1, 2, P.Npy, P.Npx, s);
+  k_widen_odd<<<stride_blocks(P.Np), 256, 0, s>>>(net->y, out, P.Np, rescale ? net->red + 4 * kRedBlocks : nullptr,
+                                                   (double)P.Np);
   CK(cudaGetLastError());
+}
+}  // namespace
+
+void guess(ins2d_cnn *net, const DevOps &P, const double *f, double *x0, cudaStream_t s) {
+  apply_odd(net, P, f, x0, false, s);
 }
 
 void precond(ins2d_cnn *net, const DevOps &P, const double *r, double *z, cudaStream_t s) {
-  reserve(net, P.Np);
-  if (net->in1_cap < P.Np) {
-    cudaFree(net->in1);
-    net->in1 = nullptr;
-    net->in1_cap = 0;
-    if (cudaMalloc(&net->in1, P.Np * sizeof(float)) != cudaSuccess) throw std::bad_alloc();
-    net->in1_cap = P.Np;
-  }
-  prepare(P, r, nullptr, 0, net->in1, nullptr, net->red, s);
-  forward(net, net->in1, 1, P.Npy, P.Npx, s);
-  k_widen_scaled<<<stride_blocks(P.Np), 256, 0, s>>>(net->y, z, P.Np, net->red + 4 * kRedBlocks, (double)P.Np);
-  CK(cudaGetLastError());
+  apply_odd(net, P, r, z, true, s);
 }
 
 namespace {

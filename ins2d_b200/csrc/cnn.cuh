@@ -83,7 +83,9 @@ double loss_grad(ins2d_cnn *net, const float *in, const float *tgt, int B, int H
                  const DevOps *P);
 // one Adam step from net->g
 void adam(ins2d_cnn *net, float lr, cudaStream_t s);
-// the solver's initial guess: x0 = network(prepare(f)) as fp64
+// the solver's initial guess: x0 = (N(v) - N(-v)) / 2 with v = prepare(f),
+// the odd part of the network N (A^-1 is linear, so the odd part of an
+// approximation of it is never a worse approximation), as fp64
 void guess(ins2d_cnn *net, const DevOps &P, const double *f, double *x0, cudaStream_t s);
 // ensures the buffers hold `pixels` pixels (throws std::bad_alloc)
 void reserve(ins2d_cnn *net, long long pixels);
@@ -93,8 +95,8 @@ void check(ins2d_cnn *net, cudaStream_t s);
 // the host; synchronises the stream):
 //   d[0] = x.f, d[1] = x.q, d[2] = f.f, d[3] = max|f|
 void dots(long long n, const double *x, const double *f, const double *q, double *red, double d[4], cudaStream_t s);
-// z = M(r): the network applied to r (prepared like f), rescaled by the rms of
-// r / diag A so that M(c r) = c M(r) for c > 0
+// z = M(r): the odd part of the network applied to r (prepared like f),
+// rescaled by the rms of r / diag A so that M(c r) = c M(r) for every real c
 void precond(ins2d_cnn *net, const DevOps &P, const double *r, double *z, cudaStream_t s);
 // flexible CG steps (each synchronises and returns its reductions):
 //   d = {p.q, p.r};  x += a p, r -= a q, d = {r.r, max|r|};  z.q;  p = z + b p

@@ -1152,7 +1152,7 @@ int ins2d_set_learned_guess(ins2d_ctx *ctx, ins2d_cnn *net) {
     ctx->lg_z = dalloc<double>(ctx, Np);
     if (!ctx->lg_red) ctx->lg_red = dalloc<double>(ctx, cnn::red_doubles());
   }
-  if (net) cnn::reserve(net, ctx->P.Np);
+  if (net) cnn::reserve(net, 2 * ctx->P.Np);
   ctx->cnn = net;
   return INS2D_OK;
   API_END

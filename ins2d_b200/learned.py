@@ -193,7 +193,9 @@ def prepare_pairs(options, f, p, n=None):
 def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None, options=None):
     """Adam on random mini-batches of the pairs (cosine-decayed learning
     rate).  With ``options`` the loss is the residual loss on its grid
-    (``tgt`` unused; out_scale first matched to the inputs' rms), else the
+    (``tgt`` unused; out_scale first matched to the inputs' rms; every batch
+    holds each input and its negation, since the solver applies the network's
+    odd part), else the
     squared error against ``tgt`` (out_scale first set to the targets' rms).
     Returns the losses relative to the first one."""
     import torch
@@ -212,7 +214,10 @@ def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None
     losses = []
     for k in range(int(steps)):
         idx = torch.randint(0, n, (min(batch, n),), generator=gen).to(inp.device)
-        xb = inp.index_select(0, idx).contiguous()
+        xb = inp.index_select(0, idx)
+        if options is not None:
+            xb = torch.cat([xb, -xb])  # the solver uses the odd part (N(v) - N(-v)) / 2
+        xb = xb.contiguous()
         rate = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(steps - 1, 1)))
         if options is None:
             yb = tgt.index_select(0, idx).contiguous()
