@@ -190,12 +190,14 @@ def prepare_pairs(options, f, p, n=None):
     return inp, tgt
 
 
-def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None, options=None):
+def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None, options=None, noise=0):
     """Adam on random mini-batches of the pairs (cosine-decayed learning
     rate).  With ``options`` the loss is the residual loss on its grid
     (``tgt`` unused; out_scale first matched to the inputs' rms; every batch
     holds each input and its negation, since the solver applies the network's
-    odd part), else the
+    odd part; ``noise`` white-noise fields are added to every batch -- the
+    residual loss needs no targets, and the residuals a preconditioner sees
+    inside CG are rougher than the right-hand sides), else the
     squared error against ``tgt`` (out_scale first set to the targets' rms).
     Returns the losses relative to the first one."""
     import torch
@@ -216,6 +218,9 @@ def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None
         idx = torch.randint(0, n, (min(batch, n),), generator=gen).to(inp.device)
         xb = inp.index_select(0, idx)
         if options is not None:
+            if noise:
+                z = torch.randn((int(noise),) + tuple(inp.shape[1:]), generator=gen).to(inp.device)
+                xb = torch.cat([xb, z])
             xb = torch.cat([xb, -xb])  # the solver uses the odd part (N(v) - N(-v)) / 2
         xb = xb.contiguous()
         rate = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(steps - 1, 1)))
