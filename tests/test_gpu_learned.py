@@ -162,8 +162,9 @@ def test_training_gains_over_plain_pcg():
     """Pairs from the solver's own first steps (a stretched lid-driven cavity);
     the network trained on the first 80% and judged on the held-out rest: the
     same tolerance is reached in fewer iterations than the Jacobi-PCG without
-    it from the learned guess; the flexible CG with the network as the
-    preconditioner reaches it too; the solutions agree within the tolerance."""
+    it from the learned guess, and in far fewer by the flexible CG with the
+    network (trained with white-noise fields as well) as its preconditioner;
+    the solutions agree within the tolerance."""
     from ins2d_b200 import learned
     torch = _torch()
     m = _cavity()
@@ -201,7 +202,10 @@ def test_training_gains_over_plain_pcg():
     # the learned guess saves iterations on the held-out solves; the flexible
     # CG reaches the same tolerance with the network as its preconditioner
     assert np.mean(it_learned) < np.mean(it_plain)
-    assert max(it_fcg) < 2000 and max(it_fcg_n) < 2000
+    assert max(it_fcg) < 2000
+    # trained with noise fields, the network is a better preconditioner than
+    # the Jacobi diagonal (measured on a B200: 153.6 against 224.3 iterations)
+    assert np.mean(it_fcg_n) < 0.85 * np.mean(it_plain)
 
 
 def test_learned_guess_with_multigrid_and_time_steps():
