@@ -286,10 +286,13 @@ int ins2d_ens_solve_shape(const ins2d_ens *e, int32_t *threads, int32_t *blocks,
  * convolutional network (six 3x3 convolutions, 1 -> 32 -> 32 -> 32 -> 32 -> 32
  * -> 1 channels, ReLU between, no biases, zero padding; BF16 tensor-core
  * layers accumulating in FP32) maps the Jacobi-scaled right-hand side to an
- * approximation of the solution.  The PCG starts from that guess (scaled by
- * the Rayleigh-Ritz factor (x0'f)/(x0'A x0)) and still stops on the
- * reference's rule ||r|| <= CG_acc ||f||, so a solution changes only within
- * the tolerance.  Parameters (INS2D_CNN_NPARAM floats): W1 [32][9],
+ * approximation of the solution.  The solver uses the network's odd part
+ * (N(v) - N(-v))/2 (one forward pass over the pair v, -v), since A^-1 is
+ * linear.  The PCG starts from that guess (scaled by the Rayleigh-Ritz factor
+ * (x0'f)/(x0'A x0)) and still stops on the reference's rule
+ * ||r|| <= CG_acc ||f||, so a solution changes only within the tolerance.
+ * One network serves one context at a time (its activation buffers are
+ * shared).  Parameters (INS2D_CNN_NPARAM floats): W1 [32][9],
  * W2..W5 [32][9][32] ([out][tap][in]), W6 [9][32]; tap t = (dy+1)*3 + (dx+1).
  * Inputs, targets and outputs of the network are fp32 device arrays of B
  * fields of H x W (x fastest). */
