@@ -114,6 +114,29 @@ def test_residual_loss_gradient_matches_oracle(path):
     assert _rel(g[N.OFF_W6:], g_ref[N.OFF_W6:]) < 1e-4
 
 
+@pytest.mark.parametrize("path", ["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 2, 5), (1, 9, 1), (2, 1, 33)])
+def test_degenerate_field_shapes(shape, path):
+    """Fields thinner than a tile and than the 3x3 stencil: every tap falls on
+    the zero padding somewhere."""
+    net, w, scale = _net(seed=4, scale=1.1, path=path)
+    inp, _, ti, _ = _inputs(5, *shape)
+    y = net.forward(ti).cpu().numpy()
+    _check_layers(net, w, scale, inp, y)
+
+
+def test_params_round_trip_and_reuse_after_larger_batch():
+    torch = _torch()
+    net, w, _ = _net(seed=6, scale=0.5)
+    w2, sc = net.params()
+    assert np.array_equal(w2, w.astype(np.float32)) and sc == 0.5
+    big = torch.randn(3, 64, 80, dtype=torch.float32, device="cuda")
+    small = big[1:2, :17, :23].contiguous()
+    y_small = net.forward(small)
+    net.forward(big)  # grows the buffers
+    assert torch.equal(net.forward(small), y_small)
+
+
 def test_tensor_core_paths_agree_on_large_field():
     """Both instruction paths on a field larger than the persistent grid
     (several tiles per block) give the same network output."""
