@@ -30,7 +30,11 @@ __global__ void k_factor_y(MgLevelD L) {
 
 constexpr int kLineThreads = 128;
 constexpr int kTailThreads = 512;
-constexpr long long kTailMaxCells = 16384;
+// levels with at most this many cells run in the single-block tail
+#ifndef INS2D_MG_TAIL_CELLS
+#define INS2D_MG_TAIL_CELLS 4096
+#endif
+constexpr long long kTailMaxCells = INS2D_MG_TAIL_CELLS;
 
 __device__ __forceinline__ bool is_done(const int *done) { return done && *(volatile const int *)done; }
 
