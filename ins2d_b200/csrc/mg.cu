@@ -62,6 +62,12 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
   mg_vcycle_block(M, b0, l0, ysh);
 }
 
+// unrolling of the segment walks in the multi-block y-line kernel (the
+// in-block solvers keep kMgUnroll)
+#ifndef INS2D_MG_YCOLS_UNROLL
+#define INS2D_MG_YCOLS_UNROLL 8
+#endif
+constexpr int kYcolsUnroll = INS2D_MG_YCOLS_UNROLL;
 // y-lines of 32 columns per block (kColThreads threads: one segment of rows per warp)
 constexpr int kColThreads = 1024;
 __global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, const double *__restrict__ b,
@@ -69,12 +75,16 @@ __global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, cons
                                                           double omega, const int *done) {
   __shared__ double ysh[2 * kColThreads];
   if (is_done(done)) return;
-  mg_ycols_block(L, b, xold, xnew, omega, blockIdx.x * 32, ysh);
+  mg_ycols_block<kYcolsUnroll>(L, b, xold, xnew, omega, blockIdx.x * 32, ysh);
 }
 
-// warps per column block: one segment of about 16 rows each, at most 32
+// warps per column block: one segment of about INS2D_MG_YSEG rows each, at
+// most 32
+#ifndef INS2D_MG_YSEG
+#define INS2D_MG_YSEG 8
+#endif
 int col_threads(int ny) {
-  int w = ny / 16;
+  int w = ny / INS2D_MG_YSEG;
   if (w < 1) w = 1;
   if (w > kColThreads / 32) w = kColThreads / 32;
   return 32 * w;

@@ -321,6 +321,7 @@ constexpr int kMgUnroll = INS2D_MG_UNROLL;  // unrolling of the column segment w
 // (sh: 2 x warps x 32 doubles), then each thread re-walks its segment.  The
 // dependent chain per thread is about 4 n / warps + 2 warps steps.  All
 // threads of the block must call it.
+template <int U = kMgUnroll>
 __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restrict__ b,
                                       const double *__restrict__ xold, double *__restrict__ xnew, double omega,
                                       int i0, double *sh) {
@@ -351,7 +352,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   // forward pass 1: composite of the segment, d_{j1-1} = A d_{j0-1} + B
   double A = 1.0, B = 0.0;
   if (col)
-#pragma unroll kMgUnroll
+#pragma unroll U
     for (int j = j0; j < j1; ++j) {
       double al, be;
       fwd(j, al, be);
@@ -374,7 +375,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   double d = sA[w * 32 + lane];
   __syncthreads();
   if (col)
-#pragma unroll kMgUnroll
+#pragma unroll U
     for (int j = j0; j < j1; ++j) {
       double al, be;
       fwd(j, al, be);
@@ -385,7 +386,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   A = 1.0;
   B = 0.0;
   if (col)
-#pragma unroll kMgUnroll
+#pragma unroll U
     for (int j = j1 - 1; j >= j0; --j) {
       const long long k = (long long)j * nx + i;
       const double ga = -L.fyc[k];
@@ -407,7 +408,7 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
   double x = sA[w * 32 + lane];
   __syncthreads();
   if (col)
-#pragma unroll kMgUnroll
+#pragma unroll U
     for (int j = j1 - 1; j >= j0; --j) {
       const long long k = (long long)j * nx + i;
       x = -L.fyc[k] * x + xnew[k];
