@@ -38,11 +38,17 @@ constexpr long long kTailMaxCells = INS2D_MG_TAIL_CELLS;
 
 __device__ __forceinline__ bool is_done(const int *done) { return done && *(volatile const int *)done; }
 
+// unrolling of the chunk loops of the multi-block x-line kernel (the
+// in-block solvers keep 2)
+#ifndef INS2D_MG_XUNROLL
+#define INS2D_MG_XUNROLL 2
+#endif
+constexpr int kXlineUnroll = INS2D_MG_XUNROLL;
 __global__ void __launch_bounds__(kLineThreads) k_mg_xline(const MgLevelD L, const double *__restrict__ b,
                                                            const double *__restrict__ xold, double *__restrict__ xnew,
                                                            double omega, const int *done) {
   if (is_done(done)) return;
-  mg_xline(L, b, xold, xnew, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  mg_xline<kXlineUnroll>(L, b, xold, xnew, omega, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 __global__ void __launch_bounds__(256) k_mg_restrict(const MgLevelD F, const MgLevelD C, const double *__restrict__ b,
                                                      const double *__restrict__ x, double *__restrict__ bc,
@@ -68,6 +74,12 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
 #define INS2D_MG_YCOLS_UNROLL 8
 #endif
 constexpr int kYcolsUnroll = INS2D_MG_YCOLS_UNROLL;
+// columns per block of the multi-block y-line kernel (32, or 16: two row
+// segments per warp)
+#ifndef INS2D_MG_YCW
+#define INS2D_MG_YCW 32
+#endif
+constexpr int kYcolsCols = INS2D_MG_YCW;
 // y-lines of 32 columns per block (kColThreads threads: one segment of rows per warp)
 constexpr int kColThreads = 1024;
 __global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, const double *__restrict__ b,
@@ -75,7 +87,7 @@ __global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, cons
                                                           double omega, const int *done) {
   __shared__ double ysh[2 * kColThreads];
   if (is_done(done)) return;
-  mg_ycols_block<kYcolsUnroll>(L, b, xold, xnew, omega, blockIdx.x * 32, ysh);
+  mg_ycols_block<kYcolsUnroll, kYcolsCols>(L, b, xold, xnew, omega, blockIdx.x * kYcolsCols, ysh);
 }
 
 // warps per column block: one segment of about INS2D_MG_YSEG rows each, at
@@ -84,7 +96,7 @@ __global__ void __launch_bounds__(kColThreads) k_mg_ycols(const MgLevelD L, cons
 #define INS2D_MG_YSEG 8
 #endif
 int col_threads(int ny) {
-  int w = ny / INS2D_MG_YSEG;
+  int w = ny / (INS2D_MG_YSEG * (32 / kYcolsCols));
   if (w < 1) w = 1;
   if (w > kColThreads / 32) w = kColThreads / 32;
   return 32 * w;
@@ -111,7 +123,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     const double *b = (l == 0) ? r0 : L.b;
     k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x,
                                                                                                   M.omega, done);
-    k_mg_ycols<<<(L.nx + 31) / 32, col_threads(L.ny), 0, s>>>(L, b, L.x, L.t, M.omega, done);
+    k_mg_ycols<<<(L.nx + kYcolsCols - 1) / kYcolsCols, col_threads(L.ny), 0, s>>>(L, b, L.x, L.t, M.omega, done);
     const MgLevelD &C = M.L[l + 1];
     k_mg_restrict<<<blocks_for((long long)C.nx * C.ny, 256), 256, 0, s>>>(L, C, b, L.t, C.b, done);
   }
@@ -123,7 +135,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
     k_mg_prolong<<<blocks_for((long long)L.nx * L.ny, 256), 256, 0, s>>>(L, C, L.t,
                                                                          (l + 1 == M.nlev - 1) ? C.x : C.t,
                                                                          M.alpha, done);
-    k_mg_ycols<<<(L.nx + 31) / 32, col_threads(L.ny), 0, s>>>(L, b, L.t, L.x, M.omega, done);
+    k_mg_ycols<<<(L.nx + kYcolsCols - 1) / kYcolsCols, col_threads(L.ny), 0, s>>>(L, b, L.t, L.x, M.omega, done);
     k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
                                                                                                   M.omega, done);
   }

@@ -228,6 +228,7 @@ __device__ __forceinline__ MgLine mg_make_yline(const MgLevelD &L, int i) {
 // warp-wide scan of affine maps (5 shuffle steps) carried from chunk to chunk.
 // The dependent chain is n/32 chunk steps instead of n cell steps, and the
 // loads of a chunk are coalesced along x-lines.  All 32 lanes must call it.
+template <int U = 2>
 static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const double *__restrict__ b,
                                                     const double *__restrict__ xold, double *__restrict__ xnew,
                                                     double omega) {
@@ -237,7 +238,7 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
   const long long base = ln.base, st = ln.st;
   const bool hasold = xold != nullptr, cyc = ln.cyc;
   double carry = 0.0;
-#pragma unroll 2
+#pragma unroll U
   for (int c0 = 0; c0 < n; c0 += 32) {
     const int q = c0 + lane;
     const long long k = base + (long long)q * st;
@@ -262,7 +263,7 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
     carry = __shfl_sync(FULL, d, 31);
   }
   carry = 0.0;
-#pragma unroll 2
+#pragma unroll U
   for (int c0 = ((n - 1) >> 5) << 5; c0 >= 0; c0 -= 32) {
     const int q = c0 + lane;
     const long long k = base + (long long)q * st;
@@ -302,9 +303,10 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
 
 // x-line relaxations: a warp per row (first = warp index j0 >> 5, step =
 // warps (js + 31) >> 5 when called with thread indices)
+template <int U = 2>
 __device__ inline void mg_xline(const MgLevelD &L, const double *__restrict__ b, const double *__restrict__ xold,
                                 double *__restrict__ xnew, double omega, int j0, int js) {
-  for (int j = j0 >> 5; j < L.ny; j += (js + 31) >> 5) mg_line_warp(mg_make_xline(L, j), b, xold, xnew, omega);
+  for (int j = j0 >> 5; j < L.ny; j += (js + 31) >> 5) mg_line_warp<U>(mg_make_xline(L, j), b, xold, xnew, omega);
 }
 // threads per line of the warp solves
 constexpr int kMgLineThreads = 32;
@@ -321,16 +323,21 @@ constexpr int kMgUnroll = INS2D_MG_UNROLL;  // unrolling of the column segment w
 // (sh: 2 x warps x 32 doubles), then each thread re-walks its segment.  The
 // dependent chain per thread is about 4 n / warps + 2 warps steps.  All
 // threads of the block must call it.
-template <int U = kMgUnroll>
+// CW = columns per block (32, or 16: each warp then walks two segments, one
+// per half-warp, so twice as many blocks share a level's columns).
+template <int U = kMgUnroll, int CW = 32>
 __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restrict__ b,
                                       const double *__restrict__ xold, double *__restrict__ xnew, double omega,
                                       int i0, double *sh) {
+  static_assert(CW == 32 || CW == 16, "columns per block");
+  constexpr int SPW = 32 / CW;  // segments per warp
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
+  const int cl = lane % CW, seg = w * SPW + lane / CW, S = W * SPW;
   const int nx = L.nx, n = L.ny;
-  const int i = i0 + lane;
+  const int i = i0 + cl;
   const bool col = i < nx;
-  const int m = (n + W - 1) / W;
-  const int j0 = min(n, w * m), j1 = min(n, j0 + m);
+  const int m = (n + S - 1) / S;
+  const int j0 = min(n, seg * m), j1 = min(n, j0 + m);
   const bool hasold = xold != nullptr, cyc = L.pery && n >= 3;
   double hx = 0.0, xmv = 0.0, xpv = 0.0;
   int im = 0, ip = 0;
@@ -359,20 +366,20 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
       B = al * B + be;
       A = al * A;
     }
-  double *sA = sh, *sB = sh + W * 32;
-  sA[w * 32 + lane] = A;
-  sB[w * 32 + lane] = B;
+  double *sA = sh, *sB = sh + W * 32;  // [segment][column], S * CW = W * 32 entries each
+  sA[seg * CW + cl] = A;
+  sB[seg * CW + cl] = B;
   __syncthreads();
-  if (w == 0) {
+  if (w == 0 && lane < CW) {
     double d = 0.0;
-    for (int q = 0; q < W; ++q) {
-      const double Aq = sA[q * 32 + lane], Bq = sB[q * 32 + lane];
-      sA[q * 32 + lane] = d;  // value entering segment q
+    for (int q = 0; q < S; ++q) {
+      const double Aq = sA[q * CW + lane], Bq = sB[q * CW + lane];
+      sA[q * CW + lane] = d;  // value entering segment q
       d = Aq * d + Bq;
     }
   }
   __syncthreads();
-  double d = sA[w * 32 + lane];
+  double d = sA[seg * CW + cl];
   __syncthreads();
   if (col)
 #pragma unroll U
@@ -393,19 +400,19 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
       B = ga * B + xnew[k];
       A = ga * A;
     }
-  sA[w * 32 + lane] = A;
-  sB[w * 32 + lane] = B;
+  sA[seg * CW + cl] = A;
+  sB[seg * CW + cl] = B;
   __syncthreads();
-  if (w == 0) {
+  if (w == 0 && lane < CW) {
     double x = 0.0;
-    for (int q = W - 1; q >= 0; --q) {
-      const double Aq = sA[q * 32 + lane], Bq = sB[q * 32 + lane];
-      sA[q * 32 + lane] = x;  // value above segment q
+    for (int q = S - 1; q >= 0; --q) {
+      const double Aq = sA[q * CW + lane], Bq = sB[q * CW + lane];
+      sA[q * CW + lane] = x;  // value above segment q
       x = Aq * x + Bq;
     }
   }
   __syncthreads();
-  double x = sA[w * 32 + lane];
+  double x = sA[seg * CW + cl];
   __syncthreads();
   if (col)
 #pragma unroll U
@@ -415,9 +422,12 @@ __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restric
       xnew[k] = cyc ? x : (hasold ? (1.0 - omega) * xold[k] + omega * x : omega * x);
     }
   if (cyc) {
+    // every segment reads the column's first and last values before any
+    // segment overwrites them
+    __syncthreads();
+    const double s = col ? (xnew[i] + L.gy[i] * xnew[(long long)(n - 1) * nx + i]) * L.ky[i] : 0.0;
     __syncthreads();
     if (col) {
-      const double s = (xnew[i] + L.gy[i] * xnew[(long long)(n - 1) * nx + i]) * L.ky[i];
       for (int j = j0; j < j1; ++j) {
         const long long k = (long long)j * nx + i;
         const double v = xnew[k] - s * L.zy[k];
