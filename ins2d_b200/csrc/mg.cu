@@ -77,7 +77,7 @@ constexpr int kYcolsUnroll = INS2D_MG_YCOLS_UNROLL;
 // columns per block of the multi-block y-line kernel (32, or 16: two row
 // segments per warp)
 #ifndef INS2D_MG_YCW
-#define INS2D_MG_YCW 32
+#define INS2D_MG_YCW 16
 #endif
 constexpr int kYcolsCols = INS2D_MG_YCW;
 // y-lines of 32 columns per block (kColThreads threads: one segment of rows per warp)

@@ -329,7 +329,7 @@ template <int U = kMgUnroll, int CW = 32>
 __device__ inline void mg_ycols_block(const MgLevelD &L, const double *__restrict__ b,
                                       const double *__restrict__ xold, double *__restrict__ xnew, double omega,
                                       int i0, double *sh) {
-  static_assert(CW == 32 || CW == 16, "columns per block");
+  static_assert(CW == 32 || CW == 16 || CW == 8, "columns per block");
   constexpr int SPW = 32 / CW;  // segments per warp
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, W = blockDim.x >> 5;
   const int cl = lane % CW, seg = w * SPW + lane / CW, S = W * SPW;
