@@ -29,7 +29,10 @@ __global__ void k_factor_y(MgLevelD L) {
 }
 
 constexpr int kLineThreads = 128;
-constexpr int kTailThreads = 512;
+#ifndef INS2D_MG_TAIL_THREADS
+#define INS2D_MG_TAIL_THREADS 512
+#endif
+constexpr int kTailThreads = INS2D_MG_TAIL_THREADS;
 // levels with at most this many cells run in the single-block tail
 #ifndef INS2D_MG_TAIL_CELLS
 #define INS2D_MG_TAIL_CELLS 4096
