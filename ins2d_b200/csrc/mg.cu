@@ -47,6 +47,21 @@ __device__ __forceinline__ bool is_done(const int *done) { return done && *(vola
 #define INS2D_MG_XUNROLL 2
 #endif
 constexpr int kXlineUnroll = INS2D_MG_XUNROLL;
+// x-lines split over kXlineSplit warps each (1 = a warp per row, the
+// original kernel); blocks of one line each
+#ifndef INS2D_MG_XSPLIT
+#define INS2D_MG_XSPLIT 1
+#endif
+constexpr int kXlineSplit = INS2D_MG_XSPLIT;
+template <int P>
+__global__ void __launch_bounds__(32 * P) k_mg_xline_split(const MgLevelD L, const double *__restrict__ b,
+                                                           const double *__restrict__ xold,
+                                                           double *__restrict__ xnew, double omega, const int *done) {
+  __shared__ double sh[4 * P];
+  if (is_done(done)) return;
+  mg_line_split<P>(mg_make_xline(L, blockIdx.x), b, xold, xnew, omega, threadIdx.x >> 5, sh);
+}
+
 __global__ void __launch_bounds__(kLineThreads) k_mg_xline(const MgLevelD L, const double *__restrict__ b,
                                                            const double *__restrict__ xold, double *__restrict__ xnew,
                                                            double omega, const int *done) {
@@ -111,6 +126,15 @@ unsigned blocks_for(long long n, int t) {
   return (unsigned)(b < 1 ? 1 : b);
 }
 
+void launch_xline(const MgLevelD &L, const double *b, const double *xold, double *xnew, double omega, const int *done,
+                  cudaStream_t s) {
+  if (kXlineSplit > 1)
+    k_mg_xline_split<kXlineSplit><<<L.ny, 32 * kXlineSplit, 0, s>>>(L, b, xold, xnew, omega, done);
+  else
+    k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, xold, xnew,
+                                                                                                  omega, done);
+}
+
 }  // namespace
 
 int mg_tail_level(const MgD &M) {
@@ -124,8 +148,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
   for (int l = 0; l < lt; ++l) {
     const MgLevelD &L = M.L[l];
     const double *b = (l == 0) ? r0 : L.b;
-    k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, nullptr, L.x,
-                                                                                                  M.omega, done);
+    launch_xline(L, b, nullptr, L.x, M.omega, done, s);
     k_mg_ycols<<<(L.nx + kYcolsCols - 1) / kYcolsCols, col_threads(L.ny), 0, s>>>(L, b, L.x, L.t, M.omega, done);
     const MgLevelD &C = M.L[l + 1];
     k_mg_restrict<<<blocks_for((long long)C.nx * C.ny, 256), 256, 0, s>>>(L, C, b, L.t, C.b, done);
@@ -139,8 +162,7 @@ void mg_vcycle_launch(const MgD &M, const double *r0, const int *done, cudaStrea
                                                                          (l + 1 == M.nlev - 1) ? C.x : C.t,
                                                                          M.alpha, done);
     k_mg_ycols<<<(L.nx + kYcolsCols - 1) / kYcolsCols, col_threads(L.ny), 0, s>>>(L, b, L.t, L.x, M.omega, done);
-    k_mg_xline<<<blocks_for((long long)L.ny * kMgLineThreads, kLineThreads), kLineThreads, 0, s>>>(L, b, L.x, L.t,
-                                                                                                  M.omega, done);
+    launch_xline(L, b, L.x, L.t, M.omega, done, s);
   }
 }
 

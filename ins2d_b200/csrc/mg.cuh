@@ -301,6 +301,139 @@ static __device__ __forceinline__ void mg_line_warp(const MgLine ln, const doubl
   }
 }
 
+// One line relaxed by P warps of a thread block (warps q = 0..P-1 of the
+// calling group own consecutive ranges of the line's 32-cell chunks).  Each
+// warp first composes the affine maps of the Thomas recurrence over its
+// range (forward: lane 31's inclusive scan of every chunk; backward: lane
+// 0's), the range composites are chained through shared memory (sh: 4 P
+// doubles of this line), then each warp re-walks its range from the value
+// entering it.  The dependent chain per warp is about 2 chunks / P + P chunk
+// steps in each direction instead of chunks.  Every thread of the block must
+// call it (block barriers).
+template <int P>
+__device__ inline void mg_line_split(const MgLine ln, const double *__restrict__ b, const double *__restrict__ xold,
+                                     double *__restrict__ xnew, double omega, int q, double *sh) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int n = ln.n;
+  const long long base = ln.base, st = ln.st;
+  const bool hasold = xold != nullptr, cyc = ln.cyc;
+  const int chunks = (n + 31) >> 5, per = (chunks + P - 1) / P;
+  const int c_lo = min(chunks, q * per), c_hi = min(chunks, c_lo + per);
+  // forward map of one chunk at lane level (inclusive scan), cell c*32+lane
+  auto fscan = [&](int c, double &A, double &B) {
+    const int i = c * 32 + lane;
+    const long long k = base + (long long)i * st;
+    A = 1.0;
+    B = 0.0;
+    if (i < n) {
+      double rhs = b[k];
+      if (hasold) rhs += ln.cross_w[i] * (ln.cm * xold[k + ln.lo] + ln.cp * xold[k + ln.hi]);
+      const double f = ln.fi[k];
+      A = (i > 0) ? (ln.ascale * ln.am[i]) * f : 0.0;
+      B = rhs * f;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double Ap = __shfl_up_sync(FULL, A, off), Bp = __shfl_up_sync(FULL, B, off);
+      if (lane >= off) {
+        B = A * Bp + B;
+        A = A * Ap;
+      }
+    }
+  };
+  // backward map of one chunk (suffix scan): x_i = -fc_i x_{i+1} + xnew_i
+  auto bscan = [&](int c, double &A, double &B) {
+    const int i = c * 32 + lane;
+    const long long k = base + (long long)i * st;
+    A = 1.0;
+    B = 0.0;
+    if (i < n) {
+      A = -ln.fc[k];
+      B = xnew[k];
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double An = __shfl_down_sync(FULL, A, off), Bn = __shfl_down_sync(FULL, B, off);
+      if (lane + off < 32) {
+        B = A * Bn + B;
+        A = A * An;
+      }
+    }
+  };
+  double *fA = sh, *fB = sh + P, *gA = sh + 2 * P, *gB = sh + 3 * P;
+  // forward, pass 1: composite of the range
+  double SA = 1.0, SB = 0.0;
+  for (int c = c_lo; c < c_hi; ++c) {
+    double A, B;
+    fscan(c, A, B);
+    const double Ac = __shfl_sync(FULL, A, 31), Bc = __shfl_sync(FULL, B, 31);
+    SB = Ac * SB + Bc;
+    SA = Ac * SA;
+  }
+  if (lane == 0) {
+    fA[q] = SA;
+    fB[q] = SB;
+  }
+  __syncthreads();
+  double carry = 0.0;
+  for (int r = 0; r < q; ++r) carry = fA[r] * carry + fB[r];
+  // forward, pass 2
+  for (int c = c_lo; c < c_hi; ++c) {
+    double A, B;
+    fscan(c, A, B);
+    const double d = A * carry + B;
+    const int i = c * 32 + lane;
+    if (i < n) xnew[base + (long long)i * st] = d;
+    carry = __shfl_sync(FULL, d, 31);
+  }
+  __syncthreads();
+  // backward, pass 1: composite of the range (right to left)
+  SA = 1.0;
+  SB = 0.0;
+  for (int c = c_hi - 1; c >= c_lo; --c) {
+    double A, B;
+    bscan(c, A, B);
+    const double Ac = __shfl_sync(FULL, A, 0), Bc = __shfl_sync(FULL, B, 0);
+    SB = Ac * SB + Bc;
+    SA = Ac * SA;
+  }
+  if (lane == 0) {
+    gA[q] = SA;
+    gB[q] = SB;
+  }
+  __syncthreads();
+  carry = 0.0;
+  for (int r = P - 1; r > q; --r) carry = gA[r] * carry + gB[r];
+  // backward, pass 2: solution and relaxation
+  for (int c = c_hi - 1; c >= c_lo; --c) {
+    double A, B;
+    bscan(c, A, B);
+    const double x = A * carry + B;
+    carry = __shfl_sync(FULL, x, 0);
+    const int i = c * 32 + lane;
+    if (i < n) {
+      const long long k = base + (long long)i * st;
+      xnew[k] = cyc ? x : (hasold ? (1.0 - omega) * xold[k] + omega * x : omega * x);
+    }
+  }
+  if (cyc) {
+    // the line's first and last values are read by every warp before any
+    // warp updates its range
+    __syncthreads();
+    const double s = (xnew[base] + ln.g * xnew[base + (long long)(n - 1) * st]) * ln.k;
+    __syncthreads();
+    for (int c = c_lo; c < c_hi; ++c) {
+      const int i = c * 32 + lane;
+      if (i < n) {
+        const long long k = base + (long long)i * st;
+        const double v = xnew[k] - s * ln.z[k];
+        xnew[k] = hasold ? (1.0 - omega) * xold[k] + omega * v : omega * v;
+      }
+    }
+  }
+}
+
 // x-line relaxations: a warp per row (first = warp index j0 >> 5, step =
 // warps (js + 31) >> 5 when called with thread indices)
 template <int U = 2>
