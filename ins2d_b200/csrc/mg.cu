@@ -50,7 +50,7 @@ constexpr int kXlineUnroll = INS2D_MG_XUNROLL;
 // x-lines split over kXlineSplit warps each (1 = a warp per row, the
 // original kernel); blocks of one line each
 #ifndef INS2D_MG_XSPLIT
-#define INS2D_MG_XSPLIT 4
+#define INS2D_MG_XSPLIT 8
 #endif
 constexpr int kXlineSplit = INS2D_MG_XSPLIT;
 template <int P>
