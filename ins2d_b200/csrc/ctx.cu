@@ -1316,7 +1316,9 @@ void ens_build_batch(ins2d_ens *e, const std::vector<int> &order) {
     auto C = [&](int m) -> const MgLevelD & { return lev[(size_t)m * kMgMaxLevels + l + 1]; };
     pl.xl[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).ny : 0LL; });
     pl.yl[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).nx : 0LL; });
-    pl.yg[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)(L(m).nx + 31) / 32 : 0LL; });
+    pl.yg[l] = make_seg([&](int m) {
+      return nlev[m] - 1 > l ? (long long)(L(m).nx + kEnsYcols - 1) / kEnsYcols : 0LL;
+    });
     pl.rs[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)C(m).nx * C(m).ny : 0LL; });
     pl.pr[l] = make_seg([&](int m) { return nlev[m] - 1 > l ? (long long)L(m).nx * L(m).ny : 0LL; });
   }

@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(128) k_emg_line(const EnsMemberD *__restrict__
   mg_line_warp(ln, b, xold, xnew, omega);
 }
 
-// y-lines in groups of 32 columns, one thread block per (member, group);
+// y-lines in groups of kEnsYcols columns, one thread block per (member, group);
 // kind 1: x -> t, 2: t -> x
 constexpr int kColThreadsEns = 256;
 __global__ void __launch_bounds__(kColThreadsEns) k_emg_ycols(const EnsMemberD *__restrict__ mem, const EnsMgD G,
@@ -273,9 +273,9 @@ __global__ void __launch_bounds__(kColThreadsEns) k_emg_ycols(const EnsMemberD *
   const MgLevelD &L = lev(G, m, l);
   const double *b = level_rhs(mem, G, m, l);
   if (kind == 1)
-    mg_ycols_block(L, b, L.x, L.t, omega, grp * 32, ysh);
+    mg_ycols_block<kMgUnroll, kEnsYcols>(L, b, L.x, L.t, omega, grp * kEnsYcols, ysh);
   else
-    mg_ycols_block(L, b, L.t, L.x, omega, grp * 32, ysh);
+    mg_ycols_block<kMgUnroll, kEnsYcols>(L, b, L.t, L.x, omega, grp * kEnsYcols, ysh);
 }
 
 // kind 0: restriction into level l+1; 1: prolongation into level l;

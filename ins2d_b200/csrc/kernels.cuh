@@ -154,6 +154,12 @@ struct EnsStats {
   int status, pad;
 };
 // --- batched ensemble solves (ens_pcg.cu) ----------------------------------
+// columns per thread block of the batched y-line solves (32, or 16: two row
+// segments per warp)
+#ifndef INS2D_ENS_YCW
+#define INS2D_ENS_YCW 32
+#endif
+constexpr int kEnsYcols = INS2D_ENS_YCW;
 // per-member CG scalars and accumulators
 struct EnsCg {
   double acc_pq, acc_rr, acc_rz, maxf;
