@@ -157,7 +157,7 @@ struct EnsStats {
 // columns per thread block of the batched y-line solves (32, or 16: two row
 // segments per warp)
 #ifndef INS2D_ENS_YCW
-#define INS2D_ENS_YCW 32
+#define INS2D_ENS_YCW 16
 #endif
 constexpr int kEnsYcols = INS2D_ENS_YCW;
 // per-member CG scalars and accumulators
