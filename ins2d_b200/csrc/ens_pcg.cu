@@ -258,6 +258,25 @@ __global__ void __launch_bounds__(128) k_emg_line(const EnsMemberD *__restrict__
   mg_line_warp(ln, b, xold, xnew, omega);
 }
 
+// x-lines split over P warps each (mg_line_split), one thread block per line
+// of any member; kind 0: from zero (x), 3: x -> t
+template <int P>
+__global__ void __launch_bounds__(32 * P) k_emg_xline_split(const EnsMemberD *__restrict__ mem, const EnsMgD G,
+                                                            const EnsCg *__restrict__ cg, EnsSeg S, int l, int kind,
+                                                            double omega) {
+  __shared__ double sh[4 * P];
+  const long long g = blockIdx.x;
+  const int s = seg_find(S.start, S.n, g);
+  const int m = S.mem[s];
+  if (cg[m].done) return;
+  const int line = (int)(g - S.start[s]);
+  const MgLevelD &L = lev(G, m, l);
+  const double *b = level_rhs(mem, G, m, l);
+  const double *xold = kind == 0 ? nullptr : L.x;
+  double *xnew = kind == 0 ? L.x : L.t;
+  mg_line_split<P>(mg_make_xline(L, line), b, xold, xnew, omega, threadIdx.x >> 5, sh);
+}
+
 // y-lines in groups of kEnsYcols columns, one thread block per (member, group);
 // kind 1: x -> t, 2: t -> x
 constexpr int kColThreadsEns = 256;
@@ -328,6 +347,20 @@ __global__ void __launch_bounds__(kTailThreadsEns) k_emg_tail(const EnsMemberD *
 
 unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// warps per x-line of the batched solves (1 = a warp per line)
+#ifndef INS2D_ENS_XSPLIT
+#define INS2D_ENS_XSPLIT 1
+#endif
+constexpr int kEnsXsplit = INS2D_ENS_XSPLIT;
+
+void launch_ens_xline(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const EnsSeg &X, int l, int kind,
+                      double omega, cudaStream_t s) {
+  if (kEnsXsplit > 1)
+    k_emg_xline_split<kEnsXsplit><<<(unsigned)X.total, 32 * kEnsXsplit, 0, s>>>(mem, G, cg, X, l, kind, omega);
+  else
+    k_emg_line<<<nblk(X.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, X, l, kind, omega);
+}
+
 }  // namespace
 
 void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const EnsMgPlan &pl, double omega,
@@ -335,7 +368,7 @@ void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const E
   const int lb = pl.ltail;  // batched levels 0 .. lb-1
   for (int l = 0; l < lb; ++l) {
     const EnsSeg &X = pl.xl[l], &Y = pl.yg[l], &R = pl.rs[l];
-    if (X.total) k_emg_line<<<nblk(X.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, X, l, 0, omega);
+    if (X.total) launch_ens_xline(mem, G, cg, X, l, 0, omega, s);
     if (Y.total) k_emg_ycols<<<(unsigned)Y.total, kColThreadsEns, 0, s>>>(mem, G, cg, Y, l, 1, omega);
     if (R.total) k_emg_cells<<<nblk(R.total, 256), 256, 0, s>>>(mem, G, cg, R, l, 0, alpha);
   }
@@ -344,7 +377,7 @@ void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const E
     const EnsSeg &X = pl.xl[l], &Y = pl.yg[l], &P = pl.pr[l];
     if (P.total) k_emg_cells<<<nblk(P.total, 256), 256, 0, s>>>(mem, G, cg, P, l, 1, alpha);
     if (Y.total) k_emg_ycols<<<(unsigned)Y.total, kColThreadsEns, 0, s>>>(mem, G, cg, Y, l, 2, omega);
-    if (X.total) k_emg_line<<<nblk(X.total * kMgLineThreads, 128), 128, 0, s>>>(mem, G, cg, X, l, 3, omega);
+    if (X.total) launch_ens_xline(mem, G, cg, X, l, 3, omega, s);
   }
 }
 
