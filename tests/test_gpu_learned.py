@@ -183,7 +183,7 @@ def _record(m, steps, capacity):
 
 def test_training_gains_over_plain_pcg():
     """Pairs from the solver's own first steps (a stretched lid-driven cavity);
-    the network trained on the first 80% and judged on the held-out rest: the
+    the network trained on the first 80% and evaluated on the held-out rest: the
     same tolerance is reached in fewer iterations than the Jacobi-PCG without
     it from the learned guess, and in far fewer by the flexible CG with the
     network (trained with white-noise fields as well) as its preconditioner;
