@@ -164,7 +164,7 @@ def bfs_profile(y):
 
 
 def bfs_dt(x, y, Re, dt_max, umax=1.5, safety=0.7):
-    """The configuration's dt = 1e-3 is beyond explicit RK4's stability limit
+    """The backward-facing step's nominal dt = 1e-3 is beyond explicit RK4's stability limit
     on a 1024-cell unit height (diffusion: |lambda dt| = 4 dt (1/hx^2 + 1/hy^2)
     / Re must stay below 2.78, convection: umax dt (1/hx + 1/hy) below 2.83),
     so the step is the smaller of dt_max and 0.7 times those limits on the
