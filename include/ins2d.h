@@ -360,6 +360,19 @@ int ins2d_set_learned_mode(ins2d_ctx *ctx, int32_t mode);
  * capacity 0 stops recording.  ins2d_recorded_pairs gives the count. */
 int ins2d_record_pairs(ins2d_ctx *ctx, double *f_buf, double *p_buf, int32_t capacity);
 int32_t ins2d_recorded_pairs(const ins2d_ctx *ctx);
+/* The whole training recipe in one call, for callers without device buffers
+ * of their own (a MATLAB gateway): from the state (V, p) at time t (host or
+ * device arrays per mem; not modified) the context runs record_steps time
+ * steps of dt, recording up to max_pairs (f, dp) pairs of its PCG solves
+ * (the attached network, if any, is not used meanwhile), then trains net
+ * for train_steps Adam steps on the residual loss: batches of `batch`
+ * recorded inputs and `noise` white-noise fields, each with its negation,
+ * rate cosine-decayed from lr to lr/20, batch draws seeded by `seed`.
+ * loss_first / loss_last (may be NULL): the loss of the first and last step.
+ * Allocates its work arrays for the duration of the call. */
+int ins2d_learned_train(ins2d_ctx *ctx, ins2d_cnn *net, const double *V, const double *p, double t, double dt,
+                        int32_t record_steps, int32_t max_pairs, int32_t train_steps, int32_t batch, float lr,
+                        int32_t noise, uint64_t seed, int mem, double *loss_first, double *loss_last);
 
 #ifdef __cplusplus
 }

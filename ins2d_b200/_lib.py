@@ -31,7 +31,7 @@ EXPORTED = [
     "ins2d_cnn_create", "ins2d_cnn_destroy", "ins2d_cnn_last_error", "ins2d_cnn_set_stream", "ins2d_cnn_set_path",
     "ins2d_cnn_get_params", "ins2d_cnn_set_params", "ins2d_cnn_get_activations", "ins2d_cnn_forward", "ins2d_cnn_loss_grad",
     "ins2d_cnn_train_step", "ins2d_cnn_loss_grad_residual", "ins2d_cnn_train_step_residual", "ins2d_cnn_prepare_pairs", "ins2d_set_learned_guess", "ins2d_set_learned_mode", "ins2d_record_pairs",
-    "ins2d_recorded_pairs",
+    "ins2d_recorded_pairs", "ins2d_learned_train",
 ]
 CNN_NPARAM = 37440
 CNN_PATH_TCGEN05, CNN_PATH_MMA_SYNC = 0, 1
@@ -157,6 +157,10 @@ def load():
         "ins2d_set_learned_mode": (ctypes.c_int, [vp, ctypes.c_int32]),
         "ins2d_record_pairs": (ctypes.c_int, [vp, vp, vp, ctypes.c_int32]),
         "ins2d_recorded_pairs": (ctypes.c_int32, [vp]),
+        "ins2d_learned_train": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                               ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                               ctypes.c_int32, ctypes.c_uint64, ctypes.c_int, P(ctypes.c_double),
+                                               P(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

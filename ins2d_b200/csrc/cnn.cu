@@ -746,6 +746,29 @@ __global__ void k_negate(float *__restrict__ a, long long n) {
     a[n + k] = -a[k];
 }
 
+// standard normal values from a counter-based generator (splitmix64 of the
+// index and the seed, Box-Muller), for the noise fields of training batches
+__device__ __forceinline__ double u01(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return ((z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+__global__ void k_gaussian(float *__restrict__ a, long long n, unsigned long long seed) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const double u1 = u01(seed ^ (2ull * (unsigned long long)k)), u2 = u01(seed ^ (2ull * (unsigned long long)k + 1));
+    a[k] = (float)(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2));
+  }
+}
+__global__ void __launch_bounds__(256) k_sumsq_f(const float *__restrict__ a, long long n, double *__restrict__ part) {
+  double v[1] = {0.0};
+  const bool mx[1] = {false};
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    v[0] += (double)a[k] * a[k];
+  block_sum<1>(v, mx, part + blockIdx.x);
+}
+
 __global__ void __launch_bounds__(256) k_dots(long long n, const double *__restrict__ x, const double *__restrict__ f,
                                               const double *__restrict__ q, double *__restrict__ part) {
   double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1030,6 +1053,28 @@ double fcg_zq(long long n, const double *z, const double *q, double *red, cudaSt
 void fcg_p(long long n, double b, const double *z, double *p, cudaStream_t s) {
   k_fcg_p<<<stride_blocks(n), 256, 0, s>>>(n, b, z, p);
   CK(cudaGetLastError());
+}
+
+void negate_tail(float *a, long long n, cudaStream_t s) {
+  k_negate<<<stride_blocks(n), 256, 0, s>>>(a, n);
+  CK(cudaGetLastError());
+}
+
+void gaussian(float *a, long long n, uint64_t seed, cudaStream_t s) {
+  k_gaussian<<<stride_blocks(n), 256, 0, s>>>(a, n, (unsigned long long)seed);
+  CK(cudaGetLastError());
+}
+
+double sumsq(const float *a, long long n, double *red, cudaStream_t s) {
+  const unsigned gb = stride_blocks(n);
+  double *part = red, *res = red + 4 * kRedBlocks;
+  k_sumsq_f<<<gb, 256, 0, s>>>(a, n, part);
+  k_finish<1><<<1, 256, 0, s>>>(part, (int)gb, 0, res);
+  CK(cudaGetLastError());
+  double h = 0.0;
+  CK(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return h;
 }
 
 void dots(long long n, const double *x, const double *f, const double *q, double *red, double d[4], cudaStream_t s) {

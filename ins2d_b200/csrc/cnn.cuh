@@ -98,6 +98,12 @@ void dots(long long n, const double *x, const double *f, const double *q, double
 // z = M(r): the odd part of the network applied to r (prepared like f),
 // rescaled by the rms of r / diag A so that M(c r) = c M(r) for every real c
 void precond(ins2d_cnn *net, const DevOps &P, const double *r, double *z, cudaStream_t s);
+// a[n + k] = -a[k] for k < n
+void negate_tail(float *a, long long n, cudaStream_t s);
+// n standard normal values (counter-based generator with this seed)
+void gaussian(float *a, long long n, uint64_t seed, cudaStream_t s);
+// sum of squares of n floats (synchronises)
+double sumsq(const float *a, long long n, double *red, cudaStream_t s);
 // flexible CG steps (each synchronises and returns its reductions):
 //   d = {p.q, p.r};  x += a p, r -= a q, d = {r.r, max|r|};  z.q;  p = z + b p
 void fcg_pq(long long n, const double *p, const double *q, const double *r, double *red, double d[2],

@@ -1166,6 +1166,98 @@ int ins2d_set_learned_mode(ins2d_ctx *ctx, int32_t mode) {
   return INS2D_OK;
 }
 
+// The training recipe of the learned guess in one call, for callers without
+// device buffers of their own (a MATLAB gateway): record the solver's pairs
+// over record_steps time steps from (V, p) (the caller's arrays are not
+// modified), prepare them, and train with the residual loss.
+int ins2d_learned_train(ins2d_ctx *ctx, ins2d_cnn *net, const double *V, const double *p, double t, double dt,
+                        int32_t record_steps, int32_t max_pairs, int32_t train_steps, int32_t batch, float lr,
+                        int32_t noise, uint64_t seed, int mem, double *loss_first, double *loss_last) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!net || !V || !p || record_steps < 1 || max_pairs < 1 || train_steps < 1 || batch < 1 || noise < 0 ||
+      !(lr > 0.0f) || !(dt > 0.0))
+    return fail(ctx, INS2D_EINVAL, "learned_train: bad argument");
+  if (net->device != ctx->device) return fail(ctx, INS2D_EINVAL, "learned_train: network on another device");
+  const long long Np = ctx->P.Np;
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv);
+  const int fields = 2 * (batch + noise);
+  if ((long long)fields * Np > (1LL << 26)) return fail(ctx, INS2D_EINVAL, "learned_train: batch too large");
+  cudaStream_t s = ctx->stream;
+  std::vector<void *> tmp;
+  auto talloc = [&](size_t bytes) {
+    void *q = nullptr;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) throw std::bad_alloc();
+    tmp.push_back(q);
+    return q;
+  };
+  struct Free {
+    std::vector<void *> &v;
+    ~Free() {
+      for (void *q : v) cudaFree(q);
+    }
+  } guard{tmp};
+  double *dV = (double *)talloc(NV * sizeof(double)), *dP = (double *)talloc(Np * sizeof(double));
+  const cudaMemcpyKind kind = mem == INS2D_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(dV, V, NV * sizeof(double), kind, s));
+  CK(cudaMemcpyAsync(dP, p, Np * sizeof(double), kind, s));
+  double *fb = (double *)talloc((size_t)max_pairs * Np * sizeof(double));
+  double *pb = (double *)talloc((size_t)max_pairs * Np * sizeof(double));
+  ins2d_cnn *saved = ctx->cnn;
+  ctx->cnn = nullptr;  // record the plain solver's pairs
+  ctx->rec_f = fb;
+  ctx->rec_p = pb;
+  ctx->rec_cap = max_pairs;
+  ctx->rec_n = 0;
+  int rc = ins2d_erk_run(ctx, dV, dP, t, dt, record_steps, nullptr, INS2D_MEM_DEVICE);
+  const int n = ctx->rec_n;
+  ctx->rec_f = ctx->rec_p = nullptr;
+  ctx->rec_cap = ctx->rec_n = 0;
+  ctx->cnn = saved;
+  if (rc) return rc;
+  if (n < 1) return fail(ctx, INS2D_EINVAL, "learned_train: no PCG solves to record (FFT path?)");
+  if (!ctx->lg_red) ctx->lg_red = dalloc<double>(ctx, cnn::red_doubles());
+  float *in = (float *)talloc((size_t)n * Np * sizeof(float));
+  for (int k = 0; k < n; ++k)
+    cnn::prepare(ctx->P, fb + (size_t)k * Np, nullptr, 0, in + (size_t)k * Np, nullptr, ctx->lg_red, s);
+  float *xb = (float *)talloc((size_t)fields * Np * sizeof(float));
+  CK(cudaStreamSynchronize(s));
+  // output scale: the inputs' rms over the network's at out_scale 1
+  net->out_scale = 1.0f;
+  const int b0 = std::min(batch, n);
+  cnn::forward(net, in, b0, ctx->P.Npy, ctx->P.Npx, s);
+  const double sx = cnn::sumsq(in, (long long)b0 * Np, ctx->lg_red, s);
+  const double sy = cnn::sumsq(net->y, (long long)b0 * Np, ctx->lg_red, s);
+  net->out_scale = (float)(sy > 0.0 ? std::sqrt(sx / sy) : 1.0);
+  // Adam on random batches (splitmix64 from the seed), cosine-decayed rate
+  uint64_t st = seed;
+  auto next = [&]() {
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  const double lr_final = 0.05 * lr;
+  for (int it = 0; it < train_steps; ++it) {
+    for (int j = 0; j < batch; ++j) {
+      const int k = (int)(next() % (uint64_t)n);
+      CK(cudaMemcpyAsync(xb + (size_t)j * Np, in + (size_t)k * Np, Np * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
+    if (noise) cnn::gaussian(xb + (size_t)batch * Np, (long long)noise * Np, next(), s);
+    cnn::negate_tail(xb, (long long)(batch + noise) * Np, s);
+    const double l = cnn::loss_grad(net, xb, nullptr, fields, ctx->P.Npy, ctx->P.Npx, s, &ctx->P);
+    if (!std::isfinite(l)) return fail(ctx, INS2D_ENONFINITE, "learned_train: non-finite loss");
+    if (it == 0 && loss_first) *loss_first = l;
+    if (loss_last) *loss_last = l;
+    const double rate =
+        lr_final + 0.5 * (lr - lr_final) * (1.0 + std::cos(3.141592653589793 * it / std::max(train_steps - 1, 1)));
+    cnn::adam(net, (float)rate, s);
+  }
+  CK(cudaStreamSynchronize(s));
+  return INS2D_OK;
+  API_END
+}
+
 int ins2d_record_pairs(ins2d_ctx *ctx, double *f_buf, double *p_buf, int32_t capacity) {
   API_BEGIN
   if (capacity < 0 || (capacity > 0 && (!f_buf || !p_buf)))

@@ -232,6 +232,21 @@ def train(net, inp, tgt=None, steps=300, batch=4, lr=2e-3, seed=0, lr_final=None
     return [l / losses[0] for l in losses] if losses and losses[0] > 0 else losses
 
 
+def train_from_steps(options, net, V, p, t, dt, record_steps=24, max_pairs=200, steps=300, batch=4, lr=2e-3,
+                     noise=0, seed=0):
+    """The library's own training recipe (``ins2d_learned_train``): record the
+    pairs of ``record_steps`` time steps from (V, p) (host arrays, not
+    modified), then train on the residual loss.  Returns (first, last) loss."""
+    V = np.ascontiguousarray(np.asarray(V, dtype=np.float64))
+    p = np.ascontiguousarray(np.asarray(p, dtype=np.float64))
+    l0, l1 = ctypes.c_double(), ctypes.c_double()
+    options._check(options._lib.ins2d_learned_train(
+        options._ctx, net.handle, V.ctypes.data, p.ctypes.data, float(t), float(dt), int(record_steps),
+        int(max_pairs), int(steps), int(batch), float(lr), int(noise), ctypes.c_uint64(int(seed)), _lib.MEM_HOST,
+        ctypes.byref(l0), ctypes.byref(l1)))
+    return l0.value, l1.value
+
+
 def attach(options, net, mode="guess"):
     """Use ``net`` in ``options``' PCG solves (None detaches): mode 'guess'
     starts the context's PCG from the network's guess; 'precond' runs a

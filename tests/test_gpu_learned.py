@@ -231,6 +231,38 @@ def test_training_gains_over_plain_pcg():
     assert np.mean(it_fcg_n) < 0.85 * np.mean(it_plain)
 
 
+def test_library_training_recipe():
+    """ins2d_learned_train (the one-call recipe a MATLAB gateway uses):
+    records the solver's pairs, trains with noise fields, and the network
+    then preconditions the flexible CG better than the Jacobi diagonal on
+    right-hand sides from later steps."""
+    from ins2d_b200 import learned
+    m = _cavity()
+    V = np.zeros(m.NV)
+    p = m.pressure_additional_solve(V, np.zeros(m.Np), 0.0)
+    net = learned.ConvNet(device=0, seed=11)
+    l0, l1 = learned.train_from_steps(m, net, V, p, 0.0, 2e-3, record_steps=20, max_pairs=120, steps=400,
+                                      batch=8, lr=3e-3, noise=8, seed=1)
+    assert l1 < 0.5 * l0, (l0, l1)
+    V1, p1 = m.time_ERK(V, p, 0.0, 2e-3, nsteps=20)
+    f_buf, p_buf = learned.record_pairs(m, 12)
+    m.time_ERK(V1, p1, 0.04, 2e-3, nsteps=3)
+    n = learned.recorded_pairs(m)
+    learned.stop_recording(m)
+    it_plain, it_fcg = [], []
+    for k in range(n):
+        f = f_buf[k].contiguous()
+        learned.attach(m, None)
+        it_plain.append(m.pressure_poisson(f, return_stats=True)[1]["iters"])
+        learned.attach(m, net, "precond")
+        dp, st = m.pressure_poisson(f, return_stats=True)
+        it_fcg.append(st["iters"])
+        assert st["norm1"] <= 1e-10 * (1 + 1e-9)
+    learned.attach(m, None)
+    print(f"\nlibrary recipe: Jacobi-PCG {np.mean(it_plain):.1f}, network-preconditioned FCG {np.mean(it_fcg):.1f}")
+    assert np.mean(it_fcg) < 0.85 * np.mean(it_plain)
+
+
 def test_learned_guess_with_multigrid_and_time_steps():
     """With the multigrid preconditioner and inside time steps the learned
     guess leaves the flow unchanged within the solver tolerance."""
