@@ -7,6 +7,11 @@
 //   p = ins2d_mex('pressure_additional_solve', h, V, p, t)
 //   [V,p] = ins2d_mex('time_ERK', h, V, p, t, dt)       % time_ERK.m:1
 //   [maxdiv,umom,vmom,k] = ins2d_mex('check_conservation', h, V, t)
+//   [l0,l1] = ins2d_mex('learned_train', h, V, p, t, dt, record_steps, train_steps, mode)
+//       % no counterpart in the reference: trains the learned initial guess on
+//       % the pairs of the first record_steps steps and attaches it to the
+//       % PCG solves; mode 'guess' (default) or 'precond' (flexible CG)
+//   ins2d_mex('learned_detach', h)
 //   ins2d_mex('destroy', h)
 //
 // The gateway flattens the options struct (grid x/y, BC types, fluid.Re,
@@ -55,6 +60,7 @@ double field_d(const mxArray *s, const char *a, const char *b, double dflt) {
 struct Handle {
   ins2d_ctx *ctx = nullptr;
   mxArray *options = nullptr;  // persistent copy (uBC/vBC handles, grid)
+  ins2d_cnn *net = nullptr;    // learned initial guess / preconditioner, if trained
 };
 
 void check(Handle *h, int rc) {
@@ -172,8 +178,31 @@ void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[]) {
   ins2d_get_sizes(h->ctx, &sz);
   if (!strcmp(cmd, "destroy")) {
     ins2d_ctx_destroy(h->ctx);
+    if (h->net) ins2d_cnn_destroy(h->net);
     mxDestroyArray(h->options);
     delete h;
+  } else if (!strcmp(cmd, "learned_train")) {
+    if (nrhs < 6) mexErrMsgIdAndTxt("ins2d:args", "learned_train: h, V, p, t, dt[, record_steps, train_steps, mode]");
+    const int rec = nrhs > 6 ? (int)mxGetScalar(prhs[6]) : 24;
+    const int steps = nrhs > 7 ? (int)mxGetScalar(prhs[7]) : 300;
+    char mode[16] = "guess";
+    if (nrhs > 8 && mxIsChar(prhs[8])) mxGetString(prhs[8], mode, sizeof mode);
+    if (!h->net) {
+      int32_t dev = 0;
+      const mxArray *dv = mxGetField(h->options, 0, "device");
+      if (dv && mxIsNumeric(dv)) dev = (int32_t)mxGetScalar(dv);
+      if (ins2d_cnn_create(dev, 0, &h->net) != INS2D_OK) mexErrMsgIdAndTxt("ins2d:cnn", "cnn_create failed");
+    }
+    double l0 = 0.0, l1 = 0.0;
+    check(h, ins2d_learned_train(h->ctx, h->net, mxGetPr(prhs[2]), mxGetPr(prhs[3]), mxGetScalar(prhs[4]),
+                                 mxGetScalar(prhs[5]), rec, 4 * rec + 8, steps, 4, 2e-3f, 4, 0, INS2D_MEM_HOST, &l0,
+                                 &l1));
+    check(h, ins2d_set_learned_guess(h->ctx, h->net));
+    check(h, ins2d_set_learned_mode(h->ctx, strcmp(mode, "precond") ? INS2D_LEARNED_GUESS : INS2D_LEARNED_PRECOND));
+    plhs[0] = mxCreateDoubleScalar(l0);
+    if (nlhs > 1) plhs[1] = mxCreateDoubleScalar(l1);
+  } else if (!strcmp(cmd, "learned_detach")) {
+    check(h, ins2d_set_learned_guess(h->ctx, nullptr));
   } else if (!strcmp(cmd, "F")) {
     std::vector<double> F(sz.NV);
     double maxres = 0;
