@@ -16,14 +16,18 @@
 // everything else is FP32.
 //
 // Tensor cores: the 32 -> 32 layers are implicit GEMMs on BF16 tensor cores
-// (mma.sync m16n8k16, FP32 accumulators):
+// with FP32 accumulators:
 //   forward        Z[p][co]   = sum_{t,ci} W[co][t][ci] A[p+t][ci]    M = pixels, N = 32, K = 288
 //   backward-data  dA[p][ci]  = sum_{t,co} W[co][8-t][ci] dZ[p+t][co] (the same kernel, transposed weights)
 //   weight grad    dW[co][t,ci] = sum_p dZ[p][co] A[p+t][ci]          M = 32, N = 288, K = pixels
-// The 1 -> 32 and 32 -> 1 layers (2 x 288 MACs per pixel) are FP32 CUDA-core
-// kernels.  Every kernel is bandwidth-light next to the solver's stencils;
-// the per-pixel traffic is one read of the input activations and one write of
-// the output (64 bytes each in BF16).
+// The first two run on tcgen05.mma with TMEM accumulators (k_conv_mid_tc,
+// the default) or on mma.sync m16n8k16 (k_conv_mid); the weight gradient on
+// mma.sync (k_wgrad_mid).  The 1 -> 32 and 32 -> 1 layers (2 x 288 MACs per
+// pixel), the losses (squared error; the residual loss with the context's
+// operator tables), the solver's odd-part application and Adam are FP32 /
+// FP64 CUDA-core kernels.  Per pixel and 32 -> 32 layer the traffic is one
+// read of the input activations and one write of the output (64 bytes each
+// in BF16).
 #include <cuda_bf16.h>
 
 #include <algorithm>
