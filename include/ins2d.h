@@ -159,6 +159,18 @@ const char *ins2d_last_error(const ins2d_ctx *ctx);
 int ins2d_get_sizes(const ins2d_ctx *ctx, ins2d_sizes *out);
 /* stream: a cudaStream_t (NULL = the context's own stream) */
 int ins2d_set_stream(ins2d_ctx *ctx, void *stream);
+/* Orders the context's later work after all work queued so far on the
+ * cudaStream_t `stream` (an event recorded there, waited on by the context's
+ * stream).  For device inputs produced on another stream, e.g. by a torch
+ * kernel that may still be running: the context's own stream does not wait
+ * for other streams by itself.  No-op when `stream` is the context's stream. */
+int ins2d_wait_stream(ins2d_ctx *ctx, void *stream);
+/* Grids whose PCG runs one launch per phase (more than 65536 cells with the
+ * multigrid preconditioner) are driven by the host, which polls a device
+ * convergence flag between chunks of iterations.  This bounds the iterations
+ * the host launches while the flag stays unset; past it the solve returns
+ * INS2D_ETIMEOUT.  iterations < 0 restores the default, CG_maxit + 1024. */
+int ins2d_set_poll_limit(ins2d_ctx *ctx, int64_t iterations);
 /* set_bc_vectors.m:1 -- boundary values at time t (steady cases call it once) */
 int ins2d_set_bc_values(ins2d_ctx *ctx, double t, const ins2d_bc_values *vals);
 /* Unsteady boundary conditions (options.BC.BC_unsteady = 1): the context calls
@@ -210,6 +222,10 @@ int ins2d_erk_step(ins2d_ctx *ctx, double *V, double *p, double t, double dt,
  * without process_iteration); V, p device pointers updated in place. */
 int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int32_t nsteps,
                   ins2d_step_stats *stats, int mem);
+/* The initial projection of input_check.m:95-111: when max|M V + yM| (also
+ * returned in *maxdiv, may be NULL) exceeds 1e-12, V -= Om_inv .* (G dp) with
+ * dp = pressure_poisson(M V + yM, t); V in place. */
+int ins2d_initial_projection(ins2d_ctx *ctx, double *V, double t, double *maxdiv, int mem);
 /* out[4] = {maxdiv, umom, vmom, k} (check_conservation.m:1-76) */
 int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4], int mem);
 
@@ -227,9 +243,15 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
  * and sizes the FFT path supports; other sizes return INS2D_EINVAL.
  * The first call on a device looks up the array's device address and sets
  * kernel attributes; make that first call before any stream capture.
+ * A call whose (Nx, Ny, dx, dy) differ from the previous call's on that
+ * device builds the twiddle and symbol tables on the host and copies them
+ * in from pageable memory, waiting for the copies; a call with the same
+ * values reuses the tables already on the device.  Every call blocks until
+ * the stream has finished its work.
  * All calls share the array: calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialised by the caller.  Returns
- * after the stream has finished the call's work. */
+ * other host threads) race and must be serialised by the caller.  An error
+ * already pending on the calling thread (cudaGetLastError) is left to the
+ * caller, neither cleared nor reported as this call's failure. */
 #define INS2D_NOALLOC_MAX_N 4096
 #define INS2D_NOALLOC_MAX_CELLS (1 << 20)
 int ins2d_fft_poisson_noalloc(const double *f, double *dp, int32_t Nx, int32_t Ny, double dx, double dy,
@@ -257,6 +279,8 @@ int32_t ins2d_ens_size(const ins2d_ens *e);
 /* member context (owned by the ensemble; NULL when m is out of range) */
 ins2d_ctx *ins2d_ens_member(ins2d_ens *e, int32_t m);
 int ins2d_ens_set_stream(ins2d_ens *e, void *stream);
+/* as ins2d_wait_stream, for the ensemble's stream */
+int ins2d_ens_wait_stream(ins2d_ens *e, void *stream);
 /* member state V (NV values), p (Np values) in or out */
 int ins2d_ens_set_state(ins2d_ens *e, int32_t m, const double *V, const double *p, int mem);
 int ins2d_ens_get_state(ins2d_ens *e, int32_t m, double *V, double *p, int mem);

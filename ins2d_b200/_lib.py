@@ -21,12 +21,12 @@ MAX_STAGES = 8
 # every symbol include/ins2d.h declares
 EXPORTED = [
     "ins2d_ctx_create", "ins2d_ctx_destroy", "ins2d_last_error", "ins2d_get_sizes",
-    "ins2d_set_stream", "ins2d_set_bc_values", "ins2d_set_bc_sampler", "ins2d_F",
+    "ins2d_set_stream", "ins2d_wait_stream", "ins2d_set_poll_limit", "ins2d_set_bc_values", "ins2d_set_bc_sampler", "ins2d_F",
     "ins2d_divergence", "ins2d_laplacian", "ins2d_pressure_poisson",
-    "ins2d_pressure_additional_solve", "ins2d_erk_step", "ins2d_erk_run", "ins2d_conservation",
+    "ins2d_pressure_additional_solve", "ins2d_erk_step", "ins2d_erk_run", "ins2d_conservation", "ins2d_initial_projection",
     "ins2d_profile", "ins2d_profile_read", "ins2d_fft_poisson_noalloc",
     "ins2d_ens_create", "ins2d_ens_destroy", "ins2d_ens_last_error", "ins2d_ens_size", "ins2d_ens_member",
-    "ins2d_ens_set_stream", "ins2d_ens_set_state", "ins2d_ens_get_state", "ins2d_ens_state_ptr", "ins2d_ens_set_member_dt",
+    "ins2d_ens_set_stream", "ins2d_ens_wait_stream", "ins2d_ens_set_state", "ins2d_ens_get_state", "ins2d_ens_state_ptr", "ins2d_ens_set_member_dt",
     "ins2d_ens_erk_run", "ins2d_ens_set_solver", "ins2d_ens_solve_shape",
     "ins2d_cnn_create", "ins2d_cnn_destroy", "ins2d_cnn_last_error", "ins2d_cnn_set_stream", "ins2d_cnn_set_path",
     "ins2d_cnn_get_params", "ins2d_cnn_set_params", "ins2d_cnn_get_activations", "ins2d_cnn_forward", "ins2d_cnn_loss_grad",
@@ -105,6 +105,8 @@ def load():
         "ins2d_last_error": (ctypes.c_char_p, [vp]),
         "ins2d_get_sizes": (ctypes.c_int, [vp, P(Sizes)]),
         "ins2d_set_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_wait_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_set_poll_limit": (ctypes.c_int, [vp, ctypes.c_int64]),
         "ins2d_set_bc_values": (ctypes.c_int, [vp, ctypes.c_double, P(BcValues)]),
         "ins2d_set_bc_sampler": (ctypes.c_int, [vp, SAMPLER_FN, vp]),
         "ins2d_F": (ctypes.c_int, [vp, vp, vp, vp, ctypes.c_double, ctypes.c_int, vp, P(ctypes.c_double),
@@ -119,6 +121,7 @@ def load():
         "ins2d_erk_run": (ctypes.c_int, [vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                          P(StepStats), ctypes.c_int]),
         "ins2d_conservation": (ctypes.c_int, [vp, vp, ctypes.c_double, P(ctypes.c_double), ctypes.c_int]),
+        "ins2d_initial_projection": (ctypes.c_int, [vp, vp, ctypes.c_double, P(ctypes.c_double), ctypes.c_int]),
         "ins2d_profile": (ctypes.c_int, [vp, ctypes.c_int]),
         "ins2d_profile_read": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_int64)]),
         "ins2d_fft_poisson_noalloc": (ctypes.c_int, [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
@@ -129,6 +132,7 @@ def load():
         "ins2d_ens_size": (ctypes.c_int32, [vp]),
         "ins2d_ens_member": (vp, [vp, ctypes.c_int32]),
         "ins2d_ens_set_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_ens_wait_stream": (ctypes.c_int, [vp, vp]),
         "ins2d_ens_set_state": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int]),
         "ins2d_ens_get_state": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int]),
         "ins2d_ens_state_ptr": (ctypes.c_int, [vp, ctypes.c_int32, P(vp), P(vp)]),

@@ -117,6 +117,8 @@ class Options:
             raise TypeError(f"unexpected options: {bad}")  # keys starting with '_' are annotations of a case
         self._lib = _lib.load()
         self._owner = _handle is None
+        self._stream = None  # the cudaStream_t handle set by set_stream (None: the context's own)
+        self.device = int(device)
         self.x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
         self.y = np.ascontiguousarray(np.asarray(y, dtype=np.float64))
         self.BC = {"u": dict(BC["u"]), "v": dict(BC["v"])}
@@ -215,12 +217,17 @@ class Options:
         except Exception:
             pass
 
-    @staticmethod
-    def _mem(*arrs):
+    def _mem(self, *arrs):
+        """MEM_HOST or MEM_DEVICE for the call's arrays; for device tensors the
+        context's stream is first ordered after torch's current stream, so an
+        input still being written by a torch kernel is read only when done."""
         kinds = {a.dev for a in arrs if a is not None}
         if len(kinds) > 1:
             raise ValueError("mix of host and device arrays")
-        return _lib.MEM_DEVICE if kinds == {True} else _lib.MEM_HOST
+        if kinds == {True}:
+            _order_after_torch(self._lib.ins2d_wait_stream, self._ctx, self._stream, self.device)
+            return _lib.MEM_DEVICE
+        return _lib.MEM_HOST
 
     def _like(self, ref, n):
         if ref.dev:
@@ -242,6 +249,7 @@ class Options:
     def set_stream(self, stream):
         """Issue work on a CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self._lib.ins2d_set_stream(self._ctx, ctypes.c_void_p(stream)))
+        self._stream = int(stream) if stream else None
 
     # -- boundary conditions ----------------------------------------------------
     def bc_samples(self, t):
@@ -350,32 +358,16 @@ class Options:
         self._check(self._lib.ins2d_conservation(self._ctx, Va.ptr, float(t), out, self._mem(Va)))
         return tuple(out)
 
-    def initial_projection(self, V, t=0.0):
-        """input_check.m:95-111: project V when max|div| > 1e-12."""
-        f, maxdiv = self.divergence(V)
-        if maxdiv > 1e-12:
-            dp = self.pressure_poisson(f, t)
-            G_dp_scaled = self.F(np.zeros(self.NV), None, dp, t)[1] - self.F(np.zeros(self.NV), None, np.zeros(self.Np), t)[1]
-            # F(0,.,dp) - F(0,.,0) = -G*dp ; V - Om^-1 G dp = V + Om^-1 (that difference)
-            V = np.asarray(V, dtype=np.float64) + self.Om_inv() * G_dp_scaled
-        return V
-
-    def Om_inv(self):
-        """Om_inv (operator_mesh.m:331-352) as a host vector."""
-        hx, hy = np.diff(self.x), np.diff(self.y)
-        gx = np.zeros(len(hx) + 1)
-        gx[0], gx[-1] = hx[0] / 2, hx[-1] / 2
-        gx[1:-1] = (hx[:-1] + hx[1:]) / 2
-        gy = np.zeros(len(hy) + 1)
-        gy[0], gy[-1] = hy[0] / 2, hy[-1] / 2
-        gy[1:-1] = (hy[:-1] + hy[1:]) / 2
-        L, R = self.BC["u"]["left"], self.BC["u"]["right"]
-        gxi = {("dir", "dir"): gx[1:-1], ("dir", "pres"): gx[1:], ("pres", "dir"): gx[:-1], ("pres", "pres"): gx,
-               ("per", "per"): np.r_[gx[0] + gx[-1], gx[1:-1]]}[(L, R)]
-        Lo, Up = self.BC["v"]["low"], self.BC["v"]["up"]
-        gyi = {("dir", "dir"): gy[1:-1], ("dir", "pres"): gy[1:], ("pres", "dir"): gy[:-1], ("pres", "pres"): gy,
-               ("per", "per"): np.r_[gy[0] + gy[-1], gy[1:-1]]}[(Lo, Up)]
-        return 1.0 / np.r_[np.kron(hy, gxi), np.kron(gyi, hx)]
+    def initial_projection(self, V, t=0.0, return_maxdiv=False):
+        """input_check.m:95-111: project V when max|M V + yM| > 1e-12 (a new
+        array for host input, a device tensor in place)."""
+        Va = _Arr(V if _is_torch_cuda(V) else np.array(V, dtype=np.float64), self.NV, "V")
+        md = ctypes.c_double()
+        self._check(self._lib.ins2d_initial_projection(self._ctx, Va.ptr, float(t), ctypes.byref(md),
+                                                       self._mem(Va)))
+        if return_maxdiv:
+            return Va.obj, md.value
+        return Va.obj
 
 
 class Ensemble:
@@ -389,6 +381,8 @@ class Ensemble:
     def __init__(self, members):
         self._lib = _lib.load()
         self.members = []
+        self._stream = None
+        self._device = int(members[0].get("device", 0)) if members else 0
         # describe every member with an Options-like set of descriptors (no
         # context is created for the descriptors themselves)
         descs = [_describe(**kw) for kw in members]
@@ -436,11 +430,21 @@ class Ensemble:
 
     def set_stream(self, stream):
         self._check(self._lib.ins2d_ens_set_stream(self._e, ctypes.c_void_p(stream)))
+        self._stream = int(stream) if stream else None
+
+    def _mem(self, *arrs):
+        kinds = {a.dev for a in arrs if a is not None}
+        if len(kinds) > 1:
+            raise ValueError("mix of host and device arrays")
+        if kinds == {True}:
+            _order_after_torch(self._lib.ins2d_ens_wait_stream, self._e, self._stream, self._device)
+            return _lib.MEM_DEVICE
+        return _lib.MEM_HOST
 
     def set_state(self, m, V, p):
         o = self.members[m]
         Va, pa = _Arr(V, o.NV, "V"), _Arr(p, o.Np, "p")
-        self._check(self._lib.ins2d_ens_set_state(self._e, m, Va.ptr, pa.ptr, Options._mem(Va, pa)))
+        self._check(self._lib.ins2d_ens_set_state(self._e, m, Va.ptr, pa.ptr, self._mem(Va, pa)))
 
     def set_member_dt(self, m, dt):
         """Give member m its own time step (0: the run's dt)."""
@@ -455,7 +459,7 @@ class Ensemble:
         for a, arr in ((Va, V), (pa, p)):
             if not a.dev and (not isinstance(arr, np.ndarray) or a.ptr != arr.ctypes.data):
                 raise ValueError("get_state: output arrays must be contiguous float64")
-        self._check(self._lib.ins2d_ens_get_state(self._e, m, Va.ptr, pa.ptr, Options._mem(Va, pa)))
+        self._check(self._lib.ins2d_ens_get_state(self._e, m, Va.ptr, pa.ptr, self._mem(Va, pa)))
         return V, p
 
     def state_tensors(self, m):
@@ -513,6 +517,19 @@ def _describe(x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_ad
     o.device = int(device)
     o.precond = _lib.PRECOND_CODES[precond]
     return g, b, o, x, y
+
+
+def _order_after_torch(wait_fn, handle, stream, device):
+    """Makes the library's stream wait for the work queued so far on torch's
+    current stream of `device` (a no-op when the library was given that very
+    stream through set_stream)."""
+    import torch
+    cur = torch.cuda.current_stream(device).cuda_stream
+    if stream is not None and int(stream) == int(cur):
+        return
+    rc = wait_fn(handle, ctypes.c_void_p(cur))
+    if rc != 0:
+        raise Ins2dError(rc, "ordering the library's stream after torch's current stream failed")
 
 
 def _cuda_view(ptr, n):

@@ -1169,7 +1169,8 @@ int ins2d_cnn_create(int32_t device, uint64_t seed, ins2d_cnn **out) {
   if (!n) return INS2D_ENOMEM;
   try {
     n->device = device;
-    CK(cudaSetDevice(device));
+    DeviceGuard dg(device);
+    CK(dg.err);
     const size_t pb = cnn::kNParam * sizeof(float);
     for (float **p : {&n->w, &n->g, &n->m, &n->v})
       if (cudaMalloc(p, pb) != cudaSuccess) throw std::bad_alloc();
@@ -1200,7 +1201,7 @@ int ins2d_cnn_create(int32_t device, uint64_t seed, ins2d_cnn **out) {
 
 int ins2d_cnn_destroy(ins2d_cnn *n) {
   if (!n) return INS2D_OK;
-  cudaSetDevice(n->device);
+  DeviceGuard dg(n->device);
   for (float *p : {n->w, n->g, n->m, n->v, n->y, n->dy, n->dres, n->in1, n->partials}) cudaFree(p);
   cudaFree(n->wf);
   cudaFree(n->wb);
@@ -1231,7 +1232,8 @@ int ins2d_cnn_set_path(ins2d_cnn *n, int32_t path) {
 int ins2d_cnn_get_params(ins2d_cnn *n, float *w, float *out_scale) {
   if (!n) return INS2D_EINVAL;
   try {
-    CK(cudaSetDevice(n->device));
+    DeviceGuard dg(n->device);
+    CK(dg.err);
     if (w) {
       CK(cudaMemcpyAsync(w, n->w, cnn::kNParam * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
       CK(cudaStreamSynchronize(n->stream));
@@ -1247,7 +1249,8 @@ int ins2d_cnn_set_params(ins2d_cnn *n, const float *w, float out_scale) {
   if (!n) return INS2D_EINVAL;
   if (!(out_scale > 0.0f) || !std::isfinite(out_scale)) return cnn_fail(n, INS2D_EINVAL, "cnn: out_scale must be > 0");
   try {
-    CK(cudaSetDevice(n->device));
+    DeviceGuard dg(n->device);
+    CK(dg.err);
     if (w) {
       CK(cudaMemcpyAsync(n->w, w, cnn::kNParam * sizeof(float), cudaMemcpyHostToDevice, n->stream));
       CK(cudaStreamSynchronize(n->stream));
@@ -1266,7 +1269,8 @@ int ins2d_cnn_forward(ins2d_cnn *n, const float *in, float *y, int32_t B, int32_
   if (rc) return rc;
   if (!y) return cnn_fail(n, INS2D_EINVAL, "cnn_forward: null output");
   try {
-    CK(cudaSetDevice(n->device));
+    DeviceGuard dg(n->device);
+    CK(dg.err);
     cnn::forward(n, in, B, H, W, n->stream);
     CK(cudaMemcpyAsync(y, n->y, (size_t)B * H * W * sizeof(float), cudaMemcpyDeviceToDevice, n->stream));
     CK(cudaStreamSynchronize(n->stream));
@@ -1284,7 +1288,8 @@ int ins2d_cnn_get_activations(ins2d_cnn *n, int32_t layer, int64_t pixels, uint1
   if (layer < 1 || layer > 5 || !out || pixels < 1 || pixels > n->cap)
     return cnn_fail(n, INS2D_EINVAL, "cnn_get_activations: layer 1..5, pixels of the last forward pass");
   try {
-    CK(cudaSetDevice(n->device));
+    DeviceGuard dg(n->device);
+    CK(dg.err);
     CK(cudaMemcpyAsync(out, n->act[layer - 1], (size_t)pixels * cnn::kC * sizeof(uint16_t), cudaMemcpyDeviceToHost,
                        n->stream));
     CK(cudaStreamSynchronize(n->stream));
@@ -1301,7 +1306,8 @@ int ins2d_cnn_loss_grad(ins2d_cnn *n, const float *in, const float *tgt, int32_t
   if (rc) return rc;
   if (!tgt) return cnn_fail(n, INS2D_EINVAL, "cnn_loss_grad: null targets");
   try {
-    CK(cudaSetDevice(n->device));
+    DeviceGuard dg(n->device);
+    CK(dg.err);
     const double l = cnn::loss_grad(n, in, tgt, B, H, W, n->stream, nullptr);
     if (loss) *loss = l;
     if (grad) {
@@ -1324,7 +1330,8 @@ int ins2d_cnn_train_step(ins2d_cnn *n, const float *in, const float *tgt, int32_
   if (!tgt) return cnn_fail(n, INS2D_EINVAL, "cnn_train_step: null targets");
   if (!(lr > 0.0f) || !std::isfinite(lr)) return cnn_fail(n, INS2D_EINVAL, "cnn_train_step: lr must be > 0");
   try {
-    CK(cudaSetDevice(n->device));
+    DeviceGuard dg(n->device);
+    CK(dg.err);
     const double l = cnn::loss_grad(n, in, tgt, B, H, W, n->stream, nullptr);
     if (!std::isfinite(l)) return cnn_fail(n, INS2D_ENONFINITE, "cnn_train_step: non-finite loss");
     cnn::adam(n, lr, n->stream);

@@ -21,10 +21,6 @@
 #include "setup.hpp"
 #include "mg_host.hpp"
 
-namespace ins2d {
-void fft_prepare();
-}
-
 using namespace ins2d;
 
 // a captured time step (erk_run on the FFT path)
@@ -79,6 +75,8 @@ struct ins2d_ctx {
   };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
+  cudaEvent_t order_ev = nullptr;  // ins2d_wait_stream
+  long long poll_limit = -1;       // ins2d_set_poll_limit (-1: CG_maxit + 1024)
   StepGraph step_graph[2];
   // learned initial guess of the PCG (borrowed network) and its work arrays
   ins2d_cnn *cnn = nullptr;
@@ -267,8 +265,9 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
     CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (c->h_sc->done) break;
-    if (launched > (long long)c->opts.CG_maxit + 1024)
-      return fail(c, INS2D_ETIMEOUT, "PCG: device convergence flag never set");
+    const long long limit = c->poll_limit >= 0 ? c->poll_limit : (long long)c->opts.CG_maxit + 1024;
+    if (launched >= limit)
+      return fail(c, INS2D_ETIMEOUT, "PCG: device convergence flag not set within the host's iteration limit");
     if (c->use_mg) {
       pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->stream);
       c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
@@ -412,7 +411,7 @@ int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solv
   if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
   if (c->poisson == INS2D_POISSON_FFT) {
     Prof pr(c, INS2D_PROF_POISSON, 3);
-    launch_fft_poisson(c->P, c->fft, f, dp, accumulate, c->stream);
+    CK(launch_fft_poisson(c->P, c->fft, f, dp, accumulate, c->stream));
     CK(cudaGetLastError());
     return INS2D_OK;
   }
@@ -436,7 +435,7 @@ int solve_div(ins2d_ctx *c, const double *W, double alpha, double beta, double g
   if (c->poisson == INS2D_POISSON_FFT && fft_fuses_div(c->fft)) {
     if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
     Prof pr(c, INS2D_PROF_POISSON, 3);
-    launch_fft_poisson_div(c->P, c->fft, W, alpha, beta, gamma, dp, accumulate, c->stream);
+    CK(launch_fft_poisson_div(c->P, c->fft, W, alpha, beta, gamma, dp, accumulate, c->stream));
     CK(cudaGetLastError());
     return INS2D_OK;
   }
@@ -558,11 +557,12 @@ int check_mem(ins2d_ctx *c, int mem) {
   return INS2D_OK;
 }
 
-#define API_BEGIN \
+#define API_BEGIN                \
   if (!ctx) return INS2D_EINVAL; \
   ctx->err.clear();              \
+  DeviceGuard dguard_(ctx->device); \
   try {                          \
-    CK(cudaSetDevice(ctx->device));
+    CK(dguard_.err);
 #define API_END                                                  \
   }                                                              \
   catch (const CudaError &e) {                                   \
@@ -592,6 +592,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
   c->device = opts->device;
   c->fp32 = opts->precision == INS2D_PREC_FP32_STENCIL;
   c->poisson = opts->poisson;
+  DeviceGuard dg(c->device);
   int rc = INS2D_OK;
   try {
     if (!(opts->Re > 0)) throw std::invalid_argument("Re must be positive");
@@ -606,7 +607,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     for (int i = 0; i < opts->rk_stages; ++i)
       for (int j = i; j < opts->rk_stages; ++j)
         if (opts->rk_A[i * opts->rk_stages + j] != 0.0) throw std::invalid_argument("Butcher tableau is not explicit");
-    CK(cudaSetDevice(c->device));
+    CK(dg.err);
     int bcs[8] = {bc->u_left, bc->u_right, bc->u_low, bc->u_up, bc->v_left, bc->v_right, bc->v_low, bc->v_up};
     build_host_ops(c->H, grid->Nx, grid->Ny, grid->x, grid->y, bcs, opts->Re);
     if (c->poisson == INS2D_POISSON_FFT) {
@@ -705,7 +706,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     c->red.max_blocks = maxb;
     CK(cudaMemset(c->red.counter, 0, sizeof(unsigned int)));
     if (c->poisson == INS2D_POISSON_FFT) {
-      fft_prepare();
+      CK(fft_prepare());
       FftPlan &F = c->fft;
       F.Nx = H.Nx;
       F.Ny = H.Ny;
@@ -769,7 +770,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
 
 int ins2d_ctx_destroy(ins2d_ctx *ctx) {
   if (!ctx) return INS2D_OK;
-  cudaSetDevice(ctx->device);
+  DeviceGuard dg(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto &g : ctx->step_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -779,6 +780,7 @@ int ins2d_ctx_destroy(ins2d_ctx *ctx) {
     cudaEventDestroy(r.b);
   }
   for (auto e : ctx->pool) cudaEventDestroy(e);
+  if (ctx->order_ev) cudaEventDestroy(ctx->order_ev);
   if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -804,9 +806,26 @@ int ins2d_set_stream(ins2d_ctx *ctx, void *stream) {
   return INS2D_OK;
 }
 
+int ins2d_set_poll_limit(ins2d_ctx *ctx, int64_t iterations) {
+  if (!ctx) return INS2D_EINVAL;
+  ctx->poll_limit = iterations < 0 ? -1 : (long long)iterations;
+  return INS2D_OK;
+}
+
+int ins2d_wait_stream(ins2d_ctx *ctx, void *stream) {
+  API_BEGIN
+  const cudaStream_t other = (cudaStream_t)stream;
+  if (other == ctx->stream) return INS2D_OK;
+  if (!ctx->order_ev) CK(cudaEventCreateWithFlags(&ctx->order_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ctx->order_ev, other));
+  CK(cudaStreamWaitEvent(ctx->stream, ctx->order_ev, 0));
+  return INS2D_OK;
+  API_END
+}
+
 int ins2d_profile(ins2d_ctx *ctx, int enable) {
   if (!ctx) return INS2D_EINVAL;
-  cudaSetDevice(ctx->device);
+  DeviceGuard dg(ctx->device);
   for (auto &r : ctx->recs) {
     ctx->pool.push_back(r.a);
     ctx->pool.push_back(r.b);
@@ -1054,6 +1073,41 @@ int ins2d_erk_step(ins2d_ctx *ctx, double *V, double *p, double t, double dt, in
   return ins2d_erk_run(ctx, V, p, t, dt, 1, stats, mem);
 }
 
+// input_check.m:95-111: when max|M V + yM| > 1e-12, V -= Om_inv .* (G dp)
+// with dp = pressure_poisson(M V + yM); V in place.
+int ins2d_initial_projection(ins2d_ctx *ctx, double *V, double t, double *maxdiv, int mem) {
+  API_BEGIN
+  if (check_mem(ctx, mem)) return INS2D_EINVAL;
+  if (!V) return fail(ctx, INS2D_EINVAL, "initial_projection: null argument");
+  int rc = sample_bc(ctx, t);
+  if (rc) return rc;
+  const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv);
+  const double *dV = in_dev(ctx, V, ctx->stV, NV, mem);
+  {
+    Prof pr(ctx, INS2D_PROF_OTHER, 1);
+    launch_div(ctx->P, dV, 1.0, 0.0, 1.0, ctx->f, true, ctx->red, ctx->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->h_red, ctx->red.result, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const double md = ctx->h_red[0];
+  if (maxdiv) *maxdiv = md;
+  if (!(md > 1e-12)) return INS2D_OK;
+  ins2d_solve_stats st;
+  rc = solve(ctx, ctx->f, ctx->dp, false, &st);
+  if (rc) return rc;
+  {
+    Prof pr(ctx, INS2D_PROF_OTHER, 1);
+    launch_correct(ctx->P, dV, ctx->dp, ctx->stO, ctx->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(V, ctx->stO, NV * sizeof(double),
+                     mem == INS2D_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return INS2D_OK;
+  API_END
+}
+
 int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4], int mem) {
   API_BEGIN
   if (check_mem(ctx, mem)) return INS2D_EINVAL;
@@ -1289,6 +1343,7 @@ int32_t ins2d_recorded_pairs(const ins2d_ctx *ctx) { return ctx ? ctx->rec_n : 0
 struct ins2d_ens {
   int device = 0;
   cudaStream_t own_stream = nullptr, stream = nullptr;
+  cudaEvent_t order_ev = nullptr;  // ins2d_ens_wait_stream
   std::vector<ins2d_ctx *> mem;
   std::vector<double *> V, p;  // member state (owned by the member contexts' allocations)
   std::vector<double> dt_member;  // per-member time step (0: the run's dt)
@@ -1625,8 +1680,9 @@ void ens_autotune(ins2d_ens *e) {
 #define ENS_BEGIN                 \
   if (!e) return INS2D_EINVAL;    \
   e->err.clear();                 \
+  DeviceGuard dguard_(e->device); \
   try {                           \
-    CK(cudaSetDevice(e->device));
+    CK(dguard_.err);
 #define ENS_END                                                     \
   }                                                                 \
   catch (const CudaError &x) {                                      \
@@ -1684,7 +1740,8 @@ int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_des
   if (rc == INS2D_OK) {
     try {
       e->device = opts[0].device;
-      CK(cudaSetDevice(e->device));
+      DeviceGuard dg(e->device);
+      CK(dg.err);
       e->fp32 = e->mem[0]->fp32;
       e->tol2 = opts[0].CG_acc * opts[0].CG_acc;
       e->maxit = opts[0].CG_maxit;
@@ -1725,9 +1782,10 @@ int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_des
 
 int ins2d_ens_destroy(ins2d_ens *e) {
   if (!e) return INS2D_OK;
-  cudaSetDevice(e->device);
+  DeviceGuard dg(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   ens_release_graphs(e);
+  if (e->order_ev) cudaEventDestroy(e->order_ev);
   if (e->h_active) cudaFreeHost(e->h_active);
   for (void *p : e->allocs) cudaFree(p);
   for (ins2d_ctx *c : e->mem) ins2d_ctx_destroy(c);
@@ -1750,6 +1808,17 @@ int ins2d_ens_set_stream(ins2d_ens *e, void *stream) {
   e->stream = stream ? (cudaStream_t)stream : e->own_stream;
   ens_release_graphs(e);
   return INS2D_OK;
+}
+
+int ins2d_ens_wait_stream(ins2d_ens *e, void *stream) {
+  ENS_BEGIN
+  const cudaStream_t other = (cudaStream_t)stream;
+  if (other == e->stream) return INS2D_OK;
+  if (!e->order_ev) CK(cudaEventCreateWithFlags(&e->order_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(e->order_ev, other));
+  CK(cudaStreamWaitEvent(e->stream, e->order_ev, 0));
+  return INS2D_OK;
+  ENS_END
 }
 
 int ins2d_ens_set_state(ins2d_ens *e, int32_t m, const double *V, const double *p, int mem) {

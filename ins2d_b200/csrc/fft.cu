@@ -710,29 +710,35 @@ bool fft_supported(int Nx, int Ny) {
 }
 
 // Opt the transform kernels in to large dynamic shared memory on the current
-// device (called once per context).
-void fft_prepare() {
+// device (called once per context); returns the first failure.
+cudaError_t fft_prepare() {
+  cudaError_t first = cudaSuccess;
+  auto opt_in = [&](const void *k) {
+    const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (first == cudaSuccess) first = e;
+  };
   for (int l = kFusedMinLog; l <= 13; ++l)
-    with_log2<kFusedMinLog>(l, [](auto c) {
+    with_log2<kFusedMinLog>(l, [&](auto c) {
       constexpr int L = decltype(c)::value;
-      cudaFuncSetAttribute(k_rows_r2c_t<L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      cudaFuncSetAttribute(k_rows_r2c_t<L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      cudaFuncSetAttribute(k_cols_t<L, cols_per_block<L>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           200 * 1024);
-      cudaFuncSetAttribute(k_rows_c2r_t<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      opt_in((const void *)k_rows_r2c_t<L, false>);
+      opt_in((const void *)k_rows_r2c_t<L, true>);
+      opt_in((const void *)k_cols_t<L, cols_per_block<L>()>);
+      opt_in((const void *)k_rows_c2r_t<L>);
     });
-  cudaFuncSetAttribute(k_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  opt_in((const void *)k_rows_r2c);
+  opt_in((const void *)k_cols);
+  opt_in((const void *)k_rows_c2r);
+  return first;
 }
 
 namespace {
-void fft_passes(const DevOps &P, const FftPlan &plan, const double *src, bool div, double alpha, double beta,
-                double gamma, double *dp, bool accumulate, cudaStream_t s) {
+cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, bool div, double alpha, double beta,
+                       double gamma, double *dp, bool accumulate, cudaStream_t s) {
   const int Nx = plan.Nx, Ny = plan.Ny;
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
-  cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
+  const cudaError_t ms = cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
+  if (ms != cudaSuccess) return ms;
   unsigned long long *maxbits = (unsigned long long *)plan.maxabs;
   // rows, real -> half spectrum
   const int fastdiv = P.rMX.lo <= 0 && P.rMX.hi >= Nx && P.rMY.lo <= 0 && P.rMY.hi >= Ny && P.rMX.two && P.rMY.two;
@@ -767,19 +773,20 @@ void fft_passes(const DevOps &P, const FftPlan &plan, const double *src, bool di
   });
   if (!fx2)
     k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0, maxbits);
+  return cudaSuccess;
 }
 }  // namespace
 
-void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
-                        cudaStream_t s) {
-  fft_passes(P, plan, f, false, 0.0, 0.0, 0.0, dp, accumulate, s);
+cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
+                               cudaStream_t s) {
+  return fft_passes(P, plan, f, false, 0.0, 0.0, 0.0, dp, accumulate, s);
 }
 
 bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= kFusedMinLog && plan.logx <= 13; }
 
-void launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha, double beta,
-                            double gamma, double *dp, bool accumulate, cudaStream_t s) {
-  fft_passes(P, plan, W, true, alpha, beta, gamma, dp, accumulate, s);
+cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
+                                   double beta, double gamma, double *dp, bool accumulate, cudaStream_t s) {
+  return fft_passes(P, plan, W, true, alpha, beta, gamma, dp, accumulate, s);
 }
 
 }  // namespace ins2d

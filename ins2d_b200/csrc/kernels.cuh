@@ -12,6 +12,24 @@ namespace ins2d {
 
 constexpr int kMaxStages = 8;
 
+// Makes `dev` the calling thread's current device for the lifetime of the
+// guard and restores the device that was current before (every C-ABI entry
+// point leaves the caller's current device as it found it).
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) err = cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+};
+
 // Deterministic reduction scratch: per-block partials, a completion counter
 // and the final values (written by the last block to finish).
 struct RedScratch {
@@ -108,13 +126,18 @@ bool fft_supported(int Nx, int Ny);
 std::vector<double> fft_twiddle_table(int n);
 // dp = real(ifft2(-fft2(f)./Ahat)) (pressure_poisson.m:92-104); dp += result when
 // accumulate.  Returns 0 (dp untouched / zero) when max|fhat| < 1e-14 (:21-32).
-void launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
-                        cudaStream_t s);
+// The return value is the error of the enqueued memset (kernel launch errors
+// are left to cudaGetLastError as for every launch).
+cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
+                               cudaStream_t s);
 // Same with the right-hand side f = (M W + alpha yM + beta ydM) gamma computed
 // inside the first pass (only when fft_fuses_div(plan): power-of-two rows >= 64).
 bool fft_fuses_div(const FftPlan &plan);
-void launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha, double beta,
-                            double gamma, double *dp, bool accumulate, cudaStream_t s);
+cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
+                                   double beta, double gamma, double *dp, bool accumulate, cudaStream_t s);
+// Opts the transform kernels in to large dynamic shared memory on the current
+// device; returns the first failure.
+cudaError_t fft_prepare();
 
 // --- PCG (pcg.cu) ---------------------------------------------------------------
 struct PcgScalars {

@@ -11,9 +11,9 @@
 //
 // The reference preconditions with a diagonal incomplete Cholesky factor
 // whose forward/backward sweeps are sequential (cg.F:317-390).  Here the
-// preconditioner is the diagonal of A (Jacobi), which is parallel; iteration
-// counts therefore differ from the reference, the converged solution agrees
-// to the stated tolerance.
+// preconditioner is a multigrid V-cycle (mg.cuh, the default) or the
+// diagonal of A (Jacobi), both parallel; iteration counts therefore differ
+// from the reference, the converged solution agrees to the stated tolerance.
 //
 // Three kernels per iteration (SpMV + p'q; x/r update + r'r, r'z and the
 // norm2 extrema; p update); scalars live on the device and each kernel's last

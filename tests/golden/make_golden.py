@@ -1,6 +1,7 @@
 """Extracts the reference's logged per-step results into small fixtures.
 
-Reads (only in the build container, where the reference checkout exists):
+Reads, from the reference checkout named by the INS2D_REFERENCE environment
+variable (required; the script stops with an error when it is unset):
   results/LDC_unsteady_1.000e+02_20x20_0/convergence.txt
   results/shear_layer01/convergence.txt
 and writes tests/golden/{ldc_re100_20x20,shear_layer_40x40}.json with the
@@ -16,7 +17,6 @@ import json
 import os
 import sys
 
-REF = os.environ.get("INS2D_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 LOGS = {
@@ -36,6 +36,9 @@ def parse(path):
 
 
 def main():
+    REF = os.environ.get("INS2D_REFERENCE")
+    if not REF or not os.path.isdir(REF):
+        sys.exit("make_golden.py: set INS2D_REFERENCE to the reference checkout (the directory holding results/)")
     for out, rel in LOGS.items():
         rows = parse(os.path.join(REF, rel))
         with open(os.path.join(HERE, out), "w") as fh:

@@ -19,7 +19,11 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.mark.parametrize("Nx,Ny,Lx,Ly", [(256, 128, 2 * np.pi, 1.0), (40, 40, 1.0, 1.0)])
+# sizes at the static scratch's limits: the longest rows and columns (4096)
+# at the cell limit 2^20, the largest size of the generic (non-power-of-two)
+# transform, and a generic size close to the cell limit
+@pytest.mark.parametrize("Nx,Ny,Lx,Ly", [(256, 128, 2 * np.pi, 1.0), (40, 40, 1.0, 1.0), (4096, 256, 4.0, 1.0),
+                                         (256, 4096, 1.0, 4.0), (2048, 512, 2.0, 1.0), (1536, 640, 3.0, 1.25)])
 def test_noalloc_matches_context_path(Nx, Ny, Lx, Ly):
     import torch
     import ins2d_b200
