@@ -1,0 +1,181 @@
+"""Parity at the benchmark configurations' own sizes and run lengths, through
+the C-ABI, against the oracle:
+
+  lid-driven cavity 64x64, Re=1000, RK44, dt=1e-3, 1000 steps, PCG to 1e-12
+      vs the scipy restatement (direct solves), at steps 100 and 1000;
+  inviscid Taylor-Green 512x512 on [0,2pi]^2, RK44, dt=1e-3, 2000 steps, FFT
+      vs the OpenMP C restatement: the same kinetic-energy drift
+      (check_conservation.m:62-76) and max|div| < 1e-12 throughout;
+  decaying turbulence 2048x2048, Re=2000, CFL 0.5, FFT, 10 FP64 steps from the
+      seeded spectral initial field vs the C restatement at 1e-12;
+  the same turbulence over 1000 steps with FP32 stencils against the FP64
+      path: kinetic-energy deviation below 1e-6 (velocity deviation reported);
+  the 256-member ensemble of tanh-stretched cavities and channels (seed 4),
+      5 steps: every member against its own single-context run, and eight
+      members (both boundary kinds, the smallest and largest grids) against
+      the scipy restatement directly.
+
+Each case runs well under a minute on one B200 plus its CPU oracle."""
+import numpy as np
+import pytest
+
+from oracle import ins2d_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_ldc64_1000_steps():
+    import ins2d_b200
+    from ins2d_b200 import cases
+    x = cases.uniform_grid(64, 0.0, 1.0)
+    uBC = cases.lid_uBC(1.0, 1.0)
+    o = R.make_options(x, x.copy(), cases.BC_CAVITY, Re=1000.0, poisson=1, uBC=uBC, RK="RK44")
+    m = ins2d_b200.Options(x, x.copy(), cases.BC_CAVITY, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=20000,
+                           uBC=uBC, RK="RK44")
+    dt = 1e-3
+    V = np.zeros(o.grid.NV)
+    p = R.pressure_additional_solve(V, np.zeros(o.grid.Np), 0.0, o)
+    Vg, pg = V.copy(), p.copy()
+    n = 0
+    for target in (100, 1000):
+        Vg, pg = m.time_ERK(Vg, pg, n * dt, dt, nsteps=target - n)
+        while n < target:
+            V, p = R.time_ERK(V, p, n * dt, dt, o)
+            n += 1
+        err = _rel(Vg, V)
+        print(f"ldc64 step {target}: velocity rel {err:.3e}, pressure rel {_rel(pg - pg.mean(), p - p.mean()):.3e}")
+        assert err < 1e-10, target
+        assert m.check_conservation(Vg, target * dt)[0] < 1e-12
+
+
+def test_tg512_2000_steps_energy():
+    import ins2d_b200
+    from ins2d_b200 import cases
+    N, dt, nsteps = 512, 1e-3, 2000
+    L = 2 * np.pi
+    x = cases.uniform_grid(N, 0.0, L)
+    m = ins2d_b200.Options(x, x.copy(), cases.BC_PERIODIC, Re=1e100, poisson=6)
+    V0 = cases.taylor_green(m)
+    p0 = np.zeros(m.Np)
+    k0 = m.check_conservation(V0, 0.0)[3]
+    Vg, pg = V0.copy(), p0.copy()
+    chunk = 500
+    for c in range(nsteps // chunk):
+        Vg, pg = m.time_ERK(Vg, pg, c * chunk * dt, dt, nsteps=chunk)
+        assert m.check_conservation(Vg, (c + 1) * chunk * dt)[0] < 1e-12
+    Vc, pc = R.erk_periodic_c(V0, p0, N, N, L, L, 1e100, dt, nsteps)
+    kg = m.check_conservation(Vg, nsteps * dt)[3]
+    kc = m.check_conservation(Vc, nsteps * dt)[3]
+    print(f"tg512 2000 steps: energy drift GPU {(kg - k0) / k0:.3e}, C oracle {(kc - k0) / k0:.3e}, "
+          f"velocity rel {_rel(Vg, Vc):.3e}")
+    assert abs((kg - k0) - (kc - k0)) <= 1e-14 * k0
+    assert abs(kg - k0) <= 1e-9 * k0  # RK4's O(dt^5) per-step energy error, no blow-up
+    assert _rel(Vg, Vc) < 1e-11
+
+
+def _turbulence(precision="fp64"):
+    import ins2d_b200
+    from ins2d_b200 import cases
+    x = cases.uniform_grid(2048, 0.0, 1.0)
+    m = ins2d_b200.Options(x, x.copy(), cases.BC_PERIODIC, Re=2000.0, poisson=6, precision=precision)
+    return m
+
+
+def test_turb2048_fp64_vs_c_oracle():
+    import torch
+    from ins2d_b200 import cases
+    m = _turbulence()
+    V0 = cases.decaying_turbulence_ic(m, k0=10.0, seed=2048)
+    dt = cases.cfl_dt(m, V0, 0.5)
+    p0 = m.pressure_additional_solve(V0, np.zeros(m.Np), 0.0)
+    Vd = torch.tensor(V0, dtype=torch.float64, device="cuda")
+    pd = torch.tensor(p0, dtype=torch.float64, device="cuda")
+    m.time_ERK(Vd, pd, 0.0, dt, nsteps=10)
+    Vc, pc = R.erk_periodic_c(V0, p0, 2048, 2048, 1.0, 1.0, 2000.0, dt, 10)
+    err = _rel(Vd.cpu().numpy(), Vc)
+    perr = _rel(pd.cpu().numpy() - pd.mean().item(), pc - pc.mean())
+    print(f"turb2048 10 FP64 steps vs C oracle: velocity rel {err:.3e}, pressure rel {perr:.3e}")
+    assert err < 1e-12
+    assert perr < 1e-10
+
+
+def test_turb2048_fp32_1000_steps():
+    import torch
+    from ins2d_b200 import cases
+    m64 = _turbulence("fp64")
+    m32 = _turbulence("fp32")
+    V0 = cases.decaying_turbulence_ic(m64, k0=10.0, seed=2048)
+    dt = cases.cfl_dt(m64, V0, 0.5)
+    p0 = m64.pressure_additional_solve(V0, np.zeros(m64.Np), 0.0)
+    k0 = m64.check_conservation(V0, 0.0)[3]
+    runs = {}
+    for name, m in (("fp64", m64), ("fp32", m32)):
+        Vd = torch.tensor(V0, dtype=torch.float64, device="cuda")
+        pd = torch.tensor(p0, dtype=torch.float64, device="cuda")
+        m.time_ERK(Vd, pd, 0.0, dt, nsteps=1000)
+        runs[name] = (Vd, pd, m.check_conservation(Vd, 1000 * dt))
+    V64, _, c64 = runs["fp64"]
+    V32, _, c32 = runs["fp32"]
+    de = abs(c32[3] - c64[3]) / c64[3]
+    dv = float(torch.linalg.norm(V32 - V64) / torch.linalg.norm(V64))
+    print(f"turb2048 1000 steps: k0 {k0:.6e}, k64 {c64[3]:.9e}, k32 {c32[3]:.9e}, energy vs FP64 {de:.3e}, "
+          f"velocity L2 vs FP64 {dv:.3e}, max|div| FP32 {c32[0]:.2e}")
+    assert de < 1e-6
+    assert dv < 1e-4
+    assert c32[0] < 1e-12  # the FP64 projection keeps the FP32-stencil run divergence-free
+
+
+def test_ensemble256_members():
+    import ins2d_b200
+    from ins2d_b200 import ensembles
+    members = ensembles.random_members(256, seed=4, CG_acc=1e-10)
+    dt, nsteps = 5e-4, 5
+    ens = ins2d_b200.Ensemble(members)
+    dts = []
+    for k, kw in enumerate(members):
+        dtm = min(dt, ensembles.stable_dt(kw, kw["_U"]))
+        dts.append(dtm)
+        if dtm < dt:
+            ens.set_member_dt(k, dtm)
+        o = ens.member(k)
+        ens.set_state(k, np.zeros(o.NV), np.zeros(o.Np))
+    stats = ens.time_ERK(0.0, dt, nsteps)
+    worst = 0.0
+    for k, kw in enumerate(members):
+        single = ins2d_b200.Options(**{a: b for a, b in kw.items() if not a.startswith("_")})
+        V0 = np.zeros(single.NV)
+        Vs, ps = single.time_ERK(V0, np.zeros(single.Np), 0.0, dts[k], nsteps=nsteps)
+        Ve, pe = ens.get_state(k)
+        e = np.max(np.abs(Ve - Vs)) / max(np.max(np.abs(Vs)), 1e-30)
+        worst = max(worst, e)
+        assert e <= 1e-10, k
+        assert stats[k]["n_solves"] == 4 * nsteps
+        single.close()
+    # eight members against the oracle: both kinds, smallest and largest grids
+    cells = [ensembles.member_cost(kw) for kw in members]
+    cav = [k for k in range(256) if k % 2 == 0]
+    chan = [k for k in range(256) if k % 2 == 1]
+    pick = set()
+    for group in (cav, chan):
+        by = sorted(group, key=lambda k: cells[k])
+        pick.update(by[:2] + by[-2:])
+    worst_o = 0.0
+    for k in sorted(pick):
+        kw = members[k]
+        o = R.make_options(kw["x"], kw["y"], kw["BC"], Re=kw["Re"], poisson=1, uBC=kw["uBC"], RK="RK44")
+        V, p = np.zeros(o.grid.NV), np.zeros(o.grid.Np)
+        for n in range(nsteps):
+            V, p = R.time_ERK(V, p, n * dts[k], dts[k], o)
+        Ve, _ = ens.get_state(k)
+        e = _rel(Ve, V)
+        worst_o = max(worst_o, e)
+        assert e < 1e-8, (k, e)
+    print(f"ens256: worst member vs single context {worst:.3e}; worst of {len(pick)} members vs oracle "
+          f"{worst_o:.3e}")
+    ens.close()
