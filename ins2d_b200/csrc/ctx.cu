@@ -50,6 +50,10 @@ struct ins2d_ctx {
   bool need_store[kMaxStages] = {};
   // device work arrays
   double *Vs = nullptr, *Wt = nullptr, *kV[kMaxStages] = {};
+  // FP32 storage of the stage quantities (FP32-stencil contexts): the stage
+  // velocity, each stage's kV and the combined Vtemp
+  bool store32 = false;
+  float *Vs32 = nullptr, *kV32[kMaxStages] = {}, *Vt32 = nullptr;
   double *f = nullptr, *dp = nullptr, *wres = nullptr;
   double *stV = nullptr, *stC = nullptr, *stO = nullptr, *stP = nullptr, *stQ = nullptr;  // host-mode staging
   double *bcblob = nullptr;
@@ -447,6 +451,24 @@ int solve_div(ins2d_ctx *c, const double *W, double alpha, double beta, double g
   return solve(c, c->f, dp, accumulate, st);
 }
 
+// the same with W = Vn sv + sa T, T in FP32 (FP32-storage stages)
+int solve_div_split(ins2d_ctx *c, const double *Vn, const float *T, double sv, double sa, double alpha, double beta,
+                    double gamma, double *dp, bool accumulate, ins2d_solve_stats *st) {
+  if (c->poisson == INS2D_POISSON_FFT && fft_fuses_div(c->fft)) {
+    if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
+    Prof pr(c, INS2D_PROF_POISSON, 3);
+    CK(launch_fft_poisson_div_split(c->P, c->fft, Vn, T, sv, sa, alpha, beta, gamma, dp, accumulate, c->stream));
+    CK(cudaGetLastError());
+    return INS2D_OK;
+  }
+  {
+    Prof pr(c, INS2D_PROF_DIV, 1);
+    launch_div_split(c->P, Vn, T, sv, sa, alpha, beta, gamma, c->f, c->stream);
+  }
+  CK(cudaGetLastError());
+  return solve(c, c->f, dp, accumulate, st);
+}
+
 void stats_add(ins2d_step_stats *s, const ins2d_solve_stats &o) {
   if (!s) return;
   s->n_solves += 1;
@@ -467,12 +489,14 @@ int sample_bc(ins2d_ctx *c, double t) {
 // kV_next is given it also receives Om^-1 R(V) (the next step's first-stage
 // right-hand side).
 int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_solve_stats *st,
-                     double *kV_next = nullptr) {
+                     bool cache = false) {
   int rc = sample_bc(c, t);
   if (rc) return rc;
   {
     Prof pr(c, INS2D_PROF_RESIDUAL, 1);
-    launch_residual(c->P, V, p, c->wres, kV_next, c->fp32, c->stream);
+    double *kn = (cache && !c->store32) ? c->kV[0] : nullptr;
+    float *kn32 = (cache && c->store32) ? c->kV32[0] : nullptr;
+    launch_residual(c->P, V, p, c->wres, kn, kn32, c->fp32, c->stream);
   }
   return solve_div(c, c->wres, 0.0, c->bcd.bc_unsteady ? 1.0 : 0.0, 1.0, p, true, st);
 }
@@ -481,8 +505,89 @@ int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_s
 // k0_cached: kV[0] already holds Om^-1 R(V) (steady BCs, the previous step of
 // the same run computed it in its additional solve); on return *cache_next
 // says whether kV[0] holds it for the next step.
+// time_ERK with FP32 storage of the stage quantities (FP32-stencil contexts):
+// the stage velocity, kV and Vtemp in FP32; Vn, p, the divergence (f =
+// (M (Vn/dt + Vtemp) + yM/dt)/c evaluated in FP64), the Poisson solve and the
+// projection (V = Vn + dt (Vtemp - c Om^-1 G dp) in FP64) as in the FP64 path.
+int erk_step32(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step_stats *stats, bool k0_cached,
+               bool *cache_next) {
+  const DevOps &P = c->P;
+  if (cache_next) *cache_next = false;
+  int rc = sample_bc(c, t);
+  if (rc) return rc;
+  const double *dpp = nullptr;
+  for (int i = 0; i < c->s; ++i) {
+    const float *Ti = nullptr;  // Vtemp_i = ai * Ti
+    double ai = 1.0;
+    if (i == 0 && k0_cached && !c->bcd.bc_unsteady) {
+      Ti = c->kV32[0];  // the previous step's residual: kV of this step's first stage
+      ai = c->A[0][0];
+    } else {
+      StageArgs a{};
+      a.V = (i == 0) ? V : nullptr;
+      a.V32 = (i == 0) ? nullptr : c->Vs32;
+      a.store32 = true;
+      a.nprev = 0;
+      for (int m = 0; m < i; ++m)
+        if (c->A[i][m] != 0.0) {
+          a.kprev32[a.nprev] = c->kV32[m];
+          a.aprev[a.nprev] = c->A[i][m];
+          ++a.nprev;
+        }
+      a.aii = c->A[i][i];
+      a.inv_dt = 1.0 / dt;
+      a.kV32 = (c->need_store[i] || a.nprev == 0) ? c->kV32[i] : nullptr;
+      a.Vt32 = a.nprev > 0 ? c->Vt32 : nullptr;
+      Prof pr(c, INS2D_PROF_STAGE, 1);
+      launch_stage(P, a, true, c->stream);
+      if (a.nprev > 0) {
+        Ti = c->Vt32;
+        ai = 1.0;
+      } else {
+        Ti = c->kV32[i];
+        ai = c->A[i][i];
+      }
+    }
+    const double ti = t + c->c[i] * dt;
+    if (c->bcd.bc_unsteady) {
+      rc = sample_bc(c, ti);
+      if (rc) return rc;
+    }
+    if (c->bcd.bc_unsteady || i > 0) {
+      // f = (M*(Vn/dt + Vtemp) + yM/dt)/c_i   (time_ERK.m:117)
+      ins2d_solve_stats st;
+      rc = solve_div_split(c, V, Ti, 1.0 / dt, ai, 1.0 / dt, 0.0, 1.0 / c->c[i], c->dp, false, &st);
+      if (rc) return rc;
+      stats_add(stats, st);
+      dpp = c->dp;
+    } else {
+      dpp = p;  // time_ERK.m:125-127
+    }
+    {
+      Prof pr(c, INS2D_PROF_PROJECT, 1);
+      if (i == c->s - 1)
+        launch_project32(P, V, Ti, ai, dpp, dt, c->c[i], V, c->stream);
+      else
+        launch_project32(P, V, Ti, ai, dpp, dt, c->c[i], c->Vs32, c->stream);
+    }
+    CK(cudaGetLastError());
+  }
+  if (c->bcd.bc_unsteady && !c->opts.p_add_solve) {
+    CK(cudaMemcpyAsync(p, dpp, P.Np * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));  // p = kp(:,end)
+  } else {
+    ins2d_solve_stats st;
+    const bool cache = cache_next && !c->bcd.bc_unsteady;
+    rc = additional_solve(c, V, p, t + dt, &st, cache);
+    if (rc) return rc;
+    stats_add(stats, st);
+    if (cache) *cache_next = true;
+  }
+  return INS2D_OK;
+}
+
 int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step_stats *stats, bool k0_cached,
              bool *cache_next) {
+  if (c->store32) return erk_step32(c, V, p, t, dt, stats, k0_cached, cache_next);
   const DevOps &P = c->P;
   if (cache_next) *cache_next = false;
   int rc = sample_bc(c, t);
@@ -536,7 +641,7 @@ int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step
   } else {
     ins2d_solve_stats st;
     const bool cache = cache_next && !c->bcd.bc_unsteady;
-    rc = additional_solve(c, V, p, t + dt, &st, cache ? c->kV[0] : nullptr);
+    rc = additional_solve(c, V, p, t + dt, &st, cache);
     if (rc) return rc;
     stats_add(stats, st);
     if (cache) *cache_next = true;
@@ -690,6 +795,12 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     c->Vs = dalloc<double>(c, NV);
     c->Wt = dalloc<double>(c, NV);
     for (int m = 0; m < c->s; ++m) c->kV[m] = (c->need_store[m] || m == 0) ? dalloc<double>(c, NV) : nullptr;
+    if (c->fp32) {
+      c->store32 = true;
+      c->Vs32 = dalloc<float>(c, NV);
+      c->Vt32 = dalloc<float>(c, NV);
+      for (int m = 0; m < c->s; ++m) c->kV32[m] = dalloc<float>(c, NV);
+    }
     c->wres = dalloc<double>(c, NV);
     c->f = dalloc<double>(c, Np);
     c->dp = dalloc<double>(c, Np);

@@ -63,6 +63,8 @@ struct DevOps {
   // rectangle [fbx0,fbx1) x [fby0,fby1) whose tiles lie inside all of them
   RegD rAUX, rSUX, rAUY, rSUY, rIVX, rIVY, rMXT, rAVX, rSVX, rAVY, rSVY, rIUX, rIUY, rMYT, rMX, rMY;
   int fbx0, fbx1, fby0, fby1;
+  int tile_ok;    // the interior tiles may use the shared-memory tiled walkers (FP64 fields)
+  int tile_ok32;  // ... on FP32 fields
 };
 
 // --- 1D table application ---------------------------------------------------
@@ -232,20 +234,69 @@ __device__ __forceinline__ double grad_y_fast(const DevOps &P, const double *__r
   return grad_y(P, p, i, j);
 }
 
+// Sources of the velocity-sized field W whose divergence a solve takes:
+// W itself (FP64), or W = Vn * sv + sa * T with T stored in FP32 (the
+// FP32-storage stages: Vn/dt + Vtemp, evaluated in FP64).
+struct WPlain {
+  const double *W;
+  __device__ __forceinline__ double operator()(long long k) const { return __ldg(W + k); }
+};
+struct WSplit {
+  const double *Vn;
+  const float *T;
+  double sv, sa;
+  __device__ __forceinline__ double operator()(long long k) const {
+    return __ldg(Vn + k) * sv + sa * (double)__ldg(T + k);
+  }
+};
+template <class F>
+__device__ __forceinline__ double reg_x_f(const RegD &r, int row, const F &f, long long base) {
+  const int c0 = wrapn(row + r.s, r.n);
+  double a = __ldg(r.w0 + row) * f(base + c0);
+  if (r.two) a += __ldg(r.w1 + row) * f(base + wrapn(c0 + 1, r.n));
+  return a;
+}
+template <class F>
+__device__ __forceinline__ double reg_y_f(const RegD &r, int row, const F &f, long long base, int stride, int i) {
+  const int c0 = wrapn(row + r.s, r.n);
+  double a = __ldg(r.w0 + row) * f(base + (long long)c0 * stride + i);
+  if (r.two) a += __ldg(r.w1 + row) * f(base + (long long)wrapn(c0 + 1, r.n) * stride + i);
+  return a;
+}
+template <class F>
+__device__ __forceinline__ double tab_x_f(const Tab &T, int r, const F &f, long long base) {
+  const int32_t *c = T.c + kT * r;
+  const double *w = T.w + kT * r;
+  return __ldg(w) * f(base + __ldg(c)) + __ldg(w + 1) * f(base + __ldg(c + 1)) + __ldg(w + 2) * f(base + __ldg(c + 2));
+}
+template <class F>
+__device__ __forceinline__ double tab_y_f(const Tab &T, int r, const F &f, long long base, int stride, int i) {
+  const int32_t *c = T.c + kT * r;
+  const double *w = T.w + kT * r;
+  return __ldg(w) * f(base + (long long)__ldg(c) * stride + i) + __ldg(w + 1) * f(base + (long long)__ldg(c + 1) * stride + i) +
+         __ldg(w + 2) * f(base + (long long)__ldg(c + 2) * stride + i);
+}
+
 // f(i,j) = (M W + alpha yM + beta ydM)(i,j) * gamma
-__device__ __forceinline__ double div_cell(const DevOps &P, const double *__restrict__ W, double alpha, double beta,
-                                           double gamma, int i, int j) {
+template <class F>
+__device__ __forceinline__ double div_cell_f(const DevOps &P, const F &W, double alpha, double beta, double gamma,
+                                             int i, int j) {
   double d;
   if (in_reg(P.rMX, i) && in_reg(P.rMY, j)) {
     // interior cell: regular rows of Mx and My, no boundary contribution
-    d = __ldg(P.hy + j) * reg_x(P.rMX, i, W, (long long)j * P.Nux) +
-        __ldg(P.hx + i) * reg_y(P.rMY, j, W + P.Nu, P.Nvx, i);
+    d = __ldg(P.hy + j) * reg_x_f(P.rMX, i, W, (long long)j * P.Nux) +
+        __ldg(P.hx + i) * reg_y_f(P.rMY, j, W, P.Nu, P.Nvx, i);
   } else {
-    d = div_in(P, W, W + P.Nu, i, j);
+    d = __ldg(P.hy + j) * tab_x_f(P.MX, i, W, (long long)j * P.Nux) +
+        __ldg(P.hx + i) * tab_y_f(P.MY, j, W, P.Nu, P.Nvx, i);
     if (alpha != 0.0) d += alpha * div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j);
     if (beta != 0.0) d += beta * div_bc(P, P.bc.dudtLe_i, P.bc.dudtRi_i, P.bc.dvdtLo_i, P.bc.dvdtUp_i, i, j);
   }
   return d * gamma;
+}
+__device__ __forceinline__ double div_cell(const DevOps &P, const double *__restrict__ W, double alpha, double beta,
+                                           double gamma, int i, int j) {
+  return div_cell_f(P, WPlain{W}, alpha, beta, gamma, i, j);
 }
 
 __device__ __forceinline__ double lap(const DevOps &P, const double *__restrict__ p, int i, int j) {

@@ -467,23 +467,33 @@ __device__ __forceinline__ void dit_passes(double2 *a, int ld, int lines, const 
 // fastdiv: every cell is a regular two-point row of Mx and My (the periodic
 // grids this solver takes): the row weights of j0, j1 and the three v rows
 // they share are set up once, the column weights once per column.
-template <int L, bool DIV>
+// SRC 0: the rows of f; 1: the divergence of W = f; 2: the divergence of
+// W = ws.Vn ws.sv + ws.sa ws.T (FP32-storage stages)
+template <int L, int SRC>
 __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
-    k_rows_r2c_t(int Ny, const double2 *__restrict__ tw, const double *__restrict__ f, double2 *__restrict__ spec,
-                 const __grid_constant__ DevOps P, double alpha, double beta, double gamma, int fastdiv) {
+    k_rows_r2c_t(int Ny, const double2 *__restrict__ tw, const double *__restrict__ f, const WSplit ws,
+                 double2 *__restrict__ spec, const __grid_constant__ DevOps P, double alpha, double beta,
+                 double gamma, int fastdiv) {
   constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
+  constexpr bool DIV = SRC != 0;
   extern __shared__ double2 sm[];
   const double2 *pyr = tw + N;
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
   const bool has1 = j1 < Ny;
+  auto W = [&](long long k) -> double {
+    if constexpr (SRC == 2)
+      return ws(k);
+    else
+      return __ldg(f + k);
+  };
   if (DIV && fastdiv) {
-    const double *u = f, *v = f + P.Nu;
     const double hy0 = __ldg(P.hy + j0), hy1 = has1 ? __ldg(P.hy + j1) : 0.0;
     const double m00 = __ldg(P.rMY.w0 + j0), m01 = __ldg(P.rMY.w1 + j0);
     const double m10 = has1 ? __ldg(P.rMY.w0 + j1) : 0.0, m11 = has1 ? __ldg(P.rMY.w1 + j1) : 0.0;
     const int r0 = wrapn(j0 + P.rMY.s, P.rMY.n), r1 = wrapn(r0 + 1, P.rMY.n), r2 = wrapn(r1 + 1, P.rMY.n);
-    const double *ua = u + (long long)j0 * P.Nux, *ub = u + (long long)(has1 ? j1 : j0) * P.Nux;
-    const double *va = v + (long long)r0 * P.Nvx, *vb = v + (long long)r1 * P.Nvx, *vc = v + (long long)r2 * P.Nvx;
+    const long long ua = (long long)j0 * P.Nux, ub = (long long)(has1 ? j1 : j0) * P.Nux;
+    const long long va = P.Nu + (long long)r0 * P.Nvx, vb = P.Nu + (long long)r1 * P.Nvx,
+                    vc = P.Nu + (long long)r2 * P.Nvx;
     for (int k = threadIdx.x; k < PER; k += kThreads) {
       double2 x[8];
 #pragma unroll
@@ -491,9 +501,9 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
         const int i = k + m * PER;
         const double w0 = __ldg(P.rMX.w0 + i), w1 = __ldg(P.rMX.w1 + i), hx = __ldg(P.hx + i);
         const int c0 = wrapn(i + P.rMX.s, P.rMX.n), c1 = wrapn(c0 + 1, P.rMX.n);
-        const double vb_i = __ldg(vb + i);
-        const double d0 = hy0 * (w0 * __ldg(ua + c0) + w1 * __ldg(ua + c1)) + hx * (m00 * __ldg(va + i) + m01 * vb_i);
-        const double d1 = hy1 * (w0 * __ldg(ub + c0) + w1 * __ldg(ub + c1)) + hx * (m10 * vb_i + m11 * __ldg(vc + i));
+        const double vb_i = W(vb + i);
+        const double d0 = hy0 * (w0 * W(ua + c0) + w1 * W(ua + c1)) + hx * (m00 * W(va + i) + m01 * vb_i);
+        const double d1 = hy1 * (w0 * W(ub + c0) + w1 * W(ub + c1)) + hx * (m10 * vb_i + m11 * W(vc + i));
         x[m] = make_double2(d0 * gamma, has1 ? d1 * gamma : 0.0);
       }
       group_dif<false>(x, 3, k, PER, pyr, false);
@@ -506,7 +516,10 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
       double2 x[8];
 #pragma unroll
       for (int m = 0; m < 8; ++m) {
-        if (DIV)
+        if constexpr (SRC == 2)
+          x[m] = make_double2(div_cell_f(P, ws, alpha, beta, gamma, k + m * PER, j0),
+                              has1 ? div_cell_f(P, ws, alpha, beta, gamma, k + m * PER, j1) : 0.0);
+        else if constexpr (SRC == 1)
           x[m] = make_double2(div_cell(P, f, alpha, beta, gamma, k + m * PER, j0),
                               has1 ? div_cell(P, f, alpha, beta, gamma, k + m * PER, j1) : 0.0);
         else
@@ -720,8 +733,9 @@ cudaError_t fft_prepare() {
   for (int l = kFusedMinLog; l <= 13; ++l)
     with_log2<kFusedMinLog>(l, [&](auto c) {
       constexpr int L = decltype(c)::value;
-      opt_in((const void *)k_rows_r2c_t<L, false>);
-      opt_in((const void *)k_rows_r2c_t<L, true>);
+      opt_in((const void *)k_rows_r2c_t<L, 0>);
+      opt_in((const void *)k_rows_r2c_t<L, 1>);
+      opt_in((const void *)k_rows_r2c_t<L, 2>);
       opt_in((const void *)k_cols_t<L, cols_per_block<L>()>);
       opt_in((const void *)k_rows_c2r_t<L>);
     });
@@ -732,8 +746,8 @@ cudaError_t fft_prepare() {
 }
 
 namespace {
-cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, bool div, double alpha, double beta,
-                       double gamma, double *dp, bool accumulate, cudaStream_t s) {
+cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, const WSplit *ws, bool div,
+                       double alpha, double beta, double gamma, double *dp, bool accumulate, cudaStream_t s) {
   const int Nx = plan.Nx, Ny = plan.Ny;
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
@@ -745,10 +759,15 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const bool fx = with_log2<kFusedMinLog>(plan.logx, [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
-    if (div)
-      k_rows_r2c_t<L, true><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, plan.spec, P, alpha, beta, gamma, fastdiv);
+    const WSplit w0{};
+    if (ws)
+      k_rows_r2c_t<L, 2><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, nullptr, *ws, plan.spec, P, alpha, beta, gamma,
+                                                     fastdiv);
+    else if (div)
+      k_rows_r2c_t<L, 1><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, alpha, beta, gamma,
+                                                     fastdiv);
     else
-      k_rows_r2c_t<L, false><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, plan.spec, P, 0.0, 0.0, 0.0, 0);
+      k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, 0.0, 0.0, 0.0, 0);
   });
   const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
   if (!fx) k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
@@ -779,14 +798,21 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
 
 cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const double *f, double *dp, bool accumulate,
                                cudaStream_t s) {
-  return fft_passes(P, plan, f, false, 0.0, 0.0, 0.0, dp, accumulate, s);
+  return fft_passes(P, plan, f, nullptr, false, 0.0, 0.0, 0.0, dp, accumulate, s);
 }
 
 bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= kFusedMinLog && plan.logx <= 13; }
 
 cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s) {
-  return fft_passes(P, plan, W, true, alpha, beta, gamma, dp, accumulate, s);
+  return fft_passes(P, plan, W, nullptr, true, alpha, beta, gamma, dp, accumulate, s);
+}
+
+cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, const double *Vn, const float *T,
+                                         double sv, double sa, double alpha, double beta, double gamma, double *dp,
+                                         bool accumulate, cudaStream_t s) {
+  const WSplit ws{Vn, T, sv, sa};
+  return fft_passes(P, plan, nullptr, &ws, true, alpha, beta, gamma, dp, accumulate, s);
 }
 
 }  // namespace ins2d

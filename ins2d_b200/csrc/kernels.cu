@@ -47,16 +47,15 @@ __global__ void __launch_bounds__(256) k_F(const __grid_constant__ DevOps P, con
   grid_reduce<1>(mx, ops, red);
 }
 
-template <bool WANTMAX>
-__global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, const double *__restrict__ W,
-                                            double alpha, double beta, double gamma, double *__restrict__ f,
-                                            const RedScratch red) {
+template <bool WANTMAX, class F>
+__global__ void __launch_bounds__(256) k_div(const __grid_constant__ DevOps P, const F W, double alpha, double beta,
+                                            double gamma, double *__restrict__ f, const RedScratch red) {
   const int i = blockIdx.x * BX + threadIdx.x;
   const int j = blockIdx.y * BY + threadIdx.y;
   double mx[1] = {0.0};
   const int ops[1] = {R_MAX};
   if (i < P.Npx && j < P.Npy) {
-    const double d = div_cell(P, W, alpha, beta, gamma, i, j);
+    const double d = div_cell_f(P, W, alpha, beta, gamma, i, j);
     f[(long long)j * P.Npx + i] = d;
     mx[0] = fabs(d);
   }
@@ -91,6 +90,30 @@ __global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps 
   const int j0 = blockIdx.y * (BY * kProjRows) + threadIdx.y;
 #pragma unroll
   for (int r = 0; r < kProjRows; ++r) project_cell(P, Wt, dp, dt, c, Vo, i, j0 + r * BY);
+}
+
+// FP32-storage stages: V_out = Vn + dt (a T - c Om^-1 G dp) in FP64 (T = the
+// stage's Vtemp / a), stored as TO: float for the next stage's stencils, double
+// for the new state (then V_out may be Vn itself: each point is read before it
+// is written by the same thread)
+template <typename TO>
+__global__ void __launch_bounds__(256) k_project32(const __grid_constant__ DevOps P, const double *Vn,
+                                                  const float *__restrict__ T, double a, const double *__restrict__ dp,
+                                                  double dt, double c, TO *Vo) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j0 = blockIdx.y * (BY * kProjRows) + threadIdx.y;
+#pragma unroll
+  for (int r = 0; r < kProjRows; ++r) {
+    const int j = j0 + r * BY;
+    if (i < P.Nux && j < P.Nuy) {
+      const long long idx = (long long)j * P.Nux + i;
+      Vo[idx] = (TO)(Vn[idx] + dt * (a * (double)T[idx] - c * om_inv_u(P, i, j) * grad_x_fast(P, dp, i, j)));
+    }
+    if (i < P.Nvx && j < P.Nvy) {
+      const long long idx = P.Nu + (long long)j * P.Nvx + i;
+      Vo[idx] = (TO)(Vn[idx] + dt * (a * (double)T[idx] - c * om_inv_v(P, i, j) * grad_y_fast(P, dp, i, j)));
+    }
+  }
 }
 
 __global__ void __launch_bounds__(256) k_correct(const __grid_constant__ DevOps P, const double *__restrict__ Vi,
@@ -212,9 +235,15 @@ void launch_div(const DevOps &P, const double *W, double alpha, double beta, dou
                 bool want_max, const RedScratch &red, cudaStream_t s) {
   dim3 g = grid_for(P.Npx, P.Npy);
   if (want_max)
-    k_div<true><<<g, dim3(BX, BY), 0, s>>>(P, W, alpha, beta, gamma, f, red);
+    k_div<true><<<g, dim3(BX, BY), 0, s>>>(P, WPlain{W}, alpha, beta, gamma, f, red);
   else
-    k_div<false><<<g, dim3(BX, BY), 0, s>>>(P, W, alpha, beta, gamma, f, red);
+    k_div<false><<<g, dim3(BX, BY), 0, s>>>(P, WPlain{W}, alpha, beta, gamma, f, red);
+}
+
+void launch_div_split(const DevOps &P, const double *Vn, const float *T, double sv, double sa, double alpha,
+                      double beta, double gamma, double *f, cudaStream_t s) {
+  k_div<false><<<grid_for(P.Npx, P.Npy), dim3(BX, BY), 0, s>>>(P, WSplit{Vn, T, sv, sa}, alpha, beta, gamma, f,
+                                                                RedScratch{});
 }
 
 void launch_project(const DevOps &P, const double *Wt, const double *dp, double dt, double c, double *V_out,
@@ -222,6 +251,22 @@ void launch_project(const DevOps &P, const double *Wt, const double *dp, double 
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project<<<g, dim3(BX, BY), 0, s>>>(P, Wt, dp, dt, c, V_out);
+}
+
+template <typename TO>
+void launch_project32_t(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
+                        double c, TO *V_out, cudaStream_t s) {
+  const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
+  k_project32<TO><<<g, dim3(BX, BY), 0, s>>>(P, Vn, T, a, dp, dt, c, V_out);
+}
+void launch_project32(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
+                      double c, float *V_out, cudaStream_t s) {
+  launch_project32_t(P, Vn, T, a, dp, dt, c, V_out, s);
+}
+void launch_project32(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
+                      double c, double *V_out, cudaStream_t s) {
+  launch_project32_t(P, Vn, T, a, dp, dt, c, V_out, s);
 }
 
 void launch_correct(const DevOps &P, const double *V_in, const double *dp, double *V_out, cudaStream_t s) {

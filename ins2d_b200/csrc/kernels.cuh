@@ -41,7 +41,8 @@ struct RedScratch {
 constexpr int kRedQ = 6;
 
 struct StageArgs {
-  const double *V;       // velocity of this stage, V = [u; v]
+  const double *V;       // velocity of this stage, V = [u; v] (FP64), or null
+  const float *V32;      // the stage velocity in FP32 (FP32-storage contexts), or null
   const double *Vn;      // velocity at t_n
   double *kV;            // out: Om^-1 R(V) of this stage (may be null)
   const double *kprev[kMaxStages];
@@ -50,6 +51,13 @@ struct StageArgs {
   double aii;            // Butcher coefficient of this stage's own kV
   double inv_dt;
   double *Wt;            // out: Vn/dt + Vtemp
+  // FP32 storage (store32): kV32 (may be null) instead of kV, the earlier
+  // stages from kprev32, and Vtemp into Vt32 (only when nprev > 0; otherwise
+  // Vtemp = aii kV32); Vn and Wt are not used
+  bool store32;
+  float *kV32;
+  const float *kprev32[kMaxStages];
+  float *Vt32;
 };
 
 // One RK stage right-hand side: kV = Om^-1 (-conv + Diff V + yDiff - y_p),
@@ -57,10 +65,10 @@ struct StageArgs {
 void launch_stage(const DevOps &P, const StageArgs &a, bool fp32, cudaStream_t s);
 // computes P.fbx0.. (the interior tile rectangle of the stencil walkers)
 void walker_rectangle(DevOps &P);
-// w = Om^-1 (R(V) - G p) (pressure_additional_solve.m:11-13); when kV_next is
-// non-null also stores Om^-1 R(V) there.
-void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next, bool fp32,
-                     cudaStream_t s);
+// w = Om^-1 (R(V) - G p) (pressure_additional_solve.m:11-13); when kV_next
+// (kV_next32) is non-null also stores Om^-1 R(V) there (rounded to FP32).
+void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next,
+                     float *kV_next32, bool fp32, cudaStream_t s);
 // F_out = -conv(V;C) + Diff V + yDiff - (G p + y_p) (F.m); maxres into red.result[0]
 void launch_F(const DevOps &P, const double *V, const double *C, const double *p, double *F_out,
               const RedScratch &red, cudaStream_t s);
@@ -71,6 +79,16 @@ void launch_div(const DevOps &P, const double *W, double alpha, double beta, dou
 // V_out = dt*(Wt - c*Om^-1*G*dp)   (time_ERK.m:132 with Vn/dt folded into Wt)
 void launch_project(const DevOps &P, const double *Wt, const double *dp, double dt, double c, double *V_out,
                     cudaStream_t s);
+// FP32-storage contexts: f = (M (Vn sv + sa T) + alpha yM + beta ydM) gamma
+// with T in FP32 (the stage's Vtemp or kV), evaluated in FP64
+void launch_div_split(const DevOps &P, const double *Vn, const float *T, double sv, double sa, double alpha,
+                      double beta, double gamma, double *f, cudaStream_t s);
+// FP32-storage contexts: V_out = Vn + dt (a T - c Om^-1 G dp) (time_ERK.m:132),
+// into the FP32 stage velocity or the FP64 new state (V_out may be Vn)
+void launch_project32(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
+                      double c, float *V_out, cudaStream_t s);
+void launch_project32(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
+                      double c, double *V_out, cudaStream_t s);
 // V_out = V_in - Om^-1 G dp   (input_check.m:107)
 void launch_correct(const DevOps &P, const double *V_in, const double *dp, double *V_out, cudaStream_t s);
 void launch_lap(const DevOps &P, const double *p, double *Ap, cudaStream_t s);
@@ -135,6 +153,10 @@ cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const doubl
 bool fft_fuses_div(const FftPlan &plan);
 cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s);
+// Same with W = Vn sv + sa T, T in FP32 (FP32-storage stages)
+cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, const double *Vn, const float *T,
+                                         double sv, double sa, double alpha, double beta, double gamma, double *dp,
+                                         bool accumulate, cudaStream_t s);
 // Opts the transform kernels in to large dynamic shared memory on the current
 // device; returns the first failure.
 cudaError_t fft_prepare();

@@ -20,7 +20,7 @@ namespace {
 
 // launch shape (compile-time tunables)
 #ifndef INS2D_WALK_RUN
-#define INS2D_WALK_RUN 16
+#define INS2D_WALK_RUN 32
 #endif
 #ifndef INS2D_WALK_MINB
 #define INS2D_WALK_MINB 5
@@ -70,8 +70,8 @@ template <typename S>
 struct Trip {
   S a0, a1, a2;
 };
-template <typename S>
-__device__ __forceinline__ Trip<S> load3(const double *__restrict__ row, const XRow<S> &x) {
+template <typename S, typename TV>
+__device__ __forceinline__ Trip<S> load3(const TV *__restrict__ row, const XRow<S> &x) {
   Trip<S> t;
   t.a0 = S(__ldg(row + x.c0));
   t.a1 = S(__ldg(row + x.c1));
@@ -110,7 +110,11 @@ __device__ __forceinline__ YRow<S> yrow(const Tab &T, int r) {
 }
 
 struct Epi {
-  int mode;  // 0: RK stage, 1: residual of the additional solve
+  // 0: RK stage, FP64 storage (kV, Wt = Vn/dt + Vtemp);
+  // 1: residual of the additional solve;
+  // 2: RK stage, FP32 storage (kV32 and, when the stage combines earlier
+  //    stages, Vt32 = Vtemp; Vn and Wt are not touched)
+  int mode;
   // stage
   const double *Vn;
   double *kV;
@@ -119,14 +123,33 @@ struct Epi {
   int nprev;
   double aii, inv_dt;
   double *Wt;
+  float *kV32;
+  const float *kprev32[kMaxStages];
+  float *Vt32;
   // residual
   const double *p;
   double *w;
   double *kV_next;
+  float *kV_next32;
 };
+
+__device__ __forceinline__ void epi_stage32(const Epi &e, long long idx, double k) {
+  const float kf = (float)k;
+  if (e.kV32) e.kV32[idx] = kf;
+  if (e.Vt32) {
+    double vt = 0.0;
+    for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * (double)__ldg(e.kprev32[m] + idx);
+    vt += e.aii * (double)kf;
+    e.Vt32[idx] = (float)vt;
+  }
+}
 
 __device__ __forceinline__ void epilogue_stage(const Epi &e, long long idx, double oi, double R) {
   const double k = oi * R;
+  if (e.mode == 2) {
+    epi_stage32(e, idx, k);
+    return;
+  }
   if (e.kV) e.kV[idx] = k;
   double vt = 0.0;
   for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * e.kprev[m][idx];
@@ -134,10 +157,16 @@ __device__ __forceinline__ void epilogue_stage(const Epi &e, long long idx, doub
   e.Wt[idx] = e.Vn[idx] * e.inv_dt + vt;
 }
 
+__device__ __forceinline__ void epi_residual(const Epi &e, long long idx, double oi, double R, double g) {
+  e.w[idx] = oi * (R - g);
+  if (e.kV_next) e.kV_next[idx] = oi * R;
+  if (e.kV_next32) e.kV_next32[idx] = (float)(oi * R);
+}
+
 // ---------------------------------------------------------------------------
 // u walker
-template <typename S>
-__device__ void walk_u(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+template <typename S, typename TV>
+__device__ void walk_u(const DevOps &P, const TV *__restrict__ u, const TV *__restrict__ v, const Epi &e,
                        int i, int j0, int j1) {
   if (i >= P.Nux) return;
   j1 = min(j1, P.Nuy);
@@ -175,7 +204,7 @@ __device__ void walk_u(const DevOps &P, const double *__restrict__ u, const doub
   for (int j = j0; j < j1; ++j) {
     S uy1, sy1, vf1;
     face(j + 1, uy1, sy1, vf1);
-    const double *__restrict__ row = u + (long long)j * P.Nux;
+    const TV *__restrict__ row = u + (long long)j * P.Nux;
     const S ule = S(__ldg(P.bc.uLe_i + j)), uri = S(__ldg(P.bc.uRi_i + j));
     const Trip<S> t0 = load3(row, ax0), t1 = load3(row, ax1);
     const S uxl = dot3(ax0, t0) + ax0.b1 * ule + ax0.b2 * uri;
@@ -191,14 +220,13 @@ __device__ void walk_u(const DevOps &P, const double *__restrict__ u, const doub
     const long long idx = (long long)j * P.Nux + i;
     const double hyd = __ldg(P.hy + j);
     const double oi = __ldg(P.rhy + j) * __ldg(P.rgxi + i);
-    if (e.mode == 0) {
+    if (e.mode != 1) {
       epilogue_stage(e, idx, oi, R);
     } else {
       const double *prow = e.p + (long long)j * P.Npx;
       const double g = -hyd * (gt.w0 * __ldg(prow + gt.c0) + gt.w1 * __ldg(prow + gt.c1) +
                                (gt.w2 != 0.0 ? gt.w2 * __ldg(prow + gt.c2) : 0.0));
-      e.w[idx] = oi * (R - g);
-      if (e.kV_next) e.kV_next[idx] = oi * R;
+      epi_residual(e, idx, oi, R, g);
     }
     uy0 = uy1;
     sy0 = sy1;
@@ -208,8 +236,8 @@ __device__ void walk_u(const DevOps &P, const double *__restrict__ u, const doub
 
 // ---------------------------------------------------------------------------
 // v walker
-template <typename S>
-__device__ void walk_v(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+template <typename S, typename TV>
+__device__ void walk_v(const DevOps &P, const TV *__restrict__ u, const TV *__restrict__ v, const Epi &e,
                        int i, int j0, int j1) {
   if (i >= P.Nvx) return;
   j1 = min(j1, P.Nvy);
@@ -238,7 +266,7 @@ __device__ void walk_v(const DevOps &P, const double *__restrict__ u, const doub
   for (int j = j0; j < j1; ++j) {
     S vy1, sy1;
     face(j + 1, vy1, sy1);
-    const double *__restrict__ row = v + (long long)j * P.Nvx;
+    const TV *__restrict__ row = v + (long long)j * P.Nvx;
     const S vle = S(__ldg(P.bc.vLe_i + j)), vri = S(__ldg(P.bc.vRi_i + j));
     const Trip<S> t0 = load3(row, vx0), t1 = load3(row, vx1);
     const S vxl = dot3(vx0, t0) + vx0.b1 * vle + vx0.b2 * vri;
@@ -249,17 +277,17 @@ __device__ void walk_v(const DevOps &P, const double *__restrict__ u, const doub
     const YRow<S> iy = yrow<S>(P.IUY, j);
     S ufl = S(0), ufr = S(0);
     if (iy.w0 != S(0)) {
-      const double *ur = u + (long long)iy.c0 * P.Nux;
+      const TV *ur = u + (long long)iy.c0 * P.Nux;
       ufl += iy.w0 * dot3(ux0, load3(ur, ux0));
       ufr += iy.w0 * dot3(ux1, load3(ur, ux1));
     }
     if (iy.w1 != S(0)) {
-      const double *ur = u + (long long)iy.c1 * P.Nux;
+      const TV *ur = u + (long long)iy.c1 * P.Nux;
       ufl += iy.w1 * dot3(ux0, load3(ur, ux0));
       ufr += iy.w1 * dot3(ux1, load3(ur, ux1));
     }
     if (iy.w2 != S(0)) {
-      const double *ur = u + (long long)iy.c2 * P.Nux;
+      const TV *ur = u + (long long)iy.c2 * P.Nux;
       ufl += iy.w2 * dot3(ux0, load3(ur, ux0));
       ufr += iy.w2 * dot3(ux1, load3(ur, ux1));
     }
@@ -273,15 +301,14 @@ __device__ void walk_v(const DevOps &P, const double *__restrict__ u, const doub
     const double R = (double)(-(duvdx + dv2dy) + d2v - ypy);
     const long long idx = P.Nu + (long long)j * P.Nvx + i;
     const double oi = __ldg(P.rgyi + j) * __ldg(P.rhx + i);
-    if (e.mode == 0) {
+    if (e.mode != 1) {
       epilogue_stage(e, idx, oi, R);
     } else {
       const YRow<double> gy = yrow<double>(P.MYT, j);
       const double g = -__ldg(P.hx + i) *
                        (gy.w0 * __ldg(e.p + (long long)gy.c0 * P.Npx + i) + gy.w1 * __ldg(e.p + (long long)gy.c1 * P.Npx + i) +
                         (gy.w2 != 0.0 ? gy.w2 * __ldg(e.p + (long long)gy.c2 * P.Npx + i) : 0.0));
-      e.w[idx] = oi * (R - g);
-      if (e.kV_next) e.kV_next[idx] = oi * R;
+      epi_residual(e, idx, oi, R, g);
     }
     vy0 = vy1;
     sy0 = sy1;
@@ -302,15 +329,18 @@ __device__ __forceinline__ S rw(const double *w, int r) {
 // y-direction weights and metrics of one tile's rows, staged in shared
 // memory once per block (faces j0..j0+RUN, rows j0..j0+RUN-1): the walkers
 // read them per row without a global-memory round trip.
-struct YRows {
-  double auy0[RUN + 1], auy1[RUN + 1], suy0[RUN + 1], suy1[RUN + 1], ivy0[RUN + 1], ivy1[RUN + 1];
-  double avy0[RUN + 1], avy1[RUN + 1], svy0[RUN + 1], svy1[RUN + 1];
-  double hy[RUN], rhy[RUN], iuy0[RUN], iuy1[RUN], gyi[RUN], rgyi[RUN], myt0[RUN], myt1[RUN];
+template <int NR>
+struct YRowsN {
+  double auy0[NR + 1], auy1[NR + 1], suy0[NR + 1], suy1[NR + 1], ivy0[NR + 1], ivy1[NR + 1];
+  double avy0[NR + 1], avy1[NR + 1], svy0[NR + 1], svy1[NR + 1];
+  double hy[NR], rhy[NR], iuy0[NR], iuy1[NR], gyi[NR], rgyi[NR], myt0[NR], myt1[NR];
 };
+using YRows = YRowsN<RUN>;
 
-__device__ __forceinline__ void stage_yrows(const DevOps &P, int j0, YRows &Y) {
+template <int NR>
+__device__ __forceinline__ void stage_yrows(const DevOps &P, int j0, YRowsN<NR> &Y) {
   const int t = threadIdx.x + blockDim.x * threadIdx.y;
-  if (t <= RUN) {
+  if (t <= NR) {
     const int r = j0 + t;
     Y.auy0[t] = __ldg(P.rAUY.w0 + r);
     Y.auy1[t] = __ldg(P.rAUY.w1 + r);
@@ -323,7 +353,7 @@ __device__ __forceinline__ void stage_yrows(const DevOps &P, int j0, YRows &Y) {
     Y.svy0[t] = __ldg(P.rSVY.w0 + r);
     Y.svy1[t] = __ldg(P.rSVY.w1 + r);
   }
-  if (t < RUN) {
+  if (t < NR) {
     const int j = j0 + t;
     Y.hy[t] = __ldg(P.hy + j);
     Y.rhy[t] = __ldg(P.rhy + j);
@@ -345,8 +375,8 @@ struct URaw {
   double ep;
 };
 
-template <typename S>
-__device__ void fast_u(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+template <typename S, typename TV>
+__device__ void fast_u(const DevOps &P, const TV *__restrict__ u, const TV *__restrict__ v, const Epi &e,
                        int i, int j0, int j1, const YRows &Y) {
   const S ire = S(P.invRe);
   // columns (modulo the row length for periodic wraps)
@@ -368,11 +398,11 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
     q.f0 = S(__ldg(u + (long long)ra * Nux + i));
     q.f1 = twoAy ? S(__ldg(u + (long long)wrapn(ra + 1, P.rAUY.n) * Nux + i)) : S(0);
     const int rv = wrapn(r + sIy, P.rIVY.n);
-    const double *vr = v + (long long)rv * Nvx;
+    const TV *vr = v + (long long)rv * Nvx;
     q.va0 = S(__ldg(vr + cI0));
     q.va1 = twoIx ? S(__ldg(vr + cI1)) : S(0);
     if (twoIy) {
-      const double *vr1 = v + (long long)wrapn(rv + 1, P.rIVY.n) * Nvx;
+      const TV *vr1 = v + (long long)wrapn(rv + 1, P.rIVY.n) * Nvx;
       q.vb0 = S(__ldg(vr1 + cI0));
       q.vb1 = twoIx ? S(__ldg(vr1 + cI1)) : S(0);
     } else {
@@ -386,7 +416,7 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
     vf = S(Y.ivy0[y]) * (iv0 * q.va0 + iv1 * q.va1) + S(Y.ivy1[y]) * (iv0 * q.vb0 + iv1 * q.vb1);
   };
   auto load_row = [&](int j, URaw<S> &q) {
-    const double *row = u + (long long)j * Nux;
+    const TV *row = u + (long long)j * Nux;
     q.um = S(__ldg(row + cA0));
     q.u0 = S(__ldg(row + cA1));
     q.up = twoA ? S(__ldg(row + cA2)) : S(0);
@@ -424,10 +454,11 @@ __device__ void fast_u(const DevOps &P, const double *__restrict__ u, const doub
       for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
       vt += e.aii * k;
       e.Wt[idx] = cur.ep * e.inv_dt + vt;
+    } else if (e.mode == 2) {
+      epi_stage32(e, idx, oi * R);
     } else {
       const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
-      e.w[idx] = oi * (R - g);
-      if (e.kV_next) e.kV_next[idx] = oi * R;
+      epi_residual(e, idx, oi, R, g);
     }
     uy0 = uy1;
     sy0 = sy1;
@@ -442,8 +473,8 @@ struct VRaw {
   double ep;
 };
 
-template <typename S>
-__device__ void fast_v(const DevOps &P, const double *__restrict__ u, const double *__restrict__ v, const Epi &e,
+template <typename S, typename TV>
+__device__ void fast_v(const DevOps &P, const TV *__restrict__ u, const TV *__restrict__ v, const Epi &e,
                        int i, int j0, int j1, const YRows &Y) {
   const S ire = S(P.invRe);
   const int cV0 = wrapn(i + P.rAVX.s, P.rAVX.n), cV1 = wrapn(cV0 + 1, P.rAVX.n), cV2 = wrapn(cV1 + 1, P.rAVX.n);
@@ -471,17 +502,17 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
     sy = S(Y.svy0[y]) * q.f0 + S(Y.svy1[y]) * q.f1;
   };
   auto load_row = [&](int j, VRaw<S> &q) {
-    const double *row = v + (long long)j * Nvx;
+    const TV *row = v + (long long)j * Nvx;
     q.vm = S(__ldg(row + cV0));
     q.v0 = S(__ldg(row + cV1));
     q.vp = twoV ? S(__ldg(row + cV2)) : S(0);
     const int ru = wrapn(j + sUy, P.rIUY.n);
-    const double *ur = u + (long long)ru * Nux;
+    const TV *ur = u + (long long)ru * Nux;
     q.ua0 = S(__ldg(ur + cU0));
     q.ua1 = S(__ldg(ur + cU1));
     q.ua2 = twoUx ? S(__ldg(ur + cU2)) : S(0);
     if (twoUy) {
-      const double *ur1 = u + (long long)wrapn(ru + 1, P.rIUY.n) * Nux;
+      const TV *ur1 = u + (long long)wrapn(ru + 1, P.rIUY.n) * Nux;
       q.ub0 = S(__ldg(ur1 + cU0));
       q.ub1 = S(__ldg(ur1 + cU1));
       q.ub2 = twoUx ? S(__ldg(ur1 + cU2)) : S(0);
@@ -526,14 +557,15 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
       for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
       vt += e.aii * k;
       e.Wt[idx] = cur.ep * e.inv_dt + vt;
+    } else if (e.mode == 2) {
+      epi_stage32(e, idx, oi * R);
     } else {
       // (G p)_v = -hx MYT p with the row's weights from shared memory
       const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
       double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
       if (P.rMYT.two) gy += Y.myt1[j - j0] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
       const double g = -hxd * gy;
-      e.w[idx] = oi * (R - g);
-      if (e.kV_next) e.kV_next[idx] = oi * R;
+      epi_residual(e, idx, oi, R, g);
     }
     vy0 = vy1;
     sy0 = sy1;
@@ -541,45 +573,274 @@ __device__ void fast_v(const DevOps &P, const double *__restrict__ u, const doub
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tiled walkers for the interior tiles of single contexts.  A block of 256
+// threads takes one WX x RUN tile: the u and v rows it reads (the tile with a
+// halo of at least two points on each side, three on the right) are copied
+// into shared memory first with cp.async in 16-byte chunks -- every chunk a
+// separate asynchronous copy, so a block has its whole tile in flight at
+// once, and a periodic wrap is only a different source address per chunk --
+// then each thread walks RUN/2 rows of one column (warps 0-3: u, 4-7: v; two
+// row segments per column) with the arithmetic of fast_u / fast_v, reading
+// its stencil values from shared memory.  Requirements (checked on the
+// host): every shift of the regular rows in [-2, 1], and rows of u and v
+// that start on 16-byte boundaries (Nux, Nvx, Nu multiples of 16 bytes /
+// sizeof(TV)).
+constexpr int kTileThreads = 256;
+constexpr int kTileSeg = RUN / 2;   // rows per thread
+constexpr int kTileRows = RUN + 5;  // staged rows j0-2 .. j0+RUN+2
+
+// staged columns i0-HL .. : HL = one 16-byte chunk of halo on the left,
+// at least WX+3-... on the right, a whole number of chunks per row
+template <typename TV>
+struct TileGeo {
+  static constexpr int EPC = 16 / (int)sizeof(TV);            // elements per chunk
+  static constexpr int HL = EPC;                              // left halo (>= 2)
+  static constexpr int COLS = ((HL + WX + 3 + EPC - 1) / EPC) * EPC;
+  static constexpr int CHUNKS = COLS / EPC;
+};
+
+template <typename TV>
+struct TileSm {
+  TV u[kTileRows][TileGeo<TV>::COLS];
+  TV v[kTileRows][TileGeo<TV>::COLS];
+};
+
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ int wrapm(int x, int n) {
+  x %= n;
+  return x < 0 ? x + n : x;
+}
+
+// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
+template <typename S, int MODE, typename TV>
+__device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
+                       const YRowsN<RUN> &Y) {
+  const S ire = S(P.invRe);
+  const int ci = i - i0 + TileGeo<TV>::HL;  // shared-memory column of u(i, .)
+  const int cA0 = ci + P.rAUX.s, cA1 = cA0 + 1, cA2 = cA1 + 1;
+  const int cI0 = ci + P.rIVX.s, cI1 = cI0 + 1;
+  const S a00 = rw<S>(P.rAUX.w0, i), a01 = rw<S>(P.rAUX.w1, i);
+  const S a10 = rw<S>(P.rAUX.w0, i + 1), a11 = rw<S>(P.rAUX.w1, i + 1);
+  const S s00 = rw<S>(P.rSUX.w0, i), s01 = rw<S>(P.rSUX.w1, i);
+  const S s10 = rw<S>(P.rSUX.w0, i + 1), s11 = rw<S>(P.rSUX.w1, i + 1);
+  const S iv0 = rw<S>(P.rIVX.w0, i), iv1 = rw<S>(P.rIVX.w1, i);
+  const S gx = S(__ldg(P.gxi + i));
+  const double rgx = __ldg(P.rgxi + i);
+  const bool twoA = P.rAUX.two, twoAy = P.rAUY.two, twoIx = P.rIVX.two, twoIy = P.rIVY.two;
+  const int sAy = P.rAUY.s - j0 + 2, sIy = P.rIVY.s - j0 + 2;  // shared-memory row of field row r: r + s
+  auto face = [&](int r, S &uy, S &sy, S &vf) {
+    const int y = r - j0;
+    const int ra = r + sAy, rv = r + sIy;
+    const S f0 = S(T.u[ra][ci]);
+    const S f1 = twoAy ? S(T.u[ra + 1][ci]) : S(0);
+    const S va0 = S(T.v[rv][cI0]);
+    const S va1 = twoIx ? S(T.v[rv][cI1]) : S(0);
+    S vb0 = S(0), vb1 = S(0);
+    if (twoIy) {
+      vb0 = S(T.v[rv + 1][cI0]);
+      vb1 = twoIx ? S(T.v[rv + 1][cI1]) : S(0);
+    }
+    uy = S(Y.auy0[y]) * f0 + S(Y.auy1[y]) * f1;
+    sy = S(Y.suy0[y]) * f0 + S(Y.suy1[y]) * f1;
+    vf = S(Y.ivy0[y]) * (iv0 * va0 + iv1 * va1) + S(Y.ivy1[y]) * (iv0 * vb0 + iv1 * vb1);
+  };
+  S uy0, sy0, vf0;
+  face(ja, uy0, sy0, vf0);
+#pragma unroll 2
+  for (int j = ja; j < jb; ++j) {
+    S uy1, sy1, vf1;
+    face(j + 1, uy1, sy1, vf1);
+    const int rr = j - j0 + 2;
+    const S um = S(T.u[rr][cA0]), u0 = S(T.u[rr][cA1]), up = twoA ? S(T.u[rr][cA2]) : S(0);
+    const S uxl = a00 * um + a01 * u0, uxr = a10 * u0 + a11 * up;
+    const S sxl = s00 * um + s01 * u0, sxr = s10 * u0 + s11 * up;
+    const double hyd = Y.hy[j - j0];
+    const S hy = S(hyd);
+    const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
+    const S duvdy = vf1 * uy1 - vf0 * uy0;
+    const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
+    const double R = (double)(-(du2dx + duvdy) + d2u);
+    const long long idx = (long long)j * P.Nux + i;
+    const double oi = Y.rhy[j - j0] * rgx;
+    if constexpr (MODE == 0) {
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+    } else if constexpr (MODE == 2) {
+      epi_stage32(e, idx, oi * R);
+    } else {
+      const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
+      epi_residual(e, idx, oi, R, g);
+    }
+    uy0 = uy1;
+    sy0 = sy1;
+    vf0 = vf1;
+  }
+}
+
+template <typename S, int MODE, typename TV>
+__device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
+                       const YRowsN<RUN> &Y) {
+  const S ire = S(P.invRe);
+  const int ci = i - i0 + TileGeo<TV>::HL;
+  const int cV0 = ci + P.rAVX.s, cV1 = cV0 + 1, cV2 = cV1 + 1;
+  const int cU0 = ci + P.rIUX.s, cU1 = cU0 + 1, cU2 = cU1 + 1;
+  const S v00 = rw<S>(P.rAVX.w0, i), v01 = rw<S>(P.rAVX.w1, i);
+  const S v10 = rw<S>(P.rAVX.w0, i + 1), v11 = rw<S>(P.rAVX.w1, i + 1);
+  const S s00 = rw<S>(P.rSVX.w0, i), s01 = rw<S>(P.rSVX.w1, i);
+  const S s10 = rw<S>(P.rSVX.w0, i + 1), s11 = rw<S>(P.rSVX.w1, i + 1);
+  const S wu00 = rw<S>(P.rIUX.w0, i), wu01 = rw<S>(P.rIUX.w1, i);
+  const S wu10 = rw<S>(P.rIUX.w0, i + 1), wu11 = rw<S>(P.rIUX.w1, i + 1);
+  const double hxd = __ldg(P.hx + i);
+  const double rhx = __ldg(P.rhx + i);
+  const S hx = S(hxd);
+  const bool twoV = P.rAVX.two, twoVy = P.rAVY.two, twoUx = P.rIUX.two, twoUy = P.rIUY.two;
+  const int sVy = P.rAVY.s - j0 + 2, sUy = P.rIUY.s - j0 + 2;
+  auto face = [&](int r, S &vy, S &sy) {
+    const int y = r - j0;
+    const int ra = r + sVy;
+    const S f0 = S(T.v[ra][ci]);
+    const S f1 = twoVy ? S(T.v[ra + 1][ci]) : S(0);
+    vy = S(Y.avy0[y]) * f0 + S(Y.avy1[y]) * f1;
+    sy = S(Y.svy0[y]) * f0 + S(Y.svy1[y]) * f1;
+  };
+  S vy0, sy0;
+  face(ja, vy0, sy0);
+#pragma unroll 2
+  for (int j = ja; j < jb; ++j) {
+    S vy1, sy1;
+    face(j + 1, vy1, sy1);
+    const int rr = j - j0 + 2;
+    const S vm = S(T.v[rr][cV0]), v0 = S(T.v[rr][cV1]), vp = twoV ? S(T.v[rr][cV2]) : S(0);
+    const int ru = j + sUy;
+    const S ua0 = S(T.u[ru][cU0]), ua1 = S(T.u[ru][cU1]), ua2 = twoUx ? S(T.u[ru][cU2]) : S(0);
+    S ub0 = S(0), ub1 = S(0), ub2 = S(0);
+    if (twoUy) {
+      ub0 = S(T.u[ru + 1][cU0]);
+      ub1 = S(T.u[ru + 1][cU1]);
+      ub2 = twoUx ? S(T.u[ru + 1][cU2]) : S(0);
+    }
+    const S vxl = v00 * vm + v01 * v0, vxr = v10 * v0 + v11 * vp;
+    const S svl = s00 * vm + s01 * v0, svr = s10 * v0 + s11 * vp;
+    const S la = wu00 * ua0 + wu01 * ua1, ra = wu10 * ua1 + wu11 * ua2;
+    const S lb = wu00 * ub0 + wu01 * ub1, rb = wu10 * ub1 + wu11 * ub2;
+    const S wy0 = S(Y.iuy0[j - j0]), wy1 = S(Y.iuy1[j - j0]);
+    const S ufl = wy0 * la + wy1 * lb, ufr = wy0 * ra + wy1 * rb;
+    const S duvdx = ufr * vxr - ufl * vxl;
+    const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
+    const double gyd = Y.gyi[j - j0];
+    const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
+    const double R = (double)(-(duvdx + dv2dy) + d2v);
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    const double oi = Y.rgyi[j - j0] * rhx;
+    if constexpr (MODE == 0) {
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+    } else if constexpr (MODE == 2) {
+      epi_stage32(e, idx, oi * R);
+    } else {
+      const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
+      double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
+      if (P.rMYT.two) gy += Y.myt1[j - j0] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
+      const double g = -hxd * gy;
+      epi_residual(e, idx, oi, R, g);
+    }
+    vy0 = vy1;
+    sy0 = sy1;
+  }
+}
+
+#ifndef INS2D_TILE_MINB
+#define INS2D_TILE_MINB 3
+#endif
+template <typename S, int MODE, typename TV>
+__global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
+    k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
+  using G = TileGeo<TV>;
+  __shared__ __align__(16) TileSm<TV> T;
+  __shared__ YRowsN<RUN> Y;
+  const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
+  const int i0 = bx * WX, j0 = by * RUN;
+  const int tid = threadIdx.x + WX * threadIdx.y;
+  const TV *u = V, *v = V + P.Nu;
+  // stage the u and v rows j0-2 .. j0+RUN+2, columns i0-HL .. (wrapped)
+  for (int q = tid; q < 2 * kTileRows * G::CHUNKS; q += kTileThreads) {
+    const int f = q >= kTileRows * G::CHUNKS;
+    const int qq = q - f * kTileRows * G::CHUNKS;
+    const int r = qq / G::CHUNKS, ch = qq - r * G::CHUNKS;
+    if (f == 0) {
+      const int gr = wrapm(j0 - 2 + r, P.Nuy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nux);
+      cp_async16(&T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
+    } else {
+      const int gr = wrapm(j0 - 2 + r, P.Nvy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nvx);
+      cp_async16(&T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
+    }
+  }
+  stage_yrows(P, j0, Y);
+  cp_async_wait_all();
+  __syncthreads();
+  const int i = i0 + threadIdx.x;
+  const int seg = threadIdx.y & 1;
+  const int ja = j0 + seg * kTileSeg, jb = ja + kTileSeg;
+  if (threadIdx.y < 2)
+    tile_u<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
+  else
+    tile_v<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
+}
+
 // one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
-template <typename S>
-__device__ __forceinline__ void tile_fast(const DevOps &P, const double *__restrict__ V, const Epi &e, int bx, int by) {
+template <typename S, typename TV>
+__device__ __forceinline__ void tile_fast(const DevOps &P, const TV *__restrict__ V, const Epi &e, int bx, int by) {
   __shared__ YRows Y;
   const int i = bx * WX + threadIdx.x;
   const int j0 = by * RUN, j1 = j0 + RUN;
-  const double *u = V, *v = V + P.Nu;
+  const TV *u = V, *v = V + P.Nu;
   stage_yrows(P, j0, Y);
   __syncthreads();
   if (threadIdx.y == 0)
-    fast_u<S>(P, u, v, e, i, j0, j1, Y);
+    fast_u<S, TV>(P, u, v, e, i, j0, j1, Y);
   else
-    fast_v<S>(P, u, v, e, i, j0, j1, Y);
+    fast_v<S, TV>(P, u, v, e, i, j0, j1, Y);
 }
-template <typename S>
-__device__ __forceinline__ void tile_generic(const DevOps &P, const double *__restrict__ V, const Epi &e, int bx,
+template <typename S, typename TV>
+__device__ __forceinline__ void tile_generic(const DevOps &P, const TV *__restrict__ V, const Epi &e, int bx,
                                              int by) {
   const int i = bx * WX + threadIdx.x;
   const int j0 = by * RUN, j1 = j0 + RUN;
-  const double *u = V, *v = V + P.Nu;
+  const TV *u = V, *v = V + P.Nu;
   if (threadIdx.y == 0)
-    walk_u<S>(P, u, v, e, i, j0, j1);
+    walk_u<S, TV>(P, u, v, e, i, j0, j1);
   else
-    walk_v<S>(P, u, v, e, i, j0, j1);
+    walk_v<S, TV>(P, u, v, e, i, j0, j1);
 }
 
-template <typename S>
-__global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_fast(const __grid_constant__ DevOps P, const double *__restrict__ V,
+template <typename S, typename TV>
+__global__ void __launch_bounds__(WX * 2, INS2D_WALK_MINB) k_walk_fast(const __grid_constant__ DevOps P, const TV *__restrict__ V,
                                                       const __grid_constant__ Epi e) {
-  tile_fast<S>(P, V, e, P.fbx0 + blockIdx.x, P.fby0 + blockIdx.y);
+  tile_fast<S, TV>(P, V, e, P.fbx0 + blockIdx.x, P.fby0 + blockIdx.y);
 }
 
-template <typename S>
-__global__ void __launch_bounds__(WX * 2) k_walk(const __grid_constant__ DevOps P, const double *__restrict__ V,
+template <typename S, typename TV>
+__global__ void __launch_bounds__(WX * 2) k_walk(const __grid_constant__ DevOps P, const TV *__restrict__ V,
                                                  const __grid_constant__ Epi e) {
   if ((int)blockIdx.x >= P.fbx0 && (int)blockIdx.x < P.fbx1 && (int)blockIdx.y >= P.fby0 &&
       (int)blockIdx.y < P.fby1)
-    return;  // interior tile: handled by k_walk_fast
-  tile_generic<S>(P, V, e, blockIdx.x, blockIdx.y);
+    return;  // interior tile: handled by k_walk_fast / k_walk_tile
+  tile_generic<S, TV>(P, V, e, blockIdx.x, blockIdx.y);
 }
 
 // --- ensembles: one launch over the tiles of all member grids ------------------
@@ -624,9 +885,9 @@ __device__ __forceinline__ void walk_ens_body(const EnsMemberD *__restrict__ mem
   if (threadIdx.x == 0 && threadIdx.y == 0) sV = ens_epi(M, w, sE);
   __syncthreads();
   if (FAST)
-    tile_fast<S>(sP, sV, sE, it.y, it.z);
+    tile_fast<S, double>(sP, sV, sE, it.y, it.z);
   else
-    tile_generic<S>(sP, sV, sE, it.y, it.z);
+    tile_generic<S, double>(sP, sV, sE, it.y, it.z);
 }
 
 template <typename S>
@@ -642,22 +903,39 @@ __global__ void __launch_bounds__(WX * 2) k_walk_ens_gen(const EnsMemberD *__res
   walk_ens_body<S, false>(mem, work, w);
 }
 
-void launch_walk(const DevOps &P, const double *V, const Epi &e, bool fp32, cudaStream_t s) {
+template <typename S, typename TV>
+void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
   const int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   dim3 g((nx + WX - 1) / WX, (ny + RUN - 1) / RUN);
   const bool has_fast = P.fbx1 > P.fbx0 && P.fby1 > P.fby0;
+  const bool tiled = (sizeof(TV) == 8 ? P.tile_ok : P.tile_ok32) && (((uintptr_t)V & 15) == 0);
   if (has_fast) {
-    dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
-    if (fp32)
-      k_walk_fast<float><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
-    else
-      k_walk_fast<double><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
+    const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
+    if (tiled) {
+      const dim3 tb(WX, kTileThreads / WX);
+      if (e.mode == 0)
+        k_walk_tile<S, 0, TV><<<gf, tb, 0, s>>>(P, V, e);
+      else if (e.mode == 1)
+        k_walk_tile<S, 1, TV><<<gf, tb, 0, s>>>(P, V, e);
+      else
+        k_walk_tile<S, 2, TV><<<gf, tb, 0, s>>>(P, V, e);
+    } else {
+      k_walk_fast<S, TV><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
+    }
   }
-  if (fp32)
-    k_walk<float><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
+  k_walk<S, TV><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
+}
+
+// FP64 contexts: FP64 fields, FP64 arithmetic; FP32-stencil contexts: FP32
+// arithmetic on FP64 fields (V32 == nullptr) or on the FP32 stage velocity
+void launch_walk(const DevOps &P, const double *V, const float *V32, const Epi &e, bool fp32, cudaStream_t s) {
+  if (V32)
+    launch_walk_t<float, float>(P, V32, e, s);
+  else if (fp32)
+    launch_walk_t<float, double>(P, V, e, s);
   else
-    k_walk<double><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
+    launch_walk_t<double, double>(P, V, e, s);
 }
 
 }  // namespace
@@ -689,6 +967,13 @@ void walker_rectangle(DevOps &P) {
     }
   }
   if (bx0 < 0 || by0 < 0) bx0 = bx1 = by0 = by1 = 0;
+  // the tiled walkers stage columns i0-2 .. i0+WX+3 and rows j0-2 .. j0+RUN+2
+  // in 16-byte chunks: every shift must keep the stencil inside that halo
+  auto shift_ok = [](const RegD &r) { return r.s >= -2 && r.s <= 1; };
+  P.tile_ok = shift_ok(P.rAUX) && shift_ok(P.rAUY) && shift_ok(P.rIVX) && shift_ok(P.rIVY) && shift_ok(P.rAVX) &&
+              shift_ok(P.rAVY) && shift_ok(P.rIUX) && shift_ok(P.rIUY) && P.Nux % 2 == 0 && P.Nvx % 2 == 0 &&
+              P.Nu % 2 == 0;
+  P.tile_ok32 = P.tile_ok && P.Nux % 4 == 0 && P.Nvx % 4 == 0 && P.Nu % 4 == 0;
   P.fbx0 = bx0;
   P.fbx1 = bx1;
   P.fby0 = by0;
@@ -724,28 +1009,32 @@ void launch_walk_ens(const EnsMemberD *mem, const int4 *fast, int nfast, const i
 
 void launch_stage(const DevOps &P, const StageArgs &a, bool fp32, cudaStream_t s) {
   Epi e{};
-  e.mode = 0;
+  e.mode = a.store32 ? 2 : 0;
   e.Vn = a.Vn;
   e.kV = a.kV;
   for (int m = 0; m < a.nprev; ++m) {
     e.kprev[m] = a.kprev[m];
+    e.kprev32[m] = a.kprev32[m];
     e.aprev[m] = a.aprev[m];
   }
   e.nprev = a.nprev;
   e.aii = a.aii;
   e.inv_dt = a.inv_dt;
   e.Wt = a.Wt;
-  launch_walk(P, a.V, e, fp32, s);
+  e.kV32 = a.kV32;
+  e.Vt32 = a.Vt32;
+  launch_walk(P, a.V, a.V32, e, fp32, s);
 }
 
-void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next, bool fp32,
-                     cudaStream_t s) {
+void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next,
+                     float *kV_next32, bool fp32, cudaStream_t s) {
   Epi e{};
   e.mode = 1;
   e.p = p;
   e.w = w;
   e.kV_next = kV_next;
-  launch_walk(P, V, e, fp32, s);
+  e.kV_next32 = kV_next32;
+  launch_walk(P, V, nullptr, e, fp32, s);
 }
 
 }  // namespace ins2d
