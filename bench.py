@@ -77,9 +77,10 @@ WORKLOADS = {
                         "members sharded over ranks longest-first"),
 }
 
-# Algorithmic DRAM bytes per pressure cell (FP64) of one launch of each kernel
+# Algorithmic DRAM bytes per pressure cell of one launch of each kernel
 # family, averaged over the family's launches in an RK44 step with steady
-# boundary conditions (each array read or written once per launch):
+# boundary conditions (each array read or written once per launch).
+# FP64 storage:
 #   stage:    first stage from the cached residual (kV0, Vn in; Wt out: 48),
 #             stages 2-3 (V_s, Vn in; Wt, kV out: 64 each), stage 4 (V_s, Vn,
 #             three earlier kV in; Wt out: 96)            -> 272 / 4 launches
@@ -88,17 +89,29 @@ WORKLOADS = {
 #   poisson_fft: rows with the divergence fused in (W in 16, half spectrum out
 #             8), columns (8 + 8), rows back (8 in, dp out 8; + 8 for the
 #             accumulating additional solve)               -> (3*56 + 64) / 4
-FAMILY_BYTES = {"stage": 272 / 4.0, "residual": 56.0, "project": 40.0, "poisson_fft": (3 * 56 + 64) / 4.0,
-                "div": 24.0}
+# FP32 storage of the stage quantities (FP32-stencil contexts; no launch for
+# the cached first stage):
+#   stage:    stages 2-3 (V_s 4+4 in, kV 8 out: 16 each), stage 4 (V_s 8, three
+#             kV 24 in, Vtemp 8 out: 40)                   -> 72 / 3
+#   residual: V 16, p 8 in; w 16, kV_next 8 out            -> 48
+#   project:  Vn 16, Vtemp 8, dp 8 in; V_s 8 out (stages 1-3) or V 16 (stage 4)
+#                                                          -> 168 / 4
+#   poisson_fft: rows from Vn 16 + Vtemp 8 (stage solves) or w 16 (additional
+#             solve) -> 3*64 + 64 over 4 solves
+FAMILY_BYTES = {
+    "fp64": {"stage": 272 / 4.0, "residual": 56.0, "project": 40.0, "poisson_fft": (3 * 56 + 64) / 4.0,
+             "div": 24.0},
+    "fp32": {"stage": 72 / 3.0, "residual": 48.0, "project": 168 / 4.0, "poisson_fft": 64.0, "div": 32.0},
+}
 # per RK44 step: all launches of the families above
-STEP_BYTES = 272 + 56 + 4 * 40 + (3 * 56 + 64)
+STEP_BYTES = {"fp64": 272 + 56 + 4 * 40 + (3 * 56 + 64), "fp32": 72 + 48 + 168 + 4 * 64}
 # the same step in the reference's operator decomposition (fused stage + divergence
 # 88, projection 40, FFT solve 64 per stage, additional solve 40 + solve)
 STEP_BYTES_REFERENCE_DECOMPOSITION = 808
 
 
-def family_bytes_per_cell(fam, rk_stats=None):
-    return FAMILY_BYTES.get(fam)
+def family_bytes_per_cell(fam, precision="fp64"):
+    return FAMILY_BYTES[precision].get(fam)
 
 
 def load_peaks():
@@ -339,6 +352,24 @@ def run_ours(args, wl, rank, world, local_rank):
         e2e_ms = float(tt.item())
     e2e_value = cells * e_steps * world / (e2e_ms / 1e3)
 
+    # the step with process_iteration.m's per-step diagnostics (one more F for
+    # the residual, process_iteration.m:4, and check_conservation, :22): each
+    # step followed by both calls on the device state
+    nd = max(2, min(args.steps, 10))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for n in range(nd):
+        opts.time_ERK(Vd, pd, t + n * dt, dt, nsteps=1)
+        opts.F(Vd, None, pd, t + (n + 1) * dt)
+        opts.check_conservation(Vd, t + (n + 1) * dt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    diag_ms = e0.elapsed_time(e1) / nd
+    t += nd * dt
+    diagnostics = {"steps": nd, "ms_per_step": round(diag_ms, 4), "value": cells / (diag_ms / 1e3),
+                   "note": "each step an ins2d_erk_step call followed by ins2d_F (maxres) and "
+                           "ins2d_conservation, as process_iteration.m runs them every step"}
+
     # per-family device time (a separate profiled run; events add a little overhead)
     nprof = max(2, min(args.steps, 10))
     opts.profile(True)
@@ -350,7 +381,8 @@ def run_ours(args, wl, rank, world, local_rank):
     dom = max(fam_ms, key=fam_ms.get)
     dom_launch_ms = fam[dom][0] / max(fam[dom][1], 1)
     fkey = "poisson_fft" if (dom == "poisson" and wl["poisson"] == 6) else dom
-    bpc = family_bytes_per_cell(fkey, None)
+    prec = wl["precision"]
+    bpc = family_bytes_per_cell(fkey, prec)
     roof = None
     if bpc is not None:
         if dom == "poisson":
@@ -369,7 +401,7 @@ def run_ours(args, wl, rank, world, local_rank):
         per_family = {}
         for k, (fms, nl) in fam.items():
             kk = "poisson_fft" if (k == "poisson" and wl["poisson"] == 6) else k
-            b = family_bytes_per_cell(kk)
+            b = family_bytes_per_cell(kk, prec)
             if b is None or nl == 0 or fms <= 0:
                 continue
             lms = fms / (nprof * 4) if k == "poisson" else fms / nl
@@ -382,14 +414,15 @@ def run_ours(args, wl, rank, world, local_rank):
                 "bytes_per_launch": bpc * cells, "launch_ms": round(launch_ms, 5),
                 "family_ms_per_step": {k: round(v / nprof, 4) for k, v in fam_ms.items()},
                 "families": per_family,
-                "step": {"bytes_per_cell": STEP_BYTES, "achieved_gbs": round(STEP_BYTES * cells / step_ms / 1e6, 1),
-                         "frac": round(STEP_BYTES * cells / step_ms / 1e6 / peak, 4),
+                "step": {"bytes_per_cell": STEP_BYTES[prec],
+                         "achieved_gbs": round(STEP_BYTES[prec] * cells / step_ms / 1e6, 1),
+                         "frac": round(STEP_BYTES[prec] * cells / step_ms / 1e6 / peak, 4),
                          "bytes_per_cell_reference_decomposition": STEP_BYTES_REFERENCE_DECOMPOSITION,
                          "frac_reference_decomposition":
                              round(STEP_BYTES_REFERENCE_DECOMPOSITION * cells / step_ms / 1e6 / peak, 4)}}
     # accuracy of this run: kinetic energy drift and divergence; for the FP32
     # stencil workload also the deviation from the FP64 path over the same steps
-    total_steps = (lw["record_steps"] if lw else 0) + args.warmup + args.steps + nprof
+    total_steps = (lw["record_steps"] if lw else 0) + args.warmup + args.steps + nd + nprof
     acc = None
     if rank == 0:
         c0 = opts.check_conservation(torch.tensor(V0, dtype=torch.float64, device="cuda"), 0.0)
@@ -403,7 +436,7 @@ def run_ours(args, wl, rank, world, local_rank):
             V64 = torch.tensor(V64_0, dtype=torch.float64, device="cuda")
             p64 = o64.pressure_additional_solve(V64, torch.zeros(o64.Np, dtype=torch.float64, device="cuda"), 0.0)
             o64.time_ERK(V64, p64, 0.0, dt, nsteps=(lw["record_steps"] if lw else 0) + args.warmup + args.steps)
-            o64.time_ERK(V64, p64, 0.0, dt, nsteps=nprof)
+            o64.time_ERK(V64, p64, 0.0, dt, nsteps=nd + nprof)
             k64 = o64.check_conservation(V64, t)[3]
             acc.update({"fp64_k": k64, "energy_vs_fp64_rel": abs(c1[3] - k64) / k64,
                         "velocity_l2_vs_fp64_rel": float(torch.linalg.norm(Vd - V64) / torch.linalg.norm(V64))})
@@ -466,6 +499,12 @@ def run_ours(args, wl, rank, world, local_rank):
                                    "frac": round(flops / fms / 1e9 / tpk[0], 4),
                                    "note": "ms includes the host synchronisation of each ins2d_cnn_forward call"}
         del net
+    # the configuration's target comparison (default workload only): FP32
+    # stencils + learned guess against the default FP64 path at the same CG
+    # residual 1e-10 (multigrid PCG), a few steps each
+    target = None
+    if rank == 0 and args.workload == "turb2048" and not args.no_target:
+        target = target_comparison(local_rank, stream)
     # CPU baseline on rank 0 only at N=1
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -486,6 +525,8 @@ def run_ours(args, wl, rank, world, local_rank):
         "roofline": roof,
         "cpu_baseline": cpu,
         "accuracy": acc,
+        "with_process_iteration": diagnostics,
+        "target": target,
         "plain_pcg": plain,
         "learned": learned_info,
         "clocks": clk,
@@ -495,6 +536,58 @@ def run_ours(args, wl, rank, world, local_rank):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def timed_steps(opts, Vd, pd, t, dt, n, stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    _, _, st = opts.time_ERK(Vd, pd, t, dt, nsteps=n, return_stats=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / n, st["iters_total"] / max(st["n_solves"], 1)
+
+
+def target_comparison(device, stream, nsteps=4):
+    """North-star comparison on the 2048^2 turbulence: the default FP64 path
+    (multigrid PCG) against FP32 stencils and against FP32 stencils with the
+    learned initial guess, every solve to the same relative residual 1e-10.
+    Each form: one warm-up step, then nsteps timed steps from the same state;
+    the network is trained first on the pairs of the FP32 run's first steps."""
+    import torch
+    out = {"workload": "decaying turbulence 2048x2048, PCG to 1e-10", "steps": nsteps}
+    forms = (("fp64_multigrid", "turb2048_pcg", None), ("fp32_multigrid", "turb2048_pcg_fp32", None),
+             ("fp32_learned", "turb2048_pcg_fp32_learned", "learned"))
+    for name, wkey, kind in forms:
+        wl = WORKLOADS[wkey]
+        opts, V0, dt = setup_case(wl, device=device)
+        opts.set_stream(stream.cuda_stream)
+        Vd = torch.tensor(V0, dtype=torch.float64, device="cuda")
+        pd = opts.pressure_additional_solve(Vd, torch.zeros(opts.Np, dtype=torch.float64, device="cuda"), 0.0)
+        t = 0.0
+        info = {}
+        net = None
+        if kind == "learned":
+            t, linfo, net = setup_learned(opts, wl["learned"], Vd, pd, t, dt, stream, device)
+            info = {"train_s": linfo["train_s"], "pairs": linfo["pairs"]}
+        opts.time_ERK(Vd, pd, t, dt, nsteps=1)
+        t += dt
+        ms, it = timed_steps(opts, Vd, pd, t, dt, nsteps, stream)
+        out[name] = dict(info, ms_per_step=round(ms, 3), cg_iters_per_solve=round(it, 2),
+                         value=opts.Npx * opts.Npy / (ms / 1e3))
+        if net is not None:
+            from ins2d_b200 import learned
+            learned.attach(opts, None)
+            net.close()
+        opts.close()
+        torch.cuda.empty_cache()
+    base = out["fp64_multigrid"]["ms_per_step"]
+    for name in ("fp32_multigrid", "fp32_learned"):
+        out[name]["speedup_vs_fp64"] = round(base / out[name]["ms_per_step"], 3)
+    out["target_speedup"] = 2.0
+    out["met"] = out["fp32_learned"]["speedup_vs_fp64"] >= 2.0
+    return out
 
 
 def run_ensemble(args, wl, rank, world, local_rank):
@@ -581,6 +674,18 @@ def run_ensemble(args, wl, rank, world, local_rank):
     all_stats = ensembles.gather_stats(local, mine, len(members)) if dist else local
     it_mean = sum(s["iters_total"] for s in all_stats) / max(sum(s["n_solves"] for s in all_stats), 1)
     it_max = max(s["iters_max"] for s in all_stats)
+    # whole-step roofline in the CG-path decomposition (552 + 4 (16 + 88 iters)
+    # B per cell and RK44 step: stages, projections and residual, plus the CG
+    # vectors of each solve; the V-cycle's own traffic is not counted)
+    peak, peak_kind = load_peaks()
+    step_bpc = 552 + 4 * (16 + 88 * it_mean)
+    ach = step_bpc * total_cells / (ms_max / args.steps / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": "whole RK44 step (CG-path decomposition)", "achieved": round(ach, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "peak_kind": peak_kind, "traffic": None,
+            "bytes_per_cell": round(step_bpc, 1)}
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        cpu = ensemble_cpu_baseline(wl)
     res = {
         "metric": "cell-updates/s per RK4 step incl. Poisson solve (sum over ensemble members)",
         "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -598,8 +703,8 @@ def run_ensemble(args, wl, rank, world, local_rank):
         # residual, 1 cached first stage, 3 divergence + 3 solve launches for stages 2-4,
         # 4 projections, 1 divergence + 1 solve for the additional solve
         "gpu_launches": args.steps * 21,
-        "roofline": None,
-        "cpu_baseline": None,
+        "roofline": roof,
+        "cpu_baseline": cpu,
         "clocks": clk,
     }
     if rank == 0:
@@ -610,37 +715,75 @@ def run_ensemble(args, wl, rank, world, local_rank):
         dist.destroy_process_group()
 
 
-def cpu_baseline(wl, budget_s=25.0, steps=None):
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def host_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def periodic_case_host(wl):
+    """(V0, dt) of a periodic workload computed on the host alone: the same
+    seeded spectral field (turbulence) or Taylor-Green field as the GPU arm."""
+    from ins2d_b200 import cases
+    N, L = wl["N"], wl["L"]
+    if wl["ic"] == "turbulence":
+        V = cases.decaying_turbulence_ic_host(N, L, k0=10.0, seed=2048)
+        h = L / N
+        dt = 0.5 * h / float(np.max(np.abs(V)))  # cases.cfl_dt
+    else:
+        x = cases.uniform_grid(N, 0.0, L)
+        xp = (x[:-1] + x[1:]) / 2
+        xu, yu = np.tile(x[:-1], N), np.repeat(xp, N)
+        xv, yv = np.tile(xp, N), np.repeat(x[:-1], N)
+        V = np.r_[np.sin(xu) * np.cos(yu), -np.cos(xv) * np.sin(yv)]
+        dt = wl["dt"]
+    return V, dt
+
+
+def cpu_baseline(wl, budget_s=25.0, steps=None, warmup=1):
     """The reference algorithm on the host cores, on a bounded sample (RK44
-    steps of the same workload).  Periodic FFT workloads: the OpenMP C
-    restatement oracle/erk_periodic.c on all host threads (checked against the
-    scipy restatement in tests/test_oracle_pins.py); other workloads: the
-    scipy/numpy restatement (single-threaded sparse matvecs, cg.F's DIC-PCG in
-    C)."""
+    steps of the same workload from the same initial field).  Periodic FFT
+    workloads: the OpenMP C restatement oracle/erk_periodic.c on all host
+    threads (checked against the scipy restatement in
+    tests/test_oracle_pins.py); other workloads: the scipy/numpy restatement
+    (single-threaded sparse matvecs, cg.F's DIC-PCG in C).  steps: the timed
+    step count (capped so the timed part stays near budget_s)."""
     from oracle import ins2d_ref as R
     from ins2d_b200 import cases
     if wl["ic"] == "bfs":
         return bfs_cpu_baseline(wl, budget_s, steps)
     N, L = wl["N"], wl["L"]
-    rng = np.random.default_rng(0)
-    dt = wl.get("dt", 1e-4)
     if wl.get("poisson") == 6 and wl["ic"] in ("turbulence", "tg"):
-        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-        V = 0.1 * rng.standard_normal(2 * N * N)
+        threads = host_threads()
+        V, dt = periodic_case_host(wl)
         p = np.zeros(N * N)
-        R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, 1, threads=threads)  # warm-up (page-in)
-        n = 0
+        if warmup > 0:
+            V, p = R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, warmup, threads=threads)
         t0 = time.perf_counter()
-        while True:
-            V, p = R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, 1, threads=threads)
-            n += 1
-            el = time.perf_counter() - t0
-            if (steps is not None and n >= steps) or (steps is None and (el > budget_s or n >= 50)):
-                break
+        V, p = R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, 1, threads=threads)
+        t1 = time.perf_counter() - t0
+        want = steps if steps is not None else 50
+        n_more = max(0, min(want - 1, int(budget_s / max(t1, 1e-9))))
+        t0 = time.perf_counter()
+        if n_more:
+            V, p = R.erk_periodic_c(V, p, N, N, L, L, wl["Re"], dt, n_more, threads=threads)
+        el = t1 + (time.perf_counter() - t0)
+        n = 1 + n_more
         return {"value": N * N * n / el, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                "sample": f"{n} RK44 step(s) of the {N}x{N} periodic workload with the OpenMP C restatement "
-                          f"of the reference algorithm (oracle/erk_periodic.c, FFT pressure solve), "
-                          f"{threads} threads; random initial velocity (timing sample)"}
+                "steps": n, "cpu_model": cpu_model(), "dt": dt,
+                "sample": f"{n} RK44 step(s) (after {warmup} untimed) of the {N}x{N} periodic workload from its own "
+                          f"initial field, with the OpenMP C restatement of the reference algorithm "
+                          f"(oracle/erk_periodic.c, FFT pressure solve), {threads} threads"}
     x = cases.uniform_grid(N, 0.0, L)
     bc = cases.BC_CAVITY if wl["ic"] == "rest" else cases.BC_PERIODIC
     uBC = cases.lid_uBC(1.0, L) if wl["ic"] == "rest" else None
@@ -650,24 +793,28 @@ def cpu_baseline(wl, budget_s=25.0, steps=None):
                        CG_maxit=100000, uBC=uBC, RK="RK44")
     setup_s = time.perf_counter() - t0
     g = o.grid
+    dt = wl.get("dt", 1e-4)
     if wl["ic"] == "rest":
         V = np.zeros(g.NV)
     elif wl["ic"] == "tg":
         V = np.r_[np.sin(g.xu) * np.cos(g.yu), -np.cos(g.xv) * np.sin(g.yv)]
     else:
-        V = R.initial_projection(0.1 * rng.standard_normal(g.NV), 0.0, o)
+        V, dt = periodic_case_host(wl)
     p = np.zeros(g.Np)
+    for n in range(warmup):
+        V, p = R.time_ERK(V, p, n * dt, dt, o)
     n = 0
     t0 = time.perf_counter()
     while True:
         V, p = R.time_ERK(V, p, n * dt, dt, o)
         n += 1
         el = time.perf_counter() - t0
-        if (steps is not None and n >= steps) or (steps is None and (el > budget_s or n >= 50)):
+        if (steps is not None and n >= steps) or el > budget_s or (steps is None and n >= 50):
             break
-    return {"value": g.Npx * g.Npy * n / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-            "sample": f"{n} RK44 step(s) of the {N}x{N} workload with the scipy/numpy restatement "
-                      f"(sparse matvecs single-threaded, cg.F's DIC-PCG in C; operator setup "
+    return {"value": g.Npx * g.Npy * n / el, "unit": "cell-updates/s", "cores": 1, "kind": "port", "steps": n,
+            "cpu_model": cpu_model(), "dt": dt,
+            "sample": f"{n} RK44 step(s) (after {warmup} untimed) of the {N}x{N} workload with the scipy/numpy "
+                      f"restatement (sparse matvecs single-threaded, cg.F's DIC-PCG in C; operator setup "
                       f"{setup_s:.1f}s excluded)"}
 
 
@@ -720,27 +867,40 @@ def ensemble_cpu_baseline(wl, nmembers=2, steps=2):
             V, p = R.time_ERK(V, p, n * dt, dt, o)
         el += time.perf_counter() - t0
         cells += o.grid.Npx * o.grid.Npy * steps
-    return {"value": cells / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+    return {"value": cells / el, "unit": "cell-updates/s", "cores": 1, "kind": "port", "steps": steps,
+            "cpu_model": cpu_model(),
             "sample": f"{steps} RK44 steps of each of the first {nmembers} members with the scipy/numpy "
                       f"restatement (cg.F's DIC-PCG in C, single-threaded)"}
 
 
 def run_reference(args, wl, rank, world):
+    """The reference algorithm's CPU restatement (the reference itself is
+    MATLAB, not runnable here) on the same workload, metric and config as the
+    GPU arm: args.warmup untimed steps, then args.steps timed steps (capped
+    to --ref-budget seconds of timed work; the cap is stated in the line)."""
     if rank != 0:
         return
-    steps = max(1, args.steps)
-    # a bounded sample: the step count is capped so the whole run takes minutes
-    warm = min(args.warmup, 1)
-    nsteps = min(steps, 3)
     if wl.get("kind") == "ensemble":
         cb = ensemble_cpu_baseline(wl)
+        config = {"workload": args.workload, "desc": wl["desc"], "members": wl["n"],
+                  "sample": cb["sample"]}
+        steps = cb.get("steps")
     else:
-        cb = cpu_baseline(wl, budget_s=1e9, steps=warm + nsteps)
+        cb = cpu_baseline(wl, budget_s=args.ref_budget, steps=max(1, args.steps), warmup=args.warmup)
+        steps = cb["steps"]
+        N = wl["N"]
+        cells = N * N
+        config = {"workload": args.workload, "desc": wl["desc"], "grid": [N, N], "dt": cb.get("dt"),
+                  "cells": cells, "l2": "working set > 126 MB L2 (no flush)" if cells >= 1 << 20 else
+                  "small grid: L2-resident", "parallelism": "host threads"}
+        if wl["ic"] == "bfs":
+            config["sample"] = cb["sample"]
     res = {
         "impl": "reference", "metric": "cell-updates/s per RK4 step incl. Poisson solve", "value": cb["value"],
-        "unit": "cell-updates/s", "n_gpus": world, "steps": nsteps, "warmup": warm, "higher_is_better": True,
+        "unit": "cell-updates/s", "n_gpus": world, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": wl["desc"]},
+        "config": config,
+        "steps_requested": args.steps,
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -755,6 +915,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="turb2048", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="--impl reference: seconds of timed CPU work at most")
+    ap.add_argument("--no-target", action="store_true",
+                    help="skip the FP32 + learned vs FP64 multigrid comparison of the default workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--members", type=int, default=None, help="ensemble workloads: number of members")
     args = ap.parse_args()

@@ -132,10 +132,7 @@ def streamfunction_velocity(psi, opts):
     return np.r_[u.ravel(), v.ravel()]
 
 
-def decaying_turbulence_ic(opts, k0=10.0, seed=2048, energy=1.0):
-    """Random-phase streamfunction with energy spectrum E(k) ~ k^4 exp(-2 (k/k0)^2)
-    on a periodic grid, turned into a discretely divergence-free velocity and
-    scaled to kinetic energy ``energy`` (check_conservation.m k)."""
+def _turbulence_velocity(opts, k0, seed):
     Nx, Ny = opts.Nx, opts.Ny
     rng = np.random.default_rng(seed)
     kx = np.fft.rfftfreq(Nx, d=1.0 / Nx)   # integer wave numbers, x (halved axis)
@@ -147,8 +144,28 @@ def decaying_turbulence_ic(opts, k0=10.0, seed=2048, energy=1.0):
         amp = np.where(K > 0, np.sqrt(E / (np.pi * K)) / K, 0.0)
     spec = amp * np.exp(2j * np.pi * rng.random(amp.shape))
     psi = np.fft.irfft2(spec, s=(Ny, Nx)).ravel()  # (j, i) -> x fastest
-    V = streamfunction_velocity(psi, opts)
+    return streamfunction_velocity(psi, opts)
+
+
+def decaying_turbulence_ic(opts, k0=10.0, seed=2048, energy=1.0):
+    """Random-phase streamfunction with energy spectrum E(k) ~ k^4 exp(-2 (k/k0)^2)
+    on a periodic grid, turned into a discretely divergence-free velocity and
+    scaled to kinetic energy ``energy`` (check_conservation.m k)."""
+    V = _turbulence_velocity(opts, k0, seed)
     k = opts.check_conservation(V, 0.0)[3]
+    return V * math.sqrt(energy / k)
+
+
+def decaying_turbulence_ic_host(N, L=1.0, k0=10.0, seed=2048, energy=1.0):
+    """The same field on the uniform periodic N x N grid of side L, computed
+    on the host alone (no device context): on that grid every u and v point
+    has the volume hx*hy, so check_conservation.m's k is hx*hy*sum(V^2)/2."""
+    from types import SimpleNamespace
+    x = uniform_grid(N, 0.0, L)
+    g = SimpleNamespace(Nx=N, Ny=N, x=x, y=x.copy())
+    V = _turbulence_velocity(g, k0, seed)
+    h = L / N
+    k = 0.5 * h * h * float(np.dot(V, V))
     return V * math.sqrt(energy / k)
 
 
