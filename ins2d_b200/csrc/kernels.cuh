@@ -65,6 +65,9 @@ struct StageArgs {
 void launch_stage(const DevOps &P, const StageArgs &a, bool fp32, cudaStream_t s);
 // computes P.fbx0.. (the interior tile rectangle of the stencil walkers)
 void walker_rectangle(DevOps &P);
+// opts the tiled walkers in to their dynamic shared memory on the current
+// device (once per context); returns the first failure
+cudaError_t walker_prepare();
 // w = Om^-1 (R(V) - G p) (pressure_additional_solve.m:11-13); when kV_next
 // (kV_next32) is non-null also stores Om^-1 R(V) there (rounded to FP32).
 void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next,

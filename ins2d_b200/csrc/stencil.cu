@@ -618,9 +618,11 @@ __device__ __forceinline__ int wrapm(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
-// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
-template <typename S, int MODE, typename TV>
-__device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
+// Phase 1 of the tiled walkers: R = -conv + Diff V (the right-hand side
+// without the pressure terms) of each point of the tile into Rs (u: Rs[0],
+// v: Rs[1]), with the arithmetic of fast_u / fast_v.
+template <typename S, typename TV>
+__device__ void tile_u(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i, int i0, int j0, int ja, int jb,
                        const YRowsN<RUN> &Y) {
   const S ire = S(P.invRe);
   const int ci = i - i0 + TileGeo<TV>::HL;  // shared-memory column of u(i, .)
@@ -632,7 +634,6 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
   const S s10 = rw<S>(P.rSUX.w0, i + 1), s11 = rw<S>(P.rSUX.w1, i + 1);
   const S iv0 = rw<S>(P.rIVX.w0, i), iv1 = rw<S>(P.rIVX.w1, i);
   const S gx = S(__ldg(P.gxi + i));
-  const double rgx = __ldg(P.rgxi + i);
   const bool twoA = P.rAUX.two, twoAy = P.rAUY.two, twoIx = P.rIVX.two, twoIy = P.rIVY.two;
   const int sAy = P.rAUY.s - j0 + 2, sIy = P.rIVY.s - j0 + 2;  // shared-memory row of field row r: r + s
   auto face = [&](int r, S &uy, S &sy, S &vf) {
@@ -661,35 +662,19 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     const S um = S(T.u[rr][cA0]), u0 = S(T.u[rr][cA1]), up = twoA ? S(T.u[rr][cA2]) : S(0);
     const S uxl = a00 * um + a01 * u0, uxr = a10 * u0 + a11 * up;
     const S sxl = s00 * um + s01 * u0, sxr = s10 * u0 + s11 * up;
-    const double hyd = Y.hy[j - j0];
-    const S hy = S(hyd);
+    const S hy = S(Y.hy[j - j0]);
     const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
     const S duvdy = vf1 * uy1 - vf0 * uy0;
     const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
-    const double R = (double)(-(du2dx + duvdy) + d2u);
-    const long long idx = (long long)j * P.Nux + i;
-    const double oi = Y.rhy[j - j0] * rgx;
-    if constexpr (MODE == 0) {
-      const double k = oi * R;
-      if (e.kV) e.kV[idx] = k;
-      double vt = 0.0;
-      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
-      vt += e.aii * k;
-      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
-    } else if constexpr (MODE == 2) {
-      epi_stage32(e, idx, oi * R);
-    } else {
-      const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
-      epi_residual(e, idx, oi, R, g);
-    }
+    Rs[j - j0][i - i0] = -(du2dx + duvdy) + d2u;
     uy0 = uy1;
     sy0 = sy1;
     vf0 = vf1;
   }
 }
 
-template <typename S, int MODE, typename TV>
-__device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
+template <typename S, typename TV>
+__device__ void tile_v(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i, int i0, int j0, int ja, int jb,
                        const YRowsN<RUN> &Y) {
   const S ire = S(P.invRe);
   const int ci = i - i0 + TileGeo<TV>::HL;
@@ -701,9 +686,7 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
   const S s10 = rw<S>(P.rSVX.w0, i + 1), s11 = rw<S>(P.rSVX.w1, i + 1);
   const S wu00 = rw<S>(P.rIUX.w0, i), wu01 = rw<S>(P.rIUX.w1, i);
   const S wu10 = rw<S>(P.rIUX.w0, i + 1), wu11 = rw<S>(P.rIUX.w1, i + 1);
-  const double hxd = __ldg(P.hx + i);
-  const double rhx = __ldg(P.rhx + i);
-  const S hx = S(hxd);
+  const S hx = S(__ldg(P.hx + i));
   const bool twoV = P.rAVX.two, twoVy = P.rAVY.two, twoUx = P.rIUX.two, twoUy = P.rIUY.two;
   const int sVy = P.rAVY.s - j0 + 2, sUy = P.rIUY.s - j0 + 2;
   auto face = [&](int r, S &vy, S &sy) {
@@ -738,41 +721,36 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     const S ufl = wy0 * la + wy1 * lb, ufr = wy0 * ra + wy1 * rb;
     const S duvdx = ufr * vxr - ufl * vxl;
     const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
-    const double gyd = Y.gyi[j - j0];
-    const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
-    const double R = (double)(-(duvdx + dv2dy) + d2v);
-    const long long idx = P.Nu + (long long)j * P.Nvx + i;
-    const double oi = Y.rgyi[j - j0] * rhx;
-    if constexpr (MODE == 0) {
-      const double k = oi * R;
-      if (e.kV) e.kV[idx] = k;
-      double vt = 0.0;
-      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
-      vt += e.aii * k;
-      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
-    } else if constexpr (MODE == 2) {
-      epi_stage32(e, idx, oi * R);
-    } else {
-      const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
-      double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
-      if (P.rMYT.two) gy += Y.myt1[j - j0] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
-      const double g = -hxd * gy;
-      epi_residual(e, idx, oi, R, g);
-    }
+    const S d2v = S(Y.gyi[j - j0]) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
+    Rs[j - j0][i - i0] = -(duvdx + dv2dy) + d2v;
     vy0 = vy1;
     sy0 = sy1;
   }
 }
 
+// shared memory of one tile: the staged fields, the right-hand sides and the
+// tile's y-weights (dynamic: more than the 48 KB of static shared memory)
+template <typename S, typename TV>
+struct TileSmem {
+  TileSm<TV> T;
+  S R[2][RUN][WX];
+  YRowsN<RUN> Y;
+};
+
 #ifndef INS2D_TILE_MINB
 #define INS2D_TILE_MINB 3
 #endif
+#ifndef INS2D_TILE_EPI_UNROLL
+#define INS2D_TILE_EPI_UNROLL 4
+#endif
+constexpr int kEpiUnroll = INS2D_TILE_EPI_UNROLL;
+// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
 template <typename S, int MODE, typename TV>
 __global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
     k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
   using G = TileGeo<TV>;
-  __shared__ __align__(16) TileSm<TV> T;
-  __shared__ YRowsN<RUN> Y;
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  TileSmem<S, TV> &M = *reinterpret_cast<TileSmem<S, TV> *>(tile_smem);
   const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
   const int i0 = bx * WX, j0 = by * RUN;
   const int tid = threadIdx.x + WX * threadIdx.y;
@@ -784,22 +762,74 @@ __global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
     const int r = qq / G::CHUNKS, ch = qq - r * G::CHUNKS;
     if (f == 0) {
       const int gr = wrapm(j0 - 2 + r, P.Nuy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nux);
-      cp_async16(&T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
+      cp_async16(&M.T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
     } else {
       const int gr = wrapm(j0 - 2 + r, P.Nvy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nvx);
-      cp_async16(&T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
+      cp_async16(&M.T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
     }
   }
-  stage_yrows(P, j0, Y);
+  stage_yrows(P, j0, M.Y);
   cp_async_wait_all();
   __syncthreads();
-  const int i = i0 + threadIdx.x;
-  const int seg = threadIdx.y & 1;
-  const int ja = j0 + seg * kTileSeg, jb = ja + kTileSeg;
-  if (threadIdx.y < 2)
-    tile_u<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
-  else
-    tile_v<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
+  // phase 1: walk the columns
+  {
+    const int i = i0 + threadIdx.x;
+    const int seg = threadIdx.y & 1;
+    const int ja = j0 + seg * kTileSeg, jb = ja + kTileSeg;
+    if (threadIdx.y < 2)
+      tile_u<S, TV>(P, M.T, M.R[0], i, i0, j0, ja, jb, M.Y);
+    else
+      tile_v<S, TV>(P, M.T, M.R[1], i, i0, j0, ja, jb, M.Y);
+  }
+  __syncthreads();
+  // phase 2: the epilogue of every point, consecutive threads on consecutive
+  // columns and all of a thread's loads independent of each other
+  const YRowsN<RUN> &Y = M.Y;
+#pragma unroll kEpiUnroll
+  for (int m = 0; m < 2 * RUN * WX / kTileThreads; ++m) {
+    const int o = tid + kTileThreads * m;
+    const int comp = o / (RUN * WX);
+    const int oo = o - comp * (RUN * WX);
+    const int jr = oo / WX, ic = oo - jr * WX;
+    const int i = i0 + ic, j = j0 + jr;
+    const double R = (double)M.R[comp][jr][ic];
+    long long idx;
+    double oi;
+    if (comp == 0) {
+      idx = (long long)j * P.Nux + i;
+      oi = Y.rhy[jr] * __ldg(P.rgxi + i);
+    } else {
+      idx = P.Nu + (long long)j * P.Nvx + i;
+      oi = Y.rgyi[jr] * __ldg(P.rhx + i);
+    }
+    if constexpr (MODE == 0) {
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int q = 0; q < e.nprev; ++q) vt += e.aprev[q] * __ldg(e.kprev[q] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+    } else if constexpr (MODE == 2) {
+      epi_stage32(e, idx, oi * R);
+    } else {
+      double g;
+      if (comp == 0) {
+        g = -Y.hy[jr] * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
+      } else {
+        const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
+        double gy = Y.myt0[jr] * __ldg(e.p + (long long)c0 * P.Npx + i);
+        if (P.rMYT.two) gy += Y.myt1[jr] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
+        g = -__ldg(P.hx + i) * gy;
+      }
+      epi_residual(e, idx, oi, R, g);
+    }
+  }
+}
+
+template <typename S, int MODE, typename TV>
+cudaError_t tile_prepare_one() {
+  return cudaFuncSetAttribute((const void *)k_walk_tile<S, MODE, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(TileSmem<S, TV>));
 }
 
 // one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
@@ -914,12 +944,13 @@ void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
     const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
     if (tiled) {
       const dim3 tb(WX, kTileThreads / WX);
+      const size_t sm = sizeof(TileSmem<S, TV>);
       if (e.mode == 0)
-        k_walk_tile<S, 0, TV><<<gf, tb, 0, s>>>(P, V, e);
+        k_walk_tile<S, 0, TV><<<gf, tb, sm, s>>>(P, V, e);
       else if (e.mode == 1)
-        k_walk_tile<S, 1, TV><<<gf, tb, 0, s>>>(P, V, e);
+        k_walk_tile<S, 1, TV><<<gf, tb, sm, s>>>(P, V, e);
       else
-        k_walk_tile<S, 2, TV><<<gf, tb, 0, s>>>(P, V, e);
+        k_walk_tile<S, 2, TV><<<gf, tb, sm, s>>>(P, V, e);
     } else {
       k_walk_fast<S, TV><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
     }
@@ -939,6 +970,21 @@ void launch_walk(const DevOps &P, const double *V, const float *V32, const Epi &
 }
 
 }  // namespace
+
+// Opts the tiled walkers in to their dynamic shared memory on the current
+// device; returns the first failure.
+cudaError_t walker_prepare() {
+  // the instances launch_walk_t launches: FP64, FP32 arithmetic on FP64
+  // fields, FP32 arithmetic on FP32 fields, each in the three modes
+  const cudaError_t r[] = {tile_prepare_one<double, 0, double>(), tile_prepare_one<double, 1, double>(),
+                           tile_prepare_one<double, 2, double>(), tile_prepare_one<float, 0, double>(),
+                           tile_prepare_one<float, 1, double>(), tile_prepare_one<float, 2, double>(),
+                           tile_prepare_one<float, 0, float>(), tile_prepare_one<float, 1, float>(),
+                           tile_prepare_one<float, 2, float>()};
+  for (cudaError_t x : r)
+    if (x != cudaSuccess) return x;
+  return cudaSuccess;
+}
 
 // The rectangle of tiles whose every column and row lies in the regular
 // ranges the fast walkers need (both walkers of a block must qualify).

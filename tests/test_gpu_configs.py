@@ -4,7 +4,7 @@ the C-ABI, against the oracle:
   lid-driven cavity 64x64, Re=1000, RK44, dt=1e-3, 1000 steps, PCG to 1e-12
       vs the scipy restatement (direct solves), at steps 100 and 1000;
   inviscid Taylor-Green 512x512 on [0,2pi]^2, RK44, dt=1e-3, 2000 steps, FFT
-      vs the OpenMP C restatement: the same kinetic-energy drift
+      vs the OpenMP C restatement: the same kinetic-energy drift to 1e-12 k0
       (check_conservation.m:62-76) and max|div| < 1e-12 throughout;
   decaying turbulence 2048x2048, Re=2000, CFL 0.5, FFT, 10 FP64 steps from the
       seeded spectral initial field vs the C restatement at 1e-12;
@@ -74,8 +74,11 @@ def test_tg512_2000_steps_energy():
     kc = m.check_conservation(Vc, nsteps * dt)[3]
     print(f"tg512 2000 steps: energy drift GPU {(kg - k0) / k0:.3e}, C oracle {(kc - k0) / k0:.3e}, "
           f"velocity rel {_rel(Vg, Vc):.3e}")
-    assert abs((kg - k0) - (kc - k0)) <= 1e-14 * k0
-    assert abs(kg - k0) <= 1e-9 * k0  # RK4's O(dt^5) per-step energy error, no blow-up
+    # the two FP64 implementations (different transform and summation orders)
+    # agree on the energy to about 1e-13 k0 after 2000 steps (measured 8e-14);
+    # the drift itself is RK4's time-discretisation error (measured -1.7e-7)
+    assert abs((kg - k0) - (kc - k0)) <= 1e-12 * k0
+    assert abs(kg - k0) <= 1e-6 * k0
     assert _rel(Vg, Vc) < 1e-11
 
 
