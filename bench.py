@@ -70,6 +70,10 @@ WORKLOADS = {
                             desc="backward-facing step 1024x1024 (as bfs1024) with the learned initial guess: "
                                  "a 6-layer 32-channel BF16 CNN trained on the GPU on the (f, dp) pairs of the "
                                  "first steps' solves; multigrid PCG to the same 1e-10"),
+    "turb2048_slab": dict(kind="slab", N=2048, L=1.0, Re=2000.0, poisson=6, precision="fp64", ic="turbulence",
+                          desc="decaying 2D turbulence 2048x2048 periodic, Re=2000, RK44, CFL 0.5, FFT Poisson, FP64, "
+                               "the one grid split into y-slabs over the ranks (halo exchanges and all-to-all "
+                               "transposes over NCCL)"),
     "ens256": dict(kind="ensemble", n=256, sizes=(64, 96, 128, 192, 256), stretch=1.05, dt=5e-4, CG_acc=1e-10,
                    poisson=4, precision="fp64",
                    desc="ensemble of 256 cavity/channel flows, tanh-stretched 1.05, nx,ny in {64..256}, "
@@ -590,6 +594,121 @@ def target_comparison(device, stream, nsteps=4):
     return out
 
 
+def run_slab(args, wl, rank, world, local_rank):
+    """One grid split into y-slabs over the ranks (ins2d_b200/slab.py): each
+    rank advances its rows; halos and the FFT's transposes move over NCCL.
+    value = the grid's cell-updates / max-over-ranks time (strong scaling)."""
+    import datetime
+    import torch
+    from ins2d_b200 import cases, slab
+    from ins2d_b200.rk import getRKmethod
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    N, L = wl["N"], wl["L"]
+    V0, dt = periodic_case_host(wl)
+    part = slab.SlabPartition(N, world, rank)
+    rows = part.global_rows()
+    dev = torch.device("cuda", local_rank)
+    u = torch.tensor(V0[:N * N].reshape(N, N)[rows], device=dev)
+    v = torch.tensor(V0[N * N:].reshape(N, N)[rows], device=dev)
+    p = torch.zeros((part.nL, N), dtype=torch.float64, device=dev)
+    ops = slab.DeviceSlabOps(N, N, L, L, wl["Re"], part, device=local_rank)
+    A, b, c = getRKmethod("RK44")
+    ex = slab.Exchange(part)
+    erk = slab.SlabERK(ops, part, ex, A, b, c, solver="fft")
+    stream = torch.cuda.current_stream()
+    t = 0.0
+    for n in range(args.warmup):
+        erk.step(u, v, p, t, dt)
+        t += dt
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for n in range(args.steps):
+        erk.step(u, v, p, t, dt)
+        t += dt
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    ms_max = float(tt.item())
+    cells = N * N
+    value = cells * args.steps / (ms_max / 1e3)
+    # end to end: each rank's slab from pinned host memory in, one step, back out
+    I = part.interior()
+    hu = torch.empty((part.n, N), dtype=torch.float64, pin_memory=True)
+    hv = torch.empty_like(hu)
+    hp = torch.empty_like(hu)
+    hu.copy_(u[I].cpu())
+    hv.copy_(v[I].cpu())
+    hp.copy_(p[I].cpu())
+    e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    tw0 = time.perf_counter()
+    for n in range(e_steps):
+        u[I].copy_(hu, non_blocking=True)
+        v[I].copy_(hv, non_blocking=True)
+        p[I].copy_(hp, non_blocking=True)
+        erk.step(u, v, p, t, dt)
+        t += dt
+        hu.copy_(u[I])
+        hv.copy_(v[I])
+        hp.copy_(p[I])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - tw0) * 1e3)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item())
+    nbytes = 8 * 3 * part.n * N
+    # divergence of the final field on this rank's rows, maximum over the ranks
+    f = ops.div(u, v)
+    md = torch.tensor([float(f[I].abs().max())], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(md, op=dist.ReduceOp.MAX)
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(WORKLOADS["turb2048"], budget_s=args.cpu_budget)
+    res = {
+        "metric": "cell-updates/s per RK4 step incl. Poisson solve", "value": value, "unit": "cell-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": wl["desc"], "grid": [N, N], "dt": dt, "cells": cells,
+                   "rows_per_rank": part.counts, "l2": "working set > 126 MB L2 (no flush)",
+                   "parallelism": f"y-slabs over {world} rank(s)"},
+        "e2e": {"value": cells * e_steps / (e2e_ms / 1e3), "unit": "cell-updates/s", "steps": e_steps,
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+        # per RK4 step on each rank: 4 right-hand sides (F), 4 projections' gradients, 4 divergences, and
+        # the 3 + 1 solves of three transform passes each (the rest are torch element-wise operations)
+        "gpu_launches": args.steps * (4 + 4 + 4 + 4 * 3),
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "accuracy": {"maxdiv": float(md.item())},
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    ops.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_ensemble(args, wl, rank, world, local_rank):
     """The batching workload: a fixed ensemble of wl['n'] members split over
     the ranks (LPT by cells); each rank advances its share as one ensemble.
@@ -930,6 +1049,8 @@ def main():
         run_reference(args, wl, rank, world)
     elif wl.get("kind") == "ensemble":
         run_ensemble(args, wl, rank, world, local_rank)
+    elif wl.get("kind") == "slab":
+        run_slab(args, wl, rank, world, local_rank)
     else:
         run_ours(args, wl, rank, world, local_rank)
 

@@ -257,6 +257,35 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
 int ins2d_fft_poisson_noalloc(const double *f, double *dp, int32_t Nx, int32_t Ny, double dx, double dy,
                               void *stream);
 
+/* --- one grid over several GPUs: FFT solve in y-slabs ---------------------
+ * The reference's only distributed path is the PETSc-MPI Poisson solve
+ * (solvers/pressure/petsc_poisson_par.c:38-52).  Here the FFT branch of
+ * pressure_poisson.m:92-104 is split at the transposes for a periodic
+ * uniform Nx x Ny grid whose rows are split over processes (one per GPU):
+ * each rank transforms its rows, an all-to-all between the calls (done by
+ * the caller, e.g. over NCCL) gives each rank whole columns of a range of
+ * wave numbers, the column transforms apply -1/Ahat, and the inverse goes
+ * back the same way.  Arrays are device arrays of the given device: spec
+ * rows nrows x (Nx/2+1) complex (interleaved doubles), cols Ny x width
+ * complex holding wave numbers I0 .. I0+width-1 (those >= Nx/2+1 are
+ * padding).  Nx, Ny powers of two from 64 to 8192.  Every call returns after
+ * the stream has finished its work. */
+typedef struct ins2d_slab_fft ins2d_slab_fft;
+int ins2d_slab_fft_create(int32_t Nx, int32_t Ny, double dx, double dy, int32_t device, ins2d_slab_fft **out);
+int ins2d_slab_fft_destroy(ins2d_slab_fft *s);
+const char *ins2d_slab_fft_last_error(const ins2d_slab_fft *s);
+/* spec = forward transforms of the rows of f (nrows x Nx, real) */
+int ins2d_slab_fft_rows_forward(ins2d_slab_fft *s, const double *f, int32_t nrows, double *spec, void *stream);
+/* in place on cols: forward column transforms, -1/Ahat (Ahat(0,0) = 1),
+ * inverse column transforms; *maxabs = max |fhat| of these columns (the
+ * caller takes the maximum over the ranks for the early return) */
+int ins2d_slab_fft_columns(ins2d_slab_fft *s, double *cols, int32_t width, int32_t I0, double *maxabs, void *stream);
+/* dp rows (nrows x Nx) = inverse row transforms of spec, scaled 1/(Nx Ny);
+ * all zero when maxabs (the maximum over all ranks) < 1e-14
+ * (pressure_poisson.m:21-32) */
+int ins2d_slab_fft_rows_inverse(ins2d_slab_fft *s, const double *spec, int32_t nrows, double maxabs, double *dp,
+                                void *stream);
+
 /* --- ensembles ------------------------------------------------------------
  * No single counterpart in the reference: the reference runs one case per
  * MATLAB process (main.m); ensembles of independent flows (different grids,

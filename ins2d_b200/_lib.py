@@ -32,6 +32,8 @@ EXPORTED = [
     "ins2d_cnn_get_params", "ins2d_cnn_set_params", "ins2d_cnn_get_activations", "ins2d_cnn_forward", "ins2d_cnn_loss_grad",
     "ins2d_cnn_train_step", "ins2d_cnn_loss_grad_residual", "ins2d_cnn_train_step_residual", "ins2d_cnn_prepare_pairs", "ins2d_set_learned_guess", "ins2d_set_learned_mode", "ins2d_record_pairs",
     "ins2d_recorded_pairs", "ins2d_learned_train",
+    "ins2d_slab_fft_create", "ins2d_slab_fft_destroy", "ins2d_slab_fft_last_error", "ins2d_slab_fft_rows_forward",
+    "ins2d_slab_fft_columns", "ins2d_slab_fft_rows_inverse",
 ]
 CNN_NPARAM = 37440
 CNN_PATH_TCGEN05, CNN_PATH_MMA_SYNC = 0, 1
@@ -132,6 +134,13 @@ def load():
         "ins2d_ens_size": (ctypes.c_int32, [vp]),
         "ins2d_ens_member": (vp, [vp, ctypes.c_int32]),
         "ins2d_ens_set_stream": (ctypes.c_int, [vp, vp]),
+        "ins2d_slab_fft_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_int32, P(vp)]),
+        "ins2d_slab_fft_destroy": (ctypes.c_int, [vp]),
+        "ins2d_slab_fft_last_error": (ctypes.c_char_p, [vp]),
+        "ins2d_slab_fft_rows_forward": (ctypes.c_int, [vp, vp, ctypes.c_int32, vp, vp]),
+        "ins2d_slab_fft_columns": (ctypes.c_int, [vp, vp, ctypes.c_int32, ctypes.c_int32, P(ctypes.c_double), vp]),
+        "ins2d_slab_fft_rows_inverse": (ctypes.c_int, [vp, vp, ctypes.c_int32, ctypes.c_double, vp, vp]),
         "ins2d_ens_wait_stream": (ctypes.c_int, [vp, vp]),
         "ins2d_ens_set_state": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int]),
         "ins2d_ens_get_state": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, ctypes.c_int]),

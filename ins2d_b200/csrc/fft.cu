@@ -541,17 +541,19 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
 
 // G spectrum columns of length 2^L: forward DIF, -1/Ahat scaling fused with
 // the last DIF and first DIT passes, inverse DIT; max |fhat| reduction
+// The columns are the first ncols of a spectrum with row stride H (complex
+// values); column c holds wave number I0 + c (I0 > 0 for a slab's column range).
 template <int L, int G>
 __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
-    k_cols_t(int Nx, const double2 *__restrict__ tw, const double *__restrict__ ax, const double *__restrict__ ay,
-             double dxdy, double2 *__restrict__ spec, unsigned long long *__restrict__ maxbits) {
+    k_cols_t(int H, int ncols, int I0, const double2 *__restrict__ tw, const double *__restrict__ ax,
+             const double *__restrict__ ay, double dxdy, double2 *__restrict__ spec,
+             unsigned long long *__restrict__ maxbits) {
   constexpr int N = 1 << L, PER = N >> 3, LD = paddedl<L>();
   extern __shared__ double2 sm[];
   __shared__ double wmax[kThreads / 32];
   const double2 *pyr = tw + N;
-  const int H = Nx / 2 + 1;
   const int c0 = blockIdx.x * G;
-  const int g_here = min(G, H - c0);
+  const int g_here = min(G, ncols - c0);
   for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
     const int k = (int)(gidx / G), line = (int)(gidx % G);
     if (line >= g_here) continue;
@@ -568,7 +570,7 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
   for (unsigned gidx = threadIdx.x; gidx < g_here * PER; gidx += kThreads) {
     const int line = (int)(gidx / PER), k = (int)(gidx % PER);
     double2 *Ls = sm + line * LD;
-    const int I = c0 + line;
+    const int I = I0 + c0 + line;
     double2 x[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) x[m] = Ls[pdl<L>(8 * k + m)];
@@ -775,8 +777,8 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const bool fy = with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
-    k_cols_t<L, G><<<(H + G - 1) / G, kThreads, sm, s>>>(Nx, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy, plan.spec,
-                                                         maxbits);
+    k_cols_t<L, G><<<(H + G - 1) / G, kThreads, sm, s>>>(H, H, 0, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
+                                                         plan.spec, maxbits);
   });
   if (!fy) {
     const int G = cols_group(Ny, plan.logy >= 0);
@@ -813,6 +815,45 @@ cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, c
                                          bool accumulate, cudaStream_t s) {
   const WSplit ws{Vn, T, sv, sa};
   return fft_passes(P, plan, nullptr, &ws, true, alpha, beta, gamma, dp, accumulate, s);
+}
+
+// --- pieces of the transform for a grid split into y-slabs ----------------------
+bool slab_fft_supported(int Nx, int Ny) {
+  const int lx = ilog2_exact(Nx), ly = ilog2_exact(Ny);
+  return lx >= kFusedMinLog && lx <= 13 && ly >= kFusedMinLog && ly <= 13;
+}
+
+cudaError_t slab_rows_forward(int Nx, const double2 *twx, const double *f, int nrows, double2 *spec, cudaStream_t s) {
+  const int pairs = (nrows + 1) / 2;
+  DevOps P{};
+  const WSplit w0{};
+  with_log2<kFusedMinLog>(ilog2_exact(Nx), [&](auto c) {
+    constexpr int L = decltype(c)::value;
+    const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
+    k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(nrows, twx, f, w0, spec, P, 0.0, 0.0, 0.0, 0);
+  });
+  return cudaPeekAtLastError();
+}
+
+cudaError_t slab_columns(int Ny, const double2 *twy, const double *ax, const double *ay, double dxdy, double2 *cols,
+                         int width, int ncols, int I0, unsigned long long *maxbits, cudaStream_t s) {
+  with_log2<kFusedMinLog>(ilog2_exact(Ny), [&](auto c) {
+    constexpr int L = decltype(c)::value, G = cols_per_block<L>();
+    const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
+    k_cols_t<L, G><<<(ncols + G - 1) / G, kThreads, sm, s>>>(width, ncols, I0, twy, ax, ay, dxdy, cols, maxbits);
+  });
+  return cudaPeekAtLastError();
+}
+
+cudaError_t slab_rows_inverse(int Nx, const double2 *twx, const double2 *spec, int nrows, double *out,
+                              const unsigned long long *maxbits, cudaStream_t s) {
+  const int pairs = (nrows + 1) / 2;
+  with_log2<kFusedMinLog>(ilog2_exact(Nx), [&](auto c) {
+    constexpr int L = decltype(c)::value;
+    const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
+    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(nrows, twx, spec, out, 0, maxbits);
+  });
+  return cudaPeekAtLastError();
 }
 
 }  // namespace ins2d

@@ -25,7 +25,8 @@ step of time_ERK (unsteady/time_ERK.m:78-168) then needs, per stage:
 The partition, the exchanges and the step are written against a backend of
 local operators (right-hand side, divergence, gradient, Laplacian, row and
 column transforms) and torch.distributed, so the same code runs on CPU ranks
-(gloo) and GPU ranks (NCCL) with any backend that provides those operators.  Data never moves between GPUs other than
+(gloo) and GPU ranks (NCCL) with any backend that provides those operators;
+DeviceSlabOps is the GPU one.  Data never moves between GPUs other than
 through these collectives; no rank reads another's memory directly.
 """
 from __future__ import annotations
@@ -195,7 +196,7 @@ class SlabERK:
         width = -(-Hc // P.world)
         cols = self.ex.rows_to_cols(spec, width)
         out, mx = ops.fft_cols_solve(cols, P.rank * width)
-        mxt = self.ex.allreduce(torch.tensor([mx], dtype=torch.float64), op="max")
+        mxt = self.ex.allreduce(torch.tensor([mx], dtype=torch.float64, device=f.device), op="max")
         dp = torch.zeros_like(f)
         if float(mxt[0]) < 1e-14:  # pressure_poisson.m:21-32
             return dp
@@ -211,10 +212,10 @@ class SlabERK:
         I = P.interior()
 
         def dots(*pairs):
-            t = torch.tensor([float((a[I] * b[I]).sum()) for a, b in pairs], dtype=torch.float64)
-            return ex.allreduce(t)
+            t = torch.stack([(a[I] * b[I]).sum() for a, b in pairs]).to(torch.float64)
+            return ex.allreduce(t).tolist()
 
-        ff = float(dots((f, f))[0])
+        ff = dots((f, f))[0]
         x = torch.zeros_like(f)
         if ff == 0.0:
             self.iters.append(0)
@@ -223,7 +224,7 @@ class SlabERK:
         z = ops.jacobi(r)
         ex.halo([z], rows=1)
         w = ops.lap(z)
-        gamma, delta, rr = (float(v) for v in dots((r, z), (z, w), (r, r)))
+        gamma, delta, rr = dots((r, z), (z, w), (r, r))
         alpha = gamma / delta
         beta = 0.0
         p = torch.zeros_like(f)
@@ -238,7 +239,7 @@ class SlabERK:
             z = ops.jacobi(r)
             ex.halo([z], rows=1)
             w = ops.lap(z)
-            g_new, delta, rr = (float(v) for v in dots((r, z), (z, w), (r, r)))
+            g_new, delta, rr = dots((r, z), (z, w), (r, r))
             if rr <= self.tol ** 2 * ff:
                 break
             if it >= self.maxit:
@@ -271,7 +272,7 @@ class SlabERK:
                 f = ops.div(un / dt + tu, vn / dt + tv) / self.c[i]
                 dp = self.solve(f)
             else:
-                dp = p  # time_ERK.m:125-127 (halo of p exchanged by the caller's previous step)
+                dp = p  # time_ERK.m:125-127 (p's halo exchanged at the start of the step)
             gu, gv = ops.grad(dp)
             us = un + dt * (tu - self.c[i] * gu)
             vs = vn + dt * (tv - self.c[i] * gv)
@@ -284,3 +285,103 @@ class SlabERK:
         f = ops.div(ku0 - gu, kv0 - gv)
         p += self.solve(f)
         ex.halo([p], rows=1)
+
+
+class DeviceSlabOps:
+    """Local operators of a rank on its GPU: a context of the rank's local
+    grid (Nx x nL cells, periodic, the global spacings) for the right-hand
+    side, divergence, gradient and Laplacian (ins2d_F, ins2d_divergence,
+    ins2d_laplacian), and the transform pieces of the global grid
+    (ins2d_slab_fft_*).  Fields are torch CUDA tensors of the rank's device."""
+
+    def __init__(self, Nx, Ny, Lx, Ly, Re, part, device=0):
+        import ctypes
+        import torch
+        from . import _lib, api, cases
+        self.lib = _lib.load()
+        hx, hy = Lx / Nx, Ly / Ny
+        x = cases.uniform_grid(Nx, 0.0, Lx)
+        y = hy * np.arange(part.nL + 1)
+        # the local context's own solver is not used: Jacobi keeps its set-up small
+        self.ctx = api.Options(x, y, cases.BC_PERIODIC, Re=Re, poisson=4, precond="jacobi", device=device)
+        self.Nx, self.Ny, self.nL = Nx, Ny, part.nL
+        self.Hc = Nx // 2 + 1
+        self.oi = (1.0 / hy) * (1.0 / hx)  # Om^-1 of the uniform periodic grid
+        self.diagA = -2.0 * (hy / hx + hx / hy)  # diagonal of A = M Om^-1 G on that grid
+        self.dev = torch.device("cuda", device)
+        self.zero = torch.zeros(2 * Nx * part.nL, dtype=torch.float64, device=self.dev)
+        self.h = ctypes.c_void_p()
+        rc = self.lib.ins2d_slab_fft_create(Nx, Ny, hx, hy, device, ctypes.byref(self.h))
+        if rc != 0:
+            msg = self.lib.ins2d_slab_fft_last_error(self.h)
+            self.lib.ins2d_slab_fft_destroy(self.h)
+            raise api.Ins2dError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if self.h:
+            self.lib.ins2d_slab_fft_destroy(self.h)
+            self.h = None
+        self.ctx.close()
+
+    def _stream(self):
+        import ctypes
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _check(self, rc):
+        if rc != 0:
+            from .api import Ins2dError
+            msg = self.lib.ins2d_slab_fft_last_error(self.h)
+            raise Ins2dError(rc, msg.decode() if msg else "")
+
+    def _split(self, V, like):
+        n = self.Nx * self.nL
+        return V[:n].view(like.shape), V[n:].view(like.shape)
+
+    def rhs(self, u, v, t=0.0):
+        """Om^-1 R(V) (F.m without the pressure terms) on the local grid"""
+        import torch
+        V = torch.cat([u.reshape(-1), v.reshape(-1)])
+        _, F = self.ctx.F(V, None, None, t, nopressure=1)
+        return self._split(F * self.oi, u)
+
+    def div(self, u, v):
+        import torch
+        f, _ = self.ctx.divergence(torch.cat([u.reshape(-1), v.reshape(-1)]))
+        return f.view(u.shape)
+
+    def grad(self, p):
+        """Om^-1 G p at the u and v points (F(0, p) = -G p on a periodic grid)"""
+        _, F = self.ctx.F(self.zero, None, p.reshape(-1).contiguous(), 0.0)
+        return self._split(F * (-self.oi), p)
+
+    def lap(self, p):
+        return self.ctx.laplacian(p.reshape(-1).contiguous()).view(p.shape)
+
+    def jacobi(self, r):
+        return r / self.diagA
+
+    def fft_rows(self, f):
+        import torch
+        f = f.contiguous()
+        spec = torch.empty((f.shape[0], self.Hc), dtype=torch.complex128, device=self.dev)
+        self._check(self.lib.ins2d_slab_fft_rows_forward(self.h, f.data_ptr(), f.shape[0], spec.data_ptr(),
+                                                         self._stream()))
+        return spec
+
+    def fft_cols_solve(self, cols, I0):
+        import ctypes
+        cols = cols.contiguous()
+        mx = ctypes.c_double()
+        self._check(self.lib.ins2d_slab_fft_columns(self.h, cols.data_ptr(), cols.shape[1], int(I0),
+                                                    ctypes.byref(mx), self._stream()))
+        return cols, mx.value
+
+    def ifft_rows(self, spec):
+        import torch
+        spec = spec.contiguous()
+        out = torch.empty((spec.shape[0], self.Nx), dtype=torch.float64, device=self.dev)
+        # the caller has already taken the early return of a vanishing spectrum
+        self._check(self.lib.ins2d_slab_fft_rows_inverse(self.h, spec.data_ptr(), spec.shape[0], 1.0,
+                                                         out.data_ptr(), self._stream()))
+        return out
