@@ -72,6 +72,13 @@ extern "C" {
 #define INS2D_PRECOND_DEFAULT 0 /* multigrid where the grid allows it, else Jacobi */
 #define INS2D_PRECOND_JACOBI 1
 #define INS2D_PRECOND_MG 2
+/* fast diagonalization: A is separable, A = -(diag(hy) (x) TX + TY (x)
+ * diag(hx)), so the generalized eigenbases of the 1D factors TX, TY give its
+ * inverse on the range of A as four dense transforms (periodic uniform grids:
+ * the Fourier basis, i.e. the FFT solve).  CG then converges in one or two
+ * iterations.  Grids up to 1024 cells per direction (set-up O(n^3) on the
+ * host), or any periodic uniform grid the FFT solver takes. */
+#define INS2D_PRECOND_FDM 3
 
 #define INS2D_PREC_FP64 0
 #define INS2D_PREC_FP32_STENCIL 1

@@ -15,7 +15,7 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOTCONV", 3: "EBREAKDOWN", 4: "ENONFI
 BC_CODES = {"dir": 0, "pres": 1, "per": 2, "sym": 3}
 MEM_HOST, MEM_DEVICE = 0, 1
 PREC_FP64, PREC_FP32_STENCIL = 0, 1
-PRECOND_CODES = {"default": 0, "jacobi": 1, "mg": 2}
+PRECOND_CODES = {"default": 0, "jacobi": 1, "mg": 2, "fdm": 3}
 MAX_STAGES = 8
 
 # every symbol include/ins2d.h declares

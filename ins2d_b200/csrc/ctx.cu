@@ -20,6 +20,7 @@
 #include "kernels.cuh"
 #include "setup.hpp"
 #include "mg_host.hpp"
+#include "fdm_host.hpp"
 
 using namespace ins2d;
 
@@ -63,6 +64,10 @@ struct ins2d_ctx {
   PcgWork pcg{};
   bool use_mg = false;
   MgD mg{};
+  // fast-diagonalization preconditioner (INS2D_PRECOND_FDM)
+  bool use_fdm = false;
+  FdmD fdm{};
+  FftPlan fdm_fft;
   PcgScalars *h_sc = nullptr;   // pinned
   double *h_red = nullptr;      // pinned
   // host copies of boundary samples (check_conservation.m boundary terms)
@@ -232,7 +237,7 @@ void setup_rk(ins2d_ctx *c) {
 // Poisson solve: dp = pressure_poisson(f) (or dp += ... when accumulate)
 // PCG to the relative residual tol (cg.F's rule ||r|| <= tol ||f||)
 int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st, double tol) {
-  const bool block = c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P);
+  const bool block = c->use_fdm ? false : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
   Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
   if (block) {
     if (c->use_mg)
@@ -258,12 +263,16 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
     if (h.status == INS2D_ENONFINITE) return fail(c, INS2D_ENONFINITE, "PCG: non-finite residual");
     return INS2D_OK;
   }
-  if (c->use_mg)
+  if (c->use_fdm)
+    pcg_init_fdm(c->P, c->fdm, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
+  else if (c->use_mg)
     pcg_init_mg(c->P, c->mg, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
   else
     pcg_init(c->P, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
   CK(cudaGetLastError());
-  int chunk = c->use_mg ? 2 : 4;
+  // the fast-diagonalization preconditioner is exact up to rounding: one
+  // iteration at a time between the polls
+  int chunk = c->use_fdm ? 1 : (c->use_mg ? 2 : 4);
   long long launched = 0;
   for (;;) {
     CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->stream));
@@ -272,7 +281,10 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
     const long long limit = c->poll_limit >= 0 ? c->poll_limit : (long long)c->opts.CG_maxit + 1024;
     if (launched >= limit)
       return fail(c, INS2D_ETIMEOUT, "PCG: device convergence flag not set within the host's iteration limit");
-    if (c->use_mg) {
+    if (c->use_fdm) {
+      pcg_iterations_fdm(c->P, c->fdm, c->pcg, chunk, c->stream);
+      c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 7LL : 8LL) * chunk;
+    } else if (c->use_mg) {
       pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->stream);
       c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
     } else {
@@ -281,7 +293,7 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
     }
     CK(cudaGetLastError());
     launched += chunk;
-    chunk = c->use_mg ? 4 : std::min(chunk * 2, 128);
+    chunk = c->use_fdm ? 1 : (c->use_mg ? 4 : std::min(chunk * 2, 128));
   }
   const PcgScalars &h = *c->h_sc;
   if (st) {
@@ -706,7 +718,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     if (opts->poisson < 1 || opts->poisson > 6) throw std::invalid_argument("wrong poisson method");
     if (opts->poisson != INS2D_POISSON_FFT && !(opts->CG_acc > 0)) throw std::invalid_argument("CG_acc must be positive");
     if (opts->poisson != INS2D_POISSON_FFT && opts->CG_maxit < 1) throw std::invalid_argument("CG_maxit must be >= 1");
-    if (opts->precond < INS2D_PRECOND_DEFAULT || opts->precond > INS2D_PRECOND_MG)
+    if (opts->precond < INS2D_PRECOND_DEFAULT || opts->precond > INS2D_PRECOND_FDM)
       throw std::invalid_argument("wrong preconditioner");
     if (opts->rk_stages < 0 || opts->rk_stages > kMaxStages) throw std::invalid_argument("rk_stages out of range");
     for (int i = 0; i < opts->rk_stages; ++i)
@@ -841,7 +853,47 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
       W.blocks = pcg_blocks(P);
       W.partials = dalloc<double>(c, (size_t)W.blocks * 8 + 16);
       CK(cudaMemset(W.sc, 0, sizeof(PcgScalars)));
-      if (opts->precond != INS2D_PRECOND_JACOBI) {
+      if (opts->precond == INS2D_PRECOND_FDM) {
+        FdmD &D = c->fdm;
+        D.nx = H.Npx;
+        D.ny = H.Npy;
+        D.z = dalloc<double>(c, Np);
+        if (H.fft_ok && fft_supported(H.Nx, H.Ny)) {
+          // periodic uniform grid: the Fourier basis, i.e. the FFT solve
+          CK(fft_prepare());
+          FftPlan &F = c->fdm_fft;
+          F.Nx = H.Nx;
+          F.Ny = H.Ny;
+          F.logx = is_pow2(H.Nx) ? (int)std::lround(std::log2((double)H.Nx)) : -1;
+          F.logy = is_pow2(H.Ny) ? (int)std::lround(std::log2((double)H.Ny)) : -1;
+          const std::vector<double> tx = fft_twiddle_table(H.Nx), ty = fft_twiddle_table(H.Ny);
+          F.twx = dalloc<double2>(c, 2 * (size_t)H.Nx);
+          F.twy = dalloc<double2>(c, 2 * (size_t)H.Ny);
+          CK(cudaMemcpy(F.twx, tx.data(), tx.size() * sizeof(double), cudaMemcpyHostToDevice));
+          CK(cudaMemcpy(F.twy, ty.data(), ty.size() * sizeof(double), cudaMemcpyHostToDevice));
+          F.spec = dalloc<double2>(c, (size_t)(H.Nx / 2 + 1) * H.Ny);
+          F.maxabs = dalloc<double>(c, 1);  // the symbol factors P.fft_ax, fft_ay are set above
+          double *gate = dalloc<double>(c, 1);
+          const double one = 1.0;
+          CK(cudaMemcpy(gate, &one, sizeof one, cudaMemcpyHostToDevice));
+          D.spectral = true;
+          D.fft = &c->fdm_fft;
+          D.gate = (const unsigned long long *)gate;
+        } else {
+          if (std::max(H.Npx, H.Npy) > kFdmMaxN)
+            throw std::invalid_argument("fast-diagonalization preconditioner: grid larger than " +
+                                        std::to_string(kFdmMaxN) + " cells in a direction");
+          const FdmHost1D fx = fdm_1d(H.TX, H.hx), fy = fdm_1d(H.TY, H.hy);
+          D.Qx = upload_vec(c, fx.Q);
+          D.Qy = upload_vec(c, fy.Q);
+          D.lx = upload_vec(c, fx.lam);
+          D.ly = upload_vec(c, fy.lam);
+          D.thr = 1e-12 * (fx.lam.back() + fy.lam.back());
+          D.t1 = dalloc<double>(c, Np);
+          D.t2 = dalloc<double>(c, Np);
+        }
+        c->use_fdm = true;
+      } else if (opts->precond != INS2D_PRECOND_JACOBI) {
         std::vector<MgHostLevel> lv;
         try {
           lv = mg_build_levels(H);

@@ -748,8 +748,11 @@ cudaError_t fft_prepare() {
 }
 
 namespace {
+// gate: the word the last pass reads for the early return (null: the
+// spectrum's own max |fhat|)
 cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, const WSplit *ws, bool div,
-                       double alpha, double beta, double gamma, double *dp, bool accumulate, cudaStream_t s) {
+                       double alpha, double beta, double gamma, double *dp, bool accumulate, cudaStream_t s,
+                       const unsigned long long *gate = nullptr) {
   const int Nx = plan.Nx, Ny = plan.Ny;
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
@@ -790,10 +793,12 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const bool fx2 = with_log2<kFusedMinLog>(plan.logx, [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
-    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, plan.spec, dp, accumulate ? 1 : 0, maxbits);
+    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
+                                                gate ? gate : maxbits);
   });
   if (!fx2)
-    k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0, maxbits);
+    k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
+                                            gate ? gate : maxbits);
   return cudaSuccess;
 }
 }  // namespace
@@ -808,6 +813,11 @@ bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= kFusedMinLog && pl
 cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s) {
   return fft_passes(P, plan, W, nullptr, true, alpha, beta, gamma, dp, accumulate, s);
+}
+
+cudaError_t launch_fft_precond(const DevOps &P, const FftPlan &plan, const double *r, double *z,
+                               const unsigned long long *gate, cudaStream_t s) {
+  return fft_passes(P, plan, r, nullptr, false, 0.0, 0.0, 0.0, z, false, s, gate);
 }
 
 cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, const double *Vn, const float *T,

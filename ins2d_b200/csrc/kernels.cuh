@@ -156,6 +156,11 @@ cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const doubl
 bool fft_fuses_div(const FftPlan &plan);
 cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s);
+// z = A^+ r by the same transform (the exact inverse of a periodic uniform
+// grid, as a PCG preconditioner): the early return is read from *gate
+// instead of the spectrum (a word holding a large value disables it)
+cudaError_t launch_fft_precond(const DevOps &P, const FftPlan &plan, const double *r, double *z,
+                               const unsigned long long *gate, cudaStream_t s);
 // Same with W = Vn sv + sa T, T in FP32 (FP32-storage stages)
 cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, const double *Vn, const float *T,
                                          double sv, double sa, double alpha, double beta, double gamma, double *dp,
@@ -163,6 +168,24 @@ cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, c
 // Opts the transform kernels in to large dynamic shared memory on the current
 // device; returns the first failure.
 cudaError_t fft_prepare();
+
+// --- fast-diagonalization preconditioner (fdm.cu) -----------------------------------
+// Generalized eigenbases of the pressure matrix's 1D factors (fdm_host.cpp)
+// and the work arrays of one application.
+struct FdmD {
+  int nx = 0, ny = 0;
+  const double *Qx = nullptr, *Qy = nullptr;  // nx x nx, ny x ny row-major (Q[i*n + a])
+  const double *lx = nullptr, *ly = nullptr;  // eigenvalues
+  double thr = 0.0;                           // lx + ly <= thr: the null mode (left out)
+  double *t1 = nullptr, *t2 = nullptr;        // nx*ny each
+  double *z = nullptr;                        // the preconditioned residual
+  // periodic uniform grids: the Fourier basis, applied by the FFT solve
+  bool spectral = false;
+  const FftPlan *fft = nullptr;
+  const unsigned long long *gate = nullptr;  // device word holding 1.0 (no early return)
+};
+// z = A^+ r (four dense products); no work once *done is set (done may be null)
+void fdm_apply(const FdmD &F, const double *r, double *z, const int *done, cudaStream_t s);
 
 // --- PCG (pcg.cu) ---------------------------------------------------------------
 struct PcgScalars {
@@ -187,6 +210,10 @@ int pcg_blocks(const DevOps &P);
 void pcg_init_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double tol, long long maxit,
                  cudaStream_t s);
 void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, cudaStream_t s);
+// The same with the fast-diagonalization preconditioner
+void pcg_init_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double *f, double tol, long long maxit,
+                  cudaStream_t s);
+void pcg_iterations_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, int n, cudaStream_t s);
 
 struct EnsMemberD {
   DevOps P;

@@ -576,6 +576,33 @@ void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, c
   }
 }
 
+namespace {
+void precond_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, cudaStream_t s) {
+  if (F.spectral)
+    launch_fft_precond(P, *F.fft, W.r, F.z, F.gate, s);
+  else
+    fdm_apply(F, W.r, F.z, &W.sc->done, s);
+}
+}  // namespace
+
+void pcg_init_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double *f, double tol, long long maxit,
+                  cudaStream_t s) {
+  k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
+  precond_fdm(P, F, W, s);
+  k_rz_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(W, F.z, P.Np, 1);
+}
+
+void pcg_iterations_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, int n, cudaStream_t s) {
+  const unsigned g = vec_blocks(P, W);
+  for (int it = 0; it < n; ++it) {
+    k_spmv<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W);
+    k_update_g<<<g, kVecThreads, 0, s>>>(W, P.Np);
+    precond_fdm(P, F, W, s);
+    k_rz_g<<<g, kVecThreads, 0, s>>>(W, F.z, P.Np, 0);
+    k_pupdate_g<<<g, kVecThreads, 0, s>>>(W, F.z, P.Np);
+  }
+}
+
 void pcg_finish(const DevOps &P, const PcgWork &W, double *dp, bool accumulate, cudaStream_t s) {
   long long n = P.Np;
   long long blocks = (n + 255) / 256;

@@ -87,3 +87,19 @@ extern "C" int probe_mg_level(void *m, int l, int *dims, int which, const double
   return 0;
 }
 extern "C" const double *probe_mg_pinv(void *m) { return ((ProbeMg *)m)->pinv.data(); }
+
+// generalized eigen-decomposition of TX (dir 0) or TY (dir 1) against the
+// cell widths hx / hy (the fast-diagonalization preconditioner's factors)
+#include "fdm_host.hpp"
+extern "C" int probe_fdm(void *h, int dir, double *Q, double *lam) {
+  HostOps *H = (HostOps *)h;
+  try {
+    FdmHost1D F = dir == 0 ? fdm_1d(H->TX, H->hx) : fdm_1d(H->TY, H->hy);
+    std::memcpy(Q, F.Q.data(), F.Q.size() * sizeof(double));
+    std::memcpy(lam, F.lam.data(), F.lam.size() * sizeof(double));
+    return F.n;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}

@@ -24,7 +24,7 @@ def probe(tmp_path_factory):
     csrc = os.path.join(ROOT, "ins2d_b200", "csrc")
     subprocess.check_call(["g++", "-O1", "-std=c++17", "-shared", "-fPIC", "-I", csrc,
                            os.path.join(ROOT, "tests", "native", "probe.cpp"), os.path.join(csrc, "setup.cpp"),
-                           os.path.join(csrc, "mg_host.cpp"), "-o", str(out)])
+                           os.path.join(csrc, "mg_host.cpp"), os.path.join(csrc, "fdm_host.cpp"), "-o", str(out)])
     lib = ctypes.CDLL(str(out))
     lib.probe_build.restype = ctypes.c_void_p
     lib.probe_build.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
