@@ -74,6 +74,18 @@ WORKLOADS = {
                           desc="decaying 2D turbulence 2048x2048 periodic, Re=2000, RK44, CFL 0.5, FFT Poisson, FP64, "
                                "the one grid split into y-slabs over the ranks (halo exchanges and all-to-all "
                                "transposes over NCCL)"),
+    "ldc64_fdm": dict(N=64, L=1.0, Re=1000.0, poisson=4, precision="fp64", ic="rest", dt=1e-3, CG_acc=1e-12,
+                      precond="fdm",
+                      desc="lid-driven cavity 64x64, Re=1000, RK44 dt=1e-3, PCG to 1e-12 with the fast-diagonalization "
+                           "preconditioner, FP64"),
+    "bfs1024_fdm": dict(N=1024, ic="bfs", Re=800.0, poisson=4, precision="fp64", dt=1e-3, CG_acc=1e-10,
+                        precond="fdm",
+                        desc="backward-facing step 1024x1024 as bfs1024, PCG to 1e-10 with the fast-diagonalization "
+                             "preconditioner, FP64"),
+    "turb2048_pcg_fdm": dict(N=2048, L=1.0, Re=2000.0, poisson=4, precision="fp64", ic="turbulence", CG_acc=1e-10,
+                             precond="fdm",
+                             desc="decaying 2D turbulence 2048x2048, PCG to 1e-10 preconditioned by the FFT solve "
+                                  "(the fast-diagonalization preconditioner's Fourier basis), FP64"),
     "ens256": dict(kind="ensemble", n=256, sizes=(64, 96, 128, 192, 256), stretch=1.05, dt=5e-4, CG_acc=1e-10,
                    poisson=4, precision="fp64",
                    desc="ensemble of 256 cavity/channel flows, tanh-stretched 1.05, nx,ny in {64..256}, "

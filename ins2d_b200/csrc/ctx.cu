@@ -781,6 +781,7 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     P.rMX = reg(H.rMX, H.MX); P.rMY = reg(H.rMY, H.MY);
     walker_rectangle(P);
     CK(walker_prepare());
+    CK(cudaDeviceGetAttribute(&P.nsm, cudaDevAttrMultiProcessorCount, c->device));
     if (H.fft_ok) {
       P.fft_ax = upload_vec(c, H.fft_ax);
       P.fft_ay = upload_vec(c, H.fft_ay);

@@ -12,6 +12,8 @@
 // their field rows in L1.  Boundary rows of the operators use the same tables
 // (the boundary elimination lives in the table entries), so there is one
 // code path for every boundary-condition combination.
+#include <algorithm>
+
 #include "kernels.cuh"
 
 namespace ins2d {
@@ -586,8 +588,6 @@ __device__ void fast_v(const DevOps &P, const TV *__restrict__ u, const TV *__re
 // host): every shift of the regular rows in [-2, 1], and rows of u and v
 // that start on 16-byte boundaries (Nux, Nvx, Nu multiples of 16 bytes /
 // sizeof(TV)).
-constexpr int kTileThreads = 256;
-constexpr int kTileSeg = RUN / 2;   // rows per thread
 constexpr int kTileRows = RUN + 5;  // staged rows j0-2 .. j0+RUN+2
 
 // staged columns i0-HL .. : HL = one 16-byte chunk of halo on the left,
@@ -728,108 +728,208 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i,
   }
 }
 
-// shared memory of one tile: the staged fields, the right-hand sides and the
-// tile's y-weights (dynamic: more than the 48 KB of static shared memory)
-template <typename S, typename TV>
-struct TileSmem {
+// Persistent, pipelined form of the tiled walkers: each thread block loops
+// over tiles (blockIdx.x, + gridDim.x, ...) and keeps two buffers, so the
+// asynchronous copies of the next tile's u/v halo tile, its y-weights and (for
+// the FP64 stage) its Vn tile are in flight while the current tile is
+// computed.  Per tile: phase 1 walks the columns (warps 0-7: u, 8-15: v, four
+// row segments per column) into R; phase 2 is the epilogue of every point,
+// consecutive threads on consecutive columns.
+constexpr int kPipeThreads = 512;
+constexpr int kPipeSegs = kPipeThreads / WX / 2;  // row segments per column and component
+constexpr int kPipeRows = RUN / kPipeSegs;        // rows per thread
+
+template <typename TV, int MODE>
+struct PipeBuf {
   TileSm<TV> T;
-  S R[2][RUN][WX];
   YRowsN<RUN> Y;
+  double Vn[MODE == 0 ? 2 : 1][MODE == 0 ? RUN : 1][WX];  // MODE 0: the tile's Vn (u, v)
+};
+template <typename S, int MODE, typename TV>
+struct PipeSmem {
+  PipeBuf<TV, MODE> buf[2];
+  S R[2][RUN][WX];
 };
 
-#ifndef INS2D_TILE_MINB
-#define INS2D_TILE_MINB 3
-#endif
-#ifndef INS2D_TILE_EPI_UNROLL
-#define INS2D_TILE_EPI_UNROLL 4
-#endif
-constexpr int kEpiUnroll = INS2D_TILE_EPI_UNROLL;
-// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
-template <typename S, int MODE, typename TV>
-__global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
-    k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// the asynchronous copies of tile (bx, by) into B
+template <int MODE, typename TV>
+__device__ __forceinline__ void pipe_issue(const DevOps &P, const TV *__restrict__ V, const Epi &e, int bx, int by,
+                                           PipeBuf<TV, MODE> &B, int tid) {
   using G = TileGeo<TV>;
-  extern __shared__ __align__(16) unsigned char tile_smem[];
-  TileSmem<S, TV> &M = *reinterpret_cast<TileSmem<S, TV> *>(tile_smem);
-  const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
   const int i0 = bx * WX, j0 = by * RUN;
-  const int tid = threadIdx.x + WX * threadIdx.y;
   const TV *u = V, *v = V + P.Nu;
-  // stage the u and v rows j0-2 .. j0+RUN+2, columns i0-HL .. (wrapped)
-  for (int q = tid; q < 2 * kTileRows * G::CHUNKS; q += kTileThreads) {
+  for (int q = tid; q < 2 * kTileRows * G::CHUNKS; q += kPipeThreads) {
     const int f = q >= kTileRows * G::CHUNKS;
     const int qq = q - f * kTileRows * G::CHUNKS;
     const int r = qq / G::CHUNKS, ch = qq - r * G::CHUNKS;
     if (f == 0) {
       const int gr = wrapm(j0 - 2 + r, P.Nuy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nux);
-      cp_async16(&M.T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
+      cp_async16(&B.T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
     } else {
       const int gr = wrapm(j0 - 2 + r, P.Nvy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nvx);
-      cp_async16(&M.T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
+      cp_async16(&B.T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
     }
   }
-  stage_yrows(P, j0, M.Y);
-  cp_async_wait_all();
-  __syncthreads();
-  // phase 1: walk the columns
-  {
-    const int i = i0 + threadIdx.x;
-    const int seg = threadIdx.y & 1;
-    const int ja = j0 + seg * kTileSeg, jb = ja + kTileSeg;
-    if (threadIdx.y < 2)
-      tile_u<S, TV>(P, M.T, M.R[0], i, i0, j0, ja, jb, M.Y);
-    else
-      tile_v<S, TV>(P, M.T, M.R[1], i, i0, j0, ja, jb, M.Y);
-  }
-  __syncthreads();
-  // phase 2: the epilogue of every point, consecutive threads on consecutive
-  // columns and all of a thread's loads independent of each other
-  const YRowsN<RUN> &Y = M.Y;
-#pragma unroll kEpiUnroll
-  for (int m = 0; m < 2 * RUN * WX / kTileThreads; ++m) {
-    const int o = tid + kTileThreads * m;
-    const int comp = o / (RUN * WX);
-    const int oo = o - comp * (RUN * WX);
-    const int jr = oo / WX, ic = oo - jr * WX;
-    const int i = i0 + ic, j = j0 + jr;
-    const double R = (double)M.R[comp][jr][ic];
-    long long idx;
-    double oi;
-    if (comp == 0) {
-      idx = (long long)j * P.Nux + i;
-      oi = Y.rhy[jr] * __ldg(P.rgxi + i);
-    } else {
-      idx = P.Nu + (long long)j * P.Nvx + i;
-      oi = Y.rgyi[jr] * __ldg(P.rhx + i);
+  if constexpr (MODE == 0) {
+    constexpr int CH = WX / 2;  // 16-byte chunks per row
+    for (int q = tid; q < 2 * RUN * CH; q += kPipeThreads) {
+      const int comp = q / (RUN * CH);
+      const int qq = q - comp * RUN * CH;
+      const int r = qq / CH, ch = qq - r * CH;
+      const double *src = comp == 0 ? e.Vn + (long long)(j0 + r) * P.Nux + i0 + 2 * ch
+                                    : e.Vn + P.Nu + (long long)(j0 + r) * P.Nvx + i0 + 2 * ch;
+      cp_async16(&B.Vn[comp][r][2 * ch], src);
     }
-    if constexpr (MODE == 0) {
-      const double k = oi * R;
-      if (e.kV) e.kV[idx] = k;
-      double vt = 0.0;
-      for (int q = 0; q < e.nprev; ++q) vt += e.aprev[q] * __ldg(e.kprev[q] + idx);
-      vt += e.aii * k;
-      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
-    } else if constexpr (MODE == 2) {
-      epi_stage32(e, idx, oi * R);
-    } else {
-      double g;
-      if (comp == 0) {
-        g = -Y.hy[jr] * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
-      } else {
-        const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
-        double gy = Y.myt0[jr] * __ldg(e.p + (long long)c0 * P.Npx + i);
-        if (P.rMYT.two) gy += Y.myt1[jr] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
-        g = -__ldg(P.hx + i) * gy;
+  }
+  // y-weights and metrics of the tile's faces (RUN + 1) and rows (RUN)
+  YRowsN<RUN> &Y = B.Y;
+  for (int q = tid; q < 10 * (RUN + 1) + 8 * RUN; q += kPipeThreads) {
+    const double *src;
+    double *dst;
+    if (q < 10 * (RUN + 1)) {
+      const int a = q / (RUN + 1), t = q - a * (RUN + 1), r = j0 + t;
+      switch (a) {
+        case 0: src = P.rAUY.w0 + r; dst = Y.auy0 + t; break;
+        case 1: src = P.rAUY.w1 + r; dst = Y.auy1 + t; break;
+        case 2: src = P.rSUY.w0 + r; dst = Y.suy0 + t; break;
+        case 3: src = P.rSUY.w1 + r; dst = Y.suy1 + t; break;
+        case 4: src = P.rIVY.w0 + r; dst = Y.ivy0 + t; break;
+        case 5: src = P.rIVY.w1 + r; dst = Y.ivy1 + t; break;
+        case 6: src = P.rAVY.w0 + r; dst = Y.avy0 + t; break;
+        case 7: src = P.rAVY.w1 + r; dst = Y.avy1 + t; break;
+        case 8: src = P.rSVY.w0 + r; dst = Y.svy0 + t; break;
+        default: src = P.rSVY.w1 + r; dst = Y.svy1 + t; break;
       }
-      epi_residual(e, idx, oi, R, g);
+    } else {
+      const int qq = q - 10 * (RUN + 1);
+      const int a = qq / RUN, t = qq - a * RUN, j = j0 + t;
+      switch (a) {
+        case 0: src = P.hy + j; dst = Y.hy + t; break;
+        case 1: src = P.rhy + j; dst = Y.rhy + t; break;
+        case 2: src = P.rIUY.w0 + j; dst = Y.iuy0 + t; break;
+        case 3: src = P.rIUY.w1 + j; dst = Y.iuy1 + t; break;
+        case 4: src = P.gyi + j; dst = Y.gyi + t; break;
+        case 5: src = P.rgyi + j; dst = Y.rgyi + t; break;
+        case 6: src = P.rMYT.w0 + j; dst = Y.myt0 + t; break;
+        default: src = P.rMYT.w1 + j; dst = Y.myt1 + t; break;
+      }
     }
+    cp_async8(dst, src);
   }
+}
+
+// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
+template <typename S, int MODE, typename TV>
+__global__ void __launch_bounds__(kPipeThreads, 1)
+    k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  PipeSmem<S, MODE, TV> &M = *reinterpret_cast<PipeSmem<S, MODE, TV> *>(tile_smem);
+  const int nbx = P.fbx1 - P.fbx0, nby = P.fby1 - P.fby0;
+  const int ntiles = nbx * nby;
+  const int tid = threadIdx.x + WX * threadIdx.y;
+  int t = blockIdx.x;
+  int cur = 0;
+  if (t < ntiles) pipe_issue<MODE, TV>(P, V, e, P.fbx0 + t % nbx, P.fby0 + t / nbx, M.buf[0], tid);
+  cp_async_commit();
+  for (; t < ntiles; t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    if (tn < ntiles) pipe_issue<MODE, TV>(P, V, e, P.fbx0 + tn % nbx, P.fby0 + tn / nbx, M.buf[cur ^ 1], tid);
+    cp_async_commit();
+    cp_async_wait<1>();  // this tile's copies have landed (the next tile's may still fly)
+    __syncthreads();
+    const PipeBuf<TV, MODE> &B = M.buf[cur];
+    const int bx = P.fbx0 + t % nbx, by = P.fby0 + t / nbx;
+    const int i0 = bx * WX, j0 = by * RUN;
+    // phase 1: walk the columns
+    {
+      const int i = i0 + threadIdx.x;
+      const int comp = threadIdx.y / kPipeSegs, seg = threadIdx.y % kPipeSegs;
+      const int ja = j0 + seg * kPipeRows, jb = ja + kPipeRows;
+      if (comp == 0)
+        tile_u<S, TV>(P, B.T, M.R[0], i, i0, j0, ja, jb, B.Y);
+      else
+        tile_v<S, TV>(P, B.T, M.R[1], i, i0, j0, ja, jb, B.Y);
+    }
+    __syncthreads();
+    // phase 2: the epilogue of every point
+    const YRowsN<RUN> &Y = B.Y;
+#pragma unroll 4
+    for (int m = 0; m < 2 * RUN * WX / kPipeThreads; ++m) {
+      const int o = tid + kPipeThreads * m;
+      const int comp = o / (RUN * WX);
+      const int oo = o - comp * (RUN * WX);
+      const int jr = oo / WX, ic = oo - jr * WX;
+      const int i = i0 + ic, j = j0 + jr;
+      const double R = (double)M.R[comp][jr][ic];
+      long long idx;
+      double oi;
+      if (comp == 0) {
+        idx = (long long)j * P.Nux + i;
+        oi = Y.rhy[jr] * __ldg(P.rgxi + i);
+      } else {
+        idx = P.Nu + (long long)j * P.Nvx + i;
+        oi = Y.rgyi[jr] * __ldg(P.rhx + i);
+      }
+      if constexpr (MODE == 0) {
+        const double k = oi * R;
+        if (e.kV) e.kV[idx] = k;
+        double vt = 0.0;
+        for (int q = 0; q < e.nprev; ++q) vt += e.aprev[q] * __ldg(e.kprev[q] + idx);
+        vt += e.aii * k;
+        e.Wt[idx] = B.Vn[comp][jr][ic] * e.inv_dt + vt;
+      } else if constexpr (MODE == 2) {
+        epi_stage32(e, idx, oi * R);
+      } else {
+        double g;
+        if (comp == 0) {
+          g = -Y.hy[jr] * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
+        } else {
+          const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
+          double gy = Y.myt0[jr] * __ldg(e.p + (long long)c0 * P.Npx + i);
+          if (P.rMYT.two) gy += Y.myt1[jr] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
+          g = -__ldg(P.hx + i) * gy;
+        }
+        epi_residual(e, idx, oi, R, g);
+      }
+    }
+    __syncthreads();  // buffer cur is refilled in the next iteration but one; R is rewritten in the next
+    cur ^= 1;
+  }
+  cp_async_wait<0>();
 }
 
 template <typename S, int MODE, typename TV>
 cudaError_t tile_prepare_one() {
   return cudaFuncSetAttribute((const void *)k_walk_tile<S, MODE, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(TileSmem<S, TV>));
+                              (int)sizeof(PipeSmem<S, MODE, TV>));
+}
+
+// resident blocks per SM of an instance (cached per instance and device)
+template <typename S, int MODE, typename TV>
+int tile_blocks_per_sm() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 1;
+  if (!cached[dev]) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk_tile<S, MODE, TV>, kPipeThreads,
+                                                      sizeof(PipeSmem<S, MODE, TV>)) != cudaSuccess ||
+        b < 1)
+      b = 1;
+    cached[dev] = b;
+  }
+  return cached[dev];
 }
 
 // one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
@@ -939,18 +1039,20 @@ void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   const int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   dim3 g((nx + WX - 1) / WX, (ny + RUN - 1) / RUN);
   const bool has_fast = P.fbx1 > P.fbx0 && P.fby1 > P.fby0;
-  const bool tiled = (sizeof(TV) == 8 ? P.tile_ok : P.tile_ok32) && (((uintptr_t)V & 15) == 0);
+  const bool tiled = (sizeof(TV) == 8 ? P.tile_ok : P.tile_ok32) && (((uintptr_t)V & 15) == 0) &&
+                     (e.mode != 0 || (((uintptr_t)e.Vn & 15) == 0)) && P.nsm > 0;
   if (has_fast) {
     const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
     if (tiled) {
-      const dim3 tb(WX, kTileThreads / WX);
-      const size_t sm = sizeof(TileSmem<S, TV>);
+      const dim3 tb(WX, kPipeThreads / WX);
+      const int ntiles = (int)(gf.x * gf.y);
+      auto blocks = [&](int per_sm) { return std::min(ntiles, P.nsm * per_sm); };
       if (e.mode == 0)
-        k_walk_tile<S, 0, TV><<<gf, tb, sm, s>>>(P, V, e);
+        k_walk_tile<S, 0, TV><<<blocks(tile_blocks_per_sm<S, 0, TV>()), tb, sizeof(PipeSmem<S, 0, TV>), s>>>(P, V, e);
       else if (e.mode == 1)
-        k_walk_tile<S, 1, TV><<<gf, tb, sm, s>>>(P, V, e);
+        k_walk_tile<S, 1, TV><<<blocks(tile_blocks_per_sm<S, 1, TV>()), tb, sizeof(PipeSmem<S, 1, TV>), s>>>(P, V, e);
       else
-        k_walk_tile<S, 2, TV><<<gf, tb, sm, s>>>(P, V, e);
+        k_walk_tile<S, 2, TV><<<blocks(tile_blocks_per_sm<S, 2, TV>()), tb, sizeof(PipeSmem<S, 2, TV>), s>>>(P, V, e);
     } else {
       k_walk_fast<S, TV><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
     }
