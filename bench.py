@@ -97,11 +97,12 @@ WORKLOADS = {
 # family, averaged over the family's launches in an RK44 step with steady
 # boundary conditions (each array read or written once per launch).
 # FP64 storage:
-#   stage:    first stage from the cached residual (kV0, Vn in; Wt out: 48),
-#             stages 2-3 (V_s, Vn in; Wt, kV out: 64 each), stage 4 (V_s, Vn,
-#             three earlier kV in; Wt out: 96)            -> 272 / 4 launches
+#   stage:    stages 2-3 (V_s, Vn in; Wt, kV out: 64 each), stage 4 (V_s, Vn,
+#             three earlier kV in; Wt out: 96)            -> 224 / 3 launches
 #   residual: V, p in; w, kV_next out                      -> 56
-#   project:  Wt, dp in; V out                             -> 40
+#   project:  the first stage from the cached residual fused into its
+#             projection (Vn, kV0, p in; V_s out: 56), stages 2-4 (Wt, dp in;
+#             V out: 40 each)                              -> 176 / 4
 #   poisson_fft: rows with the divergence fused in (W in 16, half spectrum out
 #             8), columns (8 + 8), rows back (8 in, dp out 8; + 8 for the
 #             accumulating additional solve)               -> (3*56 + 64) / 4
@@ -115,12 +116,12 @@ WORKLOADS = {
 #   poisson_fft: rows from Vn 16 + Vtemp 8 (stage solves) or w 16 (additional
 #             solve) -> 3*64 + 64 over 4 solves
 FAMILY_BYTES = {
-    "fp64": {"stage": 272 / 4.0, "residual": 56.0, "project": 40.0, "poisson_fft": (3 * 56 + 64) / 4.0,
+    "fp64": {"stage": 224 / 3.0, "residual": 56.0, "project": 176 / 4.0, "poisson_fft": (3 * 56 + 64) / 4.0,
              "div": 24.0},
     "fp32": {"stage": 72 / 3.0, "residual": 48.0, "project": 168 / 4.0, "poisson_fft": 64.0, "div": 32.0},
 }
 # per RK44 step: all launches of the families above
-STEP_BYTES = {"fp64": 272 + 56 + 4 * 40 + (3 * 56 + 64), "fp32": 72 + 48 + 168 + 4 * 64}
+STEP_BYTES = {"fp64": 224 + 56 + 176 + (3 * 56 + 64), "fp32": 72 + 48 + 168 + 4 * 64}
 # the same step in the reference's operator decomposition (fused stage + divergence
 # 88, projection 40, FFT solve 64 per stage, additional solve 40 + solve)
 STEP_BYTES_REFERENCE_DECOMPOSITION = 808

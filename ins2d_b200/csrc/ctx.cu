@@ -606,6 +606,14 @@ int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step
   if (rc) return rc;
   const double *dpp = nullptr;
   for (int i = 0; i < c->s; ++i) {
+    if (i == 0 && k0_cached && !c->bcd.bc_unsteady && c->s > 1) {
+      // first stage from the cached residual fused into its projection
+      // (dp = p: time_ERK.m:125-127); Wt is not formed
+      Prof pr(c, INS2D_PROF_PROJECT, 1);
+      launch_project_cached(P, V, c->kV[0], c->A[0][0], 1.0 / dt, p, dt, c->c[0], c->Vs, c->stream);
+      CK(cudaGetLastError());
+      continue;
+    }
     if (i == 0 && k0_cached && !c->bcd.bc_unsteady) {
       Prof pr(c, INS2D_PROF_STAGE, 1);
       launch_stage_cached(c->kV[0], V, c->A[0][0], 1.0 / dt, c->Wt, P.Nu + P.Nv, c->stream);

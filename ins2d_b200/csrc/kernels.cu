@@ -92,6 +92,33 @@ __global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps 
   for (int r = 0; r < kProjRows; ++r) project_cell(P, Wt, dp, dt, c, Vo, i, j0 + r * BY);
 }
 
+// the first stage from the cached residual fused into its projection:
+// Wt = Vn/dt + aii kV0 (k_stage_cached's expression) formed in registers, so
+// Wt is neither written nor read again (the first stage solves no Poisson
+// equation when the boundary conditions are steady: dp = p)
+__global__ void __launch_bounds__(256) k_project_cached(const __grid_constant__ DevOps P,
+                                                       const double *__restrict__ Vn,
+                                                       const double *__restrict__ kV0, double aii, double inv_dt,
+                                                       const double *__restrict__ dp, double dt, double c,
+                                                       double *__restrict__ Vo) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j0 = blockIdx.y * (BY * kProjRows) + threadIdx.y;
+#pragma unroll
+  for (int r = 0; r < kProjRows; ++r) {
+    const int j = j0 + r * BY;
+    if (i < P.Nux && j < P.Nuy) {
+      const long long idx = (long long)j * P.Nux + i;
+      const double w = Vn[idx] * inv_dt + aii * kV0[idx];
+      Vo[idx] = dt * (w - c * om_inv_u(P, i, j) * grad_x_fast(P, dp, i, j));
+    }
+    if (i < P.Nvx && j < P.Nvy) {
+      const long long idx = P.Nu + (long long)j * P.Nvx + i;
+      const double w = Vn[idx] * inv_dt + aii * kV0[idx];
+      Vo[idx] = dt * (w - c * om_inv_v(P, i, j) * grad_y_fast(P, dp, i, j));
+    }
+  }
+}
+
 // FP32-storage stages: V_out = Vn + dt (a T - c Om^-1 G dp) in FP64 (T = the
 // stage's Vtemp / a), stored as TO: float for the next stage's stencils, double
 // for the new state (then V_out may be Vn itself: each point is read before it
@@ -267,6 +294,13 @@ void launch_project32(const DevOps &P, const double *Vn, const float *T, double 
 void launch_project32(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
                       double c, double *V_out, cudaStream_t s) {
   launch_project32_t(P, Vn, T, a, dp, dt, c, V_out, s);
+}
+
+void launch_project_cached(const DevOps &P, const double *Vn, const double *kV0, double aii, double inv_dt,
+                           const double *dp, double dt, double c, double *V_out, cudaStream_t s) {
+  const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
+  const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
+  k_project_cached<<<g, dim3(BX, BY), 0, s>>>(P, Vn, kV0, aii, inv_dt, dp, dt, c, V_out);
 }
 
 void launch_correct(const DevOps &P, const double *V_in, const double *dp, double *V_out, cudaStream_t s) {

@@ -92,6 +92,10 @@ void launch_project32(const DevOps &P, const double *Vn, const float *T, double 
                       double c, float *V_out, cudaStream_t s);
 void launch_project32(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
                       double c, double *V_out, cudaStream_t s);
+// the first stage from the cached residual and its projection in one pass:
+// V_out = dt (Vn/dt + aii kV0 - c Om^-1 G dp)
+void launch_project_cached(const DevOps &P, const double *Vn, const double *kV0, double aii, double inv_dt,
+                           const double *dp, double dt, double c, double *V_out, cudaStream_t s);
 // V_out = V_in - Om^-1 G dp   (input_check.m:107)
 void launch_correct(const DevOps &P, const double *V_in, const double *dp, double *V_out, cudaStream_t s);
 void launch_lap(const DevOps &P, const double *p, double *Ap, cudaStream_t s);
