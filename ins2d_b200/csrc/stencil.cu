@@ -12,8 +12,6 @@
 // their field rows in L1.  Boundary rows of the operators use the same tables
 // (the boundary elimination lives in the table entries), so there is one
 // code path for every boundary-condition combination.
-#include <algorithm>
-
 #include "kernels.cuh"
 
 namespace ins2d {
@@ -588,6 +586,8 @@ __device__ void fast_v(const DevOps &P, const TV *__restrict__ u, const TV *__re
 // host): every shift of the regular rows in [-2, 1], and rows of u and v
 // that start on 16-byte boundaries (Nux, Nvx, Nu multiples of 16 bytes /
 // sizeof(TV)).
+constexpr int kTileThreads = 256;
+constexpr int kTileSeg = RUN / 2;   // rows per thread
 constexpr int kTileRows = RUN + 5;  // staged rows j0-2 .. j0+RUN+2
 
 // staged columns i0-HL .. : HL = one 16-byte chunk of halo on the left,
@@ -618,11 +618,9 @@ __device__ __forceinline__ int wrapm(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
-// Phase 1 of the tiled walkers: R = -conv + Diff V (the right-hand side
-// without the pressure terms) of each point of the tile into Rs (u: Rs[0],
-// v: Rs[1]), with the arithmetic of fast_u / fast_v.
-template <typename S, typename TV>
-__device__ void tile_u(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i, int i0, int j0, int ja, int jb,
+// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
+template <typename S, int MODE, typename TV>
+__device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
                        const YRowsN<RUN> &Y) {
   const S ire = S(P.invRe);
   const int ci = i - i0 + TileGeo<TV>::HL;  // shared-memory column of u(i, .)
@@ -634,6 +632,7 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i,
   const S s10 = rw<S>(P.rSUX.w0, i + 1), s11 = rw<S>(P.rSUX.w1, i + 1);
   const S iv0 = rw<S>(P.rIVX.w0, i), iv1 = rw<S>(P.rIVX.w1, i);
   const S gx = S(__ldg(P.gxi + i));
+  const double rgx = __ldg(P.rgxi + i);
   const bool twoA = P.rAUX.two, twoAy = P.rAUY.two, twoIx = P.rIVX.two, twoIy = P.rIVY.two;
   const int sAy = P.rAUY.s - j0 + 2, sIy = P.rIVY.s - j0 + 2;  // shared-memory row of field row r: r + s
   auto face = [&](int r, S &uy, S &sy, S &vf) {
@@ -662,19 +661,35 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i,
     const S um = S(T.u[rr][cA0]), u0 = S(T.u[rr][cA1]), up = twoA ? S(T.u[rr][cA2]) : S(0);
     const S uxl = a00 * um + a01 * u0, uxr = a10 * u0 + a11 * up;
     const S sxl = s00 * um + s01 * u0, sxr = s10 * u0 + s11 * up;
-    const S hy = S(Y.hy[j - j0]);
+    const double hyd = Y.hy[j - j0];
+    const S hy = S(hyd);
     const S du2dx = (hy * uxr) * uxr - (hy * uxl) * uxl;
     const S duvdy = vf1 * uy1 - vf0 * uy0;
     const S d2u = hy * (ire * sxr - ire * sxl) + gx * (ire * sy1 - ire * sy0);
-    Rs[j - j0][i - i0] = -(du2dx + duvdy) + d2u;
+    const double R = (double)(-(du2dx + duvdy) + d2u);
+    const long long idx = (long long)j * P.Nux + i;
+    const double oi = Y.rhy[j - j0] * rgx;
+    if constexpr (MODE == 0) {
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+    } else if constexpr (MODE == 2) {
+      epi_stage32(e, idx, oi * R);
+    } else {
+      const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
+      epi_residual(e, idx, oi, R, g);
+    }
     uy0 = uy1;
     sy0 = sy1;
     vf0 = vf1;
   }
 }
 
-template <typename S, typename TV>
-__device__ void tile_v(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i, int i0, int j0, int ja, int jb,
+template <typename S, int MODE, typename TV>
+__device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
                        const YRowsN<RUN> &Y) {
   const S ire = S(P.invRe);
   const int ci = i - i0 + TileGeo<TV>::HL;
@@ -686,7 +701,9 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i,
   const S s10 = rw<S>(P.rSVX.w0, i + 1), s11 = rw<S>(P.rSVX.w1, i + 1);
   const S wu00 = rw<S>(P.rIUX.w0, i), wu01 = rw<S>(P.rIUX.w1, i);
   const S wu10 = rw<S>(P.rIUX.w0, i + 1), wu11 = rw<S>(P.rIUX.w1, i + 1);
-  const S hx = S(__ldg(P.hx + i));
+  const double hxd = __ldg(P.hx + i);
+  const double rhx = __ldg(P.rhx + i);
+  const S hx = S(hxd);
   const bool twoV = P.rAVX.two, twoVy = P.rAVY.two, twoUx = P.rIUX.two, twoUy = P.rIUY.two;
   const int sVy = P.rAVY.s - j0 + 2, sUy = P.rIUY.s - j0 + 2;
   auto face = [&](int r, S &vy, S &sy) {
@@ -721,215 +738,68 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, S (*Rs)[WX], int i,
     const S ufl = wy0 * la + wy1 * lb, ufr = wy0 * ra + wy1 * rb;
     const S duvdx = ufr * vxr - ufl * vxl;
     const S dv2dy = (hx * vy1) * vy1 - (hx * vy0) * vy0;
-    const S d2v = S(Y.gyi[j - j0]) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
-    Rs[j - j0][i - i0] = -(duvdx + dv2dy) + d2v;
+    const double gyd = Y.gyi[j - j0];
+    const S d2v = S(gyd) * (ire * svr - ire * svl) + hx * (ire * sy1 - ire * sy0);
+    const double R = (double)(-(duvdx + dv2dy) + d2v);
+    const long long idx = P.Nu + (long long)j * P.Nvx + i;
+    const double oi = Y.rgyi[j - j0] * rhx;
+    if constexpr (MODE == 0) {
+      const double k = oi * R;
+      if (e.kV) e.kV[idx] = k;
+      double vt = 0.0;
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+      vt += e.aii * k;
+      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+    } else if constexpr (MODE == 2) {
+      epi_stage32(e, idx, oi * R);
+    } else {
+      const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
+      double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
+      if (P.rMYT.two) gy += Y.myt1[j - j0] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
+      const double g = -hxd * gy;
+      epi_residual(e, idx, oi, R, g);
+    }
     vy0 = vy1;
     sy0 = sy1;
   }
 }
 
-// Persistent, pipelined form of the tiled walkers: each thread block loops
-// over tiles (blockIdx.x, + gridDim.x, ...) and keeps two buffers, so the
-// asynchronous copies of the next tile's u/v halo tile, its y-weights and (for
-// the FP64 stage) its Vn tile are in flight while the current tile is
-// computed.  Per tile: phase 1 walks the columns (warps 0-7: u, 8-15: v, four
-// row segments per column) into R; phase 2 is the epilogue of every point,
-// consecutive threads on consecutive columns.
-constexpr int kPipeThreads = 512;
-constexpr int kPipeSegs = kPipeThreads / WX / 2;  // row segments per column and component
-constexpr int kPipeRows = RUN / kPipeSegs;        // rows per thread
-
-template <typename TV, int MODE>
-struct PipeBuf {
-  TileSm<TV> T;
-  YRowsN<RUN> Y;
-  double Vn[MODE == 0 ? 2 : 1][MODE == 0 ? RUN : 1][WX];  // MODE 0: the tile's Vn (u, v)
-};
+#ifndef INS2D_TILE_MINB
+#define INS2D_TILE_MINB 3
+#endif
 template <typename S, int MODE, typename TV>
-struct PipeSmem {
-  PipeBuf<TV, MODE> buf[2];
-  S R[2][RUN][WX];
-};
-
-__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// the asynchronous copies of tile (bx, by) into B
-template <int MODE, typename TV>
-__device__ __forceinline__ void pipe_issue(const DevOps &P, const TV *__restrict__ V, const Epi &e, int bx, int by,
-                                           PipeBuf<TV, MODE> &B, int tid) {
+__global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
+    k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
   using G = TileGeo<TV>;
+  __shared__ __align__(16) TileSm<TV> T;
+  __shared__ YRowsN<RUN> Y;
+  const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
   const int i0 = bx * WX, j0 = by * RUN;
+  const int tid = threadIdx.x + WX * threadIdx.y;
   const TV *u = V, *v = V + P.Nu;
-  for (int q = tid; q < 2 * kTileRows * G::CHUNKS; q += kPipeThreads) {
+  // stage the u and v rows j0-2 .. j0+RUN+2, columns i0-HL .. (wrapped)
+  for (int q = tid; q < 2 * kTileRows * G::CHUNKS; q += kTileThreads) {
     const int f = q >= kTileRows * G::CHUNKS;
     const int qq = q - f * kTileRows * G::CHUNKS;
     const int r = qq / G::CHUNKS, ch = qq - r * G::CHUNKS;
     if (f == 0) {
       const int gr = wrapm(j0 - 2 + r, P.Nuy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nux);
-      cp_async16(&B.T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
+      cp_async16(&T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
     } else {
       const int gr = wrapm(j0 - 2 + r, P.Nvy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nvx);
-      cp_async16(&B.T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
+      cp_async16(&T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
     }
   }
-  if constexpr (MODE == 0) {
-    constexpr int CH = WX / 2;  // 16-byte chunks per row
-    for (int q = tid; q < 2 * RUN * CH; q += kPipeThreads) {
-      const int comp = q / (RUN * CH);
-      const int qq = q - comp * RUN * CH;
-      const int r = qq / CH, ch = qq - r * CH;
-      const double *src = comp == 0 ? e.Vn + (long long)(j0 + r) * P.Nux + i0 + 2 * ch
-                                    : e.Vn + P.Nu + (long long)(j0 + r) * P.Nvx + i0 + 2 * ch;
-      cp_async16(&B.Vn[comp][r][2 * ch], src);
-    }
-  }
-  // y-weights and metrics of the tile's faces (RUN + 1) and rows (RUN)
-  YRowsN<RUN> &Y = B.Y;
-  for (int q = tid; q < 10 * (RUN + 1) + 8 * RUN; q += kPipeThreads) {
-    const double *src;
-    double *dst;
-    if (q < 10 * (RUN + 1)) {
-      const int a = q / (RUN + 1), t = q - a * (RUN + 1), r = j0 + t;
-      switch (a) {
-        case 0: src = P.rAUY.w0 + r; dst = Y.auy0 + t; break;
-        case 1: src = P.rAUY.w1 + r; dst = Y.auy1 + t; break;
-        case 2: src = P.rSUY.w0 + r; dst = Y.suy0 + t; break;
-        case 3: src = P.rSUY.w1 + r; dst = Y.suy1 + t; break;
-        case 4: src = P.rIVY.w0 + r; dst = Y.ivy0 + t; break;
-        case 5: src = P.rIVY.w1 + r; dst = Y.ivy1 + t; break;
-        case 6: src = P.rAVY.w0 + r; dst = Y.avy0 + t; break;
-        case 7: src = P.rAVY.w1 + r; dst = Y.avy1 + t; break;
-        case 8: src = P.rSVY.w0 + r; dst = Y.svy0 + t; break;
-        default: src = P.rSVY.w1 + r; dst = Y.svy1 + t; break;
-      }
-    } else {
-      const int qq = q - 10 * (RUN + 1);
-      const int a = qq / RUN, t = qq - a * RUN, j = j0 + t;
-      switch (a) {
-        case 0: src = P.hy + j; dst = Y.hy + t; break;
-        case 1: src = P.rhy + j; dst = Y.rhy + t; break;
-        case 2: src = P.rIUY.w0 + j; dst = Y.iuy0 + t; break;
-        case 3: src = P.rIUY.w1 + j; dst = Y.iuy1 + t; break;
-        case 4: src = P.gyi + j; dst = Y.gyi + t; break;
-        case 5: src = P.rgyi + j; dst = Y.rgyi + t; break;
-        case 6: src = P.rMYT.w0 + j; dst = Y.myt0 + t; break;
-        default: src = P.rMYT.w1 + j; dst = Y.myt1 + t; break;
-      }
-    }
-    cp_async8(dst, src);
-  }
-}
-
-// MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
-template <typename S, int MODE, typename TV>
-__global__ void __launch_bounds__(kPipeThreads, 1)
-    k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
-  extern __shared__ __align__(16) unsigned char tile_smem[];
-  PipeSmem<S, MODE, TV> &M = *reinterpret_cast<PipeSmem<S, MODE, TV> *>(tile_smem);
-  const int nbx = P.fbx1 - P.fbx0, nby = P.fby1 - P.fby0;
-  const int ntiles = nbx * nby;
-  const int tid = threadIdx.x + WX * threadIdx.y;
-  int t = blockIdx.x;
-  int cur = 0;
-  if (t < ntiles) pipe_issue<MODE, TV>(P, V, e, P.fbx0 + t % nbx, P.fby0 + t / nbx, M.buf[0], tid);
-  cp_async_commit();
-  for (; t < ntiles; t += gridDim.x) {
-    const int tn = t + gridDim.x;
-    if (tn < ntiles) pipe_issue<MODE, TV>(P, V, e, P.fbx0 + tn % nbx, P.fby0 + tn / nbx, M.buf[cur ^ 1], tid);
-    cp_async_commit();
-    cp_async_wait<1>();  // this tile's copies have landed (the next tile's may still fly)
-    __syncthreads();
-    const PipeBuf<TV, MODE> &B = M.buf[cur];
-    const int bx = P.fbx0 + t % nbx, by = P.fby0 + t / nbx;
-    const int i0 = bx * WX, j0 = by * RUN;
-    // phase 1: walk the columns
-    {
-      const int i = i0 + threadIdx.x;
-      const int comp = threadIdx.y / kPipeSegs, seg = threadIdx.y % kPipeSegs;
-      const int ja = j0 + seg * kPipeRows, jb = ja + kPipeRows;
-      if (comp == 0)
-        tile_u<S, TV>(P, B.T, M.R[0], i, i0, j0, ja, jb, B.Y);
-      else
-        tile_v<S, TV>(P, B.T, M.R[1], i, i0, j0, ja, jb, B.Y);
-    }
-    __syncthreads();
-    // phase 2: the epilogue of every point
-    const YRowsN<RUN> &Y = B.Y;
-#pragma unroll 4
-    for (int m = 0; m < 2 * RUN * WX / kPipeThreads; ++m) {
-      const int o = tid + kPipeThreads * m;
-      const int comp = o / (RUN * WX);
-      const int oo = o - comp * (RUN * WX);
-      const int jr = oo / WX, ic = oo - jr * WX;
-      const int i = i0 + ic, j = j0 + jr;
-      const double R = (double)M.R[comp][jr][ic];
-      long long idx;
-      double oi;
-      if (comp == 0) {
-        idx = (long long)j * P.Nux + i;
-        oi = Y.rhy[jr] * __ldg(P.rgxi + i);
-      } else {
-        idx = P.Nu + (long long)j * P.Nvx + i;
-        oi = Y.rgyi[jr] * __ldg(P.rhx + i);
-      }
-      if constexpr (MODE == 0) {
-        const double k = oi * R;
-        if (e.kV) e.kV[idx] = k;
-        double vt = 0.0;
-        for (int q = 0; q < e.nprev; ++q) vt += e.aprev[q] * __ldg(e.kprev[q] + idx);
-        vt += e.aii * k;
-        e.Wt[idx] = B.Vn[comp][jr][ic] * e.inv_dt + vt;
-      } else if constexpr (MODE == 2) {
-        epi_stage32(e, idx, oi * R);
-      } else {
-        double g;
-        if (comp == 0) {
-          g = -Y.hy[jr] * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
-        } else {
-          const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
-          double gy = Y.myt0[jr] * __ldg(e.p + (long long)c0 * P.Npx + i);
-          if (P.rMYT.two) gy += Y.myt1[jr] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
-          g = -__ldg(P.hx + i) * gy;
-        }
-        epi_residual(e, idx, oi, R, g);
-      }
-    }
-    __syncthreads();  // buffer cur is refilled in the next iteration but one; R is rewritten in the next
-    cur ^= 1;
-  }
-  cp_async_wait<0>();
-}
-
-template <typename S, int MODE, typename TV>
-cudaError_t tile_prepare_one() {
-  return cudaFuncSetAttribute((const void *)k_walk_tile<S, MODE, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sizeof(PipeSmem<S, MODE, TV>));
-}
-
-// resident blocks per SM of an instance (cached per instance and device)
-template <typename S, int MODE, typename TV>
-int tile_blocks_per_sm() {
-  static int cached[64] = {0};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) return 1;
-  if (!cached[dev]) {
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_walk_tile<S, MODE, TV>, kPipeThreads,
-                                                      sizeof(PipeSmem<S, MODE, TV>)) != cudaSuccess ||
-        b < 1)
-      b = 1;
-    cached[dev] = b;
-  }
-  return cached[dev];
+  stage_yrows(P, j0, Y);
+  cp_async_wait_all();
+  __syncthreads();
+  const int i = i0 + threadIdx.x;
+  const int seg = threadIdx.y & 1;
+  const int ja = j0 + seg * kTileSeg, jb = ja + kTileSeg;
+  if (threadIdx.y < 2)
+    tile_u<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
+  else
+    tile_v<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
 }
 
 // one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
@@ -1039,20 +909,17 @@ void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   const int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   dim3 g((nx + WX - 1) / WX, (ny + RUN - 1) / RUN);
   const bool has_fast = P.fbx1 > P.fbx0 && P.fby1 > P.fby0;
-  const bool tiled = (sizeof(TV) == 8 ? P.tile_ok : P.tile_ok32) && (((uintptr_t)V & 15) == 0) &&
-                     (e.mode != 0 || (((uintptr_t)e.Vn & 15) == 0)) && P.nsm > 0;
+  const bool tiled = (sizeof(TV) == 8 ? P.tile_ok : P.tile_ok32) && (((uintptr_t)V & 15) == 0);
   if (has_fast) {
     const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
     if (tiled) {
-      const dim3 tb(WX, kPipeThreads / WX);
-      const int ntiles = (int)(gf.x * gf.y);
-      auto blocks = [&](int per_sm) { return std::min(ntiles, P.nsm * per_sm); };
+      const dim3 tb(WX, kTileThreads / WX);
       if (e.mode == 0)
-        k_walk_tile<S, 0, TV><<<blocks(tile_blocks_per_sm<S, 0, TV>()), tb, sizeof(PipeSmem<S, 0, TV>), s>>>(P, V, e);
+        k_walk_tile<S, 0, TV><<<gf, tb, 0, s>>>(P, V, e);
       else if (e.mode == 1)
-        k_walk_tile<S, 1, TV><<<blocks(tile_blocks_per_sm<S, 1, TV>()), tb, sizeof(PipeSmem<S, 1, TV>), s>>>(P, V, e);
+        k_walk_tile<S, 1, TV><<<gf, tb, 0, s>>>(P, V, e);
       else
-        k_walk_tile<S, 2, TV><<<blocks(tile_blocks_per_sm<S, 2, TV>()), tb, sizeof(PipeSmem<S, 2, TV>), s>>>(P, V, e);
+        k_walk_tile<S, 2, TV><<<gf, tb, 0, s>>>(P, V, e);
     } else {
       k_walk_fast<S, TV><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
     }
@@ -1073,20 +940,10 @@ void launch_walk(const DevOps &P, const double *V, const float *V32, const Epi &
 
 }  // namespace
 
-// Opts the tiled walkers in to their dynamic shared memory on the current
-// device; returns the first failure.
-cudaError_t walker_prepare() {
-  // the instances launch_walk_t launches: FP64, FP32 arithmetic on FP64
-  // fields, FP32 arithmetic on FP32 fields, each in the three modes
-  const cudaError_t r[] = {tile_prepare_one<double, 0, double>(), tile_prepare_one<double, 1, double>(),
-                           tile_prepare_one<double, 2, double>(), tile_prepare_one<float, 0, double>(),
-                           tile_prepare_one<float, 1, double>(), tile_prepare_one<float, 2, double>(),
-                           tile_prepare_one<float, 0, float>(), tile_prepare_one<float, 1, float>(),
-                           tile_prepare_one<float, 2, float>()};
-  for (cudaError_t x : r)
-    if (x != cudaSuccess) return x;
-  return cudaSuccess;
-}
+// The tiled walkers' shared memory is static (below 48 KB per block): no
+// opt-in is needed; kept so the context's set-up has one place to prepare the
+// walkers on its device.
+cudaError_t walker_prepare() { return cudaSuccess; }
 
 // The rectangle of tiles whose every column and row lies in the regular
 // ranges the fast walkers need (both walkers of a block must qualify).
