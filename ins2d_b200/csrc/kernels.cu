@@ -164,26 +164,33 @@ __global__ void __launch_bounds__(256) k_lap(const __grid_constant__ DevOps P, c
   if (i < P.Npx && j < P.Npy) Ap[(long long)j * P.Npx + i] = lap(P, p, i, j);
 }
 
+// each thread takes kConsRows rows (BY apart) of one column, so the grid has
+// kConsRows times fewer blocks (and block partials to reduce)
+constexpr int kConsRows = 16;
 __global__ void __launch_bounds__(256) k_conservation(const __grid_constant__ DevOps P, const double *__restrict__ V,
                                                      const RedScratch red) {
   const int i = blockIdx.x * BX + threadIdx.x;
-  const int j = blockIdx.y * BY + threadIdx.y;
+  const int jb = blockIdx.y * (BY * kConsRows) + threadIdx.y;
   const double *u = V, *v = V + P.Nu;
   double q[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   const int ops[5] = {R_MAX, R_SUM, R_SUM, R_SUM, R_SUM};
-  if (i < P.Npx && j < P.Npy)
-    q[0] = fabs(div_in(P, u, v, i, j) + div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j));
-  if (i < P.Nux && j < P.Nuy) {
-    const double om = __ldg(P.hy + j) * __ldg(P.gxi + i);
-    const double x = u[(long long)j * P.Nux + i];
-    q[1] = om * x;
-    q[3] = om * x * x;
-  }
-  if (i < P.Nvx && j < P.Nvy) {
-    const double om = __ldg(P.gyi + j) * __ldg(P.hx + i);
-    const double x = v[(long long)j * P.Nvx + i];
-    q[2] = om * x;
-    q[4] = om * x * x;
+#pragma unroll 4
+  for (int r = 0; r < kConsRows; ++r) {
+    const int j = jb + r * BY;
+    if (i < P.Npx && j < P.Npy)
+      q[0] = fmax(q[0], fabs(div_in(P, u, v, i, j) + div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j)));
+    if (i < P.Nux && j < P.Nuy) {
+      const double om = __ldg(P.hy + j) * __ldg(P.gxi + i);
+      const double x = u[(long long)j * P.Nux + i];
+      q[1] += om * x;
+      q[3] += om * x * x;
+    }
+    if (i < P.Nvx && j < P.Nvy) {
+      const double om = __ldg(P.gyi + j) * __ldg(P.hx + i);
+      const double x = v[(long long)j * P.Nvx + i];
+      q[2] += om * x;
+      q[4] += om * x * x;
+    }
   }
   grid_reduce<5>(q, ops, red);
 }
@@ -315,7 +322,8 @@ void launch_lap(const DevOps &P, const double *p, double *Ap, cudaStream_t s) {
 void launch_conservation(const DevOps &P, const double *V, const RedScratch &red, cudaStream_t s) {
   int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
   int ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
-  k_conservation<<<grid_for(nx, ny), dim3(BX, BY), 0, s>>>(P, V, red);
+  const dim3 g((nx + BX - 1) / BX, (ny + BY * kConsRows - 1) / (BY * kConsRows));
+  k_conservation<<<g, dim3(BX, BY), 0, s>>>(P, V, red);
 }
 
 void launch_stage_cached(const double *kV0, const double *Vn, double aii, double inv_dt, double *Wt, long long n,
