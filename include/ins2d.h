@@ -67,9 +67,10 @@ extern "C" {
 
 /* preconditioner of the device PCG (poisson 1-5).  The reference's cg.F uses
  * a diagonal incomplete Cholesky factor (sequential sweeps, cg.F:317-390);
- * the device offers a multigrid V-cycle (default) or the Jacobi diagonal.
- * Either way CG iterates to the same relative residual CG_acc. */
-#define INS2D_PRECOND_DEFAULT 0 /* multigrid where the grid allows it, else Jacobi */
+ * the device offers fast diagonalization, a multigrid V-cycle or the Jacobi
+ * diagonal.  Either way CG iterates to the same relative residual CG_acc. */
+#define INS2D_PRECOND_DEFAULT 0 /* fast diagonalization where it applies, else multigrid, else Jacobi;
+                                   ensemble members: multigrid */
 #define INS2D_PRECOND_JACOBI 1
 #define INS2D_PRECOND_MG 2
 /* fast diagonalization: A is separable, A = -(diag(hy) (x) TX + TY (x)

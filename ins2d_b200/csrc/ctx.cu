@@ -862,7 +862,11 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
       W.blocks = pcg_blocks(P);
       W.partials = dalloc<double>(c, (size_t)W.blocks * 8 + 16);
       CK(cudaMemset(W.sc, 0, sizeof(PcgScalars)));
-      if (opts->precond == INS2D_PRECOND_FDM) {
+      // the default: fast diagonalization where it applies (periodic uniform
+      // grids the FFT takes, or up to kFdmMaxN cells per direction), else
+      // multigrid, else Jacobi
+      const bool fdm_fits = (H.fft_ok && fft_supported(H.Nx, H.Ny)) || std::max(H.Npx, H.Npy) <= kFdmMaxN;
+      if (opts->precond == INS2D_PRECOND_FDM || (opts->precond == INS2D_PRECOND_DEFAULT && fdm_fits)) {
         FdmD &D = c->fdm;
         D.nx = H.Npx;
         D.ny = H.Npy;
@@ -1898,7 +1902,11 @@ int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_des
     }
     if (rc) break;
     ins2d_ctx *c = nullptr;
-    rc = ins2d_ctx_create(&grids[m], &bcs[m], &o, &c);
+    // the ensemble's solvers (persistent per member, or batched) run the
+    // multigrid V-cycle: members take it unless Jacobi is asked for
+    ins2d_opts om = o;
+    if (om.precond != INS2D_PRECOND_JACOBI) om.precond = INS2D_PRECOND_MG;
+    rc = ins2d_ctx_create(&grids[m], &bcs[m], &om, &c);
     if (rc) {
       msg = std::string("member ") + std::to_string(m) + ": " + (c ? c->err : std::string("create failed"));
       if (c) ins2d_ctx_destroy(c);

@@ -198,9 +198,9 @@ def test_erk_fft_large_grid():
 
 @pytest.mark.parametrize("combo", ["cavity", "channel", "periodic", "per_y_open", "open_x"])
 @pytest.mark.parametrize("shape", [(24, 20), (301, 257)])
-@pytest.mark.parametrize("precond", ["mg", "jacobi"])
+@pytest.mark.parametrize("precond", ["mg", "jacobi", "fdm"])
 def test_pcg_preconditioners(combo, shape, precond):
-    """Multigrid and Jacobi preconditioned CG reach the stated tolerance and
+    """Multigrid, Jacobi and fast-diagonalization preconditioned CG reach the stated tolerance and
     agree with the oracle's direct solve, one thread block (24x20) and
     multi-block (301x257) paths; multigrid needs few iterations on stretched
     grids."""
@@ -222,13 +222,15 @@ def test_pcg_preconditioners(combo, shape, precond):
     assert res <= 2e-11
     if precond == "mg":
         assert st["iters"] <= 40, st
+    if precond == "fdm":
+        assert st["iters"] <= 4, st
     dp_ref = R.pressure_poisson(f, 0.0, o)
     if is_closed(bc):
         dp, dp_ref = dp - dp.mean(), dp_ref - dp_ref.mean()
     assert _rel(dp, dp_ref) < 1e-8
 
 
-@pytest.mark.parametrize("poisson,precond", [(4, "mg"), (4, "jacobi")])
+@pytest.mark.parametrize("poisson,precond", [(4, "mg"), (4, "jacobi"), (4, "fdm")])
 def test_nonfinite_rhs_reports_error(poisson, precond):
     """A NaN in the right-hand side ends the solve with INS2D_ENONFINITE (the
     device path reports it as a status; no fault, the context stays usable)."""
