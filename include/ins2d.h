@@ -174,10 +174,16 @@ int ins2d_set_stream(ins2d_ctx *ctx, void *stream);
  * for other streams by itself.  No-op when `stream` is the context's stream. */
 int ins2d_wait_stream(ins2d_ctx *ctx, void *stream);
 /* Grids whose PCG runs one launch per phase (more than 65536 cells with the
- * multigrid preconditioner) are driven by the host, which polls a device
- * convergence flag between chunks of iterations.  This bounds the iterations
- * the host launches while the flag stays unset; past it the solve returns
- * INS2D_ETIMEOUT.  iterations < 0 restores the default, CG_maxit + 1024. */
+ * multigrid preconditioner, or the fast-diagonalization preconditioner) are
+ * driven by the host, which polls a device convergence flag between chunks
+ * of iterations.  This bounds the iterations the host launches while the
+ * flag stays unset; past it the solve returns INS2D_ETIMEOUT.  iterations < 0
+ * restores the default, CG_maxit + 1024.  Inside the CUDA graphs of
+ * ins2d_erk_run (runs of two or more steps with steady boundary conditions)
+ * the same solves loop on the device, in a conditional WHILE node; the
+ * value bounds its passes (default CG_maxit / iterations per pass + 4) and
+ * the run reports INS2D_ETIMEOUT when a loop stopped there unconverged.
+ * Changing the value drops the captured graphs. */
 int ins2d_set_poll_limit(ins2d_ctx *ctx, int64_t iterations);
 /* set_bc_vectors.m:1 -- boundary values at time t (steady cases call it once) */
 int ins2d_set_bc_values(ins2d_ctx *ctx, double t, const ins2d_bc_values *vals);
@@ -227,7 +233,11 @@ int ins2d_pressure_additional_solve(ins2d_ctx *ctx, const double *V, double *p, 
 int ins2d_erk_step(ins2d_ctx *ctx, double *V, double *p, double t, double dt,
                    ins2d_step_stats *stats, int mem);
 /* nsteps consecutive time_ERK steps from t with a fixed dt (solver_unsteady.m:72-102
- * without process_iteration); V, p device pointers updated in place. */
+ * without process_iteration); V, p device pointers updated in place.  With
+ * steady boundary conditions and nsteps >= 2 each step is captured once as
+ * a CUDA graph and replayed (PCG iteration loops as conditional WHILE
+ * nodes); a PCG error is then reported after the step that raised it at the
+ * latest 32 steps later, or at the end of the run. */
 int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int32_t nsteps,
                   ins2d_step_stats *stats, int mem);
 /* The initial projection of input_check.m:95-111: when max|M V + yM| (also

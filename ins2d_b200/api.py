@@ -105,8 +105,10 @@ class Options:
     unsteady BCs), ``Re``, ``poisson`` (1-5: device PCG, 6: FFT), ``CG_acc``,
     ``CG_maxit``, ``p_add_solve``, the RK method name, ``precision``
     ('fp64' or 'fp32': FP32 convection/diffusion stencils) and ``precond``
-    (PCG preconditioner: 'default' = multigrid where the grid allows it,
-    'mg', or 'jacobi').
+    (PCG preconditioner: 'default' = fast diagonalization where it applies
+    -- periodic uniform grids, or at most 1024 pressure cells per direction
+    -- else multigrid where the grid allows it, else Jacobi; 'fdm', 'mg', or
+    'jacobi').
     """
 
     def __init__(self, x, y, BC, Re=1000.0, poisson=4, CG_acc=1e-12, CG_maxit=10000, p_add_solve=1, RK="RK44",

@@ -24,7 +24,8 @@
 
 using namespace ins2d;
 
-// a captured time step (erk_run on the FFT path)
+// a captured time step (erk_run: FFT solves, or PCG solves whose iteration
+// loops are conditional WHILE nodes of the graph)
 struct StepGraph {
   cudaGraphExec_t exec = nullptr;
   const double *V = nullptr, *p = nullptr;
@@ -69,6 +70,12 @@ struct ins2d_ctx {
   FdmD fdm{};
   FftPlan fdm_fft;
   PcgScalars *h_sc = nullptr;   // pinned
+  // PCG solves inside a step graph: the iteration loop is a WHILE node whose
+  // body is captured on body_stream; their statistics accumulate on the device
+  bool dev_loop = false;
+  cudaStream_t body_stream = nullptr;
+  SolveAccum *accum = nullptr;    // device
+  SolveAccum *h_accum = nullptr;  // pinned
   double *h_red = nullptr;      // pinned
   // host copies of boundary samples (check_conservation.m boundary terms)
   std::vector<double> uLe_i, uRi_i, vLo_i, vUp_i;
@@ -235,8 +242,88 @@ void setup_rk(ins2d_ctx *c) {
 
 // ---------------------------------------------------------------------------
 // Poisson solve: dp = pressure_poisson(f) (or dp += ... when accumulate)
+
+// The PCG solve inside a step being captured as a CUDA graph (c->dev_loop):
+// no host round trip.  The iterations are the body of a conditional WHILE
+// node, captured on the context's second stream into the node's body graph;
+// a one-thread kernel after the initialisation and at the end of each pass
+// sets the condition to "not converged and fewer passes than the limit", so
+// the loop ends by itself.  The solve's iterations, residual and status are
+// added to c->accum, which the host reads after the graph launches (cg.F's
+// errors are reported then).
+int solve_pcg_graph(ins2d_ctx *c, const double *f, double *dp, bool accumulate, double tol) {
+  const bool block = c->use_fdm ? false : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
+  Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
+  if (block) {
+    if (c->use_mg)
+      pcg_solve_block_mg(c->P, c->mg, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
+    else
+      pcg_solve_block(c->P, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
+    CK(cudaGetLastError());
+    launch_solve_accum(c->pcg.sc, c->accum, c->stream);
+    CK(cudaGetLastError());
+    return INS2D_OK;
+  }
+  if (c->use_fdm)
+    pcg_init_fdm(c->P, c->fdm, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
+  else if (c->use_mg)
+    pcg_init_mg(c->P, c->mg, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
+  else
+    pcg_init(c->P, c->pcg, f, tol, c->opts.CG_maxit, c->stream);
+  CK(cudaGetLastError());
+  const int chunk = (c->use_fdm || c->use_mg) ? 1 : 4;
+  const long long lim = c->poll_limit >= 0 ? c->poll_limit : (long long)c->opts.CG_maxit / chunk + 4;
+  const int limit = (int)std::min<long long>(lim, 1 << 30);
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  CK(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) return fail(c, INS2D_EINVAL, "graph-form PCG outside a stream capture");
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  launch_pcg_cond(c->pcg.sc, h, limit, 0, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+  CK(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  if (c->use_fdm) {
+    pcg_iterations_fdm(c->P, c->fdm, c->pcg, chunk, c->body_stream);
+    c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 7LL : 8LL) * chunk;
+  } else if (c->use_mg) {
+    pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->body_stream);
+    c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
+  } else {
+    pcg_iterations(c->P, c->pcg, chunk, c->body_stream);
+    c->launches[INS2D_PROF_POISSON] += 3LL * chunk;
+  }
+  launch_pcg_cond(c->pcg.sc, h, limit, 1, c->body_stream);
+  const cudaError_t le = cudaGetLastError();
+  cudaGraph_t body_out = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(c->body_stream, &body_out);
+  CK(le);
+  CK(ee);
+  pcg_finish(c->P, c->pcg, dp, accumulate, c->stream);
+  launch_solve_accum(c->pcg.sc, c->accum, c->stream);
+  c->launches[INS2D_PROF_POISSON] += 3;
+  CK(cudaGetLastError());
+  return INS2D_OK;
+}
+
 // PCG to the relative residual tol (cg.F's rule ||r|| <= tol ||f||)
 int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st, double tol) {
+  if (c->dev_loop) {
+    if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
+    return solve_pcg_graph(c, f, dp, accumulate, tol);
+  }
   const bool block = c->use_fdm ? false : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
   Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
   if (block) {
@@ -921,7 +1008,10 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     }
     CK(cudaMallocHost((void **)&c->h_sc, sizeof(PcgScalars)));
     CK(cudaMallocHost((void **)&c->h_red, sizeof(double) * kRedQ));
+    CK(cudaMallocHost((void **)&c->h_accum, sizeof(SolveAccum)));
+    c->accum = dalloc<SolveAccum>(c, 1);
     CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;
     CK(cudaDeviceSynchronize());
   } catch (const CudaError &e) {
@@ -960,7 +1050,9 @@ int ins2d_ctx_destroy(ins2d_ctx *ctx) {
   if (ctx->order_ev) cudaEventDestroy(ctx->order_ev);
   if (ctx->h_sc) cudaFreeHost(ctx->h_sc);
   if (ctx->h_red) cudaFreeHost(ctx->h_red);
+  if (ctx->h_accum) cudaFreeHost(ctx->h_accum);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->body_stream) cudaStreamDestroy(ctx->body_stream);
   delete ctx;
   return INS2D_OK;
 }
@@ -984,9 +1076,20 @@ int ins2d_set_stream(ins2d_ctx *ctx, void *stream) {
 }
 
 int ins2d_set_poll_limit(ins2d_ctx *ctx, int64_t iterations) {
-  if (!ctx) return INS2D_EINVAL;
-  ctx->poll_limit = iterations < 0 ? -1 : (long long)iterations;
+  API_BEGIN
+  const long long v = iterations < 0 ? -1 : (long long)iterations;
+  if (v != ctx->poll_limit) {
+    // captured step graphs hold the loop limit: capture again
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto &g : ctx->step_graph)
+      if (g.exec) {
+        CK(cudaGraphExecDestroy(g.exec));
+        g.exec = nullptr;
+      }
+  }
+  ctx->poll_limit = v;
   return INS2D_OK;
+  API_END
 }
 
 int ins2d_wait_stream(ins2d_ctx *ctx, void *stream) {
@@ -1189,11 +1292,36 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
     dV = ctx->stV;
     dP = ctx->stP;
   }
-  // FFT path with steady boundary conditions: a step is a fixed launch
-  // sequence without host round trips, so it is captured once as a CUDA
+  // With steady boundary conditions a step is a launch sequence without host
+  // round trips -- FFT solves, or PCG solves whose iteration loops run on the
+  // device as conditional WHILE nodes -- so it is captured once as a CUDA
   // graph (first step, and steps whose first stage comes from the cache) and
-  // replayed; the graphs are keyed by the state pointers and dt.
-  const bool graphs = ctx->poisson == INS2D_POISSON_FFT && !ctx->bcd.bc_unsteady && !ctx->prof && nsteps >= 2;
+  // replayed; the graphs are keyed by the state pointers and dt.  The PCG
+  // solves' statistics and errors accumulate on the device and are read
+  // every kAccumCheck steps and at the end of the run.
+  const bool pcg_graphs = ctx->poisson != INS2D_POISSON_FFT && !ctx->cnn && ctx->rec_n >= ctx->rec_cap;
+  const bool graphs = (ctx->poisson == INS2D_POISSON_FFT || pcg_graphs) && !ctx->bcd.bc_unsteady && !ctx->prof &&
+                      nsteps >= 2;
+  const bool dev_stats = graphs && pcg_graphs;
+  constexpr int kAccumCheck = 32;
+  auto read_accum = [&]() -> int {
+    CK(cudaMemcpyAsync(ctx->h_accum, ctx->accum, sizeof(SolveAccum), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const SolveAccum &a = *ctx->h_accum;
+    if (a.status == INS2D_ENOTCONV) {
+      char buf[160];
+      snprintf(buf, sizeof buf, "CG didn't converge in %lld iterations; residual= %g", a.fail_maxit,
+               std::sqrt(a.fail_rr));
+      return fail(ctx, INS2D_ENOTCONV, buf);
+    }
+    if (a.status == INS2D_EBREAKDOWN) return fail(ctx, INS2D_EBREAKDOWN, "PCG breakdown: p'Ap = 0");
+    if (a.status == INS2D_ENONFINITE) return fail(ctx, INS2D_ENONFINITE, "PCG: non-finite residual");
+    if (a.status == INS2D_ETIMEOUT)
+      return fail(ctx, INS2D_ETIMEOUT, "PCG: device convergence flag not set within the iteration-loop limit");
+    if (a.status != 0) return fail(ctx, a.status, "PCG failed");
+    return INS2D_OK;
+  };
+  if (dev_stats) CK(cudaMemsetAsync(ctx->accum, 0, sizeof(SolveAccum), ctx->stream));
   bool cached = false;
   for (int n = 0; n < nsteps; ++n) {
     if (graphs) {
@@ -1207,7 +1335,17 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
         cudaGraph_t gr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         bool next = false;
-        int rc = erk_step(ctx, dV, dP, t + n * dt, dt, nullptr, cached, &next);
+        ctx->dev_loop = pcg_graphs;
+        int rc;
+        try {
+          rc = erk_step(ctx, dV, dP, t + n * dt, dt, nullptr, cached, &next);
+        } catch (...) {
+          ctx->dev_loop = false;
+          cudaGraph_t junk = nullptr;
+          if (cudaStreamEndCapture(ctx->stream, &junk) == cudaSuccess && junk) cudaGraphDestroy(junk);
+          throw;
+        }
+        ctx->dev_loop = false;
         cudaError_t ce = cudaStreamEndCapture(ctx->stream, &gr);
         if (rc) {
           if (ce == cudaSuccess) cudaGraphDestroy(gr);
@@ -1227,8 +1365,13 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
       }
       CK(cudaGraphLaunch(G.exec, ctx->stream));
       for (int k = 0; k < INS2D_PROF_N; ++k) ctx->launches[k] += G.launches[k];
-      // s FFT solves per step (stages 2..s and the additional solve), no iterations
-      for (int k = 0; k < ctx->s; ++k) stats_add(stats, ins2d_solve_stats{0, 0.0, 0.0});
+      if (!dev_stats) {
+        // s FFT solves per step (stages 2..s and the additional solve), no iterations
+        for (int k = 0; k < ctx->s; ++k) stats_add(stats, ins2d_solve_stats{0, 0.0, 0.0});
+      } else if ((n + 1) % kAccumCheck == 0 && n + 1 < nsteps) {
+        const int rc = read_accum();
+        if (rc) return rc;
+      }
       cached = true;
       continue;
     }
@@ -1236,6 +1379,17 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
     int rc = erk_step(ctx, dV, dP, t + n * dt, dt, stats, cached, n + 1 < nsteps ? &next : nullptr);
     if (rc) return rc;
     cached = next;
+  }
+  if (dev_stats && nsteps > 0) {
+    const int rc = read_accum();
+    if (rc) return rc;
+    if (stats) {
+      const SolveAccum &a = *ctx->h_accum;
+      stats->n_solves = (int32_t)a.n_solves;
+      stats->iters_total = (int32_t)a.iters_total;
+      stats->iters_max = (int32_t)a.iters_max;
+      stats->norm1_max = a.norm1_max;
+    }
   }
   if (mem == INS2D_MEM_HOST) {
     CK(cudaMemcpyAsync(V, dV, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

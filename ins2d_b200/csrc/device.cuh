@@ -65,6 +65,7 @@ struct DevOps {
   int fbx0, fbx1, fby0, fby1;
   int tile_ok;    // the interior tiles may use the shared-memory tiled walkers (FP64 fields)
   int tile_ok32;  // ... on FP32 fields
+  int all_fast;   // the rectangle holds every tile of the grid (no table-walker tiles)
   int nsm;        // multiprocessors of the device (persistent launches)
 };
 

@@ -473,9 +473,10 @@ template <int L, int SRC>
 __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
     k_rows_r2c_t(int Ny, const double2 *__restrict__ tw, const double *__restrict__ f, const WSplit ws,
                  double2 *__restrict__ spec, const __grid_constant__ DevOps P, double alpha, double beta,
-                 double gamma, int fastdiv) {
+                 double gamma, int fastdiv, const int *__restrict__ skip) {
   constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
   constexpr bool DIV = SRC != 0;
+  if (skip && *(volatile const int *)skip) return;  // preconditioner of a converged CG: nothing to do
   extern __shared__ double2 sm[];
   const double2 *pyr = tw + N;
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
@@ -547,8 +548,9 @@ template <int L, int G>
 __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
     k_cols_t(int H, int ncols, int I0, const double2 *__restrict__ tw, const double *__restrict__ ax,
              const double *__restrict__ ay, double dxdy, double2 *__restrict__ spec,
-             unsigned long long *__restrict__ maxbits) {
+             unsigned long long *__restrict__ maxbits, const int *__restrict__ skip) {
   constexpr int N = 1 << L, PER = N >> 3, LD = paddedl<L>();
+  if (skip && *(volatile const int *)skip) return;
   extern __shared__ double2 sm[];
   __shared__ double wmax[kThreads / 32];
   const double2 *pyr = tw + N;
@@ -617,8 +619,9 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
 template <int L>
 __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
     k_rows_c2r_t(int Ny, const double2 *__restrict__ tw, const double2 *__restrict__ spec, double *__restrict__ out,
-                 int accumulate, const unsigned long long *__restrict__ maxbits) {
+                 int accumulate, const unsigned long long *__restrict__ maxbits, const int *__restrict__ skip) {
   constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
+  if (skip && *(volatile const int *)skip) return;
   extern __shared__ double2 sm[];
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
   const bool has1 = j1 < Ny;
@@ -752,7 +755,7 @@ namespace {
 // spectrum's own max |fhat|)
 cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, const WSplit *ws, bool div,
                        double alpha, double beta, double gamma, double *dp, bool accumulate, cudaStream_t s,
-                       const unsigned long long *gate = nullptr) {
+                       const unsigned long long *gate = nullptr, const int *skip = nullptr) {
   const int Nx = plan.Nx, Ny = plan.Ny;
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
@@ -767,12 +770,12 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
     const WSplit w0{};
     if (ws)
       k_rows_r2c_t<L, 2><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, nullptr, *ws, plan.spec, P, alpha, beta, gamma,
-                                                     fastdiv);
+                                                     fastdiv, skip);
     else if (div)
       k_rows_r2c_t<L, 1><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, alpha, beta, gamma,
-                                                     fastdiv);
+                                                     fastdiv, skip);
     else
-      k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, 0.0, 0.0, 0.0, 0);
+      k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, 0.0, 0.0, 0.0, 0, skip);
   });
   const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
   if (!fx) k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
@@ -781,7 +784,7 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
     k_cols_t<L, G><<<(H + G - 1) / G, kThreads, sm, s>>>(H, H, 0, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
-                                                         plan.spec, maxbits);
+                                                         plan.spec, maxbits, skip);
   });
   if (!fy) {
     const int G = cols_group(Ny, plan.logy >= 0);
@@ -794,7 +797,7 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
     k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
-                                                gate ? gate : maxbits);
+                                                gate ? gate : maxbits, skip);
   });
   if (!fx2)
     k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
@@ -816,8 +819,8 @@ cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const d
 }
 
 cudaError_t launch_fft_precond(const DevOps &P, const FftPlan &plan, const double *r, double *z,
-                               const unsigned long long *gate, cudaStream_t s) {
-  return fft_passes(P, plan, r, nullptr, false, 0.0, 0.0, 0.0, z, false, s, gate);
+                               const unsigned long long *gate, const int *skip, cudaStream_t s) {
+  return fft_passes(P, plan, r, nullptr, false, 0.0, 0.0, 0.0, z, false, s, gate, skip);
 }
 
 cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, const double *Vn, const float *T,
@@ -840,7 +843,7 @@ cudaError_t slab_rows_forward(int Nx, const double2 *twx, const double *f, int n
   with_log2<kFusedMinLog>(ilog2_exact(Nx), [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
-    k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(nrows, twx, f, w0, spec, P, 0.0, 0.0, 0.0, 0);
+    k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(nrows, twx, f, w0, spec, P, 0.0, 0.0, 0.0, 0, nullptr);
   });
   return cudaPeekAtLastError();
 }
@@ -850,7 +853,8 @@ cudaError_t slab_columns(int Ny, const double2 *twy, const double *ax, const dou
   with_log2<kFusedMinLog>(ilog2_exact(Ny), [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
-    k_cols_t<L, G><<<(ncols + G - 1) / G, kThreads, sm, s>>>(width, ncols, I0, twy, ax, ay, dxdy, cols, maxbits);
+    k_cols_t<L, G><<<(ncols + G - 1) / G, kThreads, sm, s>>>(width, ncols, I0, twy, ax, ay, dxdy, cols, maxbits,
+                                                             nullptr);
   });
   return cudaPeekAtLastError();
 }
@@ -861,7 +865,7 @@ cudaError_t slab_rows_inverse(int Nx, const double2 *twx, const double2 *spec, i
   with_log2<kFusedMinLog>(ilog2_exact(Nx), [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
-    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(nrows, twx, spec, out, 0, maxbits);
+    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(nrows, twx, spec, out, 0, maxbits, nullptr);
   });
   return cudaPeekAtLastError();
 }

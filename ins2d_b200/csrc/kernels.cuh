@@ -162,9 +162,10 @@ cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const d
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s);
 // z = A^+ r by the same transform (the exact inverse of a periodic uniform
 // grid, as a PCG preconditioner): the early return is read from *gate
-// instead of the spectrum (a word holding a large value disables it)
+// instead of the spectrum (a word holding a large value disables it); every
+// pass returns at once while *skip is non-zero (a converged CG)
 cudaError_t launch_fft_precond(const DevOps &P, const FftPlan &plan, const double *r, double *z,
-                               const unsigned long long *gate, cudaStream_t s);
+                               const unsigned long long *gate, const int *skip, cudaStream_t s);
 // Same with W = Vn sv + sa T, T in FP32 (FP32-storage stages)
 cudaError_t launch_fft_poisson_div_split(const DevOps &P, const FftPlan &plan, const double *Vn, const float *T,
                                          double sv, double sa, double alpha, double beta, double gamma, double *dp,
@@ -197,8 +198,24 @@ struct PcgScalars {
   long long it, maxit;
   int done, status;
   unsigned int counter;
-  int pad;
+  int loops;  // passes of a device-side iteration loop (graph form)
 };
+// Solve statistics accumulated on the device by the solves of a captured
+// step graph (the host reads them after the graph launches).
+struct SolveAccum {
+  long long n_solves, iters_total, iters_max;
+  double norm1_max;
+  int status;  // first non-zero solve status (INS2D_E*), 0 if none
+  int pad;
+  double fail_rr;
+  long long fail_maxit;
+};
+// Graph form of the PCG loop: sets the WHILE condition h to "not done and
+// fewer than limit passes" (count: this launch ends a pass of the body)
+void launch_pcg_cond(PcgScalars *sc, cudaGraphConditionalHandle h, int limit, int count, cudaStream_t s);
+// adds a finished solve's iterations, residual and status to *acc (a loop
+// that stopped at its pass limit before convergence counts as INS2D_ETIMEOUT)
+void launch_solve_accum(const PcgScalars *sc, SolveAccum *acc, cudaStream_t s);
 struct PcgWork {
   double *x, *r, *p, *q;
   PcgScalars *sc;      // device

@@ -68,6 +68,7 @@ __global__ void __launch_bounds__(256) k_init(const __grid_constant__ DevOps P, 
     s->it = 0;
     s->status = 0;
     s->maxx = s->minx = s->maxres = 0.0;
+    s->loops = 0;
     // pressure_poisson.m:33-38 and cg.F:222-227
     s->done = (out[2] < 1e-14 || out[0] <= tol2) ? 1 : 0;
     if (!isfinite(out[0]) || !isfinite(out[1])) {
@@ -579,7 +580,7 @@ void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, c
 namespace {
 void precond_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, cudaStream_t s) {
   if (F.spectral)
-    launch_fft_precond(P, *F.fft, W.r, F.z, F.gate, s);
+    launch_fft_precond(P, *F.fft, W.r, F.z, F.gate, &W.sc->done, s);
   else
     fdm_apply(F, W.r, F.z, &W.sc->done, s);
 }
@@ -601,6 +602,38 @@ void pcg_iterations_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, int n,
     k_rz_g<<<g, kVecThreads, 0, s>>>(W, F.z, P.Np, 0);
     k_pupdate_g<<<g, kVecThreads, 0, s>>>(W, F.z, P.Np);
   }
+}
+
+namespace {
+__global__ void k_pcg_cond(PcgScalars *sc, cudaGraphConditionalHandle h, int limit, int count) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int n = sc->loops;
+  if (count) sc->loops = ++n;
+  const int done = *(volatile int *)&sc->done;
+  cudaGraphSetConditional(h, (!done && n < limit) ? 1u : 0u);
+}
+__global__ void k_solve_accum(const PcgScalars *sc, SolveAccum *a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const long long it = sc->it;
+  a->n_solves += 1;
+  a->iters_total += it;
+  if (it > a->iters_max) a->iters_max = it;
+  const double n1 = sqrt(sc->rr);
+  if (n1 > a->norm1_max) a->norm1_max = n1;
+  const int st = sc->done ? sc->status : INS2D_ETIMEOUT;
+  if (st != 0 && a->status == 0) {
+    a->status = st;
+    a->fail_rr = sc->rr;
+    a->fail_maxit = sc->maxit;
+  }
+}
+}  // namespace
+
+void launch_pcg_cond(PcgScalars *sc, cudaGraphConditionalHandle h, int limit, int count, cudaStream_t s) {
+  k_pcg_cond<<<1, 32, 0, s>>>(sc, h, limit, count);
+}
+void launch_solve_accum(const PcgScalars *sc, SolveAccum *acc, cudaStream_t s) {
+  k_solve_accum<<<1, 32, 0, s>>>(sc, acc);
 }
 
 void pcg_finish(const DevOps &P, const PcgWork &W, double *dp, bool accumulate, cudaStream_t s) {

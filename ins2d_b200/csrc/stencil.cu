@@ -613,13 +613,24 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
-__device__ __forceinline__ int wrapm(int x, int n) {
-  x %= n;
-  return x < 0 ? x + n : x;
+
+// Vtemp of an FP64 stage at idx: sum over the earlier stages a_m kV_m, then
+// the stage's own aii k (time_ERK.m:96-101).  NP >= 0: that many earlier
+// stages, unrolled at compile time; NP < 0: e.nprev.
+template <int NP>
+__device__ __forceinline__ double stage_vtemp(const Epi &e, long long idx, double k) {
+  double vt = 0.0;
+  if constexpr (NP >= 0) {
+#pragma unroll
+    for (int m = 0; m < NP; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+  } else {
+    for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
+  }
+  return vt + e.aii * k;
 }
 
 // MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
-template <typename S, int MODE, typename TV>
+template <typename S, int MODE, typename TV, int NP>
 __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
                        const YRowsN<RUN> &Y) {
   const S ire = S(P.invRe);
@@ -672,9 +683,7 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     if constexpr (MODE == 0) {
       const double k = oi * R;
       if (e.kV) e.kV[idx] = k;
-      double vt = 0.0;
-      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
-      vt += e.aii * k;
+      const double vt = stage_vtemp<NP>(e, idx, k);
       e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
     } else if constexpr (MODE == 2) {
       epi_stage32(e, idx, oi * R);
@@ -688,7 +697,7 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
   }
 }
 
-template <typename S, int MODE, typename TV>
+template <typename S, int MODE, typename TV, int NP>
 __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i, int i0, int j0, int ja, int jb,
                        const YRowsN<RUN> &Y) {
   const S ire = S(P.invRe);
@@ -746,9 +755,7 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     if constexpr (MODE == 0) {
       const double k = oi * R;
       if (e.kV) e.kV[idx] = k;
-      double vt = 0.0;
-      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
-      vt += e.aii * k;
+      const double vt = stage_vtemp<NP>(e, idx, k);
       e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
     } else if constexpr (MODE == 2) {
       epi_stage32(e, idx, oi * R);
@@ -764,32 +771,42 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
   }
 }
 
+// Copies the u and v rows j0-2 .. j0+RUN+2, columns i0-HL .. (wrapped) of
+// the velocity-sized field V into T with cp.async: a thread keeps one 16-byte
+// chunk column of one field and walks its rows RSTEP apart (tiles are whole,
+// so a staged coordinate wraps once at most).
+template <typename TV>
+__device__ __forceinline__ void stage_tile_fields(const DevOps &P, const TV *__restrict__ V, TileSm<TV> &T, int i0,
+                                                  int j0, int tid) {
+  using G = TileGeo<TV>;
+  constexpr int CH2 = 2 * G::CHUNKS, RSTEP = kTileThreads / CH2;
+  if (tid >= RSTEP * CH2) return;
+  const int q = tid % CH2, f = q >= G::CHUNKS, ch = q - f * G::CHUNKS;
+  const int nx = f ? P.Nvx : P.Nux, ny = f ? P.Nvy : P.Nuy;
+  const TV *src = V + (f ? P.Nu : 0LL) + wrapn(i0 - G::HL + G::EPC * ch, nx);
+  TV *dst = (f ? &T.v[0][0] : &T.u[0][0]) + G::EPC * ch;
+  int r = tid / CH2;
+  int gr = wrapn(j0 - 2 + r, ny);
+  for (; r < kTileRows; r += RSTEP) {
+    cp_async16(dst + r * G::COLS, src + (long long)gr * nx);
+    gr += RSTEP;
+    if (gr >= ny) gr -= ny;
+  }
+}
+
 #ifndef INS2D_TILE_MINB
 #define INS2D_TILE_MINB 3
 #endif
-template <typename S, int MODE, typename TV>
+// MODE 0-2 as tile_u / tile_v
+template <typename S, int MODE, typename TV, int NP>
 __global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
     k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
-  using G = TileGeo<TV>;
   __shared__ __align__(16) TileSm<TV> T;
   __shared__ YRowsN<RUN> Y;
   const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
   const int i0 = bx * WX, j0 = by * RUN;
   const int tid = threadIdx.x + WX * threadIdx.y;
-  const TV *u = V, *v = V + P.Nu;
-  // stage the u and v rows j0-2 .. j0+RUN+2, columns i0-HL .. (wrapped)
-  for (int q = tid; q < 2 * kTileRows * G::CHUNKS; q += kTileThreads) {
-    const int f = q >= kTileRows * G::CHUNKS;
-    const int qq = q - f * kTileRows * G::CHUNKS;
-    const int r = qq / G::CHUNKS, ch = qq - r * G::CHUNKS;
-    if (f == 0) {
-      const int gr = wrapm(j0 - 2 + r, P.Nuy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nux);
-      cp_async16(&T.u[r][G::EPC * ch], u + (long long)gr * P.Nux + gc);
-    } else {
-      const int gr = wrapm(j0 - 2 + r, P.Nvy), gc = wrapm(i0 - G::HL + G::EPC * ch, P.Nvx);
-      cp_async16(&T.v[r][G::EPC * ch], v + (long long)gr * P.Nvx + gc);
-    }
-  }
+  stage_tile_fields<TV>(P, V, T, i0, j0, tid);
   stage_yrows(P, j0, Y);
   cp_async_wait_all();
   __syncthreads();
@@ -797,9 +814,9 @@ __global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
   const int seg = threadIdx.y & 1;
   const int ja = j0 + seg * kTileSeg, jb = ja + kTileSeg;
   if (threadIdx.y < 2)
-    tile_u<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
+    tile_u<S, MODE, TV, NP>(P, T, e, i, i0, j0, ja, jb, Y);
   else
-    tile_v<S, MODE, TV>(P, T, e, i, i0, j0, ja, jb, Y);
+    tile_v<S, MODE, TV, NP>(P, T, e, i, i0, j0, ja, jb, Y);
 }
 
 // one WX x RUN tile (bx, by): u walkers in warps with threadIdx.y == 0, v in 1
@@ -903,6 +920,24 @@ __global__ void __launch_bounds__(WX * 2) k_walk_ens_gen(const EnsMemberD *__res
   walk_ens_body<S, false>(mem, work, w);
 }
 
+// MODE 0 with the count of earlier stages as a template argument (0..3
+// unrolled, more at run time)
+template <typename S, int MODE, typename TV>
+void launch_tile(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
+  const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0), tb(WX, kTileThreads / WX);
+  if constexpr (MODE == 0) {
+    switch (e.nprev) {
+      case 0: k_walk_tile<S, MODE, TV, 0><<<gf, tb, 0, s>>>(P, V, e); break;
+      case 1: k_walk_tile<S, MODE, TV, 1><<<gf, tb, 0, s>>>(P, V, e); break;
+      case 2: k_walk_tile<S, MODE, TV, 2><<<gf, tb, 0, s>>>(P, V, e); break;
+      case 3: k_walk_tile<S, MODE, TV, 3><<<gf, tb, 0, s>>>(P, V, e); break;
+      default: k_walk_tile<S, MODE, TV, -1><<<gf, tb, 0, s>>>(P, V, e); break;
+    }
+  } else {
+    k_walk_tile<S, MODE, TV, -1><<<gf, tb, 0, s>>>(P, V, e);
+  }
+}
+
 template <typename S, typename TV>
 void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx;
@@ -913,18 +948,17 @@ void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   if (has_fast) {
     const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0);
     if (tiled) {
-      const dim3 tb(WX, kTileThreads / WX);
       if (e.mode == 0)
-        k_walk_tile<S, 0, TV><<<gf, tb, 0, s>>>(P, V, e);
+        launch_tile<S, 0, TV>(P, V, e, s);
       else if (e.mode == 1)
-        k_walk_tile<S, 1, TV><<<gf, tb, 0, s>>>(P, V, e);
+        launch_tile<S, 1, TV>(P, V, e, s);
       else
-        k_walk_tile<S, 2, TV><<<gf, tb, 0, s>>>(P, V, e);
+        launch_tile<S, 2, TV>(P, V, e, s);
     } else {
       k_walk_fast<S, TV><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
     }
   }
-  k_walk<S, TV><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
+  if (!P.all_fast) k_walk<S, TV><<<g, dim3(WX, 2), 0, s>>>(P, V, e);
 }
 
 // FP64 contexts: FP64 fields, FP64 arithmetic; FP32-stencil contexts: FP32
@@ -972,6 +1006,7 @@ void walker_rectangle(DevOps &P) {
     }
   }
   if (bx0 < 0 || by0 < 0) bx0 = bx1 = by0 = by1 = 0;
+  P.all_fast = bx0 == 0 && bx1 == nbx && by0 == 0 && by1 == nby && bx1 > bx0 && by1 > by0;
   // the tiled walkers stage columns i0-2 .. i0+WX+3 and rows j0-2 .. j0+RUN+2
   // in 16-byte chunks: every shift must keep the stencil inside that halo
   auto shift_ok = [](const RegD &r) { return r.s >= -2 && r.s <= 1; };

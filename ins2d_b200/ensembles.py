@@ -35,7 +35,9 @@ def random_members(n, seed=4, sizes=(64, 96, 128, 192, 256), stretch=1.05, Re_ra
             y = cases.tanh_grid(ny, -0.5, 0.5, stretch)
             kw = dict(x=x, y=y, BC=cases.BC_CHANNEL, Re=Re,
                       uBC=cases.channel_uBC(lambda yy, U=U: U * (1.0 - 4.0 * np.asarray(yy) ** 2)))
-        kw.update(poisson=4, CG_acc=CG_acc, CG_maxit=CG_maxit, RK=RK, precision=precision)
+        # multigrid-preconditioned PCG: the preconditioner of ensemble
+        # members, so single contexts built from these settings match them
+        kw.update(poisson=4, CG_acc=CG_acc, CG_maxit=CG_maxit, RK=RK, precision=precision, precond="mg")
         kw["_U"] = U
         out.append(kw)
     return out

@@ -71,6 +71,56 @@ def test_pcg_poll_limit_timeout():
     assert np.linalg.norm(m.laplacian(dp) - f) <= 1.5e-10 * np.linalg.norm(f)
 
 
+@pytest.mark.parametrize("precond", ["fdm", "mg", "jacobi"])
+def test_pcg_step_graph_matches_host_loop(precond):
+    """A run of several steps captures each step as a CUDA graph in which the
+    PCG iteration loops are conditional WHILE nodes (no host round trip);
+    single steps run the host-polled loop.  Both take the same iterations and
+    give the same states (grid above the single-block solver's size)."""
+    import ins2d_b200
+    x = grid_stretched(300, 0.0, 1.0)
+    y = grid_stretched(260, 0.0, 1.0)
+    bc = BC_COMBOS["cavity"]
+    uBC, vBC = smooth_bc(5, closed=True)
+    m = ins2d_b200.Options(x, y, bc, Re=200.0, poisson=4, CG_acc=1e-10, CG_maxit=50000, uBC=uBC, vBC=vBC,
+                           precond=precond)
+    V0 = np.zeros(m.NV)
+    p0 = np.zeros(m.Np)
+    dt = 1e-4
+    Vg, pg, sg = m.time_ERK(V0, p0, 0.0, dt, nsteps=3, return_stats=True)
+    Vh, ph = V0.copy(), p0.copy()
+    iters = 0
+    for n in range(3):
+        Vh, ph, sh = m.time_ERK(Vh, ph, n * dt, dt, nsteps=1, return_stats=True)
+        iters += sh["iters_total"]
+    assert sg["n_solves"] == 12
+    assert sg["iters_total"] == iters
+    assert _rel(Vg, Vh) < 1e-13
+    assert _rel(pg, ph) < 1e-12
+
+
+def test_pcg_step_graph_loop_limit():
+    """The device-side iteration loop of a step graph ends at its pass limit
+    (a zero poll limit: no pass) and the run reports INS2D_ETIMEOUT; the
+    context stays usable."""
+    import ins2d_b200
+    from ins2d_b200 import _lib
+    x = grid_stretched(300, 0.0, 1.0)
+    y = grid_stretched(260, 0.0, 1.0)
+    uBC, vBC = smooth_bc(5, closed=True)
+    m = ins2d_b200.Options(x, y, BC_COMBOS["cavity"], Re=200.0, poisson=4, CG_acc=1e-10, uBC=uBC, vBC=vBC,
+                           precond="mg")
+    lib = _lib.load()
+    assert lib.ins2d_set_poll_limit(m._ctx, 0) == 0
+    with pytest.raises(ins2d_b200.Ins2dError) as ei:
+        m.time_ERK(np.zeros(m.NV), np.zeros(m.Np), 0.0, 1e-4, nsteps=2)
+    assert ei.value.status == _lib.ETIMEOUT
+    assert "iteration-loop limit" in str(ei.value)
+    assert lib.ins2d_set_poll_limit(m._ctx, -1) == 0
+    V, p, st = m.time_ERK(np.zeros(m.NV), np.zeros(m.Np), 0.0, 1e-4, nsteps=2, return_stats=True)
+    assert st["n_solves"] == 8 and st["norm1_max"] <= 1e-10
+
+
 @pytest.mark.parametrize("combo", ["cavity", "channel", "periodic", "per_x_walls"])
 def test_initial_projection(combo):
     """input_check.m:95-111 on the device against the oracle: a random field

@@ -26,8 +26,10 @@ def _members(seed, n, sizes, stretch=1.05):
             y = cases.tanh_grid(ny, -0.5, 0.5, stretch)
             out.append(dict(x=x, y=y, BC=cases.BC_CHANNEL, Re=Re,
                             uBC=cases.channel_uBC(lambda yy, U=U: U * (1 - 4 * np.asarray(yy) ** 2))))
+    # members solve with the multigrid preconditioner; the single contexts
+    # they are compared with use the same one
     for kw in out:
-        kw.update(poisson=4, CG_acc=1e-12, CG_maxit=20000, RK="RK44")
+        kw.update(poisson=4, CG_acc=1e-12, CG_maxit=20000, RK="RK44", precond="mg")
     return out
 
 

@@ -110,7 +110,8 @@ def test_pcg_poisson(combo):
 
 def test_pcg_not_converged_reports_error():
     o, m = _pair("cavity", False, nx=24, ny=20)
-    m2 = _ins2d().Options(o.grid.x, o.grid.y, BC_COMBOS["cavity"], Re=45.0, poisson=4, CG_acc=1e-14, CG_maxit=2)
+    m2 = _ins2d().Options(o.grid.x, o.grid.y, BC_COMBOS["cavity"], Re=45.0, poisson=4, CG_acc=1e-14, CG_maxit=2,
+                          precond="mg")
     f = o.discretization.M @ np.random.default_rng(1).standard_normal(o.grid.NV) + o.discretization.yM
     with pytest.raises(_ins2d().Ins2dError) as ei:
         m2.pressure_poisson(f)
@@ -194,6 +195,34 @@ def test_erk_fft_large_grid():
     Vg, pg = m.time_ERK(V0, np.zeros(g.Np), 0.0, 1e-4, nsteps=3)
     assert _rel(Vg, V) < 1e-12
     assert _rel(pg - pg.mean(), p - p.mean()) < 1e-10
+
+
+@pytest.mark.parametrize("rk", ["RK44", "RK33P2"])
+@pytest.mark.parametrize("poisson,stretch", [(6, False), (4, False), (4, True)])
+def test_erk_whole_tile_grid(rk, poisson, stretch):
+    """Periodic grid of whole 64x32 walker tiles: only the tiled walkers run
+    (no table-walker launch).  Runs of several steps (first stage from the
+    cached residual; CUDA graphs, PCG loops on the device) and single steps
+    (first stage from V; host-polled PCG) against the oracle."""
+    o, m = _pair("periodic", stretch, nx=128, ny=96, Re=300.0, poisson=poisson, CG_acc=1e-13, RK=rk)
+    g = o.grid
+    rng = np.random.default_rng(21)
+    V0 = R.initial_projection(0.5 * rng.standard_normal(g.NV), 0.0, o)
+    p0 = R.pressure_additional_solve(V0, np.zeros(g.Np), 0.0, o)
+    dt = 2e-4
+    V, p = V0.copy(), p0.copy()
+    for n in range(3):
+        V, p = R.time_ERK(V, p, n * dt, dt, o)
+    Vg, pg = m.time_ERK(V0, p0, 0.0, dt, nsteps=3)
+    Vs, ps = V0.copy(), p0.copy()
+    for n in range(3):
+        Vs, ps = m.time_ERK(Vs, ps, n * dt, dt, nsteps=1)
+    tol = 1e-12 if poisson == 6 else 1e-10
+    assert _rel(Vg, V) < tol
+    assert _rel(Vs, V) < tol
+    assert _rel(pg - pg.mean(), p - p.mean()) < 1e2 * tol
+    assert _rel(ps - ps.mean(), p - p.mean()) < 1e2 * tol
+    assert m.check_conservation(Vg, 3 * dt)[0] < 1e-10
 
 
 @pytest.mark.parametrize("combo", ["cavity", "channel", "periodic", "per_y_open", "open_x"])
