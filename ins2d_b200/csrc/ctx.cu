@@ -297,7 +297,7 @@ int solve_pcg_graph(ins2d_ctx *c, const double *f, double *dp, bool accumulate, 
   CK(cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   if (c->use_fdm) {
     pcg_iterations_fdm(c->P, c->fdm, c->pcg, chunk, c->body_stream);
-    c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 7LL : 8LL) * chunk;
+    c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 4LL + fft_kernels(c->fdm_fft) : 8LL) * chunk;
   } else if (c->use_mg) {
     pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->body_stream);
     c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
@@ -370,7 +370,7 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
       return fail(c, INS2D_ETIMEOUT, "PCG: device convergence flag not set within the host's iteration limit");
     if (c->use_fdm) {
       pcg_iterations_fdm(c->P, c->fdm, c->pcg, chunk, c->stream);
-      c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 7LL : 8LL) * chunk;
+      c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 4LL + fft_kernels(c->fdm_fft) : 8LL) * chunk;
     } else if (c->use_mg) {
       pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->stream);
       c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
@@ -513,7 +513,7 @@ int solve_learned(ins2d_ctx *c, const double *f, double *dp, bool accumulate, in
 int solve(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_solve_stats *st) {
   if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
   if (c->poisson == INS2D_POISSON_FFT) {
-    Prof pr(c, INS2D_PROF_POISSON, 3);
+    Prof pr(c, INS2D_PROF_POISSON, fft_kernels(c->fft));
     CK(launch_fft_poisson(c->P, c->fft, f, dp, accumulate, c->stream));
     CK(cudaGetLastError());
     return INS2D_OK;
@@ -537,7 +537,7 @@ int solve_div(ins2d_ctx *c, const double *W, double alpha, double beta, double g
               ins2d_solve_stats *st) {
   if (c->poisson == INS2D_POISSON_FFT && fft_fuses_div(c->fft)) {
     if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
-    Prof pr(c, INS2D_PROF_POISSON, 3);
+    Prof pr(c, INS2D_PROF_POISSON, fft_kernels(c->fft));
     CK(launch_fft_poisson_div(c->P, c->fft, W, alpha, beta, gamma, dp, accumulate, c->stream));
     CK(cudaGetLastError());
     return INS2D_OK;
@@ -555,7 +555,7 @@ int solve_div_split(ins2d_ctx *c, const double *Vn, const float *T, double sv, d
                     double gamma, double *dp, bool accumulate, ins2d_solve_stats *st) {
   if (c->poisson == INS2D_POISSON_FFT && fft_fuses_div(c->fft)) {
     if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
-    Prof pr(c, INS2D_PROF_POISSON, 3);
+    Prof pr(c, INS2D_PROF_POISSON, fft_kernels(c->fft));
     CK(launch_fft_poisson_div_split(c->P, c->fft, Vn, T, sv, sa, alpha, beta, gamma, dp, accumulate, c->stream));
     CK(cudaGetLastError());
     return INS2D_OK;
@@ -1196,8 +1196,17 @@ int ins2d_F(ins2d_ctx *ctx, const double *V, const double *C, const double *p, d
   const double *dC = (C && C != V) ? in_dev(ctx, C, ctx->stC, NV, mem) : dV;
   const double *dP = nopressure ? nullptr : in_dev(ctx, p, ctx->stP, (size_t)ctx->P.Np, mem);
   double *dO = mem == INS2D_MEM_DEVICE ? F_out : ctx->stO;
-  Prof pr(ctx, INS2D_PROF_OTHER, 1);
-  launch_F(ctx->P, dV, dC, dP, dO, ctx->red, ctx->stream);
+  if (dP && dC == dV && !ctx->fp32) {
+    // the stencil walkers (the stage kernels' F) and a max|F| reduction
+    Prof pr(ctx, INS2D_PROF_OTHER, 2);
+    launch_F_walk(ctx->P, dV, dP, dO, ctx->stream);
+    launch_maxabs(dO, (long long)NV, ctx->red, ctx->stream);
+  } else {
+    // C != V (F.m's linearisation point), nopressure, or FP32-stencil
+    // contexts (diagnostics stay FP64): one thread per point
+    Prof pr(ctx, INS2D_PROF_OTHER, 1);
+    launch_F(ctx->P, dV, dC, dP, dO, ctx->red, ctx->stream);
+  }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(ctx->h_red, ctx->red.result, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   if (mem == INS2D_MEM_HOST) CK(cudaMemcpyAsync(F_out, dO, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

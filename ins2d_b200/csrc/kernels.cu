@@ -256,6 +256,38 @@ __global__ void __launch_bounds__(256) k_stage_cached_ens(const EnsMemberD *__re
 
 }  // namespace
 
+namespace {
+// VEC: x is 16-byte aligned and read two values at a time
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_maxabs(const double *__restrict__ x, long long n, const RedScratch red) {
+  double m[1] = {0.0};
+  const int ops[1] = {R_MAX};
+  constexpr int W = VEC ? 2 : 1;
+  const long long stride = (long long)gridDim.x * blockDim.x * W;
+  for (long long k = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * W; k < n; k += stride) {
+    if (VEC && k + 1 < n) {
+      const double2 v = __ldg(reinterpret_cast<const double2 *>(x + k));
+      m[0] = fmax(m[0], fmax(fabs(v.x), fabs(v.y)));
+    } else {
+      m[0] = fmax(m[0], fabs(__ldg(x + k)));
+    }
+  }
+  grid_reduce<1>(m, ops, red);
+}
+}  // namespace
+
+void launch_maxabs(const double *x, long long n, const RedScratch &red, cudaStream_t s) {
+  const bool vec = ((uintptr_t)x & 15) == 0;
+  long long b = ((vec ? n / 2 : n) + 255) / 256;
+  if (b > 148LL * 8) b = 148LL * 8;
+  if (b > red.max_blocks) b = red.max_blocks;
+  if (b < 1) b = 1;
+  if (vec)
+    k_maxabs<true><<<(unsigned)b, 256, 0, s>>>(x, n, red);
+  else
+    k_maxabs<false><<<(unsigned)b, 256, 0, s>>>(x, n, red);
+}
+
 void launch_F(const DevOps &P, const double *V, const double *C, const double *p, double *F_out,
               const RedScratch &red, cudaStream_t s) {
   dim3 g = grid_for(P.Nux > P.Nvx ? P.Nux : P.Nvx, P.Nuy > P.Nvy ? P.Nuy : P.Nvy);
@@ -280,8 +312,83 @@ void launch_div_split(const DevOps &P, const double *Vn, const float *T, double 
                                                                 RedScratch{});
 }
 
+// --- projection on grids whose gradient rows are all regular two-point rows
+// (doubly periodic grids, P.proj_cols): a thread walks kColRows rows of one
+// column i, so the column's weights and neighbour indices are set up once,
+// the rows' weights are warp-uniform loads, and the dp value shared by
+// consecutive v rows is read once.  Same expressions as project_cell (om
+// factor, two-point gradient, (c om) g), so the results equal k_project's.
+constexpr int kColRows = 16;
+struct ProjW {  // V = dt (Wt - c Om^-1 G dp)
+  const double *Wt;
+  double dt;
+  __device__ __forceinline__ double value(long long k, double cog) const { return dt * (Wt[k] - cog); }
+};
+struct ProjCached {  // V = dt (Vn/dt + aii kV0 - c Om^-1 G dp)
+  const double *Vn, *kV0;
+  double aii, inv_dt, dt;
+  __device__ __forceinline__ double value(long long k, double cog) const {
+    const double w = Vn[k] * inv_dt + aii * kV0[k];
+    return dt * (w - cog);
+  }
+};
+struct ProjSplit {  // V = Vn + dt (a T - c Om^-1 G dp), T in FP32
+  const double *Vn;
+  const float *T;
+  double a, dt;
+  __device__ __forceinline__ double value(long long k, double cog) const {
+    return Vn[k] + dt * (a * (double)T[k] - cog);
+  }
+};
+template <class SRC, typename TO>
+__global__ void __launch_bounds__(256) k_project_cols(const __grid_constant__ DevOps P, const SRC src,
+                                                     const double *__restrict__ dp, double c, TO *Vo) {
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j0 = (blockIdx.y * BY + threadIdx.y) * kColRows;
+  if (i >= P.Npx || j0 >= P.Npy) return;
+  const int jend = min(j0 + kColRows, P.Npy);
+  const double rgxi = __ldg(P.rgxi + i), wx0 = __ldg(P.rMXT.w0 + i), wx1 = __ldg(P.rMXT.w1 + i);
+  const int cx0 = wrapn(i + P.rMXT.s, P.rMXT.n), cx1 = wrapn(cx0 + 1, P.rMXT.n);
+  const double rhx = __ldg(P.rhx + i), hx = __ldg(P.hx + i);
+  int r0 = wrapn(j0 + P.rMYT.s, P.rMYT.n);
+  double pa = __ldg(dp + (long long)r0 * P.Npx + i);
+#pragma unroll 4
+  for (int j = j0; j < jend; ++j) {
+    const int r1 = wrapn(r0 + 1, P.rMYT.n);
+    const double pb = __ldg(dp + (long long)r1 * P.Npx + i);
+    const double *prow = dp + (long long)j * P.Npx;
+    {
+      const long long k = (long long)j * P.Nux + i;
+      double a = wx0 * __ldg(prow + cx0);
+      a += wx1 * __ldg(prow + cx1);
+      const double om = __ldg(P.rhy + j) * rgxi;
+      const double g = -__ldg(P.hy + j) * a;
+      Vo[k] = (TO)src.value(k, c * om * g);
+    }
+    {
+      const long long k = P.Nu + (long long)j * P.Nvx + i;
+      double a = __ldg(P.rMYT.w0 + j) * pa;
+      a += __ldg(P.rMYT.w1 + j) * pb;
+      const double om = __ldg(P.rgyi + j) * rhx;
+      const double g = -hx * a;
+      Vo[k] = (TO)src.value(k, c * om * g);
+    }
+    pa = pb;
+    r0 = r1;
+  }
+}
+template <class SRC, typename TO>
+void launch_project_cols(const DevOps &P, const SRC &src, const double *dp, double c, TO *V_out, cudaStream_t s) {
+  const dim3 g((P.Npx + BX - 1) / BX, (P.Npy + BY * kColRows - 1) / (BY * kColRows));
+  k_project_cols<SRC, TO><<<g, dim3(BX, BY), 0, s>>>(P, src, dp, c, V_out);
+}
+
 void launch_project(const DevOps &P, const double *Wt, const double *dp, double dt, double c, double *V_out,
                     cudaStream_t s) {
+  if (P.proj_cols) {
+    launch_project_cols(P, ProjW{Wt, dt}, dp, c, V_out, s);
+    return;
+  }
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project<<<g, dim3(BX, BY), 0, s>>>(P, Wt, dp, dt, c, V_out);
@@ -290,6 +397,10 @@ void launch_project(const DevOps &P, const double *Wt, const double *dp, double 
 template <typename TO>
 void launch_project32_t(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
                         double c, TO *V_out, cudaStream_t s) {
+  if (P.proj_cols) {
+    launch_project_cols(P, ProjSplit{Vn, T, a, dt}, dp, c, V_out, s);
+    return;
+  }
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project32<TO><<<g, dim3(BX, BY), 0, s>>>(P, Vn, T, a, dp, dt, c, V_out);
@@ -305,6 +416,10 @@ void launch_project32(const DevOps &P, const double *Vn, const float *T, double 
 
 void launch_project_cached(const DevOps &P, const double *Vn, const double *kV0, double aii, double inv_dt,
                            const double *dp, double dt, double c, double *V_out, cudaStream_t s) {
+  if (P.proj_cols) {
+    launch_project_cols(P, ProjCached{Vn, kV0, aii, inv_dt, dt}, dp, c, V_out, s);
+    return;
+  }
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project_cached<<<g, dim3(BX, BY), 0, s>>>(P, Vn, kV0, aii, inv_dt, dp, dt, c, V_out);

@@ -72,6 +72,11 @@ cudaError_t walker_prepare();
 // (kV_next32) is non-null also stores Om^-1 R(V) there (rounded to FP32).
 void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next,
                      float *kV_next32, bool fp32, cudaStream_t s);
+// F_out = -conv(V) + Diff V + yDiff - (G p + y_p) (F.m:137-145 with C = V and
+// the pressure) by the stencil walkers, FP64 fields and arithmetic
+void launch_F_walk(const DevOps &P, const double *V, const double *p, double *F_out, cudaStream_t s);
+// red.result[0] = max |x| over n values (deterministic)
+void launch_maxabs(const double *x, long long n, const RedScratch &red, cudaStream_t s);
 // F_out = -conv(V;C) + Diff V + yDiff - (G p + y_p) (F.m); maxres into red.result[0]
 void launch_F(const DevOps &P, const double *V, const double *C, const double *p, double *F_out,
               const RedScratch &red, cudaStream_t s);
@@ -158,6 +163,8 @@ cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const doubl
 // Same with the right-hand side f = (M W + alpha yM + beta ydM) gamma computed
 // inside the first pass (only when fft_fuses_div(plan): power-of-two rows >= 64).
 bool fft_fuses_div(const FftPlan &plan);
+// kernel launches of one solve (the column transform takes one or three)
+int fft_kernels(const FftPlan &plan);
 cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s);
 // z = A^+ r by the same transform (the exact inverse of a periodic uniform

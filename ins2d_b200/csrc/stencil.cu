@@ -112,6 +112,7 @@ __device__ __forceinline__ YRow<S> yrow(const Tab &T, int r) {
 struct Epi {
   // 0: RK stage, FP64 storage (kV, Wt = Vn/dt + Vtemp);
   // 1: residual of the additional solve;
+  // 3: F = R - G p into w (walked as mode 1);
   // 2: RK stage, FP32 storage (kV32 and, when the stage combines earlier
   //    stages, Vt32 = Vtemp; Vn and Wt are not touched)
   int mode;
@@ -133,12 +134,19 @@ struct Epi {
   float *kV_next32;
 };
 
+// NP >= 0: that many earlier stages, unrolled; NP < 0: e.nprev
+template <int NP = -1>
 __device__ __forceinline__ void epi_stage32(const Epi &e, long long idx, double k) {
   const float kf = (float)k;
   if (e.kV32) e.kV32[idx] = kf;
   if (e.Vt32) {
     double vt = 0.0;
-    for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * (double)__ldg(e.kprev32[m] + idx);
+    if constexpr (NP >= 0) {
+#pragma unroll
+      for (int m = 0; m < NP; ++m) vt += e.aprev[m] * (double)__ldg(e.kprev32[m] + idx);
+    } else {
+      for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * (double)__ldg(e.kprev32[m] + idx);
+    }
     vt += e.aii * (double)kf;
     e.Vt32[idx] = (float)vt;
   }
@@ -158,6 +166,10 @@ __device__ __forceinline__ void epilogue_stage(const Epi &e, long long idx, doub
 }
 
 __device__ __forceinline__ void epi_residual(const Epi &e, long long idx, double oi, double R, double g) {
+  if (e.mode == 3) {  // F (F.m): the momentum right-hand side with the pressure gradient
+    e.w[idx] = R - g;
+    return;
+  }
   e.w[idx] = oi * (R - g);
   if (e.kV_next) e.kV_next[idx] = oi * R;
   if (e.kV_next32) e.kV_next32[idx] = (float)(oi * R);
@@ -181,7 +193,7 @@ __device__ void walk_u(const DevOps &P, const TV *__restrict__ u, const TV *__re
   const S xvlo = S(__ldg(P.bc.XvLo + i)), xvup = S(__ldg(P.bc.XvUp + i));
   // gradient row (residual mode)
   XRow<double> gt{};
-  if (e.mode == 1) gt = xrow<double>(P.MXT, i);
+  if (e.mode == 1 || e.mode == 3) gt = xrow<double>(P.MXT, i);
   // face at row r: u_uy, du/dy, vbar_uy
   auto face = [&](int r, S &uy, S &sy, S &vf) {
     const YRow<S> ay = yrow<S>(P.AUY, r);
@@ -220,7 +232,7 @@ __device__ void walk_u(const DevOps &P, const TV *__restrict__ u, const TV *__re
     const long long idx = (long long)j * P.Nux + i;
     const double hyd = __ldg(P.hy + j);
     const double oi = __ldg(P.rhy + j) * __ldg(P.rgxi + i);
-    if (e.mode != 1) {
+    if (e.mode == 0 || e.mode == 2) {
       epilogue_stage(e, idx, oi, R);
     } else {
       const double *prow = e.p + (long long)j * P.Npx;
@@ -301,7 +313,7 @@ __device__ void walk_v(const DevOps &P, const TV *__restrict__ u, const TV *__re
     const double R = (double)(-(duvdx + dv2dy) + d2v - ypy);
     const long long idx = P.Nu + (long long)j * P.Nvx + i;
     const double oi = __ldg(P.rgyi + j) * __ldg(P.rhx + i);
-    if (e.mode != 1) {
+    if (e.mode == 0 || e.mode == 2) {
       epilogue_stage(e, idx, oi, R);
     } else {
       const YRow<double> gy = yrow<double>(P.MYT, j);
@@ -686,7 +698,7 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
       const double vt = stage_vtemp<NP>(e, idx, k);
       e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
     } else if constexpr (MODE == 2) {
-      epi_stage32(e, idx, oi * R);
+      epi_stage32<NP>(e, idx, oi * R);
     } else {
       const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
       epi_residual(e, idx, oi, R, g);
@@ -758,7 +770,7 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
       const double vt = stage_vtemp<NP>(e, idx, k);
       e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
     } else if constexpr (MODE == 2) {
-      epi_stage32(e, idx, oi * R);
+      epi_stage32<NP>(e, idx, oi * R);
     } else {
       const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
       double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
@@ -920,12 +932,12 @@ __global__ void __launch_bounds__(WX * 2) k_walk_ens_gen(const EnsMemberD *__res
   walk_ens_body<S, false>(mem, work, w);
 }
 
-// MODE 0 with the count of earlier stages as a template argument (0..3
+// MODE 0 and 2 with the count of earlier stages as a template argument (0..3
 // unrolled, more at run time)
 template <typename S, int MODE, typename TV>
 void launch_tile(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0), tb(WX, kTileThreads / WX);
-  if constexpr (MODE == 0) {
+  if constexpr (MODE == 0 || MODE == 2) {
     switch (e.nprev) {
       case 0: k_walk_tile<S, MODE, TV, 0><<<gf, tb, 0, s>>>(P, V, e); break;
       case 1: k_walk_tile<S, MODE, TV, 1><<<gf, tb, 0, s>>>(P, V, e); break;
@@ -950,10 +962,10 @@ void launch_walk_t(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
     if (tiled) {
       if (e.mode == 0)
         launch_tile<S, 0, TV>(P, V, e, s);
-      else if (e.mode == 1)
-        launch_tile<S, 1, TV>(P, V, e, s);
-      else
+      else if (e.mode == 2)
         launch_tile<S, 2, TV>(P, V, e, s);
+      else
+        launch_tile<S, 1, TV>(P, V, e, s);  // residual and F
     } else {
       k_walk_fast<S, TV><<<gf, dim3(WX, 2), 0, s>>>(P, V, e);
     }
@@ -1014,6 +1026,9 @@ void walker_rectangle(DevOps &P) {
               shift_ok(P.rAVY) && shift_ok(P.rIUX) && shift_ok(P.rIUY) && P.Nux % 2 == 0 && P.Nvx % 2 == 0 &&
               P.Nu % 2 == 0;
   P.tile_ok32 = P.tile_ok && P.Nux % 4 == 0 && P.Nvx % 4 == 0 && P.Nu % 4 == 0;
+  P.proj_cols = P.Nux == P.Npx && P.Nvx == P.Npx && P.Nuy == P.Npy && P.Nvy == P.Npy && P.rMXT.lo == 0 &&
+                P.rMXT.hi >= P.Nux && P.rMYT.lo == 0 && P.rMYT.hi >= P.Nvy && P.rMXT.two && P.rMYT.two &&
+                P.rMXT.n == P.Npx && P.rMYT.n == P.Npy;
   P.fbx0 = bx0;
   P.fbx1 = bx1;
   P.fby0 = by0;
@@ -1064,6 +1079,14 @@ void launch_stage(const DevOps &P, const StageArgs &a, bool fp32, cudaStream_t s
   e.kV32 = a.kV32;
   e.Vt32 = a.Vt32;
   launch_walk(P, a.V, a.V32, e, fp32, s);
+}
+
+void launch_F_walk(const DevOps &P, const double *V, const double *p, double *F_out, cudaStream_t s) {
+  Epi e{};
+  e.mode = 3;
+  e.p = p;
+  e.w = F_out;
+  launch_walk(P, V, nullptr, e, false, s);
 }
 
 void launch_residual(const DevOps &P, const double *V, const double *p, double *w, double *kV_next,

@@ -70,8 +70,26 @@ def test_F_divergence_laplacian(combo, stretch):
         assert abs(a - b) <= 1e-12 * max(abs(b), 1.0)
 
 
+@pytest.mark.parametrize("combo,nx,ny", [("cavity", 200, 140), ("channel", 200, 140), ("periodic", 128, 96),
+                                          ("per_y_open", 130, 96)])
+@pytest.mark.parametrize("stretch", [False, True])
+def test_F_tiled_walkers(combo, nx, ny, stretch):
+    """F with the pressure (C = V) runs through the stage walkers -- shared-
+    memory tiles inside, table walker at the boundary -- and a separate
+    max|F| reduction: against the oracle at 1e-12."""
+    o, m = _pair(combo, stretch, nx=nx, ny=ny)
+    g = o.grid
+    rng = np.random.default_rng(17)
+    V = rng.standard_normal(g.NV)
+    p = rng.standard_normal(g.Np)
+    mr_ref, F_ref = R.F(V, V, p, 0.0, o)
+    mr, Fg = m.F(V, None, p, 0.0)
+    assert _rel(Fg, F_ref) < 1e-12
+    assert abs(mr - mr_ref) <= 1e-12 * mr_ref
+
+
 @pytest.mark.parametrize("nx,ny", [(16, 8), (40, 40), (64, 32), (12, 10), (128, 128), (1024, 512), (2048, 2048),
-                                   (8192, 64), (64, 8192), (4096, 32)])
+                                   (8192, 64), (64, 8192), (4096, 32), (96, 1024), (256, 4096), (64, 2048)])
 def test_fft_poisson(nx, ny):
     x = grid_uniform(nx, 0.0, 2 * np.pi)
     y = grid_uniform(ny, 0.0, 3.0)
