@@ -66,8 +66,6 @@ struct DevOps {
   int tile_ok;    // the interior tiles may use the shared-memory tiled walkers (FP64 fields)
   int tile_ok32;  // ... on FP32 fields
   int all_fast;   // the rectangle holds every tile of the grid (no table-walker tiles)
-  int proj_cols;  // every gradient row a regular two-point row on a doubly periodic grid:
-                  // the projections walk columns (k_project_cols)
   int nsm;        // multiprocessors of the device (persistent launches)
 };
 

@@ -614,134 +614,6 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
   }
 }
 
-// --- four-step column transform for Ny = 2^L = N1 N2, N1 = 64, N2 = 2^(L-6),
-// L = 10..12 (INS2D_FFT_FOURSTEP): the column FFT of length N becomes
-// N1-point transforms over rows strided by N2 (kernel A), a twiddle
-// W_N^(n2 k1), and N2-point transforms over contiguous rows (kernel B), so
-// every global access of a warp is one 32-column row segment (512 bytes)
-// instead of 16 rows of two columns.  Row j = n1 N2 + n2 holds x[n1 N2 + n2];
-// after A row k1 N2 + n2 holds the twiddled N1-point transform y[k1][n2];
-// B transforms over n2 (frequency J = k1 + N1 k2), scales by -1/Ahat,
-// transforms back and applies W_N^(-n2 k1); A in the inverse direction
-// finishes (scaled 1/N).  Each kernel reads and writes the spectrum once
-// (L2-resident at the sizes it serves).
-#ifndef INS2D_FFT_FOURSTEP
-#define INS2D_FFT_FOURSTEP 1
-#endif
-constexpr int kFsCols = 32;  // spectrum columns per block (a warp's row segment)
-
-// A: N1 = 64-point transforms of kFsCols columns over the rows n1 N2 + n2,
-// n2 = blockIdx.y; FWD: forward then the twiddle; else inverse, scaled 1/N
-template <int L, bool FWD>
-__global__ void __launch_bounds__(256) k_cols_a(int H, const double2 *__restrict__ tw, double2 *__restrict__ spec,
-                                               const int *__restrict__ skip) {
-  constexpr int N = 1 << L, N1 = 64, N2 = N / N1;
-  if (skip && *(volatile const int *)skip) return;
-  __shared__ double2 sm[kFsCols][N1 + 1];
-  const double2 *pyr = tw + N;
-  const int c = threadIdx.x & 31, q = threadIdx.x >> 5;  // q: 0..7
-  const int I = blockIdx.x * kFsCols + c, n2 = blockIdx.y;
-  const bool ok = I < H;
-  {
-    double2 x[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m)
-      x[m] = ok ? spec[(size_t)((q + 8 * m) * N2 + n2) * H + I] : make_double2(0.0, 0.0);
-    group_dif<false>(x, 3, q, 8, pyr, !FWD);
-#pragma unroll
-    for (int m = 0; m < 8; ++m) sm[c][q + 8 * m] = x[m];
-  }
-  __syncthreads();
-  double2 x[8];
-#pragma unroll
-  for (int m = 0; m < 8; ++m) x[m] = sm[c][q * 8 + m];
-  group_dif<true>(x, 3, 0, 1, pyr, !FWD);
-  if (!ok) return;
-  constexpr double sc = 1.0 / N;
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const int k = brev(q * 8 + m, 6);  // the transform index of position q*8 + m
-    double2 v = x[m];
-    if (FWD)
-      v = cmul(v, __ldg(tw + n2 * k));
-    else
-      v = make_double2(v.x * sc, v.y * sc);
-    spec[(size_t)(k * N2 + n2) * H + I] = v;
-  }
-}
-
-// B: for k1 = blockIdx.y, the N2-point forward transforms over rows
-// k1 N2 + n2, the scaling -1/Ahat(I, k1 + N1 k2) with the max |fhat|
-// reduction, the inverse transforms and the twiddle W_N^(-n2 k1)
-template <int L>
-__global__ void __launch_bounds__(256) k_cols_b(int H, const double2 *__restrict__ tw, const double *__restrict__ ax,
-                                               const double *__restrict__ ay, double dxdy,
-                                               double2 *__restrict__ spec, unsigned long long *__restrict__ maxbits,
-                                               const int *__restrict__ skip) {
-  constexpr int N = 1 << L, N1 = 64, L2 = L - 6, N2 = 1 << L2, NS1 = L2 - 3, M1 = 1 << NS1;
-  if (skip && *(volatile const int *)skip) return;
-  __shared__ double2 sm[kFsCols][N2 + 1];
-  __shared__ double wmax[8];
-  const double2 *pyr = tw + N;
-  const int c = threadIdx.x & 31, q = threadIdx.x >> 5;  // q: 0..7
-  const int I = blockIdx.x * kFsCols + c, k1 = blockIdx.y;
-  const bool ok = I < H;
-  const size_t row0 = (size_t)k1 * N2;
-  // forward stages with half sizes N2/2 .. 8: values q + 8 m, m < M1
-  {
-    double2 x[8];
-#pragma unroll
-    for (int m = 0; m < M1; ++m) x[m] = ok ? spec[(row0 + q + 8 * m) * H + I] : make_double2(0.0, 0.0);
-    group_dif<false>(x, NS1, q, 8, pyr, false);
-#pragma unroll
-    for (int m = 0; m < M1; ++m) sm[c][q + 8 * m] = x[m];
-  }
-  __syncthreads();
-  // half sizes 4, 2, 1 (positions blk*8 + m), scaling, and back
-  double lmax = 0.0;
-  for (int blk = q; blk < N2 / 8; blk += 8) {
-    double2 x[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = sm[c][blk * 8 + m];
-    group_dif<true>(x, 3, 0, 1, pyr, false);
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const int J = k1 + N1 * brev(blk * 8 + m, L2);
-      const double2 F = x[m];
-      if (ok) lmax = fmax(lmax, F.x * F.x + F.y * F.y);
-      const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + (ok ? I : 0)) + __ldg(ay + J));
-      const double r = -1.0 / lam;
-      x[m] = make_double2(F.x * r, F.y * r);
-    }
-    group_dit<true>(x, 3, 0, 1, pyr, true);
-#pragma unroll
-    for (int m = 0; m < 8; ++m) sm[c][blk * 8 + m] = x[m];
-  }
-  __syncthreads();
-  {
-    double2 x[8];
-#pragma unroll
-    for (int m = 0; m < M1; ++m) x[m] = sm[c][q + 8 * m];
-    group_dit<false>(x, NS1, q, 8, pyr, true);
-    if (ok)
-#pragma unroll
-      for (int m = 0; m < M1; ++m) {
-        const int n2 = q + 8 * m;
-        double2 w = __ldg(tw + n2 * k1);
-        w.y = -w.y;
-        spec[(row0 + n2) * H + I] = cmul(x[m], w);
-      }
-  }
-  for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, off));
-  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mm = wmax[0];
-    for (int w = 1; w < 8; ++w) mm = fmax(mm, wmax[w]);
-    atomicMax(maxbits, (unsigned long long)__double_as_longlong(sqrt(mm)));
-  }
-}
-
 // half spectra of rows j0, j1 -> real rows (inverse DIF, bit-reversed result
 // read back in natural order)
 template <int L>
@@ -908,29 +780,13 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
   if (!fx) k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
   // columns: forward, scaling, inverse
-  if (INS2D_FFT_FOURSTEP && plan.logy >= 10 && plan.logy <= 12) {
-    const dim3 ga((H + kFsCols - 1) / kFsCols, plan.Ny / 64), gb((H + kFsCols - 1) / kFsCols, 64);
-    auto run = [&](auto c) {
-      constexpr int L = decltype(c)::value;
-      k_cols_a<L, true><<<ga, 256, 0, s>>>(H, plan.twy, plan.spec, skip);
-      k_cols_b<L><<<gb, 256, 0, s>>>(H, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy, plan.spec, maxbits, skip);
-      k_cols_a<L, false><<<ga, 256, 0, s>>>(H, plan.twy, plan.spec, skip);
-    };
-    if (plan.logy == 10)
-      run(std::integral_constant<int, 10>{});
-    else if (plan.logy == 11)
-      run(std::integral_constant<int, 11>{});
-    else
-      run(std::integral_constant<int, 12>{});
-  }
-  const bool fy = !(INS2D_FFT_FOURSTEP && plan.logy >= 10 && plan.logy <= 12) &&
-                  with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
+  const bool fy = with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
     k_cols_t<L, G><<<(H + G - 1) / G, kThreads, sm, s>>>(H, H, 0, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
                                                          plan.spec, maxbits, skip);
   });
-  if (!fy && !(INS2D_FFT_FOURSTEP && plan.logy >= 10 && plan.logy <= 12)) {
+  if (!fy) {
     const int G = cols_group(Ny, plan.logy >= 0);
     const size_t smy = (size_t)G * padded(Ny) * sizeof(double2) * (plan.logy >= 0 ? 1 : 2);
     k_cols<<<(H + G - 1) / G, kThreads, smy, s>>>(Nx, Ny, plan.logy, G, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
@@ -957,9 +813,7 @@ cudaError_t launch_fft_poisson(const DevOps &P, const FftPlan &plan, const doubl
 
 bool fft_fuses_div(const FftPlan &plan) { return plan.logx >= kFusedMinLog && plan.logx <= 13; }
 
-int fft_kernels(const FftPlan &plan) {
-  return (INS2D_FFT_FOURSTEP && plan.logy >= 10 && plan.logy <= 12) ? 5 : 3;
-}
+int fft_kernels(const FftPlan &) { return 3; }
 
 cudaError_t launch_fft_poisson_div(const DevOps &P, const FftPlan &plan, const double *W, double alpha,
                                    double beta, double gamma, double *dp, bool accumulate, cudaStream_t s) {

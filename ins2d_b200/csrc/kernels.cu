@@ -312,83 +312,8 @@ void launch_div_split(const DevOps &P, const double *Vn, const float *T, double 
                                                                 RedScratch{});
 }
 
-// --- projection on grids whose gradient rows are all regular two-point rows
-// (doubly periodic grids, P.proj_cols): a thread walks kColRows rows of one
-// column i, so the column's weights and neighbour indices are set up once,
-// the rows' weights are warp-uniform loads, and the dp value shared by
-// consecutive v rows is read once.  Same expressions as project_cell (om
-// factor, two-point gradient, (c om) g), so the results equal k_project's.
-constexpr int kColRows = 16;
-struct ProjW {  // V = dt (Wt - c Om^-1 G dp)
-  const double *Wt;
-  double dt;
-  __device__ __forceinline__ double value(long long k, double cog) const { return dt * (Wt[k] - cog); }
-};
-struct ProjCached {  // V = dt (Vn/dt + aii kV0 - c Om^-1 G dp)
-  const double *Vn, *kV0;
-  double aii, inv_dt, dt;
-  __device__ __forceinline__ double value(long long k, double cog) const {
-    const double w = Vn[k] * inv_dt + aii * kV0[k];
-    return dt * (w - cog);
-  }
-};
-struct ProjSplit {  // V = Vn + dt (a T - c Om^-1 G dp), T in FP32
-  const double *Vn;
-  const float *T;
-  double a, dt;
-  __device__ __forceinline__ double value(long long k, double cog) const {
-    return Vn[k] + dt * (a * (double)T[k] - cog);
-  }
-};
-template <class SRC, typename TO>
-__global__ void __launch_bounds__(256) k_project_cols(const __grid_constant__ DevOps P, const SRC src,
-                                                     const double *__restrict__ dp, double c, TO *Vo) {
-  const int i = blockIdx.x * BX + threadIdx.x;
-  const int j0 = (blockIdx.y * BY + threadIdx.y) * kColRows;
-  if (i >= P.Npx || j0 >= P.Npy) return;
-  const int jend = min(j0 + kColRows, P.Npy);
-  const double rgxi = __ldg(P.rgxi + i), wx0 = __ldg(P.rMXT.w0 + i), wx1 = __ldg(P.rMXT.w1 + i);
-  const int cx0 = wrapn(i + P.rMXT.s, P.rMXT.n), cx1 = wrapn(cx0 + 1, P.rMXT.n);
-  const double rhx = __ldg(P.rhx + i), hx = __ldg(P.hx + i);
-  int r0 = wrapn(j0 + P.rMYT.s, P.rMYT.n);
-  double pa = __ldg(dp + (long long)r0 * P.Npx + i);
-#pragma unroll 4
-  for (int j = j0; j < jend; ++j) {
-    const int r1 = wrapn(r0 + 1, P.rMYT.n);
-    const double pb = __ldg(dp + (long long)r1 * P.Npx + i);
-    const double *prow = dp + (long long)j * P.Npx;
-    {
-      const long long k = (long long)j * P.Nux + i;
-      double a = wx0 * __ldg(prow + cx0);
-      a += wx1 * __ldg(prow + cx1);
-      const double om = __ldg(P.rhy + j) * rgxi;
-      const double g = -__ldg(P.hy + j) * a;
-      Vo[k] = (TO)src.value(k, c * om * g);
-    }
-    {
-      const long long k = P.Nu + (long long)j * P.Nvx + i;
-      double a = __ldg(P.rMYT.w0 + j) * pa;
-      a += __ldg(P.rMYT.w1 + j) * pb;
-      const double om = __ldg(P.rgyi + j) * rhx;
-      const double g = -hx * a;
-      Vo[k] = (TO)src.value(k, c * om * g);
-    }
-    pa = pb;
-    r0 = r1;
-  }
-}
-template <class SRC, typename TO>
-void launch_project_cols(const DevOps &P, const SRC &src, const double *dp, double c, TO *V_out, cudaStream_t s) {
-  const dim3 g((P.Npx + BX - 1) / BX, (P.Npy + BY * kColRows - 1) / (BY * kColRows));
-  k_project_cols<SRC, TO><<<g, dim3(BX, BY), 0, s>>>(P, src, dp, c, V_out);
-}
-
 void launch_project(const DevOps &P, const double *Wt, const double *dp, double dt, double c, double *V_out,
                     cudaStream_t s) {
-  if (P.proj_cols) {
-    launch_project_cols(P, ProjW{Wt, dt}, dp, c, V_out, s);
-    return;
-  }
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project<<<g, dim3(BX, BY), 0, s>>>(P, Wt, dp, dt, c, V_out);
@@ -397,10 +322,6 @@ void launch_project(const DevOps &P, const double *Wt, const double *dp, double 
 template <typename TO>
 void launch_project32_t(const DevOps &P, const double *Vn, const float *T, double a, const double *dp, double dt,
                         double c, TO *V_out, cudaStream_t s) {
-  if (P.proj_cols) {
-    launch_project_cols(P, ProjSplit{Vn, T, a, dt}, dp, c, V_out, s);
-    return;
-  }
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project32<TO><<<g, dim3(BX, BY), 0, s>>>(P, Vn, T, a, dp, dt, c, V_out);
@@ -416,10 +337,6 @@ void launch_project32(const DevOps &P, const double *Vn, const float *T, double 
 
 void launch_project_cached(const DevOps &P, const double *Vn, const double *kV0, double aii, double inv_dt,
                            const double *dp, double dt, double c, double *V_out, cudaStream_t s) {
-  if (P.proj_cols) {
-    launch_project_cols(P, ProjCached{Vn, kV0, aii, inv_dt, dt}, dp, c, V_out, s);
-    return;
-  }
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
   k_project_cached<<<g, dim3(BX, BY), 0, s>>>(P, Vn, kV0, aii, inv_dt, dp, dt, c, V_out);

@@ -1026,9 +1026,6 @@ void walker_rectangle(DevOps &P) {
               shift_ok(P.rAVY) && shift_ok(P.rIUX) && shift_ok(P.rIUY) && P.Nux % 2 == 0 && P.Nvx % 2 == 0 &&
               P.Nu % 2 == 0;
   P.tile_ok32 = P.tile_ok && P.Nux % 4 == 0 && P.Nvx % 4 == 0 && P.Nu % 4 == 0;
-  P.proj_cols = P.Nux == P.Npx && P.Nvx == P.Npx && P.Nuy == P.Npy && P.Nvy == P.Npy && P.rMXT.lo == 0 &&
-                P.rMXT.hi >= P.Nux && P.rMYT.lo == 0 && P.rMYT.hi >= P.Nvy && P.rMXT.two && P.rMYT.two &&
-                P.rMXT.n == P.Npx && P.rMYT.n == P.Npy;
   P.fbx0 = bx0;
   P.fbx1 = bx1;
   P.fby0 = by0;
