@@ -90,7 +90,11 @@ WORKLOADS = {
                    poisson=4, precision="fp64",
                    desc="ensemble of 256 cavity/channel flows, tanh-stretched 1.05, nx,ny in {64..256}, "
                         "Re U[100,5000], lid/inflow U[0.5,1.5], from rest, RK44 dt=5e-4, PCG to 1e-10, FP64; "
-                        "members sharded over ranks longest-first"),
+                        "members sharded over ranks longest-first; the batched solves use fast "
+                        "diagonalization"),
+    "ens256_mg": dict(kind="ensemble", n=256, sizes=(64, 96, 128, 192, 256), stretch=1.05, dt=5e-4, CG_acc=1e-10,
+                      poisson=4, precision="fp64", precond="mg",
+                      desc="ens256 with the members' multigrid preconditioner (solve form chosen by the tuner)"),
 }
 
 # Algorithmic DRAM bytes per pressure cell of one launch of each kernel
@@ -737,7 +741,8 @@ def run_ensemble(args, wl, rank, world, local_rank):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     members = ensembles.random_members(args.members or wl["n"], seed=4, sizes=wl["sizes"], stretch=wl["stretch"],
-                                       CG_acc=wl["CG_acc"], precision=wl["precision"])
+                                       CG_acc=wl["CG_acc"], precision=wl["precision"],
+                                       precond=wl.get("precond", "default"))
     costs = [ensembles.member_cost(kw) for kw in members]
     mine = ensembles.lpt_partition(costs, world)[rank]
     t0 = time.perf_counter()

@@ -243,6 +243,48 @@ void setup_rk(ins2d_ctx *c) {
 // ---------------------------------------------------------------------------
 // Poisson solve: dp = pressure_poisson(f) (or dp += ... when accumulate)
 
+// Adds a conditional WHILE node to the graph being captured on stream s.
+// pre(h) is captured on s before the node and sets the condition's first
+// value; body(bs, h) is captured on body_stream (a second stream of the same
+// device) into the node's body graph, and its last kernel sets the condition
+// again.  Throws CudaError when s is not capturing.
+template <class Pre, class Body>
+void capture_while(cudaStream_t s, cudaStream_t body_stream, Pre pre, Body body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) throw CudaError("device-side loop outside a stream capture");
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  pre(h);
+  CK(cudaGetLastError());
+  CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, deps, nd, &np));
+  CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  CK(cudaStreamBeginCaptureToGraph(body_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  try {
+    body(body_stream, h);
+  } catch (...) {
+    cudaGraph_t junk = nullptr;
+    cudaStreamEndCapture(body_stream, &junk);
+    throw;
+  }
+  const cudaError_t le = cudaGetLastError();
+  cudaGraph_t body_out = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(body_stream, &body_out);
+  CK(le);
+  CK(ee);
+}
+
 // The PCG solve inside a step being captured as a CUDA graph (c->dev_loop):
 // no host round trip.  The iterations are the body of a conditional WHILE
 // node, captured on the context's second stream into the node's body graph;
@@ -274,43 +316,22 @@ int solve_pcg_graph(ins2d_ctx *c, const double *f, double *dp, bool accumulate, 
   const int chunk = (c->use_fdm || c->use_mg) ? 1 : 4;
   const long long lim = c->poll_limit >= 0 ? c->poll_limit : (long long)c->opts.CG_maxit / chunk + 4;
   const int limit = (int)std::min<long long>(lim, 1 << 30);
-  cudaStreamCaptureStatus cs;
-  cudaGraph_t g = nullptr;
-  const cudaGraphNode_t *deps = nullptr;
-  size_t nd = 0;
-  CK(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
-  if (cs != cudaStreamCaptureStatusActive) return fail(c, INS2D_EINVAL, "graph-form PCG outside a stream capture");
-  cudaGraphConditionalHandle h;
-  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-  launch_pcg_cond(c->pcg.sc, h, limit, 0, c->stream);
-  CK(cudaGetLastError());
-  CK(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
-  cudaGraphNodeParams np{};
-  np.type = cudaGraphNodeTypeConditional;
-  np.conditional.handle = h;
-  np.conditional.type = cudaGraphCondTypeWhile;
-  np.conditional.size = 1;
-  cudaGraphNode_t node;
-  CK(cudaGraphAddNode(&node, g, deps, nd, &np));
-  CK(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
-  cudaGraph_t body = np.conditional.phGraph_out[0];
-  CK(cudaStreamBeginCaptureToGraph(c->body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  if (c->use_fdm) {
-    pcg_iterations_fdm(c->P, c->fdm, c->pcg, chunk, c->body_stream);
-    c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 4LL + fft_kernels(c->fdm_fft) : 8LL) * chunk;
-  } else if (c->use_mg) {
-    pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, c->body_stream);
-    c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
-  } else {
-    pcg_iterations(c->P, c->pcg, chunk, c->body_stream);
-    c->launches[INS2D_PROF_POISSON] += 3LL * chunk;
-  }
-  launch_pcg_cond(c->pcg.sc, h, limit, 1, c->body_stream);
-  const cudaError_t le = cudaGetLastError();
-  cudaGraph_t body_out = nullptr;
-  const cudaError_t ee = cudaStreamEndCapture(c->body_stream, &body_out);
-  CK(le);
-  CK(ee);
+  capture_while(
+      c->stream, c->body_stream,
+      [&](cudaGraphConditionalHandle h) { launch_pcg_cond(c->pcg.sc, h, limit, 0, c->stream); },
+      [&](cudaStream_t bs, cudaGraphConditionalHandle h) {
+        if (c->use_fdm) {
+          pcg_iterations_fdm(c->P, c->fdm, c->pcg, chunk, bs);
+          c->launches[INS2D_PROF_POISSON] += (c->fdm.spectral ? 4LL + fft_kernels(c->fdm_fft) : 8LL) * chunk;
+        } else if (c->use_mg) {
+          pcg_iterations_mg(c->P, c->mg, c->pcg, chunk, bs);
+          c->launches[INS2D_PROF_POISSON] += (long long)(4 + 6 * mg_tail_level(c->mg) + 1) * chunk;
+        } else {
+          pcg_iterations(c->P, c->pcg, chunk, bs);
+          c->launches[INS2D_PROF_POISSON] += 3LL * chunk;
+        }
+        launch_pcg_cond(c->pcg.sc, h, limit, 1, bs);
+      });
   pcg_finish(c->P, c->pcg, dp, accumulate, c->stream);
   launch_solve_accum(c->pcg.sc, c->accum, c->stream);
   c->launches[INS2D_PROF_POISSON] += 3;
@@ -1718,6 +1739,17 @@ struct ins2d_ens {
   double tuned_ms[3] = {0.0, 0.0, 0.0};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t chunk_graph = nullptr;  // a chunk of batched PCG iterations
+  // fast-diagonalization preconditioner of the batched solves (every member
+  // at most kFdmMaxN cells per direction, default or fdm preconditioner)
+  bool use_fdm = false;
+  // batched solves inside a step graph: the iteration loop is a WHILE node
+  bool dev_loop = false;
+  cudaStream_t body_stream = nullptr;
+  int *d_loops = nullptr;
+  EnsFdmD *d_fdm = nullptr;
+  std::vector<double *> fdm_z;
+  int4 *d_ftiles = nullptr;
+  int n_ftiles = 0;
 };
 
 namespace {
@@ -1822,6 +1854,13 @@ void ens_build_batch(ins2d_ens *e, const std::vector<int> &order) {
   e->d_ctiles = ens_alloc<int2>(e, ct.size());
   CK(cudaMemcpy(e->d_ctiles, ct.data(), ct.size() * sizeof(int2), cudaMemcpyHostToDevice));
   e->n_ctiles = (int)ct.size();
+  if (e->use_fdm) {
+    std::vector<int4> ft;
+    for (int m : order) fdm_tiles(m, e->mem[m]->P.Npx, e->mem[m]->P.Npy, ft);
+    e->d_ftiles = ens_alloc<int4>(e, ft.size());
+    CK(cudaMemcpy(e->d_ftiles, ft.data(), ft.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    e->n_ftiles = (int)ft.size();
+  }
   std::vector<EnsCg> cg(n);
   for (int m = 0; m < n; ++m) {
     cg[m] = EnsCg{};
@@ -1841,24 +1880,47 @@ void ens_solve_batched(ins2d_ens *e, int which) {
   const MgD &M0 = e->mem[0]->mg;
   const double om = M0.omega, al = M0.alpha;
   cudaStream_t s = e->stream;
+  // the preconditioner: fast diagonalization (four products over all
+  // members' tiles) or the members' V-cycles
+  auto precond_on = [&](cudaStream_t st) {
+    if (e->use_fdm)
+      fdm_apply_ens(e->d_fdm, e->d_ftiles, e->n_ftiles, e->d_cg, st);
+    else
+      ens_vcycle(e->d_mem, e->mgd, e->d_cg, e->plan, om, al, st);
+  };
+  auto precond = [&]() { precond_on(s); };
   ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 0, s);
   ens_cg_scalar(e->d_cg, n, 0, nullptr, s);
-  ens_vcycle(e->d_mem, e->mgd, e->d_cg, e->plan, om, al, s);
+  precond();
   ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 4, s);
   ens_cg_scalar(e->d_cg, n, 1, nullptr, s);
-  const int chunk = 4;
-  auto iterations = [&]() {
+  const int chunk = e->use_fdm ? (e->dev_loop ? 1 : 2) : 4;
+  auto iterations_on = [&](cudaStream_t st) {
     for (int k = 0; k < chunk; ++k) {
-      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 1, s);
-      ens_cg_scalar(e->d_cg, n, 2, nullptr, s);
-      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 2, s);
-      ens_cg_scalar(e->d_cg, n, 3, e->d_active, s);
-      ens_vcycle(e->d_mem, e->mgd, e->d_cg, e->plan, om, al, s);
-      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 3, s);
-      ens_cg_scalar(e->d_cg, n, 4, nullptr, s);
-      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 5, s);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 1, st);
+      ens_cg_scalar(e->d_cg, n, 2, nullptr, st);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 2, st);
+      ens_cg_scalar(e->d_cg, n, 3, e->d_active, st);
+      precond_on(st);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 3, st);
+      ens_cg_scalar(e->d_cg, n, 4, nullptr, st);
+      ens_cg_vec(e->d_mem, e->mgd, e->d_ctiles, e->n_ctiles, e->d_cg, 5, st);
     }
   };
+  auto iterations = [&]() { iterations_on(s); };
+  if (e->dev_loop) {
+    // inside a step graph: the loop is a WHILE node that ends when no member
+    // iterates or after CG_maxit / chunk + 4 passes
+    const int limit = (int)std::min<long long>(e->maxit / chunk + 4, 1 << 30);
+    capture_while(
+        s, e->body_stream, [&](cudaGraphConditionalHandle h) { ens_loop_cond(e->d_cg, n, e->d_loops, limit, 0, h, s); },
+        [&](cudaStream_t bs, cudaGraphConditionalHandle h) {
+          iterations_on(bs);
+          ens_loop_cond(e->d_cg, n, e->d_loops, limit, 1, h, bs);
+        });
+    ens_cg_finish(e->d_mem, e->d_ctiles, e->n_ctiles, e->d_cg, n, which, e->d_stats, s);
+    return;
+  }
   // the chunk of iterations is one CUDA graph (its launches depend only on
   // the ensemble's device tables), replayed until no member iterates
   if (!e->chunk_graph) {
@@ -1901,6 +1963,7 @@ void ens_upload(ins2d_ens *e, double dt) {
     d.wres = c->wres;
     d.W = c->pcg;
     d.mg = c->use_mg ? e->d_mg[m] : nullptr;
+    d.zf = e->use_fdm ? e->fdm_z[m] : nullptr;
     walk_tiles(c->P, m, fast, gen);
     cell_tiles(c->P, m, cells);
   }
@@ -1988,8 +2051,9 @@ void ens_step(ins2d_ens *e, bool k0_cached) {
 // reductions) and keeps the fastest.
 void ens_autotune(ins2d_ens *e) {
   const int sms = sm_count(e->device), n = (int)e->mem.size();
-  const int cand[3] = {512, 256, 0};  // 0: batched across members
-  const int ncand = e->can_batch ? 3 : 2;
+  // 0: batched across members; fast-diagonalization ensembles solve batched
+  const int cand[3] = {e->use_fdm ? 0 : 512, 256, 0};
+  const int ncand = e->use_fdm ? 1 : (e->can_batch ? 3 : 2);
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -2104,7 +2168,42 @@ int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_des
       }
       e->can_batch = true;
       for (ins2d_ctx *c : e->mem) e->can_batch = e->can_batch && c->use_mg;
+      // fast diagonalization for the batched solves when every member takes
+      // the default (or fdm) preconditioner and is small enough for dense bases
+      bool fdm = e->can_batch;
+      for (int m = 0; m < n && fdm; ++m) {
+        const ins2d_ctx *c = e->mem[m];
+        fdm = (opts[m].precond == INS2D_PRECOND_DEFAULT || opts[m].precond == INS2D_PRECOND_FDM) &&
+              std::max(c->H.Npx, c->H.Npy) <= kFdmMaxN;
+      }
+      if (fdm) {
+        std::vector<EnsFdmD> hf(n);
+        for (int m = 0; m < n; ++m) {
+          ins2d_ctx *c = e->mem[m];
+          const HostOps &H = c->H;
+          const FdmHost1D fx = fdm_1d(H.TX, H.hx), fy = fdm_1d(H.TY, H.hy);
+          EnsFdmD &D = hf[m];
+          D.nx = H.Npx;
+          D.ny = H.Npy;
+          D.Qx = upload_vec(c, fx.Q);
+          D.Qy = upload_vec(c, fy.Q);
+          D.lx = upload_vec(c, fx.lam);
+          D.ly = upload_vec(c, fy.lam);
+          D.thr = 1e-12 * (fx.lam.back() + fy.lam.back());
+          D.r = c->pcg.r;
+          const size_t Np = (size_t)c->P.Np;
+          D.t1 = dalloc<double>(c, Np);
+          D.t2 = dalloc<double>(c, Np);
+          D.z = dalloc<double>(c, Np);
+          e->fdm_z.push_back(D.z);
+        }
+        e->d_fdm = ens_alloc<EnsFdmD>(e, n);
+        CK(cudaMemcpy(e->d_fdm, hf.data(), n * sizeof(EnsFdmD), cudaMemcpyHostToDevice));
+        e->use_fdm = true;
+      }
       CK(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking));
+      CK(cudaStreamCreateWithFlags(&e->body_stream, cudaStreamNonBlocking));
+      e->d_loops = ens_alloc<int>(e, 1);
       e->stream = e->own_stream;
       CK(cudaDeviceSynchronize());
     } catch (const CudaError &x) {
@@ -2134,6 +2233,7 @@ int ins2d_ens_destroy(ins2d_ens *e) {
   for (void *p : e->allocs) cudaFree(p);
   for (ins2d_ctx *c : e->mem) ins2d_ctx_destroy(c);
   if (e->own_stream) cudaStreamDestroy(e->own_stream);
+  if (e->body_stream) cudaStreamDestroy(e->body_stream);
   delete e;
   return INS2D_OK;
 }
@@ -2219,8 +2319,8 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
       // right-hand side it left behind (re-solving it changes no state: the
       // tuner writes dp, which every stage overwrites); the step's
       // statistics are kept
-      e->solve_threads = 512;
-      e->solve_blocks = std::min(n, sm_count(e->device));
+      e->solve_threads = e->use_fdm ? 0 : 512;
+      e->solve_blocks = e->use_fdm ? 0 : std::min(n, sm_count(e->device));
       ens_step(e, g == 1);
       std::vector<EnsStats> keep(n);
       CK(cudaMemcpyAsync(keep.data(), e->d_stats, n * sizeof(EnsStats), cudaMemcpyDeviceToHost, e->stream));
@@ -2231,18 +2331,20 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
       CK(cudaStreamSynchronize(e->stream));
       continue;
     }
-    if (e->solve_threads == 0) {  // batched solves poll the host: no graph
-      ens_step(e, g == 1);
-      continue;
-    }
     if (!e->graph[g]) {
-      if (e->graph[g]) {
-        cudaGraphExecDestroy(e->graph[g]);
-        e->graph[g] = nullptr;
-      }
+      // batched solves: their iteration loops become WHILE nodes of the graph
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
-      ens_step(e, g == 1);
+      e->dev_loop = e->solve_threads == 0;
+      try {
+        ens_step(e, g == 1);
+      } catch (...) {
+        e->dev_loop = false;
+        cudaGraph_t junk = nullptr;
+        if (cudaStreamEndCapture(e->stream, &junk) == cudaSuccess && junk) cudaGraphDestroy(junk);
+        throw;
+      }
+      e->dev_loop = false;
       CK(cudaStreamEndCapture(e->stream, &gr));
       cudaError_t ie = cudaGraphInstantiate(&e->graph[g], gr, 0);
       cudaGraphDestroy(gr);
@@ -2275,6 +2377,8 @@ int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_s
 int ins2d_ens_set_solver(ins2d_ens *e, int32_t threads) {
   if (!e || !(threads == -1 || threads == 0 || threads == 256 || threads == 512)) return INS2D_EINVAL;
   if (threads == 0 && !e->can_batch) return ens_fail(e, INS2D_EINVAL, "batched solves need the multigrid preconditioner");
+  if (threads > 0 && e->use_fdm)
+    return ens_fail(e, INS2D_EINVAL, "fast-diagonalization ensembles solve batched (threads 0 or -1)");
   e->forced = threads;
   if (threads >= 0) {
     e->solve_threads = threads;

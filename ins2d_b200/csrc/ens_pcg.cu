@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kTile) k_ecg_vec(const EnsMemberD *__restrict_
   const long long k = (long long)t.y + threadIdx.x;
   const bool in = k < E.P.Np;
   const PcgWork &W = E.W;
-  const double *z = mg_res(G, m, 0);
+  const double *z = E.zf ? E.zf : mg_res(G, m, 0);
   double a = 0.0, b = 0.0;
   if (op == 1) {  // q = A p, p'q
     for (int w = threadIdx.x; w < (int)(sizeof(DevOps) / 8); w += blockDim.x)
@@ -205,6 +205,25 @@ __global__ void k_ecg_scalar(EnsCg *__restrict__ cg, int n, int op, int *active)
   if (mine) atomicAdd(&cnt, mine);
   __syncthreads();
   if (threadIdx.x == 0 && active) *active = cnt;
+}
+
+// WHILE condition of the graph form of the batched solve: some member still
+// iterating and fewer than `limit` passes (count: this launch ends a pass;
+// the first launch resets the pass count)
+__global__ void k_ecg_loop_cond(const EnsCg *__restrict__ cg, int n, int *loops, int limit, int count,
+                                cudaGraphConditionalHandle h) {
+  __shared__ int act;
+  if (threadIdx.x == 0) act = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int m = threadIdx.x; m < n; m += blockDim.x) mine += cg[m].done ? 0 : 1;
+  if (mine) atomicAdd(&act, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int k = count ? *loops + 1 : 0;
+    *loops = k;
+    cudaGraphSetConditional(h, (act > 0 && k < limit) ? 1u : 0u);
+  }
 }
 
 // dst = x (which = 0: dp) or dst += x (which = 1: p); statistics
@@ -384,6 +403,10 @@ void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const E
 void ens_cg_vec(const EnsMemberD *mem, const EnsMgD &G, const int2 *tiles, int ntiles, EnsCg *cg, int op,
                 cudaStream_t s) {
   if (ntiles > 0) k_ecg_vec<<<ntiles, kTile, 0, s>>>(mem, G, tiles, cg, op);
+}
+void ens_loop_cond(const EnsCg *cg, int n, int *loops, int limit, int count, cudaGraphConditionalHandle h,
+                   cudaStream_t s) {
+  k_ecg_loop_cond<<<1, 256, 0, s>>>(cg, n, loops, limit, count, h);
 }
 void ens_cg_scalar(EnsCg *cg, int n, int op, int *active, cudaStream_t s) {
   k_ecg_scalar<<<1, 256, 0, s>>>(cg, n, op, active);

@@ -22,73 +22,85 @@ constexpr int kBM = 64, kBN = 64, kBK = 16, kGemmThreads = 256;
 // TA: A stored K x M (element (m,k) at A[k*lda + m]); else A[m*lda + k].
 // TB: B stored N x K (element (k,n) at B[n*ldb + k]); else B[k*ldb + n].
 // SCALE: C(b, a) *= -1/(lx[a] + ly[b]), 0 where lx[a] + ly[b] <= thr.
+// one kBM x kBN tile (rows m0.., columns n0..) of C by a block of kGemmThreads.
+// Thread (ty, tx) of 16 x 16 owns rows {2ty, 2ty+1, 32+2ty, 33+2ty} and the
+// same columns with tx, so its operands of one k are two 16-byte shared
+// loads each (conflict-free); the next k-slab's global loads are issued into
+// registers before the current slab's products (INS2D_FDM_PREFETCH).
+#ifndef INS2D_FDM_PREFETCH
+#define INS2D_FDM_PREFETCH 1
+#endif
 template <bool TA, bool TB, bool SCALE>
-__global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, const double *__restrict__ A, int lda,
-                                                       const double *__restrict__ B, int ldb, double *__restrict__ C,
-                                                       int ldc, const double *__restrict__ lx,
-                                                       const double *__restrict__ ly, double thr,
-                                                       const int *__restrict__ done) {
-  if (done && *(volatile const int *)done) return;
-  __shared__ double As[kBK][kBM];
-  __shared__ double Bs[kBK][kBN];
+__device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__restrict__ A, int lda,
+                                          const double *__restrict__ B, int ldb, double *__restrict__ C, int ldc,
+                                          const double *__restrict__ lx, const double *__restrict__ ly, double thr,
+                                          int m0, int n0) {
+  __shared__ __align__(16) double As[kBK][kBM];
+  __shared__ __align__(16) double Bs[kBK][kBN];
+  constexpr int QA = (kBM * kBK) / kGemmThreads, QB = (kBN * kBK) / kGemmThreads;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-  double acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += kBK) {
+  // global -> registers of the k-slab starting at k0
+  auto load = [&](int k0, double (&ra)[QA], double (&rb)[QB]) {
 #pragma unroll
-    for (int q = 0; q < (kBM * kBK) / kGemmThreads; ++q) {
+    for (int q = 0; q < QA; ++q) {
       const int e = tid + kGemmThreads * q;
-      int m, k;
-      if (TA) {
-        k = e / kBM;
-        m = e - k * kBM;
-      } else {
-        m = e / kBK;
-        k = e - m * kBK;
-      }
+      const int m = TA ? e % kBM : e / kBK, k = TA ? e / kBM : e % kBK;
       const int gm = m0 + m, gk = k0 + k;
-      double a = 0.0;
-      if (gm < M && gk < K) a = TA ? __ldg(A + (size_t)gk * lda + gm) : __ldg(A + (size_t)gm * lda + gk);
-      As[k][m] = a;
+      ra[q] = (gm < M && gk < K) ? (TA ? __ldg(A + (size_t)gk * lda + gm) : __ldg(A + (size_t)gm * lda + gk)) : 0.0;
     }
 #pragma unroll
-    for (int q = 0; q < (kBN * kBK) / kGemmThreads; ++q) {
+    for (int q = 0; q < QB; ++q) {
       const int e = tid + kGemmThreads * q;
-      int n, k;
-      if (TB) {
-        n = e / kBK;
-        k = e - n * kBK;
-      } else {
-        k = e / kBN;
-        n = e - k * kBN;
-      }
+      const int n = TB ? e / kBK : e % kBN, k = TB ? e % kBK : e / kBN;
       const int gn = n0 + n, gk = k0 + k;
-      double b = 0.0;
-      if (gn < N && gk < K) b = TB ? __ldg(B + (size_t)gn * ldb + gk) : __ldg(B + (size_t)gk * ldb + gn);
-      Bs[k][n] = b;
+      rb[q] = (gn < N && gk < K) ? (TB ? __ldg(B + (size_t)gn * ldb + gk) : __ldg(B + (size_t)gk * ldb + gn)) : 0.0;
     }
+  };
+  auto store = [&](const double (&ra)[QA], const double (&rb)[QB]) {
+#pragma unroll
+    for (int q = 0; q < QA; ++q) {
+      const int e = tid + kGemmThreads * q;
+      As[TA ? e / kBM : e % kBK][TA ? e % kBM : e / kBK] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < QB; ++q) {
+      const int e = tid + kGemmThreads * q;
+      Bs[TB ? e % kBK : e / kBN][TB ? e / kBK : e % kBN] = rb[q];
+    }
+  };
+  double acc[4][4] = {};
+  double ra[QA], rb[QB];
+  load(0, ra, rb);
+  for (int k0 = 0; k0 < K; k0 += kBK) {
+    store(ra, rb);
     __syncthreads();
+#if INS2D_FDM_PREFETCH
+    if (k0 + kBK < K) load(k0 + kBK, ra, rb);
+#endif
 #pragma unroll
     for (int k = 0; k < kBK; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = As[k][ty + 16 * r];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = Bs[k][tx + 16 * c];
+      const double2 a0 = *reinterpret_cast<const double2 *>(&As[k][2 * ty]);
+      const double2 a1 = *reinterpret_cast<const double2 *>(&As[k][32 + 2 * ty]);
+      const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[k][2 * tx]);
+      const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[k][32 + 2 * tx]);
+      const double a[4] = {a0.x, a0.y, a1.x, a1.y}, b[4] = {b0.x, b0.y, b1.x, b1.y};
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
     }
     __syncthreads();
+#if !INS2D_FDM_PREFETCH
+    if (k0 + kBK < K) load(k0 + kBK, ra, rb);
+#endif
   }
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    const int gm = m0 + ty + 16 * r;
+    const int gm = m0 + (r >> 1) * 32 + 2 * ty + (r & 1);
     if (gm >= M) continue;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const int gn = n0 + tx + 16 * c;
+      const int gn = n0 + (c >> 1) * 32 + 2 * tx + (c & 1);
       if (gn >= N) continue;
       double v = acc[r][c];
       if (SCALE) {
@@ -101,6 +113,39 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, cons
 }
 
 template <bool TA, bool TB, bool SCALE>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, const double *__restrict__ A, int lda,
+                                                       const double *__restrict__ B, int ldb, double *__restrict__ C,
+                                                       int ldc, const double *__restrict__ lx,
+                                                       const double *__restrict__ ly, double thr,
+                                                       const int *__restrict__ done) {
+  if (done && *(volatile const int *)done) return;
+  gemm_tile<TA, TB, SCALE>(M, N, K, A, lda, B, ldb, C, ldc, lx, ly, thr, blockIdx.y * kBM, blockIdx.x * kBN);
+}
+
+// The four products of fdm_apply for many members in one launch per product:
+// work items {member, tile row, tile column}; members whose CG has converged
+// (cg[m].done) skip their tiles.  OP 0: T1 = R Qx; 1: T2 = -(Qy' T1) ./ lam;
+// 2: T1 = Qy T2; 3: Z = T1 Qx'.
+template <int OP>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_ens(const EnsFdmD *__restrict__ F,
+                                                           const int4 *__restrict__ tiles,
+                                                           const EnsCg *__restrict__ cg) {
+  const int4 t = tiles[blockIdx.x];
+  const int m = t.x;
+  if (*(volatile const int *)&cg[m].done) return;
+  const EnsFdmD &D = F[m];
+  const int nx = D.nx, ny = D.ny, m0 = t.y * kBM, n0 = t.z * kBN;
+  if (OP == 0)
+    gemm_tile<false, false, false>(ny, nx, nx, D.r, nx, D.Qx, nx, D.t1, nx, D.lx, D.ly, D.thr, m0, n0);
+  else if (OP == 1)
+    gemm_tile<true, false, true>(ny, nx, ny, D.Qy, ny, D.t1, nx, D.t2, nx, D.lx, D.ly, D.thr, m0, n0);
+  else if (OP == 2)
+    gemm_tile<false, false, false>(ny, nx, ny, D.Qy, ny, D.t2, nx, D.t1, nx, D.lx, D.ly, D.thr, m0, n0);
+  else
+    gemm_tile<false, true, false>(ny, nx, nx, D.t1, nx, D.Qx, nx, D.z, nx, D.lx, D.ly, D.thr, m0, n0);
+}
+
+template <bool TA, bool TB, bool SCALE>
 void gemm(int M, int N, int K, const double *A, int lda, const double *B, int ldb, double *C, int ldc,
           const FdmD &F, const int *done, cudaStream_t s) {
   const dim3 g((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
@@ -108,6 +153,19 @@ void gemm(int M, int N, int K, const double *A, int lda, const double *B, int ld
 }
 
 }  // namespace
+
+void fdm_tiles(int member, int nx, int ny, std::vector<int4> &out) {
+  for (int bm = 0; bm < (ny + kBM - 1) / kBM; ++bm)
+    for (int bn = 0; bn < (nx + kBN - 1) / kBN; ++bn) out.push_back(make_int4(member, bm, bn, 0));
+}
+
+void fdm_apply_ens(const EnsFdmD *F, const int4 *tiles, int ntiles, const EnsCg *cg, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  k_gemm_ens<0><<<ntiles, kGemmThreads, 0, s>>>(F, tiles, cg);
+  k_gemm_ens<1><<<ntiles, kGemmThreads, 0, s>>>(F, tiles, cg);
+  k_gemm_ens<2><<<ntiles, kGemmThreads, 0, s>>>(F, tiles, cg);
+  k_gemm_ens<3><<<ntiles, kGemmThreads, 0, s>>>(F, tiles, cg);
+}
 
 void fdm_apply(const FdmD &F, const double *r, double *z, const int *done, cudaStream_t s) {
   const int nx = F.nx, ny = F.ny;

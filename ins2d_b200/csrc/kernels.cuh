@@ -198,6 +198,21 @@ struct FdmD {
 };
 // z = A^+ r (four dense products); no work once *done is set (done may be null)
 void fdm_apply(const FdmD &F, const double *r, double *z, const int *done, cudaStream_t s);
+// one ensemble member's fast-diagonalization data (device copy): z = A^+ r
+struct EnsFdmD {
+  int nx, ny;
+  const double *Qx, *Qy, *lx, *ly;
+  double thr;
+  const double *r;  // the member's CG residual
+  double *t1, *t2, *z;
+};
+struct EnsCg;
+// Host: the 64x64 output tiles {member, tile row, tile column, 0} of a member
+// with an ny x nx pressure grid
+void fdm_tiles(int member, int nx, int ny, std::vector<int4> &out);
+// z = A^+ r for every member not yet converged (cg[m].done == 0): the four
+// products, one launch each over all members' tiles
+void fdm_apply_ens(const EnsFdmD *F, const int4 *tiles, int ntiles, const EnsCg *cg, cudaStream_t s);
 
 // --- PCG (pcg.cu) ---------------------------------------------------------------
 struct PcgScalars {
@@ -249,6 +264,7 @@ struct EnsMemberD {
   double *V, *p, *Vs, *Wt, *kV[kMaxStages], *f, *dp, *wres;
   PcgWork W;
   const MgD *mg;  // device copy of the member's hierarchy, or null (Jacobi)
+  const double *zf;  // batched solves with fast diagonalization: the preconditioned residual
 };
 // per-member solve statistics, accumulated over a run
 struct EnsStats {
@@ -299,6 +315,10 @@ void ens_vcycle(const EnsMemberD *mem, const EnsMgD &G, const EnsCg *cg, const E
 void ens_cg_vec(const EnsMemberD *mem, const EnsMgD &G, const int2 *tiles, int ntiles, EnsCg *cg, int op,
                 cudaStream_t s);
 // op 0 after init, 1 first r'z, 2 alpha, 3 convergence, 4 beta; *active = members still iterating
+// WHILE condition of the batched solve's graph form (some member iterating,
+// fewer than limit passes; count 0 resets the pass counter *loops)
+void ens_loop_cond(const EnsCg *cg, int n, int *loops, int limit, int count, cudaGraphConditionalHandle h,
+                   cudaStream_t s);
 void ens_cg_scalar(EnsCg *cg, int n, int op, int *active, cudaStream_t s);
 void ens_cg_finish(const EnsMemberD *mem, const int2 *tiles, int ntiles, EnsCg *cg, int n, int which,
                    EnsStats *stats, cudaStream_t s);

@@ -14,12 +14,15 @@ from . import cases
 
 
 def random_members(n, seed=4, sizes=(64, 96, 128, 192, 256), stretch=1.05, Re_range=(100.0, 5000.0),
-                   U_range=(0.5, 1.5), CG_acc=1e-10, CG_maxit=20000, RK="RK44", precision="fp64"):
+                   U_range=(0.5, 1.5), CG_acc=1e-10, CG_maxit=20000, RK="RK44", precision="fp64",
+                   precond="default"):
     """Cavity and channel flows on tanh-stretched grids with nx, ny drawn from
     ``sizes``, Re and the lid / inflow velocity drawn uniformly (seeded):
     the batching configuration of the benchmark.  Even members are lid-driven
     cavities on [0,1]^2, odd members channels on [0,4] x [-0.5,0.5] with a
-    parabolic inflow and an outflow at p = 0."""
+    parabolic inflow and an outflow at p = 0.  ``precond``: the members'
+    PCG preconditioner ('default': fast diagonalization in the batched
+    ensemble solves, the same as single contexts of these sizes; 'mg')."""
     rng = np.random.default_rng(seed)
     out = []
     for m in range(n):
@@ -35,9 +38,7 @@ def random_members(n, seed=4, sizes=(64, 96, 128, 192, 256), stretch=1.05, Re_ra
             y = cases.tanh_grid(ny, -0.5, 0.5, stretch)
             kw = dict(x=x, y=y, BC=cases.BC_CHANNEL, Re=Re,
                       uBC=cases.channel_uBC(lambda yy, U=U: U * (1.0 - 4.0 * np.asarray(yy) ** 2)))
-        # multigrid-preconditioned PCG: the preconditioner of ensemble
-        # members, so single contexts built from these settings match them
-        kw.update(poisson=4, CG_acc=CG_acc, CG_maxit=CG_maxit, RK=RK, precision=precision, precond="mg")
+        kw.update(poisson=4, CG_acc=CG_acc, CG_maxit=CG_maxit, RK=RK, precision=precision, precond=precond)
         kw["_U"] = U
         out.append(kw)
     return out

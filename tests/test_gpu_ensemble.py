@@ -10,7 +10,7 @@ from ins2d_b200 import cases
 pytestmark = pytest.mark.gpu
 
 
-def _members(seed, n, sizes, stretch=1.05):
+def _members(seed, n, sizes, stretch=1.05, precond="default"):
     rng = np.random.default_rng(seed)
     out = []
     for m in range(n):
@@ -26,20 +26,22 @@ def _members(seed, n, sizes, stretch=1.05):
             y = cases.tanh_grid(ny, -0.5, 0.5, stretch)
             out.append(dict(x=x, y=y, BC=cases.BC_CHANNEL, Re=Re,
                             uBC=cases.channel_uBC(lambda yy, U=U: U * (1 - 4 * np.asarray(yy) ** 2))))
-    # members solve with the multigrid preconditioner; the single contexts
-    # they are compared with use the same one
+    # the single contexts the members are compared with take the same
+    # preconditioner setting (default: fast diagonalization; mg: multigrid)
     for kw in out:
-        kw.update(poisson=4, CG_acc=1e-12, CG_maxit=20000, RK="RK44", precond="mg")
+        kw.update(poisson=4, CG_acc=1e-12, CG_maxit=20000, RK="RK44", precond=precond)
     return out
 
 
 @pytest.mark.parametrize("seed,n,sizes", [(4, 6, [24, 32, 40, 64]), (5, 9, [16, 48, 96, 130])])
-@pytest.mark.parametrize("solver", [-1, 0, 512])
-def test_ensemble_matches_single_runs(seed, n, sizes, solver):
+@pytest.mark.parametrize("solver,precond", [(-1, "default"), (0, "default"), (-1, "mg"), (0, "mg"), (512, "mg")])
+def test_ensemble_matches_single_runs(seed, n, sizes, solver, precond):
     """solver -1: tuned form; 0: solves batched across members; 512:
-    persistent member solve."""
+    persistent member solve.  precond default: the batched solves with fast
+    diagonalization (four products over all members' tiles per application);
+    mg: the members' V-cycles."""
     import ins2d_b200
-    members = _members(seed, n, sizes)
+    members = _members(seed, n, sizes, precond=precond)
     ens = ins2d_b200.Ensemble(members)
     ens.set_solver(solver)
     singles, states = [], []
@@ -63,9 +65,22 @@ def test_ensemble_matches_single_runs(seed, n, sizes, solver):
         assert np.max(np.abs(Ve - V)) <= 1e-10 * scale, m
         assert np.max(np.abs(pe - p)) <= 1e-8 * max(np.max(np.abs(p)), 1e-30), m
         assert stats[m]["n_solves"] == 4 * nsteps  # 3 stage solves + 1 additional per RK4 step
-        assert stats[m]["iters_max"] <= 60
+        assert stats[m]["iters_max"] <= (4 if precond == "default" else 60)
         # the member context still serves the single-flow API on the ensemble's state
         assert ens.member(m).check_conservation(Ve, nsteps * dt)[0] < 1e-10
+
+
+def test_ensemble_fdm_solves_batched():
+    """An ensemble with the fast-diagonalization preconditioner refuses the
+    persistent per-member solve form (its V-cycle is not the same
+    preconditioner) and keeps the batched form."""
+    import ins2d_b200
+    ens = ins2d_b200.Ensemble(_members(2, 3, [24, 32]))
+    with pytest.raises(ins2d_b200.Ins2dError) as ei:
+        ens.set_solver(512)
+    assert ei.value.status == 1
+    ens.set_solver(0)
+    ens.close()
 
 
 def test_ensemble_rejects_unsupported_members():
