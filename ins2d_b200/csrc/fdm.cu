@@ -9,7 +9,9 @@
 // a singular A (closed or periodic domains) is left out.  Applied exactly this
 // is the inverse on the range of A, so the PCG -- which keeps cg.F's control
 // flow and stopping rule -- converges in one or two iterations.  Four dense
-// products per application, run by a tiled FP64 GEMM (CUDA cores).
+// products per application, run by a tiled FP64 GEMM on the FP64 tensor cores
+// (mma.sync m8n8k4 .f64; a CUDA-core form of the same tile stays available
+// with INS2D_FDM_DMMA=0).
 #include "kernels.cuh"
 
 namespace ins2d {
@@ -112,6 +114,98 @@ __device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__r
   }
 }
 
+// The same tile on the FP64 tensor cores (INS2D_FDM_DMMA): mma.sync
+// m8n8k4 .f64, each warp a 32 x 16 block of C (4 x 2 fragments of 8 x 8).
+// Fragment layout of m8n8k4 .f64 (group g = lane / 4, t = lane % 4): A holds
+// (row g, col t), B (row t, col g), C/D (row g, cols 2t, 2t+1).  The operand
+// slabs are staged with padded rows (kBM + 4) so a warp's fragment loads hit
+// distinct banks.
+#ifndef INS2D_FDM_DMMA
+#define INS2D_FDM_DMMA 1
+#endif
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+template <bool TA, bool TB, bool SCALE>
+__device__ __forceinline__ void gemm_tile_tc(int M, int N, int K, const double *__restrict__ A, int lda,
+                                             const double *__restrict__ B, int ldb, double *__restrict__ C, int ldc,
+                                             const double *__restrict__ lx, const double *__restrict__ ly,
+                                             double thr, int m0, int n0) {
+  constexpr int PA = kBM + 4, PB = kBN + 4;
+  __shared__ __align__(16) double As[kBK][PA];
+  __shared__ __align__(16) double Bs[kBK][PB];
+  constexpr int QA = (kBM * kBK) / kGemmThreads, QB = (kBN * kBK) / kGemmThreads;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  double ra[QA], rb[QB];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < QA; ++q) {
+      const int e = tid + kGemmThreads * q;
+      const int m = TA ? e % kBM : e / kBK, k = TA ? e / kBM : e % kBK;
+      const int gm = m0 + m, gk = k0 + k;
+      ra[q] = (gm < M && gk < K) ? (TA ? __ldg(A + (size_t)gk * lda + gm) : __ldg(A + (size_t)gm * lda + gk)) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < QB; ++q) {
+      const int e = tid + kGemmThreads * q;
+      const int n = TB ? e / kBK : e % kBN, k = TB ? e % kBK : e / kBN;
+      const int gn = n0 + n, gk = k0 + k;
+      rb[q] = (gn < N && gk < K) ? (TB ? __ldg(B + (size_t)gn * ldb + gk) : __ldg(B + (size_t)gk * ldb + gn)) : 0.0;
+    }
+  };
+  double acc[4][2][2] = {};
+  load(0);
+  for (int k0 = 0; k0 < K; k0 += kBK) {
+#pragma unroll
+    for (int q = 0; q < QA; ++q) {
+      const int e = tid + kGemmThreads * q;
+      As[TA ? e / kBM : e % kBK][TA ? e % kBM : e / kBK] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < QB; ++q) {
+      const int e = tid + kGemmThreads * q;
+      Bs[TB ? e % kBK : e / kBN][TB ? e / kBK : e % kBN] = rb[q];
+    }
+    __syncthreads();
+    if (k0 + kBK < K) load(k0 + kBK);
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 4) {
+      double a[4], b[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk + t][wm + 8 * i + g];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) b[j] = Bs[kk + t][wn + 8 * j + g];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + wm + 8 * i + g;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gn = n0 + wn + 8 * j + 2 * t + h;
+        if (gn >= N) continue;
+        double v = acc[i][j][h];
+        if (SCALE) {
+          const double lam = __ldg(lx + gn) + __ldg(ly + gm);
+          v = lam > thr ? -v / lam : 0.0;
+        }
+        C[(size_t)gm * ldc + gn] = v;
+      }
+  }
+}
+
 template <bool TA, bool TB, bool SCALE>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, const double *__restrict__ A, int lda,
                                                        const double *__restrict__ B, int ldb, double *__restrict__ C,
@@ -119,13 +213,22 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, cons
                                                        const double *__restrict__ ly, double thr,
                                                        const int *__restrict__ done) {
   if (done && *(volatile const int *)done) return;
+#if INS2D_FDM_DMMA
+  gemm_tile_tc<TA, TB, SCALE>(M, N, K, A, lda, B, ldb, C, ldc, lx, ly, thr, blockIdx.y * kBM, blockIdx.x * kBN);
+#else
   gemm_tile<TA, TB, SCALE>(M, N, K, A, lda, B, ldb, C, ldc, lx, ly, thr, blockIdx.y * kBM, blockIdx.x * kBN);
+#endif
 }
 
 // The four products of fdm_apply for many members in one launch per product:
 // work items {member, tile row, tile column}; members whose CG has converged
 // (cg[m].done) skip their tiles.  OP 0: T1 = R Qx; 1: T2 = -(Qy' T1) ./ lam;
 // 2: T1 = Qy T2; 3: Z = T1 Qx'.
+#if INS2D_FDM_DMMA
+#define GEMM_TILE gemm_tile_tc
+#else
+#define GEMM_TILE gemm_tile
+#endif
 template <int OP>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_ens(const EnsFdmD *__restrict__ F,
                                                            const int4 *__restrict__ tiles,
@@ -136,13 +239,13 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_ens(const EnsFdmD *__rest
   const EnsFdmD &D = F[m];
   const int nx = D.nx, ny = D.ny, m0 = t.y * kBM, n0 = t.z * kBN;
   if (OP == 0)
-    gemm_tile<false, false, false>(ny, nx, nx, D.r, nx, D.Qx, nx, D.t1, nx, D.lx, D.ly, D.thr, m0, n0);
+    GEMM_TILE<false, false, false>(ny, nx, nx, D.r, nx, D.Qx, nx, D.t1, nx, D.lx, D.ly, D.thr, m0, n0);
   else if (OP == 1)
-    gemm_tile<true, false, true>(ny, nx, ny, D.Qy, ny, D.t1, nx, D.t2, nx, D.lx, D.ly, D.thr, m0, n0);
+    GEMM_TILE<true, false, true>(ny, nx, ny, D.Qy, ny, D.t1, nx, D.t2, nx, D.lx, D.ly, D.thr, m0, n0);
   else if (OP == 2)
-    gemm_tile<false, false, false>(ny, nx, ny, D.Qy, ny, D.t2, nx, D.t1, nx, D.lx, D.ly, D.thr, m0, n0);
+    GEMM_TILE<false, false, false>(ny, nx, ny, D.Qy, ny, D.t2, nx, D.t1, nx, D.lx, D.ly, D.thr, m0, n0);
   else
-    gemm_tile<false, true, false>(ny, nx, nx, D.t1, nx, D.Qx, nx, D.z, nx, D.lx, D.ly, D.thr, m0, n0);
+    GEMM_TILE<false, true, false>(ny, nx, nx, D.t1, nx, D.Qx, nx, D.z, nx, D.lx, D.ly, D.thr, m0, n0);
 }
 
 template <bool TA, bool TB, bool SCALE>
