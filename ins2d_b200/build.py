@@ -12,7 +12,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libins2d.so")
 SOURCES = ["setup.cpp", "kernels.cu", "stencil.cu", "fft.cu", "pcg.cu", "mg_host.cpp", "mg.cu", "fdm_host.cpp", "fdm.cu", "ens_pcg.cu", "cnn.cu", "ctx.cu", "noalloc.cu", "slab.cu"]
-HEADERS = ["setup.hpp", "device.cuh", "kernels.cuh", "reduce.cuh", "mg.cuh", "mg_host.hpp", "cnn.cuh", "fdm_host.hpp"]
+HEADERS = ["setup.hpp", "device.cuh", "kernels.cuh", "reduce.cuh", "mg.cuh", "mg_host.hpp", "cnn.cuh", "fdm_host.hpp",
+           "fdm_block.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

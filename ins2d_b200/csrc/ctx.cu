@@ -294,10 +294,13 @@ void capture_while(cudaStream_t s, cudaStream_t body_stream, Pre pre, Body body)
 // added to c->accum, which the host reads after the graph launches (cg.F's
 // errors are reported then).
 int solve_pcg_graph(ins2d_ctx *c, const double *f, double *dp, bool accumulate, double tol) {
-  const bool block = c->use_fdm ? false : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
+  const bool block = c->use_fdm ? pcg_use_block_fdm(c->fdm)
+                                : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
   Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
   if (block) {
-    if (c->use_mg)
+    if (c->use_fdm)
+      pcg_solve_block_fdm(c->P, c->fdm, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
+    else if (c->use_mg)
       pcg_solve_block_mg(c->P, c->mg, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
     else
       pcg_solve_block(c->P, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
@@ -345,10 +348,13 @@ int solve_pcg(ins2d_ctx *c, const double *f, double *dp, bool accumulate, ins2d_
     if (st) *st = ins2d_solve_stats{0, 0.0, 0.0};
     return solve_pcg_graph(c, f, dp, accumulate, tol);
   }
-  const bool block = c->use_fdm ? false : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
+  const bool block = c->use_fdm ? pcg_use_block_fdm(c->fdm)
+                                : (c->use_mg ? (c->P.Np <= kPcgBlockMgMaxCells) : pcg_use_block(c->P));
   Prof pr(c, INS2D_PROF_POISSON, block ? 1 : 2);
   if (block) {
-    if (c->use_mg)
+    if (c->use_fdm)
+      pcg_solve_block_fdm(c->P, c->fdm, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
+    else if (c->use_mg)
       pcg_solve_block_mg(c->P, c->mg, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);
     else
       pcg_solve_block(c->P, c->pcg, f, dp, tol, c->opts.CG_maxit, accumulate, c->stream);

@@ -18,13 +18,13 @@ namespace ins2d {
 
 namespace {
 
-constexpr int kBM = 64, kBN = 64, kBK = 16, kGemmThreads = 256;
+constexpr int kBM = 64, kBN = 64, kBK = 16, kCoreThreads = 256;
 
 // C (M x N, row-major, ldc) = op(A) op(B), op(A) M x K, op(B) K x N.
 // TA: A stored K x M (element (m,k) at A[k*lda + m]); else A[m*lda + k].
 // TB: B stored N x K (element (k,n) at B[n*ldb + k]); else B[k*ldb + n].
 // SCALE: C(b, a) *= -1/(lx[a] + ly[b]), 0 where lx[a] + ly[b] <= thr.
-// one kBM x kBN tile (rows m0.., columns n0..) of C by a block of kGemmThreads.
+// one kBM x kBN tile (rows m0.., columns n0..) of C by a block of kCoreThreads.
 // Thread (ty, tx) of 16 x 16 owns rows {2ty, 2ty+1, 32+2ty, 33+2ty} and the
 // same columns with tx, so its operands of one k are two 16-byte shared
 // loads each (conflict-free); the next k-slab's global loads are issued into
@@ -39,20 +39,20 @@ __device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__r
                                           int m0, int n0) {
   __shared__ __align__(16) double As[kBK][kBM];
   __shared__ __align__(16) double Bs[kBK][kBN];
-  constexpr int QA = (kBM * kBK) / kGemmThreads, QB = (kBN * kBK) / kGemmThreads;
+  constexpr int QA = (kBM * kBK) / kCoreThreads, QB = (kBN * kBK) / kCoreThreads;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   // global -> registers of the k-slab starting at k0
   auto load = [&](int k0, double (&ra)[QA], double (&rb)[QB]) {
 #pragma unroll
     for (int q = 0; q < QA; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kCoreThreads * q;
       const int m = TA ? e % kBM : e / kBK, k = TA ? e / kBM : e % kBK;
       const int gm = m0 + m, gk = k0 + k;
       ra[q] = (gm < M && gk < K) ? (TA ? __ldg(A + (size_t)gk * lda + gm) : __ldg(A + (size_t)gm * lda + gk)) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < QB; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kCoreThreads * q;
       const int n = TB ? e / kBK : e % kBN, k = TB ? e % kBK : e / kBN;
       const int gn = n0 + n, gk = k0 + k;
       rb[q] = (gn < N && gk < K) ? (TB ? __ldg(B + (size_t)gn * ldb + gk) : __ldg(B + (size_t)gk * ldb + gn)) : 0.0;
@@ -61,12 +61,12 @@ __device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__r
   auto store = [&](const double (&ra)[QA], const double (&rb)[QB]) {
 #pragma unroll
     for (int q = 0; q < QA; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kCoreThreads * q;
       As[TA ? e / kBM : e % kBK][TA ? e % kBM : e / kBK] = ra[q];
     }
 #pragma unroll
     for (int q = 0; q < QB; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kCoreThreads * q;
       Bs[TB ? e % kBK : e / kBN][TB ? e / kBK : e % kBN] = rb[q];
     }
   };
@@ -115,7 +115,8 @@ __device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__r
 }
 
 // The same tile on the FP64 tensor cores (INS2D_FDM_DMMA): mma.sync
-// m8n8k4 .f64, each warp a 32 x 16 block of C (4 x 2 fragments of 8 x 8).
+// m8n8k4 .f64, each warp a 32 x kTcWarpN block of C (4 x kTcWarpN/8
+// fragments of 8 x 8; INS2D_FDM_WARP_N 32: four warps per tile, 16: eight).
 // Fragment layout of m8n8k4 .f64 (group g = lane / 4, t = lane % 4): A holds
 // (row g, col t), B (row t, col g), C/D (row g, cols 2t, 2t+1).  The operand
 // slabs are staged with padded rows (kBM + 4) so a warp's fragment loads hit
@@ -123,6 +124,11 @@ __device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__r
 #ifndef INS2D_FDM_DMMA
 #define INS2D_FDM_DMMA 1
 #endif
+#ifndef INS2D_FDM_WARP_N
+#define INS2D_FDM_WARP_N 32
+#endif
+constexpr int kTcWarpN = INS2D_FDM_WARP_N, kTcThreads = 32 * (kBM / 32) * (kBN / kTcWarpN);
+constexpr int kGemmThreads = INS2D_FDM_DMMA ? kTcThreads : kCoreThreads;
 __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                : "+d"(d0), "+d"(d1)
@@ -136,53 +142,54 @@ __device__ __forceinline__ void gemm_tile_tc(int M, int N, int K, const double *
   constexpr int PA = kBM + 4, PB = kBN + 4;
   __shared__ __align__(16) double As[kBK][PA];
   __shared__ __align__(16) double Bs[kBK][PB];
-  constexpr int QA = (kBM * kBK) / kGemmThreads, QB = (kBN * kBK) / kGemmThreads;
+  constexpr int QA = (kBM * kBK) / kTcThreads, QB = (kBN * kBK) / kTcThreads;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  constexpr int NJ = kTcWarpN / 8;  // fragments per warp along n
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * kTcWarpN;
   double ra[QA], rb[QB];
   auto load = [&](int k0) {
 #pragma unroll
     for (int q = 0; q < QA; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kTcThreads * q;
       const int m = TA ? e % kBM : e / kBK, k = TA ? e / kBM : e % kBK;
       const int gm = m0 + m, gk = k0 + k;
       ra[q] = (gm < M && gk < K) ? (TA ? __ldg(A + (size_t)gk * lda + gm) : __ldg(A + (size_t)gm * lda + gk)) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < QB; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kTcThreads * q;
       const int n = TB ? e / kBK : e % kBN, k = TB ? e % kBK : e / kBN;
       const int gn = n0 + n, gk = k0 + k;
       rb[q] = (gn < N && gk < K) ? (TB ? __ldg(B + (size_t)gn * ldb + gk) : __ldg(B + (size_t)gk * ldb + gn)) : 0.0;
     }
   };
-  double acc[4][2][2] = {};
+  double acc[4][NJ][2] = {};
   load(0);
   for (int k0 = 0; k0 < K; k0 += kBK) {
 #pragma unroll
     for (int q = 0; q < QA; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kTcThreads * q;
       As[TA ? e / kBM : e % kBK][TA ? e % kBM : e / kBK] = ra[q];
     }
 #pragma unroll
     for (int q = 0; q < QB; ++q) {
-      const int e = tid + kGemmThreads * q;
+      const int e = tid + kTcThreads * q;
       Bs[TB ? e % kBK : e / kBN][TB ? e / kBK : e % kBN] = rb[q];
     }
     __syncthreads();
     if (k0 + kBK < K) load(k0 + kBK);
 #pragma unroll
     for (int kk = 0; kk < kBK; kk += 4) {
-      double a[4], b[2];
+      double a[4], b[NJ];
 #pragma unroll
       for (int i = 0; i < 4; ++i) a[i] = As[kk + t][wm + 8 * i + g];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) b[j] = Bs[kk + t][wn + 8 * j + g];
+      for (int j = 0; j < NJ; ++j) b[j] = Bs[kk + t][wn + 8 * j + g];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        for (int j = 0; j < NJ; ++j) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
     __syncthreads();
   }
@@ -191,7 +198,7 @@ __device__ __forceinline__ void gemm_tile_tc(int M, int N, int K, const double *
     const int gm = m0 + wm + 8 * i + g;
     if (gm >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < NJ; ++j)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int gn = n0 + wn + 8 * j + 2 * t + h;

@@ -257,6 +257,11 @@ void pcg_iterations_mg(const DevOps &P, const MgD &M, const PcgWork &W, int n, c
 void pcg_init_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double *f, double tol, long long maxit,
                   cudaStream_t s);
 void pcg_iterations_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, int n, cudaStream_t s);
+// small grids (at most 128 cells per direction, not the spectral form): the
+// whole fast-diagonalization PCG solve in one thread block
+bool pcg_use_block_fdm(const FdmD &F);
+void pcg_solve_block_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double *f, double *dp, double tol,
+                         long long maxit, bool accumulate, cudaStream_t s);
 
 struct EnsMemberD {
   DevOps P;

@@ -22,6 +22,7 @@
 #include "ins2d.h"
 #include "kernels.cuh"
 #include "mg.cuh"
+#include "fdm_block.cuh"
 #include "reduce.cuh"
 
 namespace ins2d {
@@ -185,18 +186,27 @@ __device__ void block_reduce(double (&v)[NQ], const int (&ops)[NQ], double (*sh)
   __syncthreads();
 }
 
-// The whole solve by one thread block.  MG = false: Jacobi preconditioner
-// (z = r / diag A); MG = true: one multigrid V-cycle per application
-// (mg.cuh).  Results go to out (the PcgScalars of this solve).
-template <bool MG>
-__device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, const double *__restrict__ f,
-                               double *__restrict__ dp, double tol2, long long maxit, int accumulate,
-                               PcgScalars *out, double (*sh)[5], double *ysh) {
+// The whole solve by one thread block.  PK 0: Jacobi preconditioner
+// (z = r / diag A); 1: one multigrid V-cycle per application (mg.cuh);
+// 2: fast diagonalization (fdm_block.cuh).  Results go to out (the
+// PcgScalars of this solve).
+template <int PK>
+__device__ void pcg_block_body(const DevOps &P, const MgD *M, const FdmD *F, const PcgWork &W,
+                               const double *__restrict__ f, double *__restrict__ dp, double tol2, long long maxit,
+                               int accumulate, PcgScalars *out, double (*sh)[5], double *ysh) {
+  constexpr bool MG = PK != 0;  // a preconditioner with its own z buffer
   const int Npx = P.Npx;
   const long long Np = P.Np;
   const int tid = threadIdx.x, nt = blockDim.x;
   double *__restrict__ x = W.x, *__restrict__ r = W.r, *__restrict__ p = W.p, *__restrict__ q = W.q;
-  const double *z = MG ? mg_result(*M, 0) : nullptr;
+  double *zw = PK == 1 ? mg_result(*M, 0) : (PK == 2 ? F->z : nullptr);
+  const double *z = zw;
+  auto precond = [&]() {
+    if constexpr (PK == 1)
+      mg_vcycle_block(*M, r, 0, ysh);
+    else if constexpr (PK == 2)
+      fdm_apply_block(*F, r, zw);
+  };
   // init (cg.F:207-229 with x_in = 0)
   double a3[3] = {0.0, 0.0, 0.0};
   const int op3[3] = {R_SUM, R_SUM, R_MAX};
@@ -226,7 +236,8 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
   }
   const int op1[1] = {R_SUM};
   if (MG && !done) {
-    mg_vcycle_block(*M, r, 0, ysh);
+    __syncthreads();
+    precond();
     double a1[1] = {0.0};
     for (long long k = tid; k < Np; k += nt) {
       p[k] = z[k];
@@ -293,7 +304,7 @@ __device__ void pcg_block_body(const DevOps &P, const MgD *M, const PcgWork &W, 
     double rz_new = a5[1];
     if (MG) {
       MG_TICK(124);
-      mg_vcycle_block(*M, r, 0, ysh);
+      precond();
       MG_TICK(125);
       double b1[1] = {0.0};
       for (long long k = tid; k < Np; k += nt) b1[0] += r[k] * z[k];
@@ -335,7 +346,7 @@ __global__ void __launch_bounds__(kBlockThreads, 1) k_pcg_block(const __grid_con
                                                                const double *__restrict__ f, double *__restrict__ dp,
                                                                double tol2, long long maxit, int accumulate) {
   __shared__ double sh[kBlockThreads / 32][5];
-  pcg_block_body<false>(P, nullptr, W, f, dp, tol2, maxit, accumulate, W.sc, sh, nullptr);
+  pcg_block_body<0>(P, nullptr, nullptr, W, f, dp, tol2, maxit, accumulate, W.sc, sh, nullptr);
 }
 
 // multigrid variant: 512 threads (the chunked line solves need ~128 registers)
@@ -350,7 +361,18 @@ __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_block_mg(const __gri
                                                                   long long maxit, int accumulate) {
   __shared__ double sh[kBlockThreads / 32][5];
   __shared__ double ysh[2 * kBlockThreadsMg];
-  pcg_block_body<true>(P, &M, W, f, dp, tol2, maxit, accumulate, W.sc, sh, ysh);
+  pcg_block_body<1>(P, &M, nullptr, W, f, dp, tol2, maxit, accumulate, W.sc, sh, ysh);
+}
+
+// fast-diagonalization variant for grids up to kFdmBlockMaxN cells per direction
+constexpr int kBlockThreadsFdm = 512;
+__global__ void __launch_bounds__(kBlockThreadsFdm, 1) k_pcg_block_fdm(const __grid_constant__ DevOps P,
+                                                                    const __grid_constant__ FdmD F, const PcgWork W,
+                                                                    const double *__restrict__ f,
+                                                                    double *__restrict__ dp, double tol2,
+                                                                    long long maxit, int accumulate) {
+  __shared__ double sh[kBlockThreads / 32][5];
+  pcg_block_body<2>(P, nullptr, &F, W, f, dp, tol2, maxit, accumulate, W.sc, sh, nullptr);
 }
 
 // Grid-stride CG kernels of the multigrid path for large grids: the SpMV uses
@@ -477,9 +499,9 @@ __global__ void __launch_bounds__(kBlockThreadsMg, 1) k_pcg_members(const EnsMem
     __syncthreads();
     double *dst = which ? E.p : E.dp;
     if (mg)
-      pcg_block_body<true>(sP, &sM, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh, ysh);
+      pcg_block_body<1>(sP, &sM, nullptr, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh, ysh);
     else
-      pcg_block_body<false>(sP, nullptr, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh, ysh);
+      pcg_block_body<0>(sP, nullptr, nullptr, E.W, E.f, dst, tol2, maxit, which, E.W.sc, sh, ysh);
     __syncthreads();
     if (tid == 0) {
       const PcgScalars &o = *E.W.sc;
@@ -527,6 +549,13 @@ extern "C" int ins2d_debug_mg_clocks(unsigned long long out[128], int reset) {
 void pcg_solve_block_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double *dp, double tol,
                         long long maxit, bool accumulate, cudaStream_t s) {
   k_pcg_block_mg<<<1, kBlockThreadsMg, 0, s>>>(P, M, W, f, dp, tol * tol, maxit, accumulate ? 1 : 0);
+}
+
+bool pcg_use_block_fdm(const FdmD &F) { return !F.spectral && F.nx <= kFdmBlockMaxN && F.ny <= kFdmBlockMaxN; }
+
+void pcg_solve_block_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double *f, double *dp, double tol,
+                         long long maxit, bool accumulate, cudaStream_t s) {
+  k_pcg_block_fdm<<<1, kBlockThreadsFdm, 0, s>>>(P, F, W, f, dp, tol * tol, maxit, accumulate ? 1 : 0);
 }
 
 int pcg_blocks(const DevOps &P) {
