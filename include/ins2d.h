@@ -316,7 +316,13 @@ int ins2d_slab_fft_rows_inverse(ins2d_slab_fft *s, const double *spec, int32_t n
  * ins2d_ens_member); the ensemble owns each member's state V, p.
  * Restrictions: steady boundary conditions, the PCG pressure solver
  * (poisson 1-5), the same device, precision, CG_acc, CG_maxit and RK method
- * for all members, at most 262144 pressure cells per member. */
+ * for all members, at most 262144 pressure cells per member.
+ * Preconditioner: when every member's opts.precond is INS2D_PRECOND_DEFAULT
+ * or INS2D_PRECOND_FDM and every member has at most 1024 pressure cells per
+ * direction, the solves are batched across members with fast
+ * diagonalization; otherwise the members use multigrid (or Jacobi when
+ * asked for) in the form the tuner picks.  Each time step is captured once as
+ * a CUDA graph. */
 typedef struct ins2d_ens ins2d_ens;
 int ins2d_ens_create(int32_t n, const ins2d_grid_desc *grids, const ins2d_bc_desc *bcs,
                      const ins2d_opts *opts, ins2d_ens **out);
@@ -343,7 +349,8 @@ int ins2d_ens_state_ptr(ins2d_ens *e, int32_t m, double **V, double **p);
 int ins2d_ens_erk_run(ins2d_ens *e, double t, double dt, int32_t nsteps, ins2d_step_stats *stats);
 /* form of the member solves: -1 = chosen by the tuner on the first run
  * (default), 0 = batched across members, 256 or 512 = persistent launch with
- * that many threads per member */
+ * that many threads per member (multigrid ensembles only: a
+ * fast-diagonalization ensemble returns INS2D_EINVAL) */
 int ins2d_ens_set_solver(ins2d_ens *e, int32_t threads);
 /* form of the member solves chosen by the tuner on the first run: threads
  * per member of the persistent solve (512 or 256; 0 = solves batched across

@@ -18,7 +18,10 @@ namespace ins2d {
 
 namespace {
 
-constexpr int kBM = 64, kBN = 64, kBK = 16, kCoreThreads = 256;
+#ifndef INS2D_FDM_BM
+#define INS2D_FDM_BM 64
+#endif
+constexpr int kBM = INS2D_FDM_BM, kBN = 64, kBK = 16, kCoreThreads = 256;
 
 // C (M x N, row-major, ldc) = op(A) op(B), op(A) M x K, op(B) K x N.
 // TA: A stored K x M (element (m,k) at A[k*lda + m]); else A[m*lda + k].
@@ -128,6 +131,7 @@ __device__ __forceinline__ void gemm_tile(int M, int N, int K, const double *__r
 #define INS2D_FDM_WARP_N 32
 #endif
 constexpr int kTcWarpN = INS2D_FDM_WARP_N, kTcThreads = 32 * (kBM / 32) * (kBN / kTcWarpN);
+static_assert(INS2D_FDM_DMMA || (kBM == 64 && kBN == 64), "the CUDA-core tile is 64 x 64");
 constexpr int kGemmThreads = INS2D_FDM_DMMA ? kTcThreads : kCoreThreads;
 __device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -146,7 +150,8 @@ __device__ __forceinline__ void gemm_tile_tc(int M, int N, int K, const double *
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   constexpr int NJ = kTcWarpN / 8;  // fragments per warp along n
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * kTcWarpN;
+  constexpr int WM = kBM / 32;  // warps along m
+  const int wm = (warp % WM) * 32, wn = (warp / WM) * kTcWarpN;
   double ra[QA], rb[QB];
   auto load = [&](int k0) {
 #pragma unroll

@@ -79,19 +79,41 @@ __global__ void __launch_bounds__(256) k_init(const __grid_constant__ DevOps P, 
   }
 }
 
-__global__ void __launch_bounds__(256) k_spmv(const __grid_constant__ DevOps P, const PcgWork W) {
+// q = A p and p'q (alpha), walking columns: a thread takes one column i and
+// kSpmvRows rows, so the x-row of TX at i (columns and weights) is read once,
+// the TY row of each j is a warp-uniform read, and the p values of a column
+// reach the thread through L1.  Same arithmetic per cell as lap().
+constexpr int kSpmvRows = 16;
+__global__ void __launch_bounds__(256) k_spmv_cols(const __grid_constant__ DevOps P, const PcgWork W) {
   if (*(volatile int *)&W.sc->done) return;
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-  double q[1] = {0.0};
+  const int i = blockIdx.x * BX + threadIdx.x;
+  const int j0 = (blockIdx.y * BY + threadIdx.y) * kSpmvRows;
+  double q1[1] = {0.0};
   const int ops[1] = {R_SUM};
-  if (i < P.Npx && j < P.Npy) {
-    const long long k = (long long)j * P.Npx + i;
-    const double aq = lap(P, W.p, i, j);
-    W.q[k] = aq;
-    q[0] = W.p[k] * aq;
+  if (i < P.Npx && j0 < P.Npy) {
+    const int32_t *cx = P.TX.c + kT * i;
+    const double *wx = P.TX.w + kT * i;
+    const int cx0 = __ldg(cx), cx1 = __ldg(cx + 1), cx2 = __ldg(cx + 2);
+    const double wx0 = __ldg(wx), wx1 = __ldg(wx + 1), wx2 = __ldg(wx + 2);
+    const double hxi = __ldg(P.hx + i);
+    const int j1 = min(j0 + kSpmvRows, P.Npy);
+    const double *__restrict__ p = W.p;
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const long long base = (long long)j * P.Npx;
+      const double tx = wx0 * __ldg(p + base + cx0) + wx1 * __ldg(p + base + cx1) + wx2 * __ldg(p + base + cx2);
+      const int32_t *cy = P.TY.c + kT * j;
+      const double *wy = P.TY.w + kT * j;
+      const double ty = __ldg(wy) * __ldg(p + (long long)__ldg(cy) * P.Npx + i) +
+                        __ldg(wy + 1) * __ldg(p + (long long)__ldg(cy + 1) * P.Npx + i) +
+                        __ldg(wy + 2) * __ldg(p + (long long)__ldg(cy + 2) * P.Npx + i);
+      const double aq = -(__ldg(P.hy + j) * tx + hxi * ty);
+      W.q[base + i] = aq;
+      q1[0] += __ldg(p + base + i) * aq;
+    }
   }
   double out[1];
-  if (grid_reduce<1>(q, ops, red_of(W), out)) {
+  if (grid_reduce<1>(q1, ops, red_of(W), out)) {
     PcgScalars *s = W.sc;
     s->pq = out[0];
     if (!isfinite(out[0])) {
@@ -104,6 +126,9 @@ __global__ void __launch_bounds__(256) k_spmv(const __grid_constant__ DevOps P, 
       s->alpha = s->rz / out[0];
     }
   }
+}
+inline dim3 spmv_grid(const DevOps &P) {
+  return dim3((P.Npx + BX - 1) / BX, (P.Npy + BY * kSpmvRows - 1) / (BY * kSpmvRows));
 }
 
 __global__ void __launch_bounds__(256) k_update(const __grid_constant__ DevOps P, const PcgWork W) {
@@ -570,7 +595,7 @@ void pcg_init(const DevOps &P, const PcgWork &W, const double *f, double tol, lo
 void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
   const dim3 g = pgrid(P), b(BX, BY);
   for (int it = 0; it < n; ++it) {
-    k_spmv<<<g, b, 0, s>>>(P, W);
+    k_spmv_cols<<<spmv_grid(P), b, 0, s>>>(P, W);
     k_update<<<g, b, 0, s>>>(P, W);
     k_pupdate<<<g, b, 0, s>>>(P, W);
   }
@@ -625,7 +650,7 @@ void pcg_init_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double
 void pcg_iterations_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, int n, cudaStream_t s) {
   const unsigned g = vec_blocks(P, W);
   for (int it = 0; it < n; ++it) {
-    k_spmv<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W);
+    k_spmv_cols<<<spmv_grid(P), dim3(BX, BY), 0, s>>>(P, W);
     k_update_g<<<g, kVecThreads, 0, s>>>(W, P.Np);
     precond_fdm(P, F, W, s);
     k_rz_g<<<g, kVecThreads, 0, s>>>(W, F.z, P.Np, 0);
