@@ -42,43 +42,6 @@ __device__ __forceinline__ RedScratch red_of(const PcgWork &W) {
   return r;
 }
 
-__global__ void __launch_bounds__(256) k_init(const __grid_constant__ DevOps P, const PcgWork W,
-                                              const double *__restrict__ f, double tol2, long long maxit) {
-  const int i = blockIdx.x * BX + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-  double q[3] = {0.0, 0.0, 0.0};
-  const int ops[3] = {R_SUM, R_SUM, R_MAX};
-  if (i < P.Npx && j < P.Npy) {
-    const long long k = (long long)j * P.Npx + i;
-    const double fv = f[k];
-    const double z = fv / lap_diag(P, i, j);
-    W.x[k] = 0.0;
-    W.r[k] = fv;
-    W.p[k] = z;
-    q[0] = fv * fv;
-    q[1] = fv * z;
-    q[2] = fabs(fv);
-  }
-  double out[3];
-  if (grid_reduce<3>(q, ops, red_of(W), out)) {
-    PcgScalars *s = W.sc;
-    s->tol2 = tol2;
-    s->maxit = maxit;
-    s->rr0 = out[0];
-    s->rz = out[1];
-    s->rr = 0.0;
-    s->it = 0;
-    s->status = 0;
-    s->maxx = s->minx = s->maxres = 0.0;
-    s->loops = 0;
-    // pressure_poisson.m:33-38 and cg.F:222-227
-    s->done = (out[2] < 1e-14 || out[0] <= tol2) ? 1 : 0;
-    if (!isfinite(out[0]) || !isfinite(out[1])) {
-      s->status = INS2D_ENONFINITE;
-      s->done = 1;
-    }
-  }
-}
-
 // q = A p and p'q (alpha), walking columns: a thread takes one column i and
 // kSpmvRows rows, so the x-row of TX at i (columns and weights) is read once,
 // the TY row of each j is a warp-uniform read, and the p values of a column
@@ -432,6 +395,47 @@ __global__ void __launch_bounds__(kVecThreads) k_spmv_g(const MgLevelD L0, const
   }
 }
 
+// PCG initialisation over a grid-stride loop (a few blocks per SM, so the final
+// reduction combines few partials): x = 0, r = f, p = f / diag A; f'f,
+// f'(f / diag A), max|f|
+__global__ void __launch_bounds__(kVecThreads) k_init_g(const __grid_constant__ DevOps P, const PcgWork W,
+                                                      const double *__restrict__ f, double tol2, long long maxit) {
+  double q[3] = {0.0, 0.0, 0.0};
+  const int ops[3] = {R_SUM, R_SUM, R_MAX};
+  const int Npx = P.Npx;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < P.Np;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(k / Npx), i = (int)(k - (long long)j * Npx);
+    const double fv = f[k];
+    const double z = fv / lap_diag(P, i, j);
+    W.x[k] = 0.0;
+    W.r[k] = fv;
+    W.p[k] = z;
+    q[0] += fv * fv;
+    q[1] += fv * z;
+    q[2] = fmax(q[2], fabs(fv));
+  }
+  double out[3];
+  if (grid_reduce<3>(q, ops, red_of(W), out)) {
+    PcgScalars *s = W.sc;
+    s->tol2 = tol2;
+    s->maxit = maxit;
+    s->rr0 = out[0];
+    s->rz = out[1];
+    s->rr = 0.0;
+    s->it = 0;
+    s->status = 0;
+    s->maxx = s->minx = s->maxres = 0.0;
+    s->loops = 0;
+    // pressure_poisson.m:33-38 and cg.F:222-227
+    s->done = (out[2] < 1e-14 || out[0] <= tol2) ? 1 : 0;
+    if (!isfinite(out[0]) || !isfinite(out[1])) {
+      s->status = INS2D_ENONFINITE;
+      s->done = 1;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kVecThreads) k_update_g(const PcgWork W, long long n) {
   if (*(volatile int *)&W.sc->done) return;
   const double alpha = W.sc->alpha;
@@ -588,19 +592,6 @@ int pcg_blocks(const DevOps &P) {
   return (int)(g.x * g.y);
 }
 
-void pcg_init(const DevOps &P, const PcgWork &W, const double *f, double tol, long long maxit, cudaStream_t s) {
-  k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
-}
-
-void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
-  const dim3 g = pgrid(P), b(BX, BY);
-  for (int it = 0; it < n; ++it) {
-    k_spmv_cols<<<spmv_grid(P), b, 0, s>>>(P, W);
-    k_update<<<g, b, 0, s>>>(P, W);
-    k_pupdate<<<g, b, 0, s>>>(P, W);
-  }
-}
-
 namespace {
 // blocks of the grid-stride kernels: at most 8 per SM and at most the
 // reduction scratch's capacity
@@ -612,9 +603,23 @@ unsigned vec_blocks(const DevOps &P, const PcgWork &W) {
 }
 }  // namespace
 
+void pcg_init(const DevOps &P, const PcgWork &W, const double *f, double tol, long long maxit, cudaStream_t s) {
+  k_init_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(P, W, f, tol * tol, maxit);
+}
+
+void pcg_iterations(const DevOps &P, const PcgWork &W, int n, cudaStream_t s) {
+  const dim3 g = pgrid(P), b(BX, BY);
+  for (int it = 0; it < n; ++it) {
+    k_spmv_cols<<<spmv_grid(P), b, 0, s>>>(P, W);
+    k_update<<<g, b, 0, s>>>(P, W);
+    k_pupdate<<<g, b, 0, s>>>(P, W);
+  }
+}
+
+
 void pcg_init_mg(const DevOps &P, const MgD &M, const PcgWork &W, const double *f, double tol, long long maxit,
                  cudaStream_t s) {
-  k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
+  k_init_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(P, W, f, tol * tol, maxit);
   mg_vcycle_launch(M, W.r, &W.sc->done, s);
   k_rz_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(W, mg_result_host(M, 0), P.Np, 1);
 }
@@ -642,7 +647,7 @@ void precond_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, cudaStream_t 
 
 void pcg_init_fdm(const DevOps &P, const FdmD &F, const PcgWork &W, const double *f, double tol, long long maxit,
                   cudaStream_t s) {
-  k_init<<<pgrid(P), dim3(BX, BY), 0, s>>>(P, W, f, tol * tol, maxit);
+  k_init_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(P, W, f, tol * tol, maxit);
   precond_fdm(P, F, W, s);
   k_rz_g<<<vec_blocks(P, W), kVecThreads, 0, s>>>(W, F.z, P.Np, 1);
 }

@@ -58,7 +58,20 @@ __device__ bool grid_reduce(double (&v)[NQ], const int (&ops)[NQ], const RedScra
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     double a = red_identity(ops[q]);
-    for (int b = tid; b < nb; b += nthr) a = red_combine(a, ((volatile double *)red.partials)[(size_t)b * NQ + q], ops[q]);
+    // partials read through L2 (ld.global.cg: written by other blocks before
+    // their fence), four loads in flight, combined in block order
+    int b = tid;
+    for (; b + 3 * nthr < nb; b += 4 * nthr) {
+      const double v0 = __ldcg(red.partials + (size_t)b * NQ + q);
+      const double v1 = __ldcg(red.partials + (size_t)(b + nthr) * NQ + q);
+      const double v2 = __ldcg(red.partials + (size_t)(b + 2 * nthr) * NQ + q);
+      const double v3 = __ldcg(red.partials + (size_t)(b + 3 * nthr) * NQ + q);
+      a = red_combine(a, v0, ops[q]);
+      a = red_combine(a, v1, ops[q]);
+      a = red_combine(a, v2, ops[q]);
+      a = red_combine(a, v3, ops[q]);
+    }
+    for (; b < nb; b += nthr) a = red_combine(a, __ldcg(red.partials + (size_t)b * NQ + q), ops[q]);
     for (int off = 16; off > 0; off >>= 1) a = red_combine(a, __shfl_down_sync(0xffffffffu, a, off), ops[q]);
     if (lane == 0) sh[warp][q] = a;
   }
