@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(256) k_conservation(const __grid_constant__ De
 #pragma unroll 4
   for (int r = 0; r < kConsRows; ++r) {
     const int j = jb + r * BY;
-    if (i < P.Npx && j < P.Npy)
-      q[0] = fmax(q[0], fabs(div_in(P, u, v, i, j) + div_bc(P, P.bc.uLe_i, P.bc.uRi_i, P.bc.vLo_i, P.bc.vUp_i, i, j)));
+    if (i < P.Npx && j < P.Npy)  // M V + yM; interior cells by their regular two-point rows
+      q[0] = fmax(q[0], fabs(div_cell_f(P, WPlain{V}, 1.0, 0.0, 1.0, i, j)));
     if (i < P.Nux && j < P.Nuy) {
       const double om = __ldg(P.hy + j) * __ldg(P.gxi + i);
       const double x = u[(long long)j * P.Nux + i];
