@@ -76,6 +76,15 @@ struct ins2d_ctx {
   cudaStream_t body_stream = nullptr;
   SolveAccum *accum = nullptr;    // device
   SolveAccum *h_accum = nullptr;  // pinned
+  // steps on host memory: p's copy in runs on copy_stream while the first
+  // stage's right-hand side is computed (the step waits on ev_p before it
+  // reads p), and V's copy out starts on copy_stream after the last
+  // projection, while the additional pressure solve runs
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_p = nullptr, ev_v = nullptr;
+  bool p_pending = false;
+  double *v_out_host = nullptr;  // erk_step copies V there after its last projection
+  bool v_out_done = false;
   double *h_red = nullptr;      // pinned
   // host copies of boundary samples (check_conservation.m boundary terms)
   std::vector<double> uLe_i, uRi_i, vLo_i, vUp_i;
@@ -627,6 +636,25 @@ int additional_solve(ins2d_ctx *c, const double *V, double *p, double t, ins2d_s
   return solve_div(c, c->wres, 0.0, c->bcd.bc_unsteady ? 1.0 : 0.0, 1.0, p, true, st);
 }
 
+// The step reads or writes p only after wait_p: on host memory p is still
+// being copied in on copy_stream while the first stage's right-hand side runs.
+void wait_p(ins2d_ctx *c) {
+  if (!c->p_pending) return;
+  CK(cudaStreamWaitEvent(c->stream, c->ev_p, 0));
+  c->p_pending = false;
+}
+// after the step's last projection: V is final, so its copy to the host
+// (when requested) starts on copy_stream beside the additional solve
+void copy_v_out(ins2d_ctx *c, const double *V) {
+  if (!c->v_out_host) return;
+  CK(cudaEventRecord(c->ev_v, c->stream));
+  CK(cudaStreamWaitEvent(c->copy_stream, c->ev_v, 0));
+  CK(cudaMemcpyAsync(c->v_out_host, V, (size_t)(c->P.Nu + c->P.Nv) * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->copy_stream));
+  c->v_out_host = nullptr;
+  c->v_out_done = true;
+}
+
 // [V,p] = time_ERK(V,p,T,t,dt,options) on device pointers, in place.
 // k0_cached: kV[0] already holds Om^-1 R(V) (steady BCs, the previous step of
 // the same run computed it in its additional solve); on return *cache_next
@@ -689,6 +717,7 @@ int erk_step32(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_st
     } else {
       dpp = p;  // time_ERK.m:125-127
     }
+    wait_p(c);
     {
       Prof pr(c, INS2D_PROF_PROJECT, 1);
       if (i == c->s - 1)
@@ -697,7 +726,9 @@ int erk_step32(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_st
         launch_project32(P, V, Ti, ai, dpp, dt, c->c[i], c->Vs32, c->stream);
     }
     CK(cudaGetLastError());
+    if (i == c->s - 1) copy_v_out(c, V);
   }
+  wait_p(c);
   if (c->bcd.bc_unsteady && !c->opts.p_add_solve) {
     CK(cudaMemcpyAsync(p, dpp, P.Np * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));  // p = kp(:,end)
   } else {
@@ -723,6 +754,7 @@ int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step
     if (i == 0 && k0_cached && !c->bcd.bc_unsteady && c->s > 1) {
       // first stage from the cached residual fused into its projection
       // (dp = p: time_ERK.m:125-127); Wt is not formed
+      wait_p(c);
       Prof pr(c, INS2D_PROF_PROJECT, 1);
       launch_project_cached(P, V, c->kV[0], c->A[0][0], 1.0 / dt, p, dt, c->c[0], c->Vs, c->stream);
       CK(cudaGetLastError());
@@ -764,12 +796,15 @@ int erk_step(ins2d_ctx *c, double *V, double *p, double t, double dt, ins2d_step
     } else {
       dpp = p;  // time_ERK.m:125-127
     }
+    wait_p(c);
     {
       Prof pr(c, INS2D_PROF_PROJECT, 1);
       launch_project(P, c->Wt, dpp, dt, c->c[i], (i == c->s - 1) ? V : c->Vs, c->stream);
     }
     CK(cudaGetLastError());
+    if (i == c->s - 1) copy_v_out(c, V);
   }
+  wait_p(c);
   if (c->bcd.bc_unsteady && !c->opts.p_add_solve) {
     CK(cudaMemcpyAsync(p, dpp, P.Np * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));  // p = kp(:,end)
   } else {
@@ -1039,6 +1074,9 @@ int ins2d_ctx_create(const ins2d_grid_desc *grid, const ins2d_bc_desc *bc, const
     c->accum = dalloc<SolveAccum>(c, 1);
     CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&c->body_stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_p, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_v, cudaEventDisableTiming));
     c->stream = c->own_stream;
     CK(cudaDeviceSynchronize());
   } catch (const CudaError &e) {
@@ -1066,6 +1104,7 @@ int ins2d_ctx_destroy(ins2d_ctx *ctx) {
   if (!ctx) return INS2D_OK;
   DeviceGuard dg(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   for (auto &g : ctx->step_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (void *p : ctx->allocs) cudaFree(p);
@@ -1080,6 +1119,9 @@ int ins2d_ctx_destroy(ins2d_ctx *ctx) {
   if (ctx->h_accum) cudaFreeHost(ctx->h_accum);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   if (ctx->body_stream) cudaStreamDestroy(ctx->body_stream);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->ev_p) cudaEventDestroy(ctx->ev_p);
+  if (ctx->ev_v) cudaEventDestroy(ctx->ev_v);
   delete ctx;
   return INS2D_OK;
 }
@@ -1321,10 +1363,26 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
   if (!(dt > 0)) return fail(ctx, INS2D_EINVAL, "dt must be positive");
   if (stats) *stats = ins2d_step_stats{0, 0, 0, 0.0};
   const size_t NV = (size_t)(ctx->P.Nu + ctx->P.Nv), Np = (size_t)ctx->P.Np;
+  // every return leaves copy_stream idle (no copy into the caller's memory
+  // outlives the call)
+  struct CopyGuard {
+    ins2d_ctx *c;
+    ~CopyGuard() {
+      cudaStreamSynchronize(c->copy_stream);
+      c->p_pending = false;
+      c->v_out_host = nullptr;
+      c->v_out_done = false;
+    }
+  } copy_guard{ctx};
   double *dV = V, *dP = p;
   if (mem == INS2D_MEM_HOST) {
     CK(cudaMemcpyAsync(ctx->stV, V, NV * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->stP, p, Np * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    // p after V on the copy stream, beside the first stage (wait_p)
+    CK(cudaEventRecord(ctx->ev_p, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_p, 0));
+    CK(cudaMemcpyAsync(ctx->stP, p, Np * sizeof(double), cudaMemcpyHostToDevice, ctx->copy_stream));
+    CK(cudaEventRecord(ctx->ev_p, ctx->copy_stream));
+    ctx->p_pending = true;
     dV = ctx->stV;
     dP = ctx->stP;
   }
@@ -1358,6 +1416,7 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
     return INS2D_OK;
   };
   if (dev_stats) CK(cudaMemsetAsync(ctx->accum, 0, sizeof(SolveAccum), ctx->stream));
+  if (graphs) wait_p(ctx);  // before any capture: the graphs read p
   bool cached = false;
   for (int n = 0; n < nsteps; ++n) {
     if (graphs) {
@@ -1412,6 +1471,7 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
       continue;
     }
     bool next = false;
+    if (mem == INS2D_MEM_HOST && n + 1 == nsteps) ctx->v_out_host = V;
     int rc = erk_step(ctx, dV, dP, t + n * dt, dt, stats, cached, n + 1 < nsteps ? &next : nullptr);
     if (rc) return rc;
     cached = next;
@@ -1427,11 +1487,13 @@ int ins2d_erk_run(ins2d_ctx *ctx, double *V, double *p, double t, double dt, int
       stats->norm1_max = a.norm1_max;
     }
   }
+  wait_p(ctx);
   if (mem == INS2D_MEM_HOST) {
-    CK(cudaMemcpyAsync(V, dV, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (!ctx->v_out_done) CK(cudaMemcpyAsync(V, dV, NV * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(p, dP, Np * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   }
   CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamSynchronize(ctx->copy_stream));
   return INS2D_OK;
   API_END
 }

@@ -45,6 +45,15 @@ struct RegD {
 };
 __device__ __forceinline__ int wrapn(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
 
+// Programmatic dependent launch (kernels started by launch_k with the
+// attribute set): pdl_wait returns once the previous kernel in the stream has
+// completed and its writes are visible; it is a no-op for a plain launch.  A
+// kernel that calls it touches no global memory before it.  pdl_trigger,
+// after the wait, lets the next kernel's blocks be scheduled while this
+// kernel's last blocks run (they wait in their own pdl_wait).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 struct DevOps {
   int Nx, Ny, Nux, Nuy, Nvx, Nvy, Npx, Npy;
   long long Nu, Nv, Np;

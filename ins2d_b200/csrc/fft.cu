@@ -473,9 +473,12 @@ template <int L, int SRC>
 __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
     k_rows_r2c_t(int Ny, const double2 *__restrict__ tw, const double *__restrict__ f, const WSplit ws,
                  double2 *__restrict__ spec, const __grid_constant__ DevOps P, double alpha, double beta,
-                 double gamma, int fastdiv, const int *__restrict__ skip) {
+                 double gamma, int fastdiv, const int *__restrict__ skip, unsigned long long *__restrict__ zero_max) {
   constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
   constexpr bool DIV = SRC != 0;
+  pdl_wait();
+  pdl_trigger();
+  if (zero_max && blockIdx.x == 0 && threadIdx.x == 0) *zero_max = 0ull;  // the column pass's max |fhat|
   if (skip && *(volatile const int *)skip) return;  // preconditioner of a converged CG: nothing to do
   extern __shared__ double2 sm[];
   const double2 *pyr = tw + N;
@@ -550,6 +553,8 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
              const double *__restrict__ ay, double dxdy, double2 *__restrict__ spec,
              unsigned long long *__restrict__ maxbits, const int *__restrict__ skip) {
   constexpr int N = 1 << L, PER = N >> 3, LD = paddedl<L>();
+  pdl_wait();
+  pdl_trigger();
   if (skip && *(volatile const int *)skip) return;
   extern __shared__ double2 sm[];
   __shared__ double wmax[kThreads / 32];
@@ -621,6 +626,8 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
     k_rows_c2r_t(int Ny, const double2 *__restrict__ tw, const double2 *__restrict__ spec, double *__restrict__ out,
                  int accumulate, const unsigned long long *__restrict__ maxbits, const int *__restrict__ skip) {
   constexpr int N = 1 << L, PER = N >> 3, H = N / 2 + 1;
+  pdl_wait();
+  pdl_trigger();
   if (skip && *(volatile const int *)skip) return;
   extern __shared__ double2 sm[];
   const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
@@ -759,23 +766,29 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const int Nx = plan.Nx, Ny = plan.Ny;
   const int pairs = (Ny + 1) / 2;
   const int H = Nx / 2 + 1;
-  const cudaError_t ms = cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
-  if (ms != cudaSuccess) return ms;
   unsigned long long *maxbits = (unsigned long long *)plan.maxabs;
+  // the fused row pass zeroes max |fhat| itself (no memset node between the
+  // passes, so the step's kernels chain by programmatic launch)
+  if (!(plan.logx >= kFusedMinLog && plan.logx <= 13)) {
+    const cudaError_t ms = cudaMemsetAsync(plan.maxabs, 0, sizeof(double), s);
+    if (ms != cudaSuccess) return ms;
+  }
   // rows, real -> half spectrum
   const int fastdiv = P.rMX.lo <= 0 && P.rMX.hi >= Nx && P.rMY.lo <= 0 && P.rMY.hi >= Ny && P.rMX.two && P.rMY.two;
   const bool fx = with_log2<kFusedMinLog>(plan.logx, [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
     const WSplit w0{};
+    const double *none = nullptr;
     if (ws)
-      k_rows_r2c_t<L, 2><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, nullptr, *ws, plan.spec, P, alpha, beta, gamma,
-                                                     fastdiv, skip);
+      launch_k(k_rows_r2c_t<L, 2>, dim3(pairs), dim3(kThreads), sm, s, Ny, plan.twx, none, *ws, plan.spec, P, alpha,
+               beta, gamma, fastdiv, skip, maxbits);
     else if (div)
-      k_rows_r2c_t<L, 1><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, alpha, beta, gamma,
-                                                     fastdiv, skip);
+      launch_k(k_rows_r2c_t<L, 1>, dim3(pairs), dim3(kThreads), sm, s, Ny, plan.twx, src, w0, plan.spec, P, alpha,
+               beta, gamma, fastdiv, skip, maxbits);
     else
-      k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, src, w0, plan.spec, P, 0.0, 0.0, 0.0, 0, skip);
+      launch_k(k_rows_r2c_t<L, 0>, dim3(pairs), dim3(kThreads), sm, s, Ny, plan.twx, src, w0, plan.spec, P, 0.0,
+               0.0, 0.0, 0, skip, maxbits);
   });
   const size_t smx = (size_t)padded(Nx) * sizeof(double2) * (plan.logx >= 0 ? 1 : 2);
   if (!fx) k_rows_r2c<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, src, plan.spec);
@@ -783,8 +796,8 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const bool fy = with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
-    k_cols_t<L, G><<<(H + G - 1) / G, kThreads, sm, s>>>(H, H, 0, plan.twy, P.fft_ax, P.fft_ay, P.fft_dxdy,
-                                                         plan.spec, maxbits, skip);
+    launch_k(k_cols_t<L, G>, dim3((H + G - 1) / G), dim3(kThreads), sm, s, H, H, 0, plan.twy, P.fft_ax, P.fft_ay,
+             P.fft_dxdy, plan.spec, maxbits, skip);
   });
   if (!fy) {
     const int G = cols_group(Ny, plan.logy >= 0);
@@ -796,8 +809,9 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const bool fx2 = with_log2<kFusedMinLog>(plan.logx, [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
-    k_rows_c2r_t<L><<<pairs, kThreads, sm, s>>>(Ny, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
-                                                gate ? gate : maxbits, skip);
+    const unsigned long long *g = gate ? gate : maxbits;
+    launch_k(k_rows_c2r_t<L>, dim3(pairs), dim3(kThreads), sm, s, Ny, plan.twx, plan.spec, dp, accumulate ? 1 : 0, g,
+             skip);
   });
   if (!fx2)
     k_rows_c2r<<<pairs, kThreads, smx, s>>>(Nx, Ny, plan.logx, plan.twx, plan.spec, dp, accumulate ? 1 : 0,
@@ -845,7 +859,7 @@ cudaError_t slab_rows_forward(int Nx, const double2 *twx, const double *f, int n
   with_log2<kFusedMinLog>(ilog2_exact(Nx), [&](auto c) {
     constexpr int L = decltype(c)::value;
     const size_t sm = (size_t)paddedl<L>() * sizeof(double2);
-    k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(nrows, twx, f, w0, spec, P, 0.0, 0.0, 0.0, 0, nullptr);
+    k_rows_r2c_t<L, 0><<<pairs, kThreads, sm, s>>>(nrows, twx, f, w0, spec, P, 0.0, 0.0, 0.0, 0, nullptr, nullptr);
   });
   return cudaPeekAtLastError();
 }

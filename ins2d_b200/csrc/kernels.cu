@@ -8,11 +8,20 @@
 // order by the last block to finish.
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
 
 #include "kernels.cuh"
 #include "reduce.cuh"
 
 namespace ins2d {
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char *v = std::getenv("INS2D_PDL");
+    return v && v[0] == '1';
+  }();
+  return on;
+}
 
 namespace {
 
@@ -86,6 +95,8 @@ constexpr int kProjRows = INS2D_PROJ_ROWS;
 __global__ void __launch_bounds__(256) k_project(const __grid_constant__ DevOps P, const double *__restrict__ Wt,
                                                 const double *__restrict__ dp, double dt, double c,
                                                 double *__restrict__ Vo) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * BX + threadIdx.x;
   const int j0 = blockIdx.y * (BY * kProjRows) + threadIdx.y;
 #pragma unroll
@@ -101,6 +112,8 @@ __global__ void __launch_bounds__(256) k_project_cached(const __grid_constant__ 
                                                        const double *__restrict__ kV0, double aii, double inv_dt,
                                                        const double *__restrict__ dp, double dt, double c,
                                                        double *__restrict__ Vo) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * BX + threadIdx.x;
   const int j0 = blockIdx.y * (BY * kProjRows) + threadIdx.y;
 #pragma unroll
@@ -316,7 +329,7 @@ void launch_project(const DevOps &P, const double *Wt, const double *dp, double 
                     cudaStream_t s) {
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
-  k_project<<<g, dim3(BX, BY), 0, s>>>(P, Wt, dp, dt, c, V_out);
+  launch_k(k_project, g, dim3(BX, BY), 0, s, P, Wt, dp, dt, c, V_out);
 }
 
 template <typename TO>
@@ -339,7 +352,7 @@ void launch_project_cached(const DevOps &P, const double *Vn, const double *kV0,
                            const double *dp, double dt, double c, double *V_out, cudaStream_t s) {
   const int nx = P.Nux > P.Nvx ? P.Nux : P.Nvx, ny = P.Nuy > P.Nvy ? P.Nuy : P.Nvy;
   const dim3 g((nx + BX - 1) / BX, (ny + BY * kProjRows - 1) / (BY * kProjRows));
-  k_project_cached<<<g, dim3(BX, BY), 0, s>>>(P, Vn, kV0, aii, inv_dt, dp, dt, c, V_out);
+  launch_k(k_project_cached, g, dim3(BX, BY), 0, s, P, Vn, kV0, aii, inv_dt, dp, dt, c, V_out);
 }
 
 void launch_correct(const DevOps &P, const double *V_in, const double *dp, double *V_out, cudaStream_t s) {

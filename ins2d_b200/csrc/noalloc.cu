@@ -122,7 +122,7 @@ extern "C" int ins2d_fft_poisson_noalloc(const double *f, double *dp, int32_t Nx
   plan.twx = twx;
   plan.twy = twy;
   plan.spec = spec;
-  plan.maxabs = maxabs;  // launch_fft_poisson zeroes it before the passes
+  plan.maxabs = maxabs;  // zeroed by the first transform pass of each solve
   // An error already pending on this thread belongs to the caller: it is
   // neither cleared nor taken for a failure of this call.  Without one, an
   // error after the launches is this call's own (and is consumed).

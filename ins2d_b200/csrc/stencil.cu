@@ -626,19 +626,48 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Vtemp of an FP64 stage at idx: sum over the earlier stages a_m kV_m, then
-// the stage's own aii k (time_ERK.m:96-101).  NP >= 0: that many earlier
-// stages, unrolled at compile time; NP < 0: e.nprev.
+// Global operands of one row's epilogue, loaded a row ahead: the walker
+// issues row j+1's loads before row j's stencil and stores, so their latency
+// overlaps that work (issued after the stores, they would wait on them as
+// possible aliases).  MODE 0: Vn and, for NP > 0, the earlier stages' kV;
+// MODE 1: the two pressure values of the gradient.
+// The earlier stages' kV are prefetched for NP <= INS2D_TILE_AHEAD_K only:
+// with more, the two rows' operands exceed the 80-register budget of three
+// blocks per SM and spill; those stages read them in place.
+#ifndef INS2D_TILE_AHEAD_K
+#define INS2D_TILE_AHEAD_K 1
+#endif
+template <int MODE, int NP>
+struct EpiAhead {
+  static constexpr bool K = MODE == 0 && NP > 0 && NP <= INS2D_TILE_AHEAD_K;
+  double a, b;
+  double kp[K ? NP : 1];
+};
+template <int MODE, int NP>
+__device__ __forceinline__ void stage_ahead(const Epi &e, long long idx, EpiAhead<MODE, NP> &x) {
+  x.a = __ldg(e.Vn + idx);
+  if constexpr (EpiAhead<MODE, NP>::K) {
+#pragma unroll
+    for (int m = 0; m < NP; ++m) x.kp[m] = __ldg(e.kprev[m] + idx);
+  }
+}
+// the FP64 stage epilogue from prefetched operands: kV = k and
+// Wt = Vn/dt + (sum over the earlier stages a_m kV_m + aii k) (time_ERK.m:96-101);
+// NP >= 0: that many earlier stages, unrolled; NP < 0: e.nprev
 template <int NP>
-__device__ __forceinline__ double stage_vtemp(const Epi &e, long long idx, double k) {
+__device__ __forceinline__ void stage_store(const Epi &e, long long idx, double k, const EpiAhead<0, NP> &x) {
+  if (e.kV) e.kV[idx] = k;
   double vt = 0.0;
-  if constexpr (NP >= 0) {
+  if constexpr (EpiAhead<0, NP>::K) {
+#pragma unroll
+    for (int m = 0; m < NP; ++m) vt += e.aprev[m] * x.kp[m];
+  } else if constexpr (NP >= 0) {
 #pragma unroll
     for (int m = 0; m < NP; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
   } else {
     for (int m = 0; m < e.nprev; ++m) vt += e.aprev[m] * __ldg(e.kprev[m] + idx);
   }
-  return vt + e.aii * k;
+  e.Wt[idx] = x.a * e.inv_dt + (vt + e.aii * k);
 }
 
 // MODE 0: FP64-storage stage, 1: residual, 2: FP32-storage stage
@@ -674,10 +703,28 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     sy = S(Y.suy0[y]) * f0 + S(Y.suy1[y]) * f1;
     vf = S(Y.ivy0[y]) * (iv0 * va0 + iv1 * va1) + S(Y.ivy1[y]) * (iv0 * vb0 + iv1 * vb1);
   };
+  // pressure gradient columns and weights (residual mode)
+  const int pc0 = MODE == 1 ? wrapn(i + P.rMXT.s, P.rMXT.n) : 0, pc1 = MODE == 1 ? wrapn(pc0 + 1, P.rMXT.n) : 0;
+  const bool twoG = MODE == 1 && P.rMXT.two;
+  const double gw0 = MODE == 1 ? __ldg(P.rMXT.w0 + i) : 0.0, gw1 = twoG ? __ldg(P.rMXT.w1 + i) : 0.0;
+  auto ahead = [&](int j, EpiAhead<MODE, NP> &x) {
+    if constexpr (MODE == 0) {
+      stage_ahead<MODE, NP>(e, (long long)j * P.Nux + i, x);
+    } else if constexpr (MODE == 1) {
+      const double *pr = e.p + (long long)j * P.Npx;
+      x.a = __ldg(pr + pc0);
+      x.b = twoG ? __ldg(pr + pc1) : 0.0;
+    }
+  };
+  EpiAhead<MODE, NP> nxt;
+  if constexpr (MODE != 2) ahead(ja, nxt);
   S uy0, sy0, vf0;
   face(ja, uy0, sy0, vf0);
 #pragma unroll 2
   for (int j = ja; j < jb; ++j) {
+    const EpiAhead<MODE, NP> cur = nxt;
+    if constexpr (MODE != 2)
+      if (j + 1 < jb) ahead(j + 1, nxt);
     S uy1, sy1, vf1;
     face(j + 1, uy1, sy1, vf1);
     const int rr = j - j0 + 2;
@@ -693,15 +740,13 @@ __device__ void tile_u(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     const long long idx = (long long)j * P.Nux + i;
     const double oi = Y.rhy[j - j0] * rgx;
     if constexpr (MODE == 0) {
-      const double k = oi * R;
-      if (e.kV) e.kV[idx] = k;
-      const double vt = stage_vtemp<NP>(e, idx, k);
-      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+      stage_store<NP>(e, idx, oi * R, cur);
     } else if constexpr (MODE == 2) {
       epi_stage32<NP>(e, idx, oi * R);
     } else {
-      const double g = -hyd * reg_x(P.rMXT, i, e.p, (long long)j * P.Npx);
-      epi_residual(e, idx, oi, R, g);
+      double gp = gw0 * cur.a;
+      if (twoG) gp += gw1 * cur.b;
+      epi_residual(e, idx, oi, R, -hyd * gp);
     }
     uy0 = uy1;
     sy0 = sy1;
@@ -735,10 +780,25 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     vy = S(Y.avy0[y]) * f0 + S(Y.avy1[y]) * f1;
     sy = S(Y.svy0[y]) * f0 + S(Y.svy1[y]) * f1;
   };
+  const bool twoG = MODE == 1 && P.rMYT.two;
+  auto ahead = [&](int j, EpiAhead<MODE, NP> &x) {
+    if constexpr (MODE == 0) {
+      stage_ahead<MODE, NP>(e, P.Nu + (long long)j * P.Nvx + i, x);
+    } else if constexpr (MODE == 1) {
+      const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
+      x.a = __ldg(e.p + (long long)c0 * P.Npx + i);
+      x.b = twoG ? __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i) : 0.0;
+    }
+  };
+  EpiAhead<MODE, NP> nxt;
+  if constexpr (MODE != 2) ahead(ja, nxt);
   S vy0, sy0;
   face(ja, vy0, sy0);
 #pragma unroll 2
   for (int j = ja; j < jb; ++j) {
+    const EpiAhead<MODE, NP> cur = nxt;
+    if constexpr (MODE != 2)
+      if (j + 1 < jb) ahead(j + 1, nxt);
     S vy1, sy1;
     face(j + 1, vy1, sy1);
     const int rr = j - j0 + 2;
@@ -765,18 +825,13 @@ __device__ void tile_v(const DevOps &P, const TileSm<TV> &T, const Epi &e, int i
     const long long idx = P.Nu + (long long)j * P.Nvx + i;
     const double oi = Y.rgyi[j - j0] * rhx;
     if constexpr (MODE == 0) {
-      const double k = oi * R;
-      if (e.kV) e.kV[idx] = k;
-      const double vt = stage_vtemp<NP>(e, idx, k);
-      e.Wt[idx] = __ldg(e.Vn + idx) * e.inv_dt + vt;
+      stage_store<NP>(e, idx, oi * R, cur);
     } else if constexpr (MODE == 2) {
       epi_stage32<NP>(e, idx, oi * R);
     } else {
-      const int c0 = wrapn(j + P.rMYT.s, P.rMYT.n);
-      double gy = Y.myt0[j - j0] * __ldg(e.p + (long long)c0 * P.Npx + i);
-      if (P.rMYT.two) gy += Y.myt1[j - j0] * __ldg(e.p + (long long)wrapn(c0 + 1, P.rMYT.n) * P.Npx + i);
-      const double g = -hxd * gy;
-      epi_residual(e, idx, oi, R, g);
+      double gy = Y.myt0[j - j0] * cur.a;
+      if (twoG) gy += Y.myt1[j - j0] * cur.b;
+      epi_residual(e, idx, oi, R, -hxd * gy);
     }
     vy0 = vy1;
     sy0 = sy1;
@@ -815,6 +870,8 @@ __global__ void __launch_bounds__(kTileThreads, INS2D_TILE_MINB)
     k_walk_tile(const __grid_constant__ DevOps P, const TV *__restrict__ V, const __grid_constant__ Epi e) {
   __shared__ __align__(16) TileSm<TV> T;
   __shared__ YRowsN<RUN> Y;
+  pdl_wait();
+  pdl_trigger();
   const int bx = P.fbx0 + blockIdx.x, by = P.fby0 + blockIdx.y;
   const int i0 = bx * WX, j0 = by * RUN;
   const int tid = threadIdx.x + WX * threadIdx.y;
@@ -939,14 +996,14 @@ void launch_tile(const DevOps &P, const TV *V, const Epi &e, cudaStream_t s) {
   const dim3 gf(P.fbx1 - P.fbx0, P.fby1 - P.fby0), tb(WX, kTileThreads / WX);
   if constexpr (MODE == 0 || MODE == 2) {
     switch (e.nprev) {
-      case 0: k_walk_tile<S, MODE, TV, 0><<<gf, tb, 0, s>>>(P, V, e); break;
-      case 1: k_walk_tile<S, MODE, TV, 1><<<gf, tb, 0, s>>>(P, V, e); break;
-      case 2: k_walk_tile<S, MODE, TV, 2><<<gf, tb, 0, s>>>(P, V, e); break;
-      case 3: k_walk_tile<S, MODE, TV, 3><<<gf, tb, 0, s>>>(P, V, e); break;
-      default: k_walk_tile<S, MODE, TV, -1><<<gf, tb, 0, s>>>(P, V, e); break;
+      case 0: launch_k(k_walk_tile<S, MODE, TV, 0>, gf, tb, 0, s, P, V, e); break;
+      case 1: launch_k(k_walk_tile<S, MODE, TV, 1>, gf, tb, 0, s, P, V, e); break;
+      case 2: launch_k(k_walk_tile<S, MODE, TV, 2>, gf, tb, 0, s, P, V, e); break;
+      case 3: launch_k(k_walk_tile<S, MODE, TV, 3>, gf, tb, 0, s, P, V, e); break;
+      default: launch_k(k_walk_tile<S, MODE, TV, -1>, gf, tb, 0, s, P, V, e); break;
     }
   } else {
-    k_walk_tile<S, MODE, TV, -1><<<gf, tb, 0, s>>>(P, V, e);
+    launch_k(k_walk_tile<S, MODE, TV, -1>, gf, tb, 0, s, P, V, e);
   }
 }
 
