@@ -193,3 +193,35 @@ def test_semidiscrete_energy_periodic(N):
     _, F = m.F(V, None, np.zeros(m.Np), 0.0)
     prod = V @ F
     assert abs(prod) <= 1e-14 * np.linalg.norm(V) * np.linalg.norm(F)
+
+
+@pytest.mark.parametrize("case", ["fft", "fft_fp32", "pcg"])
+@pytest.mark.parametrize("nsteps", [1, 3])
+def test_host_buffers_match_device_tensors(case, nsteps):
+    """A step on host buffers copies p in on a second stream beside the first
+    stage and, for a single step, copies V out beside the additional solve;
+    its state equals the same steps run on device tensors."""
+    import torch
+    import ins2d_b200
+    if case.startswith("fft"):
+        x = grid_uniform(128, 0.0, 1.0)
+        m = ins2d_b200.Options(x, x.copy(), BC_COMBOS["periodic"], Re=500.0, poisson=6,
+                               precision="fp32" if case == "fft_fp32" else "fp64")
+        dt = 1e-3
+    else:
+        x = grid_stretched(300, 0.0, 1.0)
+        y = grid_stretched(260, 0.0, 1.0)
+        uBC, vBC = smooth_bc(5, closed=True)
+        m = ins2d_b200.Options(x, y, BC_COMBOS["cavity"], Re=200.0, poisson=4, CG_acc=1e-10, uBC=uBC, vBC=vBC)
+        dt = 1e-5
+    rng = np.random.default_rng(11)
+    V0 = 0.1 * rng.standard_normal(m.NV)
+    p0 = 0.1 * rng.standard_normal(m.Np)
+    Vh, ph = m.time_ERK(V0, p0, 0.0, dt, nsteps=nsteps)
+    Vd = torch.tensor(V0, device="cuda")
+    pd = torch.tensor(p0, device="cuda")
+    m.time_ERK(Vd, pd, 0.0, dt, nsteps=nsteps)
+    torch.cuda.synchronize()
+    assert _rel(Vh, Vd.cpu().numpy()) < 1e-13
+    assert _rel(ph, pd.cpu().numpy()) < 1e-13
+    assert not np.array_equal(Vh, V0)
