@@ -384,6 +384,91 @@ __device__ __forceinline__ void group_dit(double2 (&x)[8], int ns, int k, int h,
   }
 }
 
+// Groups of NS <= 4 radix-2 stages on 16 values (the column pass's outer
+// passes, INS2D_FFT_COLS_R16): as group_dif / group_dit with NS a
+// compile-time count; the top stage of a four-stage group multiplies by
+// sixteenth roots of unity.
+
+// a * W_16^j (conjugate root when inv), j < 8; W_16^j = cos(pi j/8) - i sin(pi j/8)
+__device__ __forceinline__ double2 rot16(double2 a, int j, bool inv) {
+  if ((j & 1) == 0) return rot(a, 4, j >> 1, inv);  // W_16^(2i) = W_8^i
+  constexpr double c = 0.92387953251128675613, s = 0.38268343236508977173;  // cos(pi/8), sin(pi/8)
+  double wr, wi;
+  if (j == 1) {
+    wr = c;
+    wi = -s;
+  } else if (j == 3) {
+    wr = s;
+    wi = -c;
+  } else if (j == 5) {
+    wr = -s;
+    wi = -c;
+  } else {
+    wr = -c;
+    wi = -s;
+  }
+  if (inv) wi = -wi;
+  return make_double2(a.x * wr - a.y * wi, a.x * wi + a.y * wr);
+}
+// w times W_{2 hh}^j, hh <= 8
+__device__ __forceinline__ double2 rot_any(double2 w, int hh, int j, bool inv) {
+  return hh == 8 ? rot16(w, j, inv) : rot(w, hh, j, inv);
+}
+// base twiddles W_{2^(st+1) h}^k of stages st < NS from the top one W_{2^NS h}^k
+template <int NS>
+__device__ __forceinline__ void group_twiddles16(int k, int h, const double2 *pyr, bool inv, double2 (&w)[4]) {
+  double2 wt = __ldg(pyr + (((1 << NS) * h) >> 1) + k);
+  if (inv) wt.y = -wt.y;
+  w[NS - 1] = wt;
+#pragma unroll
+  for (int st = NS - 2; st >= 0; --st) w[st] = csq(w[st + 1]);
+}
+template <bool UNIT, int NS>
+__device__ __forceinline__ void group_dif16(double2 (&x)[16], int k, int h, const double2 *pyr, bool inv) {
+  double2 w[4];
+  if constexpr (!UNIT) group_twiddles16<NS>(k, h, pyr, inv, w);
+#pragma unroll
+  for (int st = NS - 1; st >= 0; --st) {
+    const int hh = 1 << st;
+    double2 tw[8];
+    if constexpr (!UNIT) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (j < hh) tw[j] = rot_any(w[st], hh, j, inv);
+    }
+#pragma unroll
+    for (int m = 0; m < (1 << NS); ++m) {
+      if ((m & (2 * hh - 1)) >= hh) continue;
+      const double2 x0 = x[m], x1 = x[m + hh];
+      const double2 d = make_double2(x0.x - x1.x, x0.y - x1.y);
+      x[m] = make_double2(x0.x + x1.x, x0.y + x1.y);
+      x[m + hh] = UNIT ? rot_any(d, hh, m & (hh - 1), inv) : cmul(d, tw[m & (hh - 1)]);
+    }
+  }
+}
+template <bool UNIT, int NS>
+__device__ __forceinline__ void group_dit16(double2 (&x)[16], int k, int h, const double2 *pyr, bool inv) {
+  double2 w[4];
+  if constexpr (!UNIT) group_twiddles16<NS>(k, h, pyr, inv, w);
+#pragma unroll
+  for (int st = 0; st < NS; ++st) {
+    const int hh = 1 << st;
+    double2 tw[8];
+    if constexpr (!UNIT) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (j < hh) tw[j] = rot_any(w[st], hh, j, inv);
+    }
+#pragma unroll
+    for (int m = 0; m < (1 << NS); ++m) {
+      if ((m & (2 * hh - 1)) >= hh) continue;
+      const double2 y = UNIT ? rot_any(x[m + hh], hh, m & (hh - 1), inv) : cmul(tw[m & (hh - 1)], x[m + hh]);
+      x[m + hh] = make_double2(x[m].x - y.x, x[m].y - y.y);
+      x[m] = make_double2(x[m].x + y.x, x[m].y + y.y);
+    }
+  }
+}
+
 // --- power-of-two lengths 2^L, 6 <= L <= 13: every shape a compile-time
 // constant; the first and last radix-8 passes fused with the global loads and
 // stores, no permutation passes; tw is the table of fft_twiddle_table (the
@@ -456,6 +541,53 @@ __device__ __forceinline__ void dit_passes(double2 *a, int ld, int lines, const 
     }
     __syncthreads();
     dit_passes<L, S0 + 3, S_TOP, G>(a, ld, lines, pyr, inv);
+  }
+}
+
+// the same with up to four stages per pass (the column pass's outer passes
+// with INS2D_FFT_COLS_R16; every pass's smallest half size H >= 8)
+template <int L, int S_HI, int S_BOT, int G>
+__device__ __forceinline__ void dif16_passes(double2 *a, int ld, int lines, const double2 *pyr, bool inv) {
+  if constexpr (S_HI >= S_BOT) {
+    constexpr int NS = (S_HI - S_BOT + 1) < 4 ? (S_HI - S_BOT + 1) : 4;
+    constexpr int S_LO = S_HI - NS + 1, R = 1 << NS, H = 1 << (S_LO - 1), PER = (1 << L) >> NS;
+    const unsigned lim = (G > 1 ? lines : 1) * PER;
+    for (unsigned g = threadIdx.x; g < lim; g += kThreads) {
+      const int line = (int)(g / PER), gg = (int)(g % PER);
+      const int k = gg & (H - 1), blk = gg >> (S_LO - 1);
+      const int base = blk * R * H + k;
+      double2 *Lp = a + line * ld;
+      double2 x[16];
+#pragma unroll
+      for (int m = 0; m < R; ++m) x[m] = Lp[pdl<L>(base + m * H)];
+      group_dif16<false, NS>(x, k, H, pyr, inv);
+#pragma unroll
+      for (int m = 0; m < R; ++m) Lp[pdl<L>(base + m * H)] = x[m];
+    }
+    __syncthreads();
+    dif16_passes<L, S_HI - NS, S_BOT, G>(a, ld, lines, pyr, inv);
+  }
+}
+template <int L, int S0, int S_TOP, int G>
+__device__ __forceinline__ void dit16_passes(double2 *a, int ld, int lines, const double2 *pyr, bool inv) {
+  if constexpr (S0 < S_TOP) {
+    constexpr int NS = (S_TOP - S0) < 4 ? (S_TOP - S0) : 4;
+    constexpr int R = 1 << NS, H = 1 << S0, PER = (1 << L) >> NS;
+    const unsigned lim = (G > 1 ? lines : 1) * PER;
+    for (unsigned g = threadIdx.x; g < lim; g += kThreads) {
+      const int line = (int)(g / PER), gg = (int)(g % PER);
+      const int k = gg & (H - 1), blk = gg >> S0;
+      const int base = blk * R * H + k;
+      double2 *Lp = a + line * ld;
+      double2 x[16];
+#pragma unroll
+      for (int m = 0; m < R; ++m) x[m] = Lp[pdl<L>(base + m * H)];
+      group_dit16<false, NS>(x, k, H, pyr, inv);
+#pragma unroll
+      for (int m = 0; m < R; ++m) Lp[pdl<L>(base + m * H)] = x[m];
+    }
+    __syncthreads();
+    dit16_passes<L, S0 + NS, S_TOP, G>(a, ld, lines, pyr, inv);
   }
 }
 
@@ -547,8 +679,11 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_ROWS_MINB)
 // the last DIF and first DIT passes, inverse DIT; max |fhat| reduction
 // The columns are the first ncols of a spectrum with row stride H (complex
 // values); column c holds wave number I0 + c (I0 > 0 for a slab's column range).
-template <int L, int G>
-__global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
+// RX: 8, or 16 for outer passes of four stages (the global load and store
+// and the shared-memory passes beside them; fewer shared-memory round trips,
+// L >= 9).
+template <int L, int G, int RX = 8>
+__global__ void __launch_bounds__(kThreads, RX == 16 ? 2 : INS2D_FFT_COLS_MINB)
     k_cols_t(int H, int ncols, int I0, const double2 *__restrict__ tw, const double *__restrict__ ax,
              const double *__restrict__ ay, double dxdy, double2 *__restrict__ spec,
              unsigned long long *__restrict__ maxbits, const int *__restrict__ skip) {
@@ -561,18 +696,35 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
   const double2 *pyr = tw + N;
   const int c0 = blockIdx.x * G;
   const int g_here = min(G, ncols - c0);
-  for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
-    const int k = (int)(gidx / G), line = (int)(gidx % G);
-    if (line >= g_here) continue;
-    double2 x[8];
+  static_assert(RX == 8 || (RX == 16 && L >= 9), "radix-16 outer passes need L >= 9");
+  if constexpr (RX == 16) {
+    constexpr int P16 = N >> 4;
+    for (unsigned gidx = threadIdx.x; gidx < G * P16; gidx += kThreads) {
+      const int k = (int)(gidx / G), line = (int)(gidx % G);
+      if (line >= g_here) continue;
+      double2 x[16];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = spec[(size_t)(k + m * PER) * H + c0 + line];
-    group_dif<false>(x, 3, k, PER, pyr, false);
+      for (int m = 0; m < 16; ++m) x[m] = spec[(size_t)(k + m * P16) * H + c0 + line];
+      group_dif16<false, 4>(x, k, P16, pyr, false);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) sm[line * LD + pdl<L>(k + m * PER)] = x[m];
+      for (int m = 0; m < 16; ++m) sm[line * LD + pdl<L>(k + m * P16)] = x[m];
+    }
+    __syncthreads();
+    dif16_passes<L, L - 4, 4, G>(sm, LD, g_here, pyr, false);
+  } else {
+    for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
+      const int k = (int)(gidx / G), line = (int)(gidx % G);
+      if (line >= g_here) continue;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) x[m] = spec[(size_t)(k + m * PER) * H + c0 + line];
+      group_dif<false>(x, 3, k, PER, pyr, false);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) sm[line * LD + pdl<L>(k + m * PER)] = x[m];
+    }
+    __syncthreads();
+    dif_passes<L, L - 3, 4, G>(sm, LD, g_here, pyr, false);
   }
-  __syncthreads();
-  dif_passes<L, L - 3, 4, G>(sm, LD, g_here, pyr, false);
   double lmax = 0.0;
   for (unsigned gidx = threadIdx.x; gidx < g_here * PER; gidx += kThreads) {
     const int line = (int)(gidx / PER), k = (int)(gidx % PER);
@@ -596,18 +748,34 @@ __global__ void __launch_bounds__(kThreads, INS2D_FFT_COLS_MINB)
     for (int m = 0; m < 8; ++m) Ls[pdl<L>(8 * k + m)] = x[m];
   }
   __syncthreads();
-  dit_passes<L, 3, L - 3, G>(sm, LD, g_here, pyr, true);
   const double sc = 1.0 / N;
-  for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
-    const int k = (int)(gidx / G), line = (int)(gidx % G);
-    if (line >= g_here) continue;
-    double2 x[8];
+  if constexpr (RX == 16) {
+    constexpr int P16 = N >> 4;
+    dit16_passes<L, 3, L - 4, G>(sm, LD, g_here, pyr, true);
+    for (unsigned gidx = threadIdx.x; gidx < G * P16; gidx += kThreads) {
+      const int k = (int)(gidx / G), line = (int)(gidx % G);
+      if (line >= g_here) continue;
+      double2 x[16];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) x[m] = sm[line * LD + pdl<L>(k + m * PER)];
-    group_dit<false>(x, 3, k, PER, pyr, true);
+      for (int m = 0; m < 16; ++m) x[m] = sm[line * LD + pdl<L>(k + m * P16)];
+      group_dit16<false, 4>(x, k, P16, pyr, true);
 #pragma unroll
-    for (int m = 0; m < 8; ++m)
-      spec[(size_t)(k + m * PER) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
+      for (int m = 0; m < 16; ++m)
+        spec[(size_t)(k + m * P16) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
+    }
+  } else {
+    dit_passes<L, 3, L - 3, G>(sm, LD, g_here, pyr, true);
+    for (unsigned gidx = threadIdx.x; gidx < G * PER; gidx += kThreads) {
+      const int k = (int)(gidx / G), line = (int)(gidx % G);
+      if (line >= g_here) continue;
+      double2 x[8];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) x[m] = sm[line * LD + pdl<L>(k + m * PER)];
+      group_dit<false>(x, 3, k, PER, pyr, true);
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        spec[(size_t)(k + m * PER) * H + c0 + line] = make_double2(x[m].x * sc, x[m].y * sc);
+    }
   }
   for (int off = 16; off > 0; off >>= 1) lmax = fmax(lmax, __shfl_down_sync(0xffffffffu, lmax, off));
   if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
@@ -693,6 +861,14 @@ bool with_log2(int l, Fn &&fn) {
   }
 }
 constexpr int kFusedMinLog = 6;
+// outer radix of the column pass for length 2^L
+#ifndef INS2D_FFT_COLS_R16
+#define INS2D_FFT_COLS_R16 1
+#endif
+template <int L>
+constexpr int cols_radix() {
+  return (INS2D_FFT_COLS_R16 && L >= 9) ? 16 : 8;
+}
 
 int ilog2_exact(int n) {
   int l = 0;
@@ -748,7 +924,7 @@ cudaError_t fft_prepare() {
       opt_in((const void *)k_rows_r2c_t<L, 0>);
       opt_in((const void *)k_rows_r2c_t<L, 1>);
       opt_in((const void *)k_rows_r2c_t<L, 2>);
-      opt_in((const void *)k_cols_t<L, cols_per_block<L>()>);
+      opt_in((const void *)k_cols_t<L, cols_per_block<L>(), cols_radix<L>()>);
       opt_in((const void *)k_rows_c2r_t<L>);
     });
   opt_in((const void *)k_rows_r2c);
@@ -796,8 +972,8 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   const bool fy = with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
-    launch_k(k_cols_t<L, G>, dim3((H + G - 1) / G), dim3(kThreads), sm, s, H, H, 0, plan.twy, P.fft_ax, P.fft_ay,
-             P.fft_dxdy, plan.spec, maxbits, skip);
+    launch_k(k_cols_t<L, G, cols_radix<L>()>, dim3((H + G - 1) / G), dim3(kThreads), sm, s, H, H, 0, plan.twy,
+             P.fft_ax, P.fft_ay, P.fft_dxdy, plan.spec, maxbits, skip);
   });
   if (!fy) {
     const int G = cols_group(Ny, plan.logy >= 0);
@@ -869,8 +1045,8 @@ cudaError_t slab_columns(int Ny, const double2 *twy, const double *ax, const dou
   with_log2<kFusedMinLog>(ilog2_exact(Ny), [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
     const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
-    k_cols_t<L, G><<<(ncols + G - 1) / G, kThreads, sm, s>>>(width, ncols, I0, twy, ax, ay, dxdy, cols, maxbits,
-                                                             nullptr);
+    k_cols_t<L, G, cols_radix<L>()><<<(ncols + G - 1) / G, kThreads, sm, s>>>(width, ncols, I0, twy, ax, ay, dxdy,
+                                                                              cols, maxbits, nullptr);
   });
   return cudaPeekAtLastError();
 }
