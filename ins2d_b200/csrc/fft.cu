@@ -496,6 +496,25 @@ constexpr int cols_per_block() {
   return (L >= 10 && g8 > INS2D_FFT_COLS_G) ? INS2D_FFT_COLS_G : g8;
 }
 
+// The column scaling's y factors ay staged in shared memory (INS2D_FFT_COLS_SAY,
+// lengths up to 4096): each block copies ay once, coalesced, to slots
+// i + i/8 after its columns, and reads them at the bit-reversed J of its
+// values (32 lanes 2^(L-8) apart: two-way bank conflicts with the padding,
+// against one sector per lane for the same reads from global memory).
+#ifndef INS2D_FFT_COLS_SAY
+#define INS2D_FFT_COLS_SAY 0
+#endif
+template <int L>
+__host__ __device__ constexpr bool cols_say() {
+  return INS2D_FFT_COLS_SAY && L <= 12;
+}
+// dynamic shared memory of a column block
+template <int L, int G>
+constexpr size_t cols_smem() {
+  return (size_t)G * paddedl<L>() * sizeof(double2) +
+         (cols_say<L>() ? (size_t)((1 << L) + ((1 << L) >> 3)) * sizeof(double) : 0);
+}
+
 // DIF passes over stages S_HI down to S_BOT (three per pass) on the first
 // `lines` of G lines of stride ld
 template <int L, int S_HI, int S_BOT, int G>
@@ -697,6 +716,10 @@ __global__ void __launch_bounds__(kThreads, RX == 16 ? 2 : INS2D_FFT_COLS_MINB)
   const int c0 = blockIdx.x * G;
   const int g_here = min(G, ncols - c0);
   static_assert(RX == 8 || (RX == 16 && L >= 9), "radix-16 outer passes need L >= 9");
+  double *say = reinterpret_cast<double *>(sm + G * LD);
+  if constexpr (cols_say<L>()) {
+    for (int i = threadIdx.x; i < N; i += kThreads) say[i + (i >> 3)] = __ldg(ay + i);
+  }  // read after the __syncthreads that ends the first pass
   if constexpr (RX == 16) {
     constexpr int P16 = N >> 4;
     for (unsigned gidx = threadIdx.x; gidx < G * P16; gidx += kThreads) {
@@ -739,8 +762,14 @@ __global__ void __launch_bounds__(kThreads, RX == 16 ? 2 : INS2D_FFT_COLS_MINB)
       const int J = brev(8 * k + m, L);
       const double2 F = x[m];
       lmax = fmax(lmax, F.x * F.x + F.y * F.y);  // squared; one square root per block
-      const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + I) + __ldg(ay + J));
-      const double r = -1.0 / lam;
+      double ayJ;
+      if constexpr (cols_say<L>())
+        ayJ = say[J + (J >> 3)];
+      else
+        ayJ = __ldg(ay + J);
+      const double lam = (I == 0 && J == 0) ? 1.0 : (dxdy * 4.0) * (__ldg(ax + I) + ayJ);
+      // the correctly rounded reciprocal: the same value as -1.0 / lam
+      const double r = INS2D_FFT_COLS_SAY ? -__drcp_rn(lam) : -1.0 / lam;
       x[m] = make_double2(F.x * r, F.y * r);
     }
     group_dit<true>(x, 3, 0, 1, pyr, true);
@@ -971,7 +1000,7 @@ cudaError_t fft_passes(const DevOps &P, const FftPlan &plan, const double *src, 
   // columns: forward, scaling, inverse
   const bool fy = with_log2<kFusedMinLog>(plan.logy, [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
-    const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
+    const size_t sm = cols_smem<L, G>();
     launch_k(k_cols_t<L, G, cols_radix<L>()>, dim3((H + G - 1) / G), dim3(kThreads), sm, s, H, H, 0, plan.twy,
              P.fft_ax, P.fft_ay, P.fft_dxdy, plan.spec, maxbits, skip);
   });
@@ -1044,7 +1073,7 @@ cudaError_t slab_columns(int Ny, const double2 *twy, const double *ax, const dou
                          int width, int ncols, int I0, unsigned long long *maxbits, cudaStream_t s) {
   with_log2<kFusedMinLog>(ilog2_exact(Ny), [&](auto c) {
     constexpr int L = decltype(c)::value, G = cols_per_block<L>();
-    const size_t sm = (size_t)G * paddedl<L>() * sizeof(double2);
+    const size_t sm = cols_smem<L, G>();
     k_cols_t<L, G, cols_radix<L>()><<<(ncols + G - 1) / G, kThreads, sm, s>>>(width, ncols, I0, twy, ax, ay, dxdy,
                                                                               cols, maxbits, nullptr);
   });
