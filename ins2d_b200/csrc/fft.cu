@@ -502,7 +502,7 @@ constexpr int cols_per_block() {
 // values (32 lanes 2^(L-8) apart: two-way bank conflicts with the padding,
 // against one sector per lane for the same reads from global memory).
 #ifndef INS2D_FFT_COLS_SAY
-#define INS2D_FFT_COLS_SAY 0
+#define INS2D_FFT_COLS_SAY 1
 #endif
 template <int L>
 __host__ __device__ constexpr bool cols_say() {
