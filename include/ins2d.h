@@ -229,7 +229,10 @@ int ins2d_pressure_poisson(ins2d_ctx *ctx, const double *f, double *dp,
 /* p = pressure_additional_solve(V,p,T,t,options) (in place on p) */
 int ins2d_pressure_additional_solve(ins2d_ctx *ctx, const double *V, double *p, double t,
                                     ins2d_solve_stats *stats, int mem);
-/* [V,p] = time_ERK(V,p,T,t,dt,options), in place on V and p */
+/* [V,p] = time_ERK(V,p,T,t,dt,options), in place on V and p.  After an error
+ * status the contents of V and p are unspecified, as with device memory: with
+ * INS2D_MEM_HOST, V's copy out starts after the last projection, so V may
+ * already hold the step's velocity when the additional solve fails. */
 int ins2d_erk_step(ins2d_ctx *ctx, double *V, double *p, double t, double dt,
                    ins2d_step_stats *stats, int mem);
 /* nsteps consecutive time_ERK steps from t with a fixed dt (solver_unsteady.m:72-102
