@@ -263,12 +263,12 @@ int ins2d_conservation(ins2d_ctx *ctx, const double *V, double t, double out[4],
  * Limits: 2 <= Nx, Ny <= INS2D_NOALLOC_MAX_N, Nx*Ny <= INS2D_NOALLOC_MAX_CELLS,
  * and sizes the FFT path supports; other sizes return INS2D_EINVAL.
  * The first call on a device looks up the array's device address and sets
- * kernel attributes; make that first call before any stream capture.
- * A call whose (Nx, Ny, dx, dy) differ from the previous call's on that
- * device builds the twiddle and symbol tables on the host and copies them
- * in from pageable memory, waiting for the copies; a call with the same
- * values reuses the tables already on the device.  Every call blocks until
- * the stream has finished its work.
+ * kernel attributes.  A call whose (Nx, Ny, dx, dy) differ from the previous
+ * call's on that device builds the twiddle and symbol tables on the host and
+ * copies them in from pageable memory, waiting for the copies; a call with
+ * the same values reuses the tables already on the device.  Every call
+ * blocks until the stream has finished its work, so no call can be captured
+ * into a CUDA graph.
  * All calls share the array: calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller.  An error
  * already pending on the calling thread (cudaGetLastError) is left to the
